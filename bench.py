@@ -1,0 +1,303 @@
+"""Benchmark of the FISTA + L1 + 2-D TV reconstruction on one B200 (or N
+independent frames on N GPUs, one process per GPU).
+
+A step is one FISTA iteration (prox sweep with its backtracking checks, the
+forward operator, the momentum update and the adjoint) over the whole volume of
+the 1024x1024x1000 workload (dz=2, dx=1.1, lambda=0.632, sparsity 0.15, TV 0.1,
+5 TV iterations; 1000 synthetic disks + 1000 rods).  ``value`` is voxel
+iterations per second over all ranks, timed on the device with CUDA events;
+``e2e`` is the same metric through the C ABI from a host hologram to host
+results.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config c2|c1]
+"""
+from __future__ import annotations
+
+import argparse
+import importlib
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+PKG = "rihvr---regularized-inverse-holographic-volume-reconstruction_b200"
+sys.path.insert(0, ROOT)
+
+METRIC = "s to FP64-oracle objective ±1e-3 at 1024²×1000 voxels; voxel-iters/s; % HBM roofline"
+FALLBACK_HBM_GBS = 6650.0
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks/throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader",
+                                          "-lms", "200", "-i", str(self.idx)], stdout=subprocess.PIPE,
+                                         stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1].split()[0]))
+                smax = float(parts[2].split()[0])
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": float(np.median(sm)), "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def workload(name: str):
+    synth = importlib.import_module(PKG + ".synth")
+    return synth.config2() if name == "c2" else synth.config1()
+
+
+# algorithmic bytes per voxel of each kernel class, s = bytes per stored voxel
+def class_bytes(s: int) -> dict:
+    return {
+        "adj_col": 8,           # write the column-pass intermediate
+        "adj_row": 16,          # read it, write the gradient volume
+        "prox": 8 + 3 * s,      # read gradient, P_k, P_{k-1}; write P_{k+1}
+        "fwd_row": s + 8,       # read P_{k+1}, write the row-pass intermediate
+        "fwd_col": 8,           # read the intermediate (the z-sum stays on chip)
+    }
+
+
+def cpu_sample(cfg, b, steps: int, warmup: int):
+    """Time the FP64 oracle on a bounded sample of the workload: the first 16
+    planes of the volume, full plane size, one FISTA iteration per step."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    rihvr = importlib.import_module(PKG)
+    p = rihvr.params_from_config(cfg)
+    nz = min(16, cfg.num_planes)
+    z = rihvr.plane_list(p)[:nz]
+    op = O.OracleParams(W=cfg.W, H=cfg.H, z=z, dx=cfg.dx(), lam=cfg.lam(), l1=cfg.l1(), tv=cfg.tv(),
+                        n_tv=cfg.num_tv_iterations, mode=7, faithful=1)
+    b64 = b.astype(np.float64)
+    for _ in range(warmup):
+        O.solve(op, b64, 1, want_volumes=False)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        O.solve(op, b64, 1, want_volumes=False)
+    dt = time.perf_counter() - t0
+    vox = cfg.W * cfg.H * nz
+    return {"value": vox * steps / dt, "unit": "voxel-iters/s", "cores": O.num_threads(), "kind": "port",
+            "sample": f"FP64 oracle, {nz} of {cfg.num_planes} planes at {cfg.W}x{cfg.H}, 1 FISTA iteration "
+                      f"per step, {steps} steps ({dt:.1f} s)"}
+
+
+def run_reference(args):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return 0
+    cfg = workload(args.config)
+    synth = importlib.import_module(PKG + ".synth")
+    _, b = synth.make_hologram(cfg)
+    cb = cpu_sample(cfg, b, args.steps, args.warmup)
+    line = {"metric": METRIC, "value": cb["value"], "unit": "voxel-iters/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "impl": "reference",
+            "dtype": "f64", "data": "synthetic", "config": {"workload": cfg.name, "sample": cb["sample"]},
+            "cpu_baseline": cb, "e2e": {"value": cb["value"], "unit": "voxel-iters/s", "h2d_bytes_per_step": 0,
+                                        "d2h_bytes_per_step": 0}, "vs_baseline": None}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    ws, rank, local = dist_env()
+    import torch
+
+    torch.cuda.set_device(local)
+    pg = None
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+        pg = dist
+    rihvr = importlib.import_module(PKG)
+    synth = importlib.import_module(PKG + ".synth")
+    base = workload(args.config)
+    # independent frames: each rank reconstructs its own hologram
+    cfg = (synth.config2 if args.config == "c2" else synth.config1)(seed=base.seed + rank)
+    _, b = synth.make_hologram(cfg)
+    storage = {"f32": 0, "bf16": 1, "f16": 2}[args.storage]
+    p = rihvr.params_from_config(cfg, record_objective=0, storage=storage)
+    s = rihvr.SparseCompressiveHolo(p, cfg.W, cfg.H)
+    V = cfg.voxels()
+    s.setHologram(b)
+    s.iterate(args.warmup)
+
+    def barrier():
+        if pg is not None:
+            pg.barrier()
+        torch.cuda.synchronize()
+
+    # timed region: device time of K iterations, per-kernel events on the solver stream
+    s.set_profiling(True)
+    launches0 = s.launch_count()
+    barrier()
+    with ClockSampler(local) as clk:
+        ms = s.iterate_timed(args.steps)
+    barrier()
+    launches = s.launch_count() - launches0
+    ktimes = s.kernel_times()
+    s.set_profiling(False)
+    log = s.iterations()
+    max_ms = ms
+    if pg is not None:
+        t = torch.tensor([ms], device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        max_ms = float(t.item())
+    value = ws * V * args.steps / (max_ms / 1e3)
+
+    # end to end through the C ABI: host hologram in, host estimate + objective out
+    stream = torch.cuda.ExternalStream(s.stream())
+    hb = torch.from_numpy(b).pin_memory()
+    hout = torch.empty((cfg.H, cfg.W), dtype=torch.float32).pin_memory()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    L = rihvr.load_library()
+    import ctypes
+
+    barrier()
+    e0.record(stream)
+    rihvr._check(L.rihvr_set_hologram(s._h, ctypes.c_void_p(hb.data_ptr()), 0), "set_hologram")
+    s.iterate(args.steps)
+    rihvr._check(L.rihvr_get_estimate(s._h, ctypes.c_void_p(hout.data_ptr()), 0), "get_estimate")
+    f_final, _ = s.calcObjectiveFunction()
+    e1.record(stream)
+    e1.synchronize()
+    e2e_ms = e0.elapsed_time(e1)
+    barrier()
+    if pg is not None:
+        t = torch.tensor([e2e_ms], device="cuda")
+        pg.all_reduce(t, op=pg.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e = {"value": ws * V * args.steps / (e2e_ms / 1e3), "unit": "voxel-iters/s",
+           "h2d_bytes_per_step": int(b.nbytes) / args.steps, "d2h_bytes_per_step": (int(hout.numel() * 4) + 8) / args.steps,
+           "ms": e2e_ms, "what": "set_hologram (H2D from pinned) + K iterations + estimate and objective (D2H)"}
+
+    # roofline of the dominant kernel class
+    peak, peak_kind = peaks()
+    sbytes = 8 if storage == 0 else 4
+    cb = class_bytes(sbytes)
+    dom = max((k for k in cb if k in ktimes and ktimes[k][1] > 0), key=lambda k: ktimes[k][0])
+    tot_ms, nl = ktimes[dom]
+    avg_ms = tot_ms / nl
+    bytes_per_launch = cb[dom] * V
+    achieved = bytes_per_launch / (avg_ms / 1e3) / 1e9
+    roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
+                "bytes_per_launch": bytes_per_launch, "avg_launch_ms": avg_ms}
+    iter_bytes = (32 + 4 * sbytes) * V  # per voxel-iteration, minimal two-pass data flow
+    kernels = {k: {"ms_total": v[0], "launches": v[1]} for k, v in ktimes.items()}
+
+    if rank == 0:
+        cpu = None
+        if ws == 1 and not args.no_cpu_baseline:
+            cpu = cpu_sample(cfg, b, steps=2, warmup=1)
+        line = {
+            "metric": METRIC, "value": value, "unit": "voxel-iters/s", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32" if storage == 0 else args.storage, "data": "synthetic",
+            "config": {"workload": cfg.name, "W": cfg.W, "H": cfg.H, "Nz": cfg.num_planes,
+                       "tv_iterations": cfg.num_tv_iterations, "storage": args.storage,
+                       "parallelism": f"{ws} independent frames" if ws > 1 else "single frame",
+                       "l2": "inputs larger than L2 (volumes of %.1f GB each)" % (V * sbytes / 1e9),
+                       "record_objective": False},
+            "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu,
+            "iteration_roofline": {"bytes_per_voxel_iter": 32 + 4 * sbytes,
+                                   "achieved": iter_bytes * args.steps / (max_ms / 1e3) / 1e9, "peak": peak,
+                                   "frac": iter_bytes * args.steps / (max_ms / 1e3) / 1e9 / peak},
+            "clocks": clk.summary(), "gpu_launches": launches, "kernels": kernels,
+            "backtracks_in_timed_region": int(log["backtracks"][-args.steps:].sum()) if len(log) else 0,
+            "final_objective_e2e": f_final, "device_bytes": s.device_bytes(),
+        }
+        print(json.dumps(line), flush=True)
+    s.destroy()
+    if pg is not None:
+        pg.barrier()
+        pg.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="c2", choices=["c2", "c1"])
+    ap.add_argument("--storage", default="f32", choices=["f32", "bf16", "f16"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

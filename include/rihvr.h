@@ -1,0 +1,215 @@
+/*
+ * rihvr.h - C ABI of the B200 reconstruction core.
+ *
+ * Drop-in boundary for RIHVR's sparse inverse reconstruction path
+ * (FASTA/FISTA with L1 + TV regularisation over a Rayleigh-Sommerfeld model).
+ * Every entry point names the reference interface it replaces; paths are
+ * relative to the RIHVR source tree (src/core/...).
+ *
+ * Conventions
+ *  - Status codes: 0 on success; 1..12 are the reference's umnholo::HoloError
+ *    values (src/core/umnholo.h:132-146); 20+ are runtime conditions.  No C++
+ *    exception crosses this boundary.
+ *  - Complex arrays are interleaved float pairs (re, im), row-major,
+ *    volumes ordered [plane][row][column].
+ *  - `is_device` != 0 means the pointer is CUDA device memory borrowed for the
+ *    duration of the call; otherwise it is host memory.
+ *  - A context owns all device memory it allocates and runs on its own CUDA
+ *    stream; calls on one context are not re-entrant.
+ */
+#ifndef RIHVR_H
+#define RIHVR_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum rihvr_status {
+  RIHVR_OK = 0,
+  /* umnholo::HoloError (src/core/umnholo.h:132-146) */
+  RIHVR_ERR_UNKNOWN_TYPE = 1,
+  RIHVR_ERR_BAD_FILENAME = 2,
+  RIHVR_ERR_MISSING_DATA = 3,
+  RIHVR_ERR_INVALID_STATE = 4,
+  RIHVR_ERR_OUT_OF_MEMORY = 5,
+  RIHVR_ERR_UNKNOWN_MODE = 6,
+  RIHVR_ERR_INVALID_ARGUMENT = 7,
+  RIHVR_ERR_UNKNOWN_ERROR = 8,
+  RIHVR_ERR_INVALID_FILE = 9,
+  RIHVR_ERR_INVALID_DATA = 10,
+  RIHVR_ERR_CRITICAL_ASSUMPTION = 11,
+  RIHVR_ERR_INFINITE_LOOP = 12,
+  /* runtime conditions (the reference throws CUDA_ERROR_UNKNOWN, umnholo.h:14-34) */
+  RIHVR_ERR_CUDA = 20,
+  RIHVR_ERR_NO_DEVICE = 21,
+  RIHVR_ERR_UNSUPPORTED_SIZE = 22
+};
+
+/* Reconstruction modes: umnholo::CompressiveHoloMode (src/core/compressive_holo.h:20-29). */
+enum rihvr_mode {
+  RIHVR_MODE_FASTA_L1 = 5,
+  RIHVR_MODE_FASTA_FUSED_LASSO = 6,    /* L1 + 3-D TV */
+  RIHVR_MODE_FASTA_FUSED_LASSO_2D = 7  /* L1 + per-plane 2-D TV (the CLI default) */
+};
+
+enum rihvr_storage { RIHVR_STORE_F32 = 0, RIHVR_STORE_BF16 = 1, RIHVR_STORE_F16 = 2 };
+
+/* Solver parameters.  The first block mirrors umnholo::Parameters
+ * (src/core/holo_ui.h:83-145), kept in float like the reference; the second
+ * block selects build options that have no reference counterpart. */
+typedef struct rihvr_params {
+  float start_plane;             /* 3001  z0 */
+  float plane_stepsize;          /* 3002  dz */
+  int num_planes;                /* 3003  Nz */
+  float wavelength;              /* 3004  lambda (same length unit as dx and z) */
+  float resolution;              /* 3005  dx, pixel pitch */
+  int zero_padding;              /* 3010  pixels added on every side */
+  int num_inverse_iterations;    /* 6001  FISTA iterations */
+  float regularization_param;    /* 6002  L1 (sparsity) weight */
+  float regularization_TV_param; /* 6004  TV weight; 0 selects the L1-only prox */
+  int num_tv_iterations;         /* 6005  Chambolle iterations per prox (0..20) */
+  int mode;                      /* rihvr_mode, default 7 */
+  int storage;                   /* rihvr_storage of the volumes, default FP32 */
+  int faithful;                  /* 1 (default): reference arithmetic - separable
+                                    complex shrink and the restart statistic as the
+                                    reference sums it; 0: complex-modulus shrink
+                                    and the plain restart dot product */
+  int max_backtracks;            /* 2 in the reference (sparse_compressive_holo.cu:423) */
+  double initial_step;           /* <= 0: 1/num_planes as the reference (:247) */
+  int record_objective;          /* 1: objective terms at every iteration */
+} rihvr_params;
+
+/* Per-iteration record (what inverseReconstruct prints, :561-565, plus terms). */
+typedef struct rihvr_iter_record {
+  double f_prox;       /* objective at the accepted prox output */
+  double f_resid_prox; /* 0.5 ||A p - b||^2 */
+  double lim;          /* line-search limit (calcLineSearchLimit, :4307-4390) */
+  double ratio;        /* backtracking ratio of the accepted step (:402-403) */
+  double t;            /* step size used */
+  double beta;         /* momentum factor (alpha0 - 1) / alpha1 */
+  double f_x;          /* objective at the momentum point ("new f", :548) */
+  double f_resid_x;    /* 0.5 ||A x - b||^2 at the momentum point */
+  double l1_x, tv_x;   /* regulariser norms at the momentum point */
+  double restart_sum;  /* restart statistic (fistaRestart, :4434-4482) */
+  int backtracks;
+  int restarted;
+} rihvr_iter_record;
+
+/* File-level fields of the .param format the CLI needs (holo_ui.h:83-145). */
+typedef struct rihvr_file_params {
+  char image_filename[4096];       /* 2001, or 2002 + 2003 */
+  char image_path[4096];           /* 2002 */
+  char image_formatted_name[4096]; /* 2003 */
+  char output_path[4096];          /* 2004 */
+  char background_filename[4096];  /* 2005 */
+  int remove_background;           /* set by 2005 */
+  int image_count;                 /* 1001 */
+  int start_image;                 /* 1002 */
+  int roi_x, roi_y, roi_size;      /* 3006, 3007, 3009 */
+  int roi_rect_x, roi_rect_y, roi_rect_w, roi_rect_h; /* 3011-3014 */
+  int output_planes;               /* 7001 */
+  int output_steps;                /* 7005 */
+} rihvr_file_params;
+
+typedef struct rihvr_ctx rihvr_ctx;
+
+/* HoloUi::HoloUi defaults (src/core/holo_ui.cpp:10-62) plus mode 7, FP32,
+ * faithful arithmetic, 2 backtracks, reference step. */
+int rihvr_params_default(rihvr_params* params);
+
+/* HoloUi::readFile (src/core/holo_ui.cpp:171-486): "name code value" lines,
+ * '%' or '#' comments.  `files` may be NULL. */
+int rihvr_read_param_file(const char* path, rihvr_params* params, rihvr_file_params* files);
+
+/* Plane positions as the reference computes them in float
+ * (holo_ui.cpp:478-483): z_i = start_plane + i * plane_stepsize. */
+int rihvr_plane_list(const rihvr_params* params, double* z_out);
+
+/* SparseCompressiveHolo::SparseCompressiveHolo(Hologram)
+ * (src/core/sparse_compressive_holo.cu:58-135).  width x height is the padded
+ * hologram size; planes must be square with a supported side. */
+int rihvr_create(const rihvr_params* params, int width, int height, rihvr_ctx** out);
+
+/* SparseCompressiveHolo::destroy (:137-146). */
+void rihvr_destroy(rihvr_ctx* ctx);
+
+/* The measured hologram b (the preprocessed, padded Hologram passed to the
+ * constructor and to inverseReconstruct): real, height x width floats.  Also
+ * resets the iterate to x = 0. */
+int rihvr_set_hologram(rihvr_ctx* ctx, const float* b, int is_device);
+
+/* SparseCompressiveHolo::inverseReconstruct(Hologram, mode) (:173-633): runs
+ * num_inverse_iterations from x = 0.  final_objective (may be NULL) receives
+ * the objective at the final momentum point. */
+int rihvr_reconstruct(rihvr_ctx* ctx, double* final_objective);
+
+/* Restart from x = 0 without changing the hologram. */
+int rihvr_reset(rihvr_ctx* ctx);
+
+/* Continue the current solve by n iterations (the loop body :299-611). */
+int rihvr_iterate(rihvr_ctx* ctx, int n);
+
+/* Same, timed on the device with CUDA events around the n iterations. */
+int rihvr_iterate_timed(rihvr_ctx* ctx, int n, float* device_ms);
+
+/* Number of iterations run since the last reset. */
+int rihvr_iteration_count(const rihvr_ctx* ctx);
+
+/* calcObjectiveFunction (:2838-2899) at the current momentum point:
+ * f and its three terms (0.5||r||^2, sum|x|, TV(x)). */
+int rihvr_objective(rihvr_ctx* ctx, double* f, double* terms3);
+
+/* Iteration log since the last reset. */
+int rihvr_get_iterations(const rihvr_ctx* ctx, rihvr_iter_record* out, int max_records, int* n_out);
+
+/* SparseCompressiveHolo::getPlane (:1197-1202): plane z of the current
+ * momentum point x1, complex interleaved height x width. */
+int rihvr_get_plane(rihvr_ctx* ctx, int z, float* out, int is_device);
+
+/* The whole momentum point volume, complex interleaved Nz x height x width. */
+int rihvr_get_volume(rihvr_ctx* ctx, float* out, int is_device);
+
+/* Estimated hologram A x (estimate_final.tif, :621-622) and residual
+ * A x - b (residual_final.tif, :623-624), height x width floats. */
+int rihvr_get_estimate(rihvr_ctx* ctx, float* out, int is_device);
+int rihvr_get_residual(rihvr_ctx* ctx, float* out, int is_device);
+
+/* Operator entry points. */
+/* backPropagate (:1935-2077): d = Re(IFFT(sum_z H'_z FFT(x_z))), x complex
+ * interleaved Nz x height x width, d height x width floats. */
+int rihvr_forward(rihvr_ctx* ctx, const float* volume, float* holo_out, int is_device);
+/* SparseGradient::reconstruct + getPlane for every plane
+ * (src/core/sparse_gradient.cu:47-165): g_z = IFFT(conj(H'_z) FFT(r)). */
+int rihvr_adjoint(rihvr_ctx* ctx, const float* residual, float* volume_out, int is_device);
+/* One prox step, denoise() (:2969-2994): p = prox(x - t A^H r, t) for the
+ * configured mode.  sums3 (may be NULL) receives the line-search terms
+ * sum (p - x).g, sum |p - x|^2 and the restart statistic against y0 = x. */
+int rihvr_prox_step(rihvr_ctx* ctx, const float* x, const float* residual, double t, float* p_out,
+                    double* sums3, int is_device);
+
+/* Device time per kernel class of the iterations run with profiling on
+ * (names "adj_col", "adj_row", "prox", "fwd_row", "fwd_col", "plane").
+ * Enabling records a pair of CUDA events around each launch. */
+int rihvr_set_profiling(rihvr_ctx* ctx, int enable);
+int rihvr_kernel_times(rihvr_ctx* ctx, const char** names, double* total_ms, int* launches, int max, int* n_out);
+
+/* The context's CUDA stream (a cudaStream_t), for callers that order their own
+ * work or timing events against it. */
+void* rihvr_get_stream(rihvr_ctx* ctx);
+
+/* Number of kernels the context has launched since it was created. */
+long long rihvr_launch_count(const rihvr_ctx* ctx);
+
+/* Bytes of device memory the context holds. */
+size_t rihvr_device_bytes(const rihvr_ctx* ctx);
+
+const char* rihvr_status_string(int status);
+const char* rihvr_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* RIHVR_H */

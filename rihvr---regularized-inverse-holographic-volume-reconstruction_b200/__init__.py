@@ -1,0 +1,349 @@
+"""B200-native reconstruction core for digital inline holography.
+
+Python mirror of RIHVR's reconstruction entry points (``umnholo::
+SparseCompressiveHolo``, src/core/sparse_compressive_holo.h:30-96, and the
+``Parameters``/``HoloUi`` pair, src/core/holo_ui.h:83-214) over the C ABI in
+``include/rihvr.h``.  The compute runs in ``librihvr_b200.so`` (hand-written
+sm_100a CUDA); there is no fallback: loading fails loudly if the library is
+missing or no GPU is visible.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "librihvr_b200.so")
+CLI_PATH = os.path.join(_HERE, "sparse-inverse-recon")
+
+# status codes (include/rihvr.h)
+OK = 0
+ERR_INVALID_ARGUMENT = 7
+ERR_UNKNOWN_MODE = 6
+ERR_MISSING_DATA = 3
+ERR_INVALID_FILE = 9
+ERR_BAD_FILENAME = 2
+ERR_OUT_OF_MEMORY = 5
+ERR_CUDA = 20
+ERR_NO_DEVICE = 21
+ERR_UNSUPPORTED_SIZE = 22
+
+MODE_FASTA_L1 = 5
+MODE_FASTA_FUSED_LASSO = 6
+MODE_FASTA_FUSED_LASSO_2D = 7
+STORE_F32, STORE_BF16, STORE_F16 = 0, 1, 2
+
+SUPPORTED_SIDES = (32, 48, 64, 128, 256, 384, 512, 768, 1024)
+
+
+class RihvrParams(ctypes.Structure):
+    """``rihvr_params`` (include/rihvr.h); first block = umnholo::Parameters."""
+    _fields_ = [
+        ("start_plane", ctypes.c_float),
+        ("plane_stepsize", ctypes.c_float),
+        ("num_planes", ctypes.c_int),
+        ("wavelength", ctypes.c_float),
+        ("resolution", ctypes.c_float),
+        ("zero_padding", ctypes.c_int),
+        ("num_inverse_iterations", ctypes.c_int),
+        ("regularization_param", ctypes.c_float),
+        ("regularization_TV_param", ctypes.c_float),
+        ("num_tv_iterations", ctypes.c_int),
+        ("mode", ctypes.c_int),
+        ("storage", ctypes.c_int),
+        ("faithful", ctypes.c_int),
+        ("max_backtracks", ctypes.c_int),
+        ("initial_step", ctypes.c_double),
+        ("record_objective", ctypes.c_int),
+    ]
+
+
+class IterRecord(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_double) for n in
+                ("f_prox", "f_resid_prox", "lim", "ratio", "t", "beta", "f_x", "f_resid_x", "l1_x", "tv_x",
+                 "restart_sum")] + [("backtracks", ctypes.c_int), ("restarted", ctypes.c_int)]
+
+
+ITER_DTYPE = np.dtype([(n, "f8") for n in ("f_prox", "f_resid_prox", "lim", "ratio", "t", "beta", "f_x",
+                                             "f_resid_x", "l1_x", "tv_x", "restart_sum")]
+                      + [("backtracks", "i4"), ("restarted", "i4")])
+
+
+class FileParams(ctypes.Structure):
+    _fields_ = [
+        ("image_filename", ctypes.c_char * 4096),
+        ("image_path", ctypes.c_char * 4096),
+        ("image_formatted_name", ctypes.c_char * 4096),
+        ("output_path", ctypes.c_char * 4096),
+        ("background_filename", ctypes.c_char * 4096),
+        ("remove_background", ctypes.c_int),
+        ("image_count", ctypes.c_int),
+        ("start_image", ctypes.c_int),
+        ("roi_x", ctypes.c_int), ("roi_y", ctypes.c_int), ("roi_size", ctypes.c_int),
+        ("roi_rect_x", ctypes.c_int), ("roi_rect_y", ctypes.c_int), ("roi_rect_w", ctypes.c_int),
+        ("roi_rect_h", ctypes.c_int),
+        ("output_planes", ctypes.c_int),
+        ("output_steps", ctypes.c_int),
+    ]
+
+
+# every symbol include/rihvr.h declares
+EXPORTED = (
+    "rihvr_params_default", "rihvr_read_param_file", "rihvr_plane_list", "rihvr_create", "rihvr_destroy",
+    "rihvr_set_hologram", "rihvr_reconstruct", "rihvr_reset", "rihvr_iterate", "rihvr_iterate_timed",
+    "rihvr_iteration_count", "rihvr_objective", "rihvr_get_iterations", "rihvr_get_plane", "rihvr_get_volume",
+    "rihvr_get_estimate", "rihvr_get_residual", "rihvr_forward", "rihvr_adjoint", "rihvr_prox_step",
+    "rihvr_set_profiling", "rihvr_kernel_times", "rihvr_get_stream", "rihvr_launch_count", "rihvr_device_bytes",
+    "rihvr_status_string", "rihvr_last_error",
+)
+
+_lib = None
+
+
+class RihvrError(RuntimeError):
+    def __init__(self, code: int, where: str):
+        L = _lib
+        msg = ""
+        if L is not None:
+            msg = (L.rihvr_last_error() or b"").decode(errors="replace")
+            name = (L.rihvr_status_string(code) or b"").decode()
+        else:
+            name = str(code)
+        super().__init__(f"{where}: status {code} ({name}) {msg}".strip())
+        self.code = code
+
+
+def load_library(path: str = LIB_PATH):
+    """Load the native library (built in-tree by build.py); raises if missing."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(f"native library missing: {path} (run build.py); there is no fallback path")
+    L = ctypes.CDLL(path)
+    vp, ip, dp, fp = ctypes.c_void_p, ctypes.c_int, ctypes.c_double, ctypes.POINTER(ctypes.c_float)
+    P = ctypes.POINTER
+    L.rihvr_params_default.argtypes = [P(RihvrParams)]
+    L.rihvr_read_param_file.argtypes = [ctypes.c_char_p, P(RihvrParams), P(FileParams)]
+    L.rihvr_plane_list.argtypes = [P(RihvrParams), P(ctypes.c_double)]
+    L.rihvr_create.argtypes = [P(RihvrParams), ip, ip, P(vp)]
+    L.rihvr_destroy.argtypes = [vp]
+    L.rihvr_destroy.restype = None
+    L.rihvr_set_hologram.argtypes = [vp, vp, ip]
+    L.rihvr_reconstruct.argtypes = [vp, P(ctypes.c_double)]
+    L.rihvr_reset.argtypes = [vp]
+    L.rihvr_iterate.argtypes = [vp, ip]
+    L.rihvr_iterate_timed.argtypes = [vp, ip, fp]
+    L.rihvr_iteration_count.argtypes = [vp]
+    L.rihvr_objective.argtypes = [vp, P(ctypes.c_double), P(ctypes.c_double)]
+    L.rihvr_get_iterations.argtypes = [vp, vp, ip, P(ctypes.c_int)]
+    for n in ("rihvr_get_plane",):
+        getattr(L, n).argtypes = [vp, ip, vp, ip]
+    for n in ("rihvr_get_volume", "rihvr_get_estimate", "rihvr_get_residual"):
+        getattr(L, n).argtypes = [vp, vp, ip]
+    L.rihvr_forward.argtypes = [vp, vp, vp, ip]
+    L.rihvr_adjoint.argtypes = [vp, vp, vp, ip]
+    L.rihvr_prox_step.argtypes = [vp, vp, vp, dp, vp, P(ctypes.c_double), ip]
+    L.rihvr_set_profiling.argtypes = [vp, ip]
+    L.rihvr_kernel_times.argtypes = [vp, P(ctypes.c_char_p), P(ctypes.c_double), P(ctypes.c_int), ip,
+                                     P(ctypes.c_int)]
+    L.rihvr_get_stream.argtypes = [vp]
+    L.rihvr_get_stream.restype = vp
+    L.rihvr_launch_count.argtypes = [vp]
+    L.rihvr_launch_count.restype = ctypes.c_longlong
+    L.rihvr_device_bytes.argtypes = [vp]
+    L.rihvr_device_bytes.restype = ctypes.c_size_t
+    L.rihvr_status_string.argtypes = [ip]
+    L.rihvr_status_string.restype = ctypes.c_char_p
+    L.rihvr_last_error.restype = ctypes.c_char_p
+    _lib = L
+    return L
+
+
+def _check(rc: int, where: str):
+    if rc != OK:
+        raise RihvrError(rc, where)
+
+
+def default_params() -> RihvrParams:
+    """HoloUi defaults (holo_ui.cpp:10-62) plus mode 7 / FP32 / faithful."""
+    p = RihvrParams()
+    _check(load_library().rihvr_params_default(ctypes.byref(p)), "rihvr_params_default")
+    return p
+
+
+def read_param_file(path: str):
+    """HoloUi::readFile (holo_ui.cpp:171-486) -> (RihvrParams, FileParams)."""
+    p = default_params()
+    f = FileParams()
+    _check(load_library().rihvr_read_param_file(path.encode(), ctypes.byref(p), ctypes.byref(f)),
+           "rihvr_read_param_file")
+    return p, f
+
+
+def plane_list(p: RihvrParams) -> np.ndarray:
+    z = np.empty(p.num_planes, np.float64)
+    _check(load_library().rihvr_plane_list(ctypes.byref(p), z.ctypes.data_as(ctypes.POINTER(ctypes.c_double))),
+           "rihvr_plane_list")
+    return z
+
+
+def params_from_config(cfg, **overrides) -> RihvrParams:
+    """Parameters of a synthetic workload (``synth.HoloConfig``)."""
+    p = default_params()
+    for k in ("start_plane", "plane_stepsize", "num_planes", "wavelength", "resolution", "zero_padding",
+              "num_inverse_iterations", "regularization_param", "regularization_TV_param", "num_tv_iterations"):
+        setattr(p, k, getattr(cfg, k))
+    for k, v in overrides.items():
+        setattr(p, k, v)
+    return p
+
+
+def _ptr(a: np.ndarray):
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+class SparseCompressiveHolo:
+    """Mirror of ``umnholo::SparseCompressiveHolo`` (sparse_compressive_holo.h:30-96).
+
+    ``SparseCompressiveHolo(params, width, height)`` allocates the solver for a
+    padded ``height x width`` hologram; ``inverseReconstruct(b)`` runs the
+    configured number of FISTA iterations from x = 0 and returns the objective
+    at the final momentum point; ``getPlane(z)`` returns a plane of the volume.
+    """
+
+    def __init__(self, params: RihvrParams, width: int, height: int):
+        L = load_library()
+        self._L = L
+        self.params = params
+        self.width, self.height, self.depth = int(width), int(height), int(params.num_planes)
+        h = ctypes.c_void_p()
+        _check(L.rihvr_create(ctypes.byref(params), self.width, self.height, ctypes.byref(h)), "rihvr_create")
+        self._h = h
+
+    # lifecycle ---------------------------------------------------------------
+    def destroy(self):
+        if getattr(self, "_h", None):
+            self._L.rihvr_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.destroy()
+
+    # operations --------------------------------------------------------------
+    def setHologram(self, b: np.ndarray):
+        b = np.ascontiguousarray(b, dtype=np.float32)
+        if b.shape != (self.height, self.width):
+            raise ValueError(f"hologram shape {b.shape} != {(self.height, self.width)}")
+        _check(self._L.rihvr_set_hologram(self._h, _ptr(b), 0), "rihvr_set_hologram")
+
+    def inverseReconstruct(self, b: np.ndarray | None = None) -> float:
+        if b is not None:
+            self.setHologram(b)
+        f = ctypes.c_double()
+        _check(self._L.rihvr_reconstruct(self._h, ctypes.byref(f)), "rihvr_reconstruct")
+        return f.value
+
+    def reset(self):
+        _check(self._L.rihvr_reset(self._h), "rihvr_reset")
+
+    def iterate(self, n: int):
+        _check(self._L.rihvr_iterate(self._h, int(n)), "rihvr_iterate")
+
+    def iterate_timed(self, n: int) -> float:
+        ms = ctypes.c_float()
+        _check(self._L.rihvr_iterate_timed(self._h, int(n), ctypes.byref(ms)), "rihvr_iterate_timed")
+        return ms.value
+
+    def calcObjectiveFunction(self):
+        f = ctypes.c_double()
+        terms = (ctypes.c_double * 3)()
+        _check(self._L.rihvr_objective(self._h, ctypes.byref(f), terms), "rihvr_objective")
+        return f.value, np.array(terms[:])
+
+    def iterations(self) -> np.ndarray:
+        n = ctypes.c_int()
+        _check(self._L.rihvr_get_iterations(self._h, None, 0, ctypes.byref(n)), "rihvr_get_iterations")
+        out = np.zeros(n.value, ITER_DTYPE)
+        if n.value:
+            _check(self._L.rihvr_get_iterations(self._h, _ptr(out), n.value, ctypes.byref(n)), "rihvr_get_iterations")
+        return out
+
+    def getPlane(self, z: int) -> np.ndarray:
+        out = np.empty((self.height, self.width), np.complex64)
+        _check(self._L.rihvr_get_plane(self._h, int(z), _ptr(out), 0), "rihvr_get_plane")
+        return out
+
+    def getVolume(self) -> np.ndarray:
+        out = np.empty((self.depth, self.height, self.width), np.complex64)
+        _check(self._L.rihvr_get_volume(self._h, _ptr(out), 0), "rihvr_get_volume")
+        return out
+
+    def getEstimate(self) -> np.ndarray:
+        out = np.empty((self.height, self.width), np.float32)
+        _check(self._L.rihvr_get_estimate(self._h, _ptr(out), 0), "rihvr_get_estimate")
+        return out
+
+    def getResidual(self) -> np.ndarray:
+        out = np.empty((self.height, self.width), np.float32)
+        _check(self._L.rihvr_get_residual(self._h, _ptr(out), 0), "rihvr_get_residual")
+        return out
+
+    # operators ---------------------------------------------------------------
+    def forward(self, vol: np.ndarray) -> np.ndarray:
+        """backPropagate: d = Re(IFFT(sum_z H'_z FFT(x_z)))."""
+        vol = np.ascontiguousarray(vol, dtype=np.complex64)
+        if vol.shape != (self.depth, self.height, self.width):
+            raise ValueError("volume shape mismatch")
+        out = np.empty((self.height, self.width), np.float32)
+        _check(self._L.rihvr_forward(self._h, _ptr(vol), _ptr(out), 0), "rihvr_forward")
+        return out
+
+    def adjoint(self, r: np.ndarray) -> np.ndarray:
+        """SparseGradient: g_z = IFFT(conj(H'_z) FFT(r))."""
+        r = np.ascontiguousarray(r, dtype=np.float32)
+        out = np.empty((self.depth, self.height, self.width), np.complex64)
+        _check(self._L.rihvr_adjoint(self._h, _ptr(r), _ptr(out), 0), "rihvr_adjoint")
+        return out
+
+    def prox_step(self, x: np.ndarray, r: np.ndarray, t: float):
+        """denoise(): p = prox(x - t A^H r, t); returns (p, [lim1, lim2, restart])."""
+        x = np.ascontiguousarray(x, dtype=np.complex64)
+        r = np.ascontiguousarray(r, dtype=np.float32)
+        out = np.empty_like(x)
+        sums = (ctypes.c_double * 3)()
+        _check(self._L.rihvr_prox_step(self._h, _ptr(x), _ptr(r), float(t), _ptr(out), sums, 0),
+               "rihvr_prox_step")
+        return out, np.array(sums[:])
+
+    # profiling ---------------------------------------------------------------
+    def set_profiling(self, on: bool):
+        _check(self._L.rihvr_set_profiling(self._h, int(bool(on))), "rihvr_set_profiling")
+
+    def kernel_times(self) -> dict:
+        names = (ctypes.c_char_p * 16)()
+        ms = (ctypes.c_double * 16)()
+        cnt = (ctypes.c_int * 16)()
+        n = ctypes.c_int()
+        _check(self._L.rihvr_kernel_times(self._h, names, ms, cnt, 16, ctypes.byref(n)), "rihvr_kernel_times")
+        return {names[i].decode(): (ms[i], cnt[i]) for i in range(n.value)}
+
+    def stream(self) -> int:
+        return int(self._L.rihvr_get_stream(self._h) or 0)
+
+    def launch_count(self) -> int:
+        return int(self._L.rihvr_launch_count(self._h))
+
+    def device_bytes(self) -> int:
+        return int(self._L.rihvr_device_bytes(self._h))

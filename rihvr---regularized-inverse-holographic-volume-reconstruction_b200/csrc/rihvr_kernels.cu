@@ -1,0 +1,1132 @@
+// sm_100a kernels of the reconstruction hot path.
+//
+// Operator structure (RIHVR src/core/sparse_compressive_holo.cu:1935-2077 forward,
+// src/core/sparse_gradient.cu:47-165 adjoint), restated by linearity:
+//   forward  d   = Re( F^-1 sum_z H'_z F(x_z) ),  H'_z = exp(i z c(f))
+//   adjoint  g_z = F^-1( conj(H'_z) F(r) )
+// with c(f) = 2 pi / lambda (sqrt(1 - (lambda f)^2) - 1).  The per-plane carrier
+// factor exp(-+ i 2 pi z / lambda) that the reference applies separately is folded
+// into H'_z.  The 2-D DFT of a plane is a row pass plus a column pass; the column
+// passes carry the transfer-function multiply (regenerated from an FP64 table of
+// c/(2 pi) per frequency, phase reduced mod 1 turn in FP64) and, for the forward
+// operator, the sum over z, so the Nz transformed planes never go back to memory.
+#include "rihvr_device.cuh"
+#include "rihvr_kernels.cuh"
+
+namespace rihvr {
+
+// ---------------------------------------------------------------------------
+// line configurations: N = N1 * N2, N1 threads per line, N2 elements each
+// ---------------------------------------------------------------------------
+template <int N>
+struct LineCfg;
+#define RIHVR_LINE(NN, NN1)                                                              \
+  template <>                                                                            \
+  struct LineCfg<NN> {                                                                   \
+    static constexpr int N = NN, N1 = NN1, N2 = NN / NN1, M = (NN / NN1) / NN1;          \
+    static constexpr int LD = NN1 + 1;                                                   \
+    static_assert((NN / NN1) % NN1 == 0, "N1 must divide N2");                           \
+  };
+RIHVR_LINE(32, 4)
+RIHVR_LINE(48, 4)
+RIHVR_LINE(64, 8)
+RIHVR_LINE(128, 8)
+RIHVR_LINE(256, 16)
+RIHVR_LINE(384, 8)
+RIHVR_LINE(512, 16)
+RIHVR_LINE(768, 16)
+RIHVR_LINE(1024, 32)
+#undef RIHVR_LINE
+
+#define RIHVR_FOR_EACH_SIZE(X) X(32) X(48) X(64) X(128) X(256) X(384) X(512) X(768) X(1024)
+
+bool line_size_supported(int n) {
+  switch (n) {
+#define RIHVR_CASE(NN) case NN:
+    RIHVR_FOR_EACH_SIZE(RIHVR_CASE)
+#undef RIHVR_CASE
+    return true;
+    default:
+      return false;
+  }
+}
+
+static int g_num_sms = 0;
+static int num_sms() {
+  if (g_num_sms == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
+    if (g_num_sms <= 0) g_num_sms = 148;
+  }
+  return g_num_sms;
+}
+
+template <typename K>
+static cudaError_t allow_smem(K kernel, size_t bytes) {
+  if (bytes <= 48 * 1024) return cudaSuccess;
+  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+// ---------------------------------------------------------------------------
+// element access by kind (uniform branches)
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float2 load_elem(int kind, const void* p, size_t i) {
+  switch (kind) {
+    case ELEM_R32:
+      return make_float2(static_cast<const float*>(p)[i], 0.f);
+    case ELEM_STORE_BF16:
+      return Store<__nv_bfloat162>::ld(static_cast<const __nv_bfloat162*>(p) + i);
+    case ELEM_STORE_F16:
+      return Store<__half2>::ld(static_cast<const __half2*>(p) + i);
+    default:
+      return static_cast<const float2*>(p)[i];
+  }
+}
+__device__ __forceinline__ void store_elem(int kind, void* p, size_t i, float2 v) {
+  switch (kind) {
+    case ELEM_R32:
+      static_cast<float*>(p)[i] = v.x;
+      break;
+    case ELEM_STORE_BF16:
+      Store<__nv_bfloat162>::st(static_cast<__nv_bfloat162*>(p) + i, v);
+      break;
+    case ELEM_STORE_F16:
+      Store<__half2>::st(static_cast<__half2*>(p) + i, v);
+      break;
+    default:
+      static_cast<float2*>(p)[i] = v;
+  }
+}
+
+template <int N1, int N2, bool INV>
+__device__ __forceinline__ void stage_b_dft(float2 (&w)[N2]) {
+  constexpr int M = N2 / N1;
+#pragma unroll
+  for (int j = 0; j < M; ++j) {
+    float2 s[N1];
+#pragma unroll
+    for (int k = 0; k < N1; ++k) s[k] = w[j * N1 + k];
+    reg_fft<N1, INV>(s);
+#pragma unroll
+    for (int k = 0; k < N1; ++k) w[j * N1 + k] = s[k];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Row pass: one line per N1-thread group, lines contiguous in memory.
+// ---------------------------------------------------------------------------
+constexpr int kRowThreads = 256;
+
+template <int N>
+struct RowLayout {
+  using C = LineCfg<N>;
+  static constexpr int LPB = kRowThreads / C::N1;
+  static constexpr int base_ls = C::N2 * C::LD;
+  // pad the per-line stride so that lines sharing a half-warp hit different banks
+  static constexpr int LS = (C::N1 >= 16) ? base_ls : base_ls + (((C::N1 % 16) - (base_ls % 16) + 16) % 16);
+  static constexpr int SMEM = LPB * LS;  // float2 elements
+  static constexpr size_t SMEM_BYTES = sizeof(float2) * SMEM;
+};
+
+template <int N, bool INV>
+__global__ void __launch_bounds__(kRowThreads) k_rows(int in_kind, const void* __restrict__ in, int out_kind,
+                                                     void* __restrict__ out, long long nlines, float scale) {
+  using C = LineCfg<N>;
+  using Lay = RowLayout<N>;
+  constexpr int N1 = C::N1, N2 = C::N2, M = C::M, LD = C::LD;
+  static_assert(32 % N1 == 0, "a line must not straddle warps");
+  extern __shared__ float2 sm[];
+  const int li = threadIdx.x / N1, t = threadIdx.x % N1;
+  long long L = (long long)blockIdx.x * Lay::LPB + li;
+  const bool active = L < nlines;
+  if (!active) L = nlines - 1;
+  const size_t base = (size_t)L * N;
+  float2 v[N2];
+#pragma unroll
+  for (int n2 = 0; n2 < N2; ++n2) v[n2] = load_elem(in_kind, in, base + t + N1 * n2);
+  reg_fft<N2, INV>(v);
+  line_twiddle<N, N2, INV>(v, t);
+  float2* sl = sm + li * Lay::LS;
+#pragma unroll
+  for (int k2 = 0; k2 < N2; ++k2) sl[k2 * LD + t] = v[k2];
+  __syncwarp();
+#pragma unroll
+  for (int j = 0; j < M; ++j)
+#pragma unroll
+    for (int n1 = 0; n1 < N1; ++n1) v[j * N1 + n1] = sl[(t + N1 * j) * LD + n1];
+  stage_b_dft<N1, N2, INV>(v);
+  if (active) {
+#pragma unroll
+    for (int j = 0; j < M; ++j)
+#pragma unroll
+      for (int k1 = 0; k1 < N1; ++k1)
+        store_elem(out_kind, out, base + t + N1 * j + N2 * k1, cscale(v[j * N1 + k1], scale));
+  }
+}
+
+template <int N>
+static cudaError_t rows_n(int inverse, int in_kind, const void* in, int out_kind, void* out, long long nlines,
+                          float scale, cudaStream_t st) {
+  using Lay = RowLayout<N>;
+  const long long blocks = (nlines + Lay::LPB - 1) / Lay::LPB;
+  if (blocks <= 0) return cudaSuccess;
+  cudaError_t e;
+  if (inverse) {
+    e = allow_smem(k_rows<N, true>, Lay::SMEM_BYTES);
+    if (e != cudaSuccess) return e;
+    k_rows<N, true><<<(unsigned)blocks, kRowThreads, Lay::SMEM_BYTES, st>>>(in_kind, in, out_kind, out, nlines, scale);
+  } else {
+    e = allow_smem(k_rows<N, false>, Lay::SMEM_BYTES);
+    if (e != cudaSuccess) return e;
+    k_rows<N, false><<<(unsigned)blocks, kRowThreads, Lay::SMEM_BYTES, st>>>(in_kind, in, out_kind, out, nlines, scale);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_rows(int inverse, int in_kind, const void* in, int out_kind, void* out, int W,
+                        long long nlines, float scale, cudaStream_t st) {
+  switch (W) {
+#define RIHVR_CASE(NN) \
+  case NN:             \
+    return rows_n<NN>(inverse, in_kind, in, out_kind, out, nlines, scale, st);
+    RIHVR_FOR_EACH_SIZE(RIHVR_CASE)
+#undef RIHVR_CASE
+    default:
+      return cudaErrorInvalidValue;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Column passes: CC columns per block, N1 threads per column (lanes: column
+// fastest so each warp-wide access covers CC*8 contiguous bytes of a row).
+// Shared layout [k2][n1][c] with n1 padded to LD.
+// ---------------------------------------------------------------------------
+template <int N>
+struct ColLayout {
+  using C = LineCfg<N>;
+  static constexpr int CC = (C::N1 >= 32) ? 8 : (C::N1 >= 16 ? 16 : 32);
+  static constexpr int THREADS = CC * C::N1;
+  static constexpr int SMEM_ELEMS = C::N2 * C::LD * CC;
+  static constexpr size_t SMEM_BYTES = sizeof(float2) * SMEM_ELEMS;
+};
+
+// Phase-table reads are issued in groups separated by a compiler scheduling
+// fence so that the FP64 table values of a whole line are not all live at once.
+constexpr int kPhaseGroup = 8;
+__device__ __forceinline__ void sched_fence() { asm volatile("" ::: "memory"); }
+// Hide a pointer's loop invariance from the compiler: the z loops re-read the
+// phase table (and the residual spectrum) from L1/L2 every plane instead of
+// pinning a whole line of them in registers.
+template <typename T>
+__device__ __forceinline__ const T* launder(const T* p) {
+  asm volatile("mov.b64 %0, %0;" : "+l"(p));
+  return p;
+}
+// Same for the twiddle index: recomputing a line's inter-stage twiddles every
+// plane costs two sincospi and ~N2 complex products, far less than keeping
+// N2 complex twiddles live across the z loop.
+__device__ __forceinline__ int launder_i(int v) {
+  asm volatile("mov.b32 %0, %0;" : "+r"(v));
+  return v;
+}
+
+// Exchange + stage B shared by all column kernels.  On entry v holds the
+// twiddled stage-A output of this thread; on exit the stage-B output.
+template <int N, bool INV>
+__device__ __forceinline__ void col_exchange(float2 (&v)[LineCfg<N>::N2], float2* sm, int c, int t) {
+  using C = LineCfg<N>;
+  using Lay = ColLayout<N>;
+  constexpr int N1 = C::N1, N2 = C::N2, M = C::M, LD = C::LD, CC = Lay::CC;
+  __syncthreads();  // previous users of sm are done
+#pragma unroll
+  for (int k2 = 0; k2 < N2; ++k2) sm[(k2 * LD + t) * CC + c] = v[k2];
+  __syncthreads();
+#pragma unroll
+  for (int j = 0; j < M; ++j)
+#pragma unroll
+    for (int n1 = 0; n1 < N1; ++n1) v[j * N1 + n1] = sm[((t + N1 * j) * LD + n1) * CC + c];
+  stage_b_dft<N1, N2, INV>(v);
+}
+
+// Adjoint column pass: U_z(:, x) = IDFT_y( conj(H'_z(:, x)) * Rs(:, x) ), z in [zb, ze).
+// Square planes: the row pitch equals the line length N, so every element
+// offset below is a compile-time multiple of N.  Rs already carries 1/(W H).
+template <int N>
+__global__ void __launch_bounds__(ColLayout<N>::THREADS) k_adj_col(const float2* __restrict__ Rs,
+                                                                   const double* __restrict__ cturn,
+                                                                   const double* __restrict__ zlist,
+                                                                   float2* __restrict__ U, int z0, int z1,
+                                                                   int zpb) {
+  using C = LineCfg<N>;
+  using Lay = ColLayout<N>;
+  constexpr int N1 = C::N1, N2 = C::N2, M = C::M, CC = Lay::CC;
+  constexpr int W = N;
+  extern __shared__ float2 sm[];
+  const int c = threadIdx.x % CC, t = threadIdx.x / CC;
+  const int xr = blockIdx.x * CC + c;
+  const bool col_ok = xr < W;
+  const int x = col_ok ? xr : W - 1;
+  const int zb = z0 + blockIdx.y * zpb, ze = min(zb + zpb, z1);
+  constexpr size_t HW = (size_t)N * W;
+  const float2* rs = Rs + (size_t)t * W + x;
+  const double* ct = cturn + (size_t)t * W + x;
+#pragma unroll 1
+  for (int z = zb; z < ze; ++z) {
+    const double zz = zlist[z];
+    const float2* rsz = launder(rs);
+    const double* ctz = launder(ct);
+    float2 v[N2];
+#pragma unroll
+    for (int g = 0; g < N2; g += kPhaseGroup) {
+#pragma unroll
+      for (int q = 0; q < kPhaseGroup; ++q) {
+        const int n2 = g + q;
+        v[n2] = cmul(__ldg(rsz + (size_t)n2 * N1 * W), transfer(zz, __ldg(ctz + (size_t)n2 * N1 * W), true));
+      }
+      sched_fence();
+    }
+    reg_fft<N2, true>(v);
+    line_twiddle<N, N2, true>(v, launder_i(t));
+    col_exchange<N, true>(v, sm, c, t);
+    if (col_ok) {
+      float2* Uz = U + (size_t)z * HW + (size_t)t * W + x;
+#pragma unroll
+      for (int j = 0; j < M; ++j)
+#pragma unroll
+        for (int k1 = 0; k1 < N1; ++k1) Uz[(size_t)(N1 * j + N2 * k1) * W] = v[j * N1 + k1];
+    }
+  }
+}
+
+// Forward column pass with the z-sum: Spart[chunk](:, x) = sum_z H'_z(:, x) DFT_y(T_z(:, x)).
+template <int N>
+__global__ void __launch_bounds__(ColLayout<N>::THREADS) k_fwd_col(const float2* __restrict__ T,
+                                                                   const double* __restrict__ cturn,
+                                                                   const double* __restrict__ zlist,
+                                                                   float2* __restrict__ Spart, int z0, int z1,
+                                                                   int zpb) {
+  using C = LineCfg<N>;
+  using Lay = ColLayout<N>;
+  constexpr int N1 = C::N1, N2 = C::N2, M = C::M, CC = Lay::CC;
+  constexpr int W = N;
+  extern __shared__ float2 sm[];
+  const int c = threadIdx.x % CC, t = threadIdx.x / CC;
+  const int xr = blockIdx.x * CC + c;
+  const bool col_ok = xr < W;
+  const int x = col_ok ? xr : W - 1;
+  const int zb = z0 + blockIdx.y * zpb, ze = min(zb + zpb, z1);
+  constexpr size_t HW = (size_t)N * W;
+  const double* ct = cturn + (size_t)t * W + x;
+  float2 acc[N2];
+#pragma unroll
+  for (int i = 0; i < N2; ++i) acc[i] = make_float2(0.f, 0.f);
+#pragma unroll 1
+  for (int z = zb; z < ze; ++z) {
+    const double zz = zlist[z];
+    const float2* Tz = T + (size_t)z * HW + (size_t)t * W + x;
+    float2 v[N2];
+#pragma unroll
+    for (int n2 = 0; n2 < N2; ++n2) v[n2] = Tz[(size_t)n2 * N1 * W];
+    reg_fft<N2, false>(v);
+    line_twiddle<N, N2, false>(v, launder_i(t));
+    col_exchange<N, false>(v, sm, c, t);
+    const double* ctz = launder(ct);
+#pragma unroll
+    for (int g = 0; g < N2; g += kPhaseGroup) {
+#pragma unroll
+      for (int q = 0; q < kPhaseGroup; ++q) {
+        const int j = (g + q) / N1, k1 = (g + q) % N1;
+        const float2 h = transfer(zz, __ldg(ctz + (size_t)(N1 * j + N2 * k1) * W), false);
+        acc[j * N1 + k1] = cadd(acc[j * N1 + k1], cmul(v[j * N1 + k1], h));
+      }
+      sched_fence();
+    }
+  }
+  if (col_ok) {
+    float2* Sp = Spart + (size_t)blockIdx.y * HW + (size_t)t * W + x;
+#pragma unroll
+    for (int j = 0; j < M; ++j)
+#pragma unroll
+      for (int k1 = 0; k1 < N1; ++k1) Sp[(size_t)(N1 * j + N2 * k1) * W] = acc[j * N1 + k1];
+  }
+}
+
+// Plain column DFT of one (square) plane.
+template <int N, bool INV>
+__global__ void __launch_bounds__(ColLayout<N>::THREADS) k_plane_col(const float2* __restrict__ in,
+                                                                     float2* __restrict__ out, float scale) {
+  using C = LineCfg<N>;
+  using Lay = ColLayout<N>;
+  constexpr int N1 = C::N1, N2 = C::N2, M = C::M, CC = Lay::CC;
+  constexpr int W = N;
+  extern __shared__ float2 sm[];
+  const int c = threadIdx.x % CC, t = threadIdx.x / CC;
+  const int xr = blockIdx.x * CC + c;
+  const bool col_ok = xr < W;
+  const int x = col_ok ? xr : W - 1;
+  const float2* src = in + (size_t)t * W + x;
+  float2 v[N2];
+#pragma unroll
+  for (int n2 = 0; n2 < N2; ++n2) v[n2] = src[(size_t)n2 * N1 * W];
+  reg_fft<N2, INV>(v);
+  line_twiddle<N, N2, INV>(v, t);
+  col_exchange<N, INV>(v, sm, c, t);
+  if (col_ok) {
+    float2* dst = out + (size_t)t * W + x;
+#pragma unroll
+    for (int j = 0; j < M; ++j)
+#pragma unroll
+      for (int k1 = 0; k1 < N1; ++k1) dst[(size_t)(N1 * j + N2 * k1) * W] = cscale(v[j * N1 + k1], scale);
+  }
+}
+
+template <int N>
+static int col_strips(int W) {
+  return (W + ColLayout<N>::CC - 1) / ColLayout<N>::CC;
+}
+
+template <int N>
+static cudaError_t adj_col_n(const float2* Rs, const double* cturn, const double* zlist, float2* U, int W,
+                             int z0, int z1, cudaStream_t st) {
+  using Lay = ColLayout<N>;
+  const int nz = z1 - z0;
+  if (nz <= 0) return cudaSuccess;
+  const int strips = col_strips<N>(W);
+  const int target = 8 * num_sms();
+  int chunks = (target + strips - 1) / strips;
+  if (chunks > nz) chunks = nz;
+  if (chunks < 1) chunks = 1;
+  const int zpb = (nz + chunks - 1) / chunks;
+  chunks = (nz + zpb - 1) / zpb;
+  cudaError_t e = allow_smem(k_adj_col<N>, Lay::SMEM_BYTES);
+  if (e != cudaSuccess) return e;
+  k_adj_col<N><<<dim3(strips, chunks), Lay::THREADS, Lay::SMEM_BYTES, st>>>(Rs, cturn, zlist, U, z0, z1, zpb);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_adj_col(const float2* Rs, const double* cturn, const double* zlist, float2* U, int W, int H,
+                           int z0, int z1, cudaStream_t st) {
+  if (W != H) return cudaErrorInvalidValue;
+  switch (H) {
+#define RIHVR_CASE(NN) \
+  case NN:             \
+    return adj_col_n<NN>(Rs, cturn, zlist, U, W, z0, z1, st);
+    RIHVR_FOR_EACH_SIZE(RIHVR_CASE)
+#undef RIHVR_CASE
+    default:
+      return cudaErrorInvalidValue;
+  }
+}
+
+int fwd_col_chunks(int W, int H, int Nz) {
+  int cc = 8;
+  switch (H) {
+#define RIHVR_CASE(NN) \
+  case NN:             \
+    cc = ColLayout<NN>::CC; break;
+    RIHVR_FOR_EACH_SIZE(RIHVR_CASE)
+#undef RIHVR_CASE
+    default:
+      break;
+  }
+  const int strips = (W + cc - 1) / cc;
+  const int target = 4 * num_sms();
+  int chunks = (target + strips - 1) / strips;
+  // partial spectra cost one plane of traffic each: keep them few
+  if (chunks > 16) chunks = 16;
+  if (chunks > Nz) chunks = Nz;
+  if (chunks < 1) chunks = 1;
+  return chunks;
+}
+
+template <int N>
+static cudaError_t fwd_col_n(const float2* T, const double* cturn, const double* zlist, float2* Spart, int W,
+                             int z0, int z1, int nchunks, cudaStream_t st) {
+  using Lay = ColLayout<N>;
+  const int nz = z1 - z0;
+  if (nz <= 0) return cudaSuccess;
+  const int strips = col_strips<N>(W);
+  const int zpb = (nz + nchunks - 1) / nchunks;
+  const int chunks = (nz + zpb - 1) / zpb;
+  cudaError_t e = allow_smem(k_fwd_col<N>, Lay::SMEM_BYTES);
+  if (e != cudaSuccess) return e;
+  if (chunks < nchunks) {  // unused chunk slots must read as zero
+    e = cudaMemsetAsync(Spart + (size_t)chunks * N * W, 0, sizeof(float2) * (size_t)(nchunks - chunks) * N * W, st);
+    if (e != cudaSuccess) return e;
+  }
+  k_fwd_col<N><<<dim3(strips, chunks), Lay::THREADS, Lay::SMEM_BYTES, st>>>(T, cturn, zlist, Spart, z0, z1, zpb);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fwd_col(const float2* T, const double* cturn, const double* zlist, float2* Spart, int W, int H,
+                           int z0, int z1, int nchunks, cudaStream_t st) {
+  if (W != H) return cudaErrorInvalidValue;
+  switch (H) {
+#define RIHVR_CASE(NN) \
+  case NN:             \
+    return fwd_col_n<NN>(T, cturn, zlist, Spart, W, z0, z1, nchunks, st);
+    RIHVR_FOR_EACH_SIZE(RIHVR_CASE)
+#undef RIHVR_CASE
+    default:
+      return cudaErrorInvalidValue;
+  }
+}
+
+template <int N>
+static cudaError_t plane_col_n(int inverse, const float2* in, float2* out, int W, float scale, cudaStream_t st) {
+  using Lay = ColLayout<N>;
+  const int strips = col_strips<N>(W);
+  cudaError_t e;
+  if (inverse) {
+    e = allow_smem(k_plane_col<N, true>, Lay::SMEM_BYTES);
+    if (e != cudaSuccess) return e;
+    k_plane_col<N, true><<<strips, Lay::THREADS, Lay::SMEM_BYTES, st>>>(in, out, scale);
+  } else {
+    e = allow_smem(k_plane_col<N, false>, Lay::SMEM_BYTES);
+    if (e != cudaSuccess) return e;
+    k_plane_col<N, false><<<strips, Lay::THREADS, Lay::SMEM_BYTES, st>>>(in, out, scale);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_plane_col(int inverse, const float2* in, float2* out, int W, int H, float scale,
+                             cudaStream_t st) {
+  if (W != H) return cudaErrorInvalidValue;
+  switch (H) {
+#define RIHVR_CASE(NN) \
+  case NN:             \
+    return plane_col_n<NN>(inverse, in, out, W, scale, st);
+    RIHVR_FOR_EACH_SIZE(RIHVR_CASE)
+#undef RIHVR_CASE
+    default:
+      return cudaErrorInvalidValue;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// sum of partial spectra (fixed order: deterministic)
+// ---------------------------------------------------------------------------
+__global__ void k_sum_chunks(const float2* __restrict__ Spart, int nchunks, float2* __restrict__ S, long long n) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    float2 a = Spart[i];
+    for (int k = 1; k < nchunks; ++k) a = cadd(a, Spart[(size_t)k * n + i]);
+    S[i] = a;
+  }
+}
+
+cudaError_t launch_sum_chunks(const float2* Spart, int nchunks, float2* S, long long n, cudaStream_t st) {
+  int blocks = (int)((n + 255) / 256);
+  if (blocks > 4 * num_sms()) blocks = 4 * num_sms();
+  k_sum_chunks<<<blocks, 256, 0, st>>>(Spart, nchunks, S, n);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// block reduction of kNumSums doubles into partials[block]
+// ---------------------------------------------------------------------------
+template <int NT>
+__device__ __forceinline__ void block_write_sums(double (&acc)[kNumSums], double* partials, int block) {
+  __shared__ double red[NT / 32][kNumSums];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < kNumSums; ++k) {
+    double v = warp_sum(acc[k]);
+    if (lane == 0) red[wid][k] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < kNumSums) {
+    double s = 0;
+    for (int w = 0; w < NT / 32; ++w) s += red[w][threadIdx.x];
+    partials[(size_t)block * kNumSums + threadIdx.x] = s;
+  }
+}
+
+// Restart statistic weights: sparse_fistaRestart_kernel<512> (RIHVR
+// sparse_compressive_holo.cu:4393-4432) overwrites the second element's real
+// product with its imaginary one and re-adds the first element's imaginary
+// product (:4411-4413): within each 1024-element chunk of a plane, elements
+// 0..511 count Re + 2 Im and elements 512..1023 count Im only.
+__device__ __forceinline__ void restart_w(size_t e, int faithful, float* wr, float* wi) {
+  if (!faithful) {
+    *wr = 1.f;
+    *wi = 1.f;
+  } else if ((e & 1023u) < 512u) {
+    *wr = 1.f;
+    *wi = 2.f;
+  } else {
+    *wr = 0.f;
+    *wi = 1.f;
+  }
+}
+
+// Soft thresholds: block_soft_threshold_kernel (sparse_compressive_holo.cu:
+// 3065-3110) shrinks Re and Im separately; the non-faithful variant shrinks
+// the complex modulus.
+__device__ __forceinline__ float2 shrink(float2 v, float T, int faithful) {
+  if (T <= 0.f) return v;
+  if (faithful) {
+    const float mr = fabsf(v.x) - T, mi = fabsf(v.y) - T;
+    return make_float2(mr > 0.f ? copysignf(mr, v.x) : 0.f, mi > 0.f ? copysignf(mi, v.y) : 0.f);
+  }
+  const float a = sqrtf(v.x * v.x + v.y * v.y);
+  if (a <= T) return make_float2(0.f, 0.f);
+  const float f = (a - T) / a;
+  return make_float2(v.x * f, v.y * f);
+}
+
+__device__ __forceinline__ float cabs2(float2 a) { return a.x * a.x + a.y * a.y; }
+
+// ---------------------------------------------------------------------------
+// Fused 2-D TV prox (mode 7): proximalFusedLasso2d, sparse_compressive_holo.cu:
+// 3652-3732 with kernels :3478-3597.  Per plane tile, with the momentum point
+// formed on the fly:
+//   x = P + beta (P - Pprev);  xh = x - t g
+//   gx = gy = 0; n_tv times: y = xh - mu div(g);  g = (g + s grad y)/max(1, |.|)
+//   y = xh - mu div(g);  p = shrink(y, thr)
+// div uses forward periodic differences, grad backward periodic differences, the
+// projection norm is taken over the four real components.  Tiles are 64x64 with
+// a recomputed halo of n_tv + 1 pixels, which makes the interior exact.
+// The same sweep accumulates the line-search sums, the restart statistic and
+// (optionally) the L1/TV norms of p and x.
+// ---------------------------------------------------------------------------
+constexpr int TV_EXT = 64, TV_RUN = 16, TV_RUNS = TV_EXT / TV_RUN, TV_THREADS = TV_EXT * TV_RUNS;
+constexpr size_t TV_SMEM = sizeof(float2) * (5 * TV_EXT * TV_EXT + TV_RUNS * TV_EXT);
+
+template <typename ST>
+__global__ void __launch_bounds__(TV_THREADS, 1) k_prox_tv2d(ProxArgs a) {
+  extern __shared__ float2 smem[];
+  float2* s_y = smem;
+  float2* s_gx = s_y + TV_EXT * TV_EXT;
+  float2* s_X = s_gx + TV_EXT * TV_EXT;
+  float2* s_g = s_X + TV_EXT * TV_EXT;
+  float2* s_P = s_g + TV_EXT * TV_EXT;
+  float2* s_gyb = s_P + TV_EXT * TV_EXT;
+  const int W = a.W, H = a.H;
+  const int ex = threadIdx.x % TV_EXT, run = threadIdx.x / TV_EXT;
+  const int h = a.n_tv + 1, inner = TV_EXT - 2 * h;
+  const int ox = blockIdx.x * inner - h, oy = blockIdx.y * inner - h;
+  const size_t plane = (size_t)blockIdx.z * W * H;
+  const ST* P = static_cast<const ST*>(a.P) + plane;
+  const ST* Pp = static_cast<const ST*>(a.Pprev) + plane;
+  const float2* G = a.G + plane;
+  const int gcol = ((ox + ex) % W + W) % W;
+  float2 xh[TV_RUN], gx[TV_RUN], gy[TV_RUN], y[TV_RUN];
+#pragma unroll
+  for (int i = 0; i < TV_RUN; ++i) {
+    const int row = run * TV_RUN + i;
+    const int grow = ((oy + row) % H + H) % H;
+    const size_t idx = (size_t)grow * W + gcol;
+    const float2 p = Store<ST>::ld(P + idx), pp = Store<ST>::ld(Pp + idx), g = G[idx];
+    const float2 x = make_float2(fmaf(a.beta, p.x - pp.x, p.x), fmaf(a.beta, p.y - pp.y, p.y));
+    xh[i] = make_float2(fmaf(-a.t, g.x, x.x), fmaf(-a.t, g.y, x.y));
+    s_X[row * TV_EXT + ex] = x;
+    s_g[row * TV_EXT + ex] = g;
+    s_P[row * TV_EXT + ex] = p;
+    s_gx[row * TV_EXT + ex] = make_float2(0.f, 0.f);
+    gx[i] = make_float2(0.f, 0.f);
+    gy[i] = make_float2(0.f, 0.f);
+  }
+  s_gyb[run * TV_EXT + ex] = make_float2(0.f, 0.f);
+  __syncthreads();
+  const float mu = a.mu, s = a.s;
+  for (int it = 0;; ++it) {
+    // y = xh - mu div(g)
+#pragma unroll
+    for (int i = 0; i < TV_RUN; ++i) {
+      const int row = run * TV_RUN + i;
+      const float2 gxr = (ex < TV_EXT - 1) ? s_gx[row * TV_EXT + ex + 1] : gx[i];
+      float2 gyd;
+      if (i < TV_RUN - 1) gyd = gy[i + 1];
+      else gyd = (run < TV_RUNS - 1) ? s_gyb[(run + 1) * TV_EXT + ex] : gy[i];
+      const float dvx = (gxr.x - gx[i].x) + (gyd.x - gy[i].x);
+      const float dvy = (gxr.y - gx[i].y) + (gyd.y - gy[i].y);
+      y[i] = make_float2(fmaf(-mu, dvx, xh[i].x), fmaf(-mu, dvy, xh[i].y));
+    }
+    if (it == a.n_tv) break;
+#pragma unroll
+    for (int i = 0; i < TV_RUN; ++i) s_y[(run * TV_RUN + i) * TV_EXT + ex] = y[i];
+    __syncthreads();
+    // g = P(g + s grad y)
+#pragma unroll
+    for (int i = 0; i < TV_RUN; ++i) {
+      const int row = run * TV_RUN + i;
+      const float2 yl = (ex > 0) ? s_y[row * TV_EXT + ex - 1] : y[i];
+      float2 yu;
+      if (i > 0) yu = y[i - 1];
+      else yu = (run > 0) ? s_y[(row - 1) * TV_EXT + ex] : y[i];
+      const float2 px = make_float2(fmaf(s, yl.x - y[i].x, gx[i].x), fmaf(s, yl.y - y[i].y, gx[i].y));
+      const float2 py = make_float2(fmaf(s, yu.x - y[i].x, gy[i].x), fmaf(s, yu.y - y[i].y, gy[i].y));
+      const float n2 = cabs2(px) + cabs2(py);
+      const float sc = (n2 > 1.f) ? rsqrtf(n2) : 1.f;
+      gx[i] = cscale(px, sc);
+      gy[i] = cscale(py, sc);
+      s_gx[row * TV_EXT + ex] = gx[i];
+    }
+    s_gyb[run * TV_EXT + ex] = gy[0];
+    __syncthreads();
+  }
+  // shrink, publish p for the TV-norm neighbours
+#pragma unroll
+  for (int i = 0; i < TV_RUN; ++i) {
+    y[i] = shrink(y[i], a.thr, a.faithful);
+  }
+  __syncthreads();
+#pragma unroll
+  for (int i = 0; i < TV_RUN; ++i) s_y[(run * TV_RUN + i) * TV_EXT + ex] = y[i];
+  __syncthreads();
+  double acc[kNumSums];
+#pragma unroll
+  for (int k = 0; k < kNumSums; ++k) acc[k] = 0.0;
+  const int gx0 = ox + ex;  // unwrapped column of this thread
+  const bool col_in = (ex >= h) && (ex < h + inner) && (gx0 < W);
+  ST* Pn = static_cast<ST*>(a.Pnew) + plane;
+#pragma unroll
+  for (int i = 0; i < TV_RUN; ++i) {
+    const int row = run * TV_RUN + i;
+    const int gy0 = oy + row;
+    if (!(col_in && row >= h && row < h + inner && gy0 < H)) continue;
+    const size_t e = (size_t)gy0 * W + gx0;
+    const float2 p = y[i];
+    Store<ST>::st(Pn + e, p);
+    const float2 x = s_X[row * TV_EXT + ex], g = s_g[row * TV_EXT + ex], y0 = s_P[row * TV_EXT + ex];
+    const float2 d = csub(p, x);
+    acc[SUM_LIM1] += (double)(d.x * g.x) + (double)(d.y * g.y);
+    acc[SUM_LIM2] += (double)cabs2(d);
+    float wr, wi;
+    restart_w(e, a.faithful, &wr, &wi);
+    const float2 u = csub(x, p), v = csub(p, y0);
+    acc[SUM_RS] += (double)(wr * u.x * v.x) + (double)(wi * u.y * v.y);
+    if (a.want_norms) {
+      const float2 pl = s_y[row * TV_EXT + ex - 1], pu = s_y[(row - 1) * TV_EXT + ex];
+      const float2 xl = s_X[row * TV_EXT + ex - 1], xu = s_X[(row - 1) * TV_EXT + ex];
+      acc[SUM_L1P] += (double)sqrtf(cabs2(p));
+      acc[SUM_TVP] += (double)sqrtf(cabs2(csub(pl, p)) + cabs2(csub(pu, p)));
+      acc[SUM_L1X] += (double)sqrtf(cabs2(x));
+      acc[SUM_TVX] += (double)sqrtf(cabs2(csub(xl, x)) + cabs2(csub(xu, x)));
+    }
+  }
+  const int blk = (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
+  block_write_sums<TV_THREADS>(acc, a.partials, blk);
+}
+
+static void tv_grid(const ProxArgs& a, dim3* g) {
+  const int inner = TV_EXT - 2 * (a.n_tv + 1);
+  *g = dim3((a.W + inner - 1) / inner, (a.H + inner - 1) / inner, a.Nz);
+}
+
+size_t max_partial_blocks(int W, int H, int Nz) {
+  // the TV prox with the largest halo it accepts (n_tv <= 20) bounds all grids
+  const int inner = TV_EXT - 2 * 21;
+  size_t tv = (size_t)((W + inner - 1) / inner) * ((H + inner - 1) / inner) * Nz;
+  size_t flat = 4096;
+  return tv > flat ? tv : flat;
+}
+
+cudaError_t launch_prox_tv2d(int storage, const ProxArgs& a, int* nblocks_out, cudaStream_t st) {
+  if (a.n_tv < 0 || a.n_tv > 20) return cudaErrorInvalidValue;
+  dim3 g;
+  tv_grid(a, &g);
+  *nblocks_out = (int)(g.x * g.y * g.z);
+  cudaError_t e;
+  switch (storage) {
+    case STORE_BF16:
+      e = allow_smem(k_prox_tv2d<__nv_bfloat162>, TV_SMEM);
+      if (e != cudaSuccess) return e;
+      k_prox_tv2d<__nv_bfloat162><<<g, TV_THREADS, TV_SMEM, st>>>(a);
+      break;
+    case STORE_F16:
+      e = allow_smem(k_prox_tv2d<__half2>, TV_SMEM);
+      if (e != cudaSuccess) return e;
+      k_prox_tv2d<__half2><<<g, TV_THREADS, TV_SMEM, st>>>(a);
+      break;
+    default:
+      e = allow_smem(k_prox_tv2d<float2>, TV_SMEM);
+      if (e != cudaSuccess) return e;
+      k_prox_tv2d<float2><<<g, TV_THREADS, TV_SMEM, st>>>(a);
+  }
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Elementwise prox (mode 5): proximalL1, sparse_compressive_holo.cu:3274-3392,
+// p = shrink(x - t g, t l1), plus the same sums (TV terms absent).
+// ---------------------------------------------------------------------------
+constexpr int FLAT_THREADS = 256;
+
+template <typename ST>
+__global__ void __launch_bounds__(FLAT_THREADS) k_prox_l1(ProxArgs a) {
+  const size_t HW = (size_t)a.W * a.H, n = HW * a.Nz;
+  const ST* P = static_cast<const ST*>(a.P);
+  const ST* Pp = static_cast<const ST*>(a.Pprev);
+  ST* Pn = static_cast<ST*>(a.Pnew);
+  double acc[kNumSums];
+#pragma unroll
+  for (int k = 0; k < kNumSums; ++k) acc[k] = 0.0;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const float2 y0 = Store<ST>::ld(P + i), pp = Store<ST>::ld(Pp + i), g = a.G[i];
+    const float2 x = make_float2(fmaf(a.beta, y0.x - pp.x, y0.x), fmaf(a.beta, y0.y - pp.y, y0.y));
+    const float2 xh = make_float2(fmaf(-a.t, g.x, x.x), fmaf(-a.t, g.y, x.y));
+    const float2 p = shrink(xh, a.thr, a.faithful);
+    Store<ST>::st(Pn + i, p);
+    const float2 d = csub(p, x);
+    acc[SUM_LIM1] += (double)(d.x * g.x) + (double)(d.y * g.y);
+    acc[SUM_LIM2] += (double)cabs2(d);
+    float wr, wi;
+    restart_w(i % HW, a.faithful, &wr, &wi);
+    const float2 u = csub(x, p), v = csub(p, y0);
+    acc[SUM_RS] += (double)(wr * u.x * v.x) + (double)(wi * u.y * v.y);
+    if (a.want_norms) {
+      acc[SUM_L1P] += (double)sqrtf(cabs2(p));
+      acc[SUM_L1X] += (double)sqrtf(cabs2(x));
+    }
+  }
+  block_write_sums<FLAT_THREADS>(acc, a.partials, blockIdx.x);
+}
+
+static int flat_blocks(size_t n) {
+  size_t b = (n + FLAT_THREADS - 1) / FLAT_THREADS;
+  size_t cap = (size_t)8 * num_sms();
+  return (int)(b < cap ? (b > 0 ? b : 1) : cap);
+}
+
+cudaError_t launch_prox_l1(int storage, const ProxArgs& a, int* nblocks_out, cudaStream_t st) {
+  const int blocks = flat_blocks((size_t)a.W * a.H * a.Nz);
+  *nblocks_out = blocks;
+  switch (storage) {
+    case STORE_BF16:
+      k_prox_l1<__nv_bfloat162><<<blocks, FLAT_THREADS, 0, st>>>(a);
+      break;
+    case STORE_F16:
+      k_prox_l1<__half2><<<blocks, FLAT_THREADS, 0, st>>>(a);
+      break;
+    default:
+      k_prox_l1<float2><<<blocks, FLAT_THREADS, 0, st>>>(a);
+  }
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// final reduction of block partials (single block, fixed order)
+// ---------------------------------------------------------------------------
+__global__ void k_reduce_partials(const double* __restrict__ partials, int nblocks, double* __restrict__ out) {
+  __shared__ double red[256];
+  for (int k = 0; k < kNumSums; ++k) {
+    double s = 0;
+    for (int b = threadIdx.x; b < nblocks; b += blockDim.x) s += partials[(size_t)b * kNumSums + k];
+    red[threadIdx.x] = s;
+    __syncthreads();
+    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
+      if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) out[k] = red[0];
+    __syncthreads();
+  }
+}
+
+cudaError_t launch_reduce_partials(const double* partials, int nblocks, double* out, cudaStream_t st) {
+  k_reduce_partials<<<1, 256, 0, st>>>(partials, nblocks, out);
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// plane-level kernels
+// ---------------------------------------------------------------------------
+// d = Re(c); sum (d - b)^2.  back_propagate_finish_kernel (:1918-1933) keeps
+// only the real part; calcResidual (:2676-2723) forms r = estimate - measured.
+__global__ void __launch_bounds__(FLAT_THREADS) k_finish_forward(const float2* __restrict__ c,
+                                                                 const float* __restrict__ b,
+                                                                 float* __restrict__ dnew, long long n,
+                                                                 double* partials) {
+  double acc[kNumSums];
+#pragma unroll
+  for (int k = 0; k < kNumSums; ++k) acc[k] = 0.0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const float d = c[i].x;
+    dnew[i] = d;
+    const float r = d - b[i];
+    acc[SUM_RR] += (double)r * (double)r;
+  }
+  block_write_sums<FLAT_THREADS>(acc, partials, blockIdx.x);
+}
+
+cudaError_t launch_finish_forward(const float2* c, const float* b, float* dnew, long long n, double* partials,
+                                  int* nblocks_out, cudaStream_t st) {
+  const int blocks = flat_blocks((size_t)n);
+  *nblocks_out = blocks;
+  k_finish_forward<<<blocks, FLAT_THREADS, 0, st>>>(c, b, dnew, n, partials);
+  return cudaGetLastError();
+}
+
+// Momentum in hologram space (:480-498, fistaUpdate on holograms :4599-4642):
+// dX = d + beta (d - dY0); dY0 = d; r = dX - b.
+__global__ void __launch_bounds__(FLAT_THREADS) k_holo_momentum(const float* __restrict__ dnew, float* dY0,
+                                                                float* __restrict__ dX, const float* __restrict__ b,
+                                                                float* __restrict__ r, float beta, long long n,
+                                                                double* partials) {
+  double acc[kNumSums];
+#pragma unroll
+  for (int k = 0; k < kNumSums; ++k) acc[k] = 0.0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const float d = dnew[i], d0 = dY0[i];
+    const float x = fmaf(beta, d - d0, d);
+    dX[i] = x;
+    dY0[i] = d;
+    const float rr = x - b[i];
+    r[i] = rr;
+    acc[SUM_RR] += (double)rr * (double)rr;
+  }
+  block_write_sums<FLAT_THREADS>(acc, partials, blockIdx.x);
+}
+
+cudaError_t launch_holo_momentum(const float* dnew, float* dY0, float* dX, const float* b, float* r, float beta,
+                                 long long n, double* partials, int* nblocks_out, cudaStream_t st) {
+  const int blocks = flat_blocks((size_t)n);
+  *nblocks_out = blocks;
+  k_holo_momentum<<<blocks, FLAT_THREADS, 0, st>>>(dnew, dY0, dX, b, r, beta, n, partials);
+  return cudaGetLastError();
+}
+
+// L1 and TV norms of the momentum point x = P + beta (P - Pprev):
+// calcL1NormComplex (sparse_volume.cu:194-235), calcTVNorm2d (:365-446),
+// calcTVNorm (:240-363, periodic in z).
+template <typename ST>
+__device__ __forceinline__ float2 xval(const ST* P, const ST* Pp, float beta, size_t i) {
+  const float2 p = Store<ST>::ld(P + i), pp = Store<ST>::ld(Pp + i);
+  return make_float2(fmaf(beta, p.x - pp.x, p.x), fmaf(beta, p.y - pp.y, p.y));
+}
+
+template <typename ST>
+__global__ void __launch_bounds__(FLAT_THREADS) k_momentum_norms(const ST* __restrict__ P, const ST* __restrict__ Pp,
+                                                                 float beta, int W, int H, int Nz, int mode,
+                                                                 double* partials) {
+  double acc[kNumSums];
+#pragma unroll
+  for (int k = 0; k < kNumSums; ++k) acc[k] = 0.0;
+  const size_t HW = (size_t)W * H, n = HW * Nz;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const int z = (int)(i / HW);
+    const size_t e = i - (size_t)z * HW;
+    const int yy = (int)(e / W), xx = (int)(e - (size_t)yy * W);
+    const float2 x = xval(P, Pp, beta, i);
+    acc[SUM_L1X] += (double)sqrtf(cabs2(x));
+    if (mode == 7 || mode == 6) {
+      const int xm = xx > 0 ? xx - 1 : W - 1, ym = yy > 0 ? yy - 1 : H - 1;
+      const float2 xl = xval(P, Pp, beta, (size_t)z * HW + (size_t)yy * W + xm);
+      const float2 xu = xval(P, Pp, beta, (size_t)z * HW + (size_t)ym * W + xx);
+      float q = cabs2(csub(xl, x)) + cabs2(csub(xu, x));
+      if (mode == 6) {
+        const int zm = z > 0 ? z - 1 : Nz - 1;
+        q += cabs2(csub(xval(P, Pp, beta, (size_t)zm * HW + e), x));
+      }
+      acc[SUM_TVX] += (double)sqrtf(q);
+    }
+  }
+  block_write_sums<FLAT_THREADS>(acc, partials, blockIdx.x);
+}
+
+cudaError_t launch_momentum_norms(int storage, const void* P, const void* Pprev, float beta, int W, int H, int Nz,
+                                  int mode, double* partials, int* nblocks_out, cudaStream_t st) {
+  const int blocks = flat_blocks((size_t)W * H * Nz);
+  *nblocks_out = blocks;
+  switch (storage) {
+    case STORE_BF16:
+      k_momentum_norms<__nv_bfloat162><<<blocks, FLAT_THREADS, 0, st>>>(
+          (const __nv_bfloat162*)P, (const __nv_bfloat162*)Pprev, beta, W, H, Nz, mode, partials);
+      break;
+    case STORE_F16:
+      k_momentum_norms<__half2><<<blocks, FLAT_THREADS, 0, st>>>((const __half2*)P, (const __half2*)Pprev, beta, W,
+                                                                  H, Nz, mode, partials);
+      break;
+    default:
+      k_momentum_norms<float2><<<blocks, FLAT_THREADS, 0, st>>>((const float2*)P, (const float2*)Pprev, beta, W, H,
+                                                                 Nz, mode, partials);
+  }
+  return cudaGetLastError();
+}
+
+template <typename ST>
+__global__ void k_materialize_x(const ST* __restrict__ P, const ST* __restrict__ Pp, float beta, float2* out,
+                                long long n) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    out[i] = xval(P, Pp, beta, (size_t)i);
+}
+
+cudaError_t launch_materialize_x(int storage, const void* P, const void* Pprev, float beta, float2* out, long long n,
+                                 cudaStream_t st) {
+  const int blocks = flat_blocks((size_t)n);
+  switch (storage) {
+    case STORE_BF16:
+      k_materialize_x<<<blocks, FLAT_THREADS, 0, st>>>((const __nv_bfloat162*)P, (const __nv_bfloat162*)Pprev, beta,
+                                                       out, n);
+      break;
+    case STORE_F16:
+      k_materialize_x<<<blocks, FLAT_THREADS, 0, st>>>((const __half2*)P, (const __half2*)Pprev, beta, out, n);
+      break;
+    default:
+      k_materialize_x<<<blocks, FLAT_THREADS, 0, st>>>((const float2*)P, (const float2*)Pprev, beta, out, n);
+  }
+  return cudaGetLastError();
+}
+
+template <typename ST>
+__global__ void k_store_volume(const float2* __restrict__ in, ST* __restrict__ out, long long n) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    Store<ST>::st(out + i, in[i]);
+}
+
+cudaError_t launch_store_volume(int storage, const float2* in, void* out, long long n, cudaStream_t st) {
+  const int blocks = flat_blocks((size_t)n);
+  switch (storage) {
+    case STORE_BF16:
+      k_store_volume<<<blocks, FLAT_THREADS, 0, st>>>(in, (__nv_bfloat162*)out, n);
+      break;
+    case STORE_F16:
+      k_store_volume<<<blocks, FLAT_THREADS, 0, st>>>(in, (__half2*)out, n);
+      break;
+    default:
+      k_store_volume<<<blocks, FLAT_THREADS, 0, st>>>(in, (float2*)out, n);
+  }
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// 3-D fused lasso (mode 6): proximalFusedLasso (:3422-3475) with
+// totalVariationProjection (:3832-4018): half threshold, n_tv unnormalised dual
+// steps over the whole volume (periodic in x, y, z; the projection is disabled
+// at :3964), final estimate, half threshold.
+// ---------------------------------------------------------------------------
+template <typename ST>
+__global__ void k_prox6_init(ProxArgs a, float2* __restrict__ X1) {
+  const size_t n = (size_t)a.W * a.H * a.Nz;
+  const ST* P = static_cast<const ST*>(a.P);
+  const ST* Pp = static_cast<const ST*>(a.Pprev);
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const float2 x = xval(P, Pp, a.beta, i), g = a.G[i];
+    const float2 xh = make_float2(fmaf(-a.t, g.x, x.x), fmaf(-a.t, g.y, x.y));
+    X1[i] = shrink(xh, 0.5f * a.thr, a.faithful);
+  }
+}
+
+cudaError_t launch_prox6_init(int storage, const ProxArgs& a, float2* X1, cudaStream_t st) {
+  const int blocks = flat_blocks((size_t)a.W * a.H * a.Nz);
+  switch (storage) {
+    case STORE_BF16:
+      k_prox6_init<__nv_bfloat162><<<blocks, FLAT_THREADS, 0, st>>>(a, X1);
+      break;
+    case STORE_F16:
+      k_prox6_init<__half2><<<blocks, FLAT_THREADS, 0, st>>>(a, X1);
+      break;
+    default:
+      k_prox6_init<float2><<<blocks, FLAT_THREADS, 0, st>>>(a, X1);
+  }
+  return cudaGetLastError();
+}
+
+__global__ void k_tv3_estimate(const float2* __restrict__ X1, const float2* __restrict__ gx,
+                               const float2* __restrict__ gy, const float2* __restrict__ gz, float2* __restrict__ Y,
+                               int W, int H, int Nz, float mu) {
+  const size_t HW = (size_t)W * H, n = HW * Nz;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const int z = (int)(i / HW);
+    const size_t e = i - (size_t)z * HW;
+    const int yy = (int)(e / W), xx = (int)(e - (size_t)yy * W);
+    const int xp = xx < W - 1 ? xx + 1 : 0, yp = yy < H - 1 ? yy + 1 : 0, zp = z < Nz - 1 ? z + 1 : 0;
+    const float2 d1 = csub(gx[(size_t)z * HW + (size_t)yy * W + xp], gx[i]);
+    const float2 d2 = csub(gy[(size_t)z * HW + (size_t)yp * W + xx], gy[i]);
+    const float2 d3 = csub(gz[(size_t)zp * HW + e], gz[i]);
+    const float2 dv = cadd(cadd(d1, d2), d3);
+    Y[i] = make_float2(fmaf(-mu, dv.x, X1[i].x), fmaf(-mu, dv.y, X1[i].y));
+  }
+}
+
+cudaError_t launch_tv3_estimate(const float2* X1, const float2* gx, const float2* gy, const float2* gz, float2* Y,
+                                int W, int H, int Nz, float mu, cudaStream_t st) {
+  k_tv3_estimate<<<flat_blocks((size_t)W * H * Nz), FLAT_THREADS, 0, st>>>(X1, gx, gy, gz, Y, W, H, Nz, mu);
+  return cudaGetLastError();
+}
+
+__global__ void k_tv3_dual(const float2* __restrict__ Y, float2* gx, float2* gy, float2* gz, int W, int H, int Nz,
+                           float s) {
+  const size_t HW = (size_t)W * H, n = HW * Nz;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const int z = (int)(i / HW);
+    const size_t e = i - (size_t)z * HW;
+    const int yy = (int)(e / W), xx = (int)(e - (size_t)yy * W);
+    const int xm = xx > 0 ? xx - 1 : W - 1, ym = yy > 0 ? yy - 1 : H - 1, zm = z > 0 ? z - 1 : Nz - 1;
+    const float2 yv = Y[i];
+    const float2 a1 = csub(Y[(size_t)z * HW + (size_t)yy * W + xm], yv);
+    const float2 a2 = csub(Y[(size_t)z * HW + (size_t)ym * W + xx], yv);
+    const float2 a3 = csub(Y[(size_t)zm * HW + e], yv);
+    gx[i] = make_float2(fmaf(s, a1.x, gx[i].x), fmaf(s, a1.y, gx[i].y));
+    gy[i] = make_float2(fmaf(s, a2.x, gy[i].x), fmaf(s, a2.y, gy[i].y));
+    gz[i] = make_float2(fmaf(s, a3.x, gz[i].x), fmaf(s, a3.y, gz[i].y));
+  }
+}
+
+cudaError_t launch_tv3_dual(const float2* Y, float2* gx, float2* gy, float2* gz, int W, int H, int Nz, float s,
+                            cudaStream_t st) {
+  k_tv3_dual<<<flat_blocks((size_t)W * H * Nz), FLAT_THREADS, 0, st>>>(Y, gx, gy, gz, W, H, Nz, s);
+  return cudaGetLastError();
+}
+
+template <typename ST>
+__global__ void __launch_bounds__(FLAT_THREADS) k_prox6_finish(ProxArgs a, const float2* __restrict__ Y) {
+  const int W = a.W, H = a.H, Nz = a.Nz;
+  const size_t HW = (size_t)W * H, n = HW * Nz;
+  const ST* P = static_cast<const ST*>(a.P);
+  const ST* Pp = static_cast<const ST*>(a.Pprev);
+  ST* Pn = static_cast<ST*>(a.Pnew);
+  const float T = 0.5f * a.thr;
+  double acc[kNumSums];
+#pragma unroll
+  for (int k = 0; k < kNumSums; ++k) acc[k] = 0.0;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+    const int z = (int)(i / HW);
+    const size_t e = i - (size_t)z * HW;
+    const int yy = (int)(e / W), xx = (int)(e - (size_t)yy * W);
+    const float2 p = shrink(Y[i], T, a.faithful);
+    Store<ST>::st(Pn + i, p);
+    const float2 y0 = Store<ST>::ld(P + i);
+    const float2 x = xval(P, Pp, a.beta, i), g = a.G[i];
+    const float2 d = csub(p, x);
+    acc[SUM_LIM1] += (double)(d.x * g.x) + (double)(d.y * g.y);
+    acc[SUM_LIM2] += (double)cabs2(d);
+    float wr, wi;
+    restart_w(e, a.faithful, &wr, &wi);
+    const float2 u = csub(x, p), v = csub(p, y0);
+    acc[SUM_RS] += (double)(wr * u.x * v.x) + (double)(wi * u.y * v.y);
+    if (a.want_norms) {
+      const int xm = xx > 0 ? xx - 1 : W - 1, ym = yy > 0 ? yy - 1 : H - 1, zm = z > 0 ? z - 1 : Nz - 1;
+      const size_t il = (size_t)z * HW + (size_t)yy * W + xm, iu = (size_t)z * HW + (size_t)ym * W + xx,
+                   ib = (size_t)zm * HW + e;
+      const float2 pl = shrink(Y[il], T, a.faithful), pu = shrink(Y[iu], T, a.faithful),
+                   pb = shrink(Y[ib], T, a.faithful);
+      acc[SUM_L1P] += (double)sqrtf(cabs2(p));
+      acc[SUM_TVP] += (double)sqrtf(cabs2(csub(pl, p)) + cabs2(csub(pu, p)) + cabs2(csub(pb, p)));
+      const float2 xl = xval(P, Pp, a.beta, il), xu = xval(P, Pp, a.beta, iu), xb = xval(P, Pp, a.beta, ib);
+      acc[SUM_L1X] += (double)sqrtf(cabs2(x));
+      acc[SUM_TVX] += (double)sqrtf(cabs2(csub(xl, x)) + cabs2(csub(xu, x)) + cabs2(csub(xb, x)));
+    }
+  }
+  block_write_sums<FLAT_THREADS>(acc, a.partials, blockIdx.x);
+}
+
+cudaError_t launch_prox6_finish(int storage, const ProxArgs& a, const float2* Y, int* nblocks_out, cudaStream_t st) {
+  const int blocks = flat_blocks((size_t)a.W * a.H * a.Nz);
+  *nblocks_out = blocks;
+  switch (storage) {
+    case STORE_BF16:
+      k_prox6_finish<__nv_bfloat162><<<blocks, FLAT_THREADS, 0, st>>>(a, Y);
+      break;
+    case STORE_F16:
+      k_prox6_finish<__half2><<<blocks, FLAT_THREADS, 0, st>>>(a, Y);
+      break;
+    default:
+      k_prox6_finish<float2><<<blocks, FLAT_THREADS, 0, st>>>(a, Y);
+  }
+  return cudaGetLastError();
+}
+
+}  // namespace rihvr

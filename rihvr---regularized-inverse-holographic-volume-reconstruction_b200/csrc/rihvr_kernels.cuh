@@ -1,0 +1,74 @@
+// Kernel launchers shared by the solver (all asynchronous on the given stream).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace rihvr {
+
+// Slots of the per-block FP64 partial sums written by reduction kernels.
+constexpr int kNumSums = 8;
+enum SumIndex {
+  SUM_LIM1 = 0,  // sum over real components of (p - x) * g          (line-search term 1)
+  SUM_LIM2 = 1,  // sum |p - x|^2                                     (line-search term 2)
+  SUM_RS = 2,    // restart statistic sum (x - p) * (p - y0)
+  SUM_L1P = 3,   // sum |p|      (complex modulus)
+  SUM_TVP = 4,   // TV(p)
+  SUM_L1X = 5,   // sum |x|
+  SUM_TVX = 6,   // TV(x)
+  SUM_RR = 7,    // sum r^2 of a residual plane
+};
+
+enum StorageKind { STORE_F32 = 0, STORE_BF16 = 1, STORE_F16 = 2 };
+enum ElemKind { ELEM_C32 = 0, ELEM_R32 = 1, ELEM_STORE_F32 = 2, ELEM_STORE_BF16 = 3, ELEM_STORE_F16 = 4 };
+
+struct ProxArgs {
+  const void* P;      // previous prox output y0 (storage type)
+  const void* Pprev;  // the prox output before it (storage type)
+  const float2* G;    // gradient volume A^H r(x)
+  void* Pnew;         // new prox output (storage type)
+  int W, H, Nz;
+  float beta;         // momentum point x = P + beta (P - Pprev)
+  float t;            // step size
+  float mu;           // t * tv
+  float s;            // dual step 1 / (12 t tv)
+  float thr;          // shrink threshold (0 = no shrink)
+  int n_tv;           // Chambolle iterations
+  int faithful;       // reference quirks (separable shrink, restart weights)
+  int want_norms;     // accumulate L1/TV of p and x
+  double* partials;   // [blocks][kNumSums]
+};
+
+bool line_size_supported(int n);
+size_t max_partial_blocks(int W, int H, int Nz);
+
+cudaError_t launch_adj_col(const float2* Rs, const double* cturn, const double* zlist, float2* U, int W,
+                           int H, int z0, int z1, cudaStream_t st);
+cudaError_t launch_rows(int inverse, int in_kind, const void* in, int out_kind, void* out, int W,
+                        long long nlines, float scale, cudaStream_t st);
+cudaError_t launch_fwd_col(const float2* T, const double* cturn, const double* zlist, float2* Spart, int W,
+                           int H, int z0, int z1, int nchunks, cudaStream_t st);
+int fwd_col_chunks(int W, int H, int Nz);
+cudaError_t launch_plane_col(int inverse, const float2* in, float2* out, int W, int H, float scale,
+                             cudaStream_t st);
+cudaError_t launch_sum_chunks(const float2* Spart, int nchunks, float2* S, long long n, cudaStream_t st);
+cudaError_t launch_prox_tv2d(int storage, const ProxArgs& a, int* nblocks_out, cudaStream_t st);
+cudaError_t launch_prox_l1(int storage, const ProxArgs& a, int* nblocks_out, cudaStream_t st);
+cudaError_t launch_reduce_partials(const double* partials, int nblocks, double* out, cudaStream_t st);
+cudaError_t launch_finish_forward(const float2* c, const float* b, float* dnew, long long n, double* partials,
+                                  int* nblocks_out, cudaStream_t st);
+cudaError_t launch_holo_momentum(const float* dnew, float* dY0, float* dX, const float* b, float* r,
+                                 float beta, long long n, double* partials, int* nblocks_out, cudaStream_t st);
+cudaError_t launch_momentum_norms(int storage, const void* P, const void* Pprev, float beta, int W, int H,
+                                  int Nz, int mode, double* partials, int* nblocks_out, cudaStream_t st);
+cudaError_t launch_materialize_x(int storage, const void* P, const void* Pprev, float beta, float2* out,
+                                 long long n, cudaStream_t st);
+cudaError_t launch_store_volume(int storage, const float2* in, void* out, long long n, cudaStream_t st);
+cudaError_t launch_prox6_init(int storage, const ProxArgs& a, float2* X1, cudaStream_t st);
+cudaError_t launch_tv3_estimate(const float2* X1, const float2* gx, const float2* gy, const float2* gz, float2* Y,
+                                int W, int H, int Nz, float mu, cudaStream_t st);
+cudaError_t launch_tv3_dual(const float2* Y, float2* gx, float2* gy, float2* gz, int W, int H, int Nz, float s,
+                            cudaStream_t st);
+cudaError_t launch_prox6_finish(int storage, const ProxArgs& a, const float2* Y, int* nblocks_out,
+                                cudaStream_t st);
+
+}  // namespace rihvr

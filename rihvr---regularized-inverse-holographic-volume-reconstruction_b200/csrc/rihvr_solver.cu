@@ -1,0 +1,724 @@
+// Host side of the C ABI: context, device buffers and the FISTA/FASTA loop of
+// SparseCompressiveHolo::inverseReconstruct (RIHVR src/core/
+// sparse_compressive_holo.cu:173-633), arranged around three volume buffers.
+//
+// Volume buffers rotate through the roles P_{k-1}, P_k, P_{k+1} (prox outputs).
+// The momentum point x_k = P_k + beta_k (P_k - P_{k-1}) (fistaUpdate, :4496-4576)
+// is never stored: the prox kernel forms it on the fly, and the forward operator
+// at x_k follows by linearity from the two stored hologram estimates
+// (:480-498).  The gradient volume A^H r(x_k) is computed once per iteration and
+// reused by every backtracking attempt (the reference recomputes it per plane
+// access, sparse_gradient.cu:125-165).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/rihvr.h"
+#include "rihvr_kernels.cuh"
+
+using namespace rihvr;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string& msg) {
+  g_last_error = msg;
+  return code;
+}
+
+#define CK(call)                                                                                   \
+  do {                                                                                             \
+    cudaError_t e_ = (call);                                                                       \
+    if (e_ != cudaSuccess) {                                                                       \
+      return fail(e_ == cudaErrorMemoryAllocation ? RIHVR_ERR_OUT_OF_MEMORY : RIHVR_ERR_CUDA,      \
+                  std::string(#call) + ": " + cudaGetErrorString(e_));                            \
+    }                                                                                              \
+  } while (0)
+
+// kernel launch: check and count (one of our kernels per launcher call)
+#define KL(call)        \
+  do {                  \
+    CK(call);           \
+    ++c->launches;      \
+  } while (0)
+
+#define RC(call)                     \
+  do {                               \
+    int r_ = (call);                 \
+    if (r_ != RIHVR_OK) return r_;   \
+  } while (0)
+
+enum KernelClass { K_ADJ_COL = 0, K_ADJ_ROW, K_PROX, K_FWD_ROW, K_FWD_COL, K_PLANE, K_NUM };
+const char* kClassNames[K_NUM] = {"adj_col", "adj_row", "prox", "fwd_row", "fwd_col", "plane"};
+
+enum Slot { SLOT_PROX = 0, SLOT_FWD = 1, SLOT_MOM = 2, SLOT_NORM = 3, NUM_SLOTS = 4 };
+
+}  // namespace
+
+struct rihvr_ctx {
+  rihvr_params p{};
+  int W = 0, H = 0, Nz = 0;
+  size_t HW = 0, V = 0;
+  int mode = 7;
+  int storage = 0;
+  size_t esize = 8;
+  int device = 0;
+  cudaStream_t st = nullptr;
+
+  void* vol[3] = {nullptr, nullptr, nullptr};
+  int iPrev = 0, iCur = 1, iNew = 2;
+  float2* G = nullptr;    // gradient volume
+  float2* U = nullptr;    // column/row intermediate volume
+  float2* Spart = nullptr;
+  float2* S = nullptr;
+  float2* pc1 = nullptr;
+  float2* pc2 = nullptr;
+  float2* Rs = nullptr;   // residual spectrum / (W H)
+  float* b = nullptr;
+  float* dnew = nullptr;
+  float* dY0 = nullptr;
+  float* dX = nullptr;
+  float* r = nullptr;
+  double* cturn = nullptr;
+  double* zlist = nullptr;
+  double* partials = nullptr;
+  size_t partial_cap = 0;
+  double* sums_d = nullptr;
+  double* sums_h = nullptr;  // pinned
+  int nchunks = 1;
+  float2 *X1 = nullptr, *gx = nullptr, *gy = nullptr, *gz = nullptr, *Y = nullptr;  // mode 6
+
+  double t = 0, alpha1 = 1, beta = 0, prev_f_resid = 0;
+  int it = 0;
+  bool have_holo = false;
+  std::vector<rihvr_iter_record> log;
+  int pending_x = -1;  // record whose x-terms arrive with the next prox sweep
+
+  bool profiling = false;
+  struct Ev {
+    int cls;
+    cudaEvent_t a, b;
+  };
+  std::vector<Ev> evs;
+  std::vector<cudaEvent_t> ev_pool;
+  size_t ev_used = 0;
+  size_t bytes = 0;
+  long long launches = 0;  // kernels launched by this context
+  std::vector<void*> allocs;
+};
+
+namespace {
+
+int dalloc(rihvr_ctx* c, void** p, size_t n) {
+  cudaError_t e = cudaMalloc(p, n);
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    cudaGetLastError();
+    return fail(RIHVR_ERR_OUT_OF_MEMORY, "cudaMalloc of " + std::to_string(n) + " bytes failed: " +
+                                             cudaGetErrorString(e));
+  }
+  c->allocs.push_back(*p);
+  c->bytes += n;
+  return RIHVR_OK;
+}
+
+template <typename T>
+int dalloc_t(rihvr_ctx* c, T** p, size_t count) {
+  return dalloc(c, reinterpret_cast<void**>(p), sizeof(T) * count);
+}
+
+int elem_kind(int storage) {
+  return storage == STORE_BF16 ? ELEM_STORE_BF16 : storage == STORE_F16 ? ELEM_STORE_F16 : ELEM_STORE_F32;
+}
+
+cudaEvent_t take_event(rihvr_ctx* c) {
+  if (c->ev_used < c->ev_pool.size()) return c->ev_pool[c->ev_used++];
+  cudaEvent_t e;
+  cudaEventCreate(&e);
+  c->ev_pool.push_back(e);
+  c->ev_used++;
+  return e;
+}
+
+struct ProfScope {
+  rihvr_ctx* c;
+  int cls;
+  cudaEvent_t a = nullptr;
+  ProfScope(rihvr_ctx* c_, int cls_) : c(c_), cls(cls_) {
+    if (c->profiling) {
+      a = take_event(c);
+      cudaEventRecord(a, c->st);
+    }
+  }
+  ~ProfScope() {
+    if (c->profiling) {
+      cudaEvent_t b = take_event(c);
+      cudaEventRecord(b, c->st);
+      c->evs.push_back({cls, a, b});
+    }
+  }
+};
+
+// --- plane-level helpers ----------------------------------------------------
+
+// Rs = FFT2(r) / (W H)  (SparseGradient::reconstruct, sparse_gradient.cu:47-75)
+int residual_spectrum(rihvr_ctx* c) {
+  ProfScope ps(c, K_PLANE);
+  KL(launch_rows(0, ELEM_R32, c->r, ELEM_C32, c->pc1, c->W, c->H, 1.0f, c->st));
+  KL(launch_plane_col(0, c->pc1, c->Rs, c->W, c->H, 1.0f / (float)c->HW, c->st));
+  return RIHVR_OK;
+}
+
+int reduce_into(rihvr_ctx* c, int nblocks, int slot) {
+  KL(launch_reduce_partials(c->partials, nblocks, c->sums_d + slot * kNumSums, c->st));
+  return RIHVR_OK;
+}
+
+// G = A^H r: column pass from the spectrum, then the inverse row pass.
+int adjoint_volume(rihvr_ctx* c) {
+  {
+    ProfScope ps(c, K_ADJ_COL);
+    KL(launch_adj_col(c->Rs, c->cturn, c->zlist, c->U, c->W, c->H, 0, c->Nz, c->st));
+  }
+  {
+    ProfScope ps(c, K_ADJ_ROW);
+    KL(launch_rows(1, ELEM_C32, c->U, ELEM_C32, c->G, c->W, (long long)c->Nz * c->H, 1.0f, c->st));
+  }
+  return RIHVR_OK;
+}
+
+// dnew = A vol (the volume in `kind` layout), sum (dnew - b)^2 into SLOT_FWD.
+int forward_volume(rihvr_ctx* c, int kind, const void* vol) {
+  {
+    ProfScope ps(c, K_FWD_ROW);
+    KL(launch_rows(0, kind, vol, ELEM_C32, c->U, c->W, (long long)c->Nz * c->H, 1.0f, c->st));
+  }
+  {
+    ProfScope ps(c, K_FWD_COL);
+    KL(launch_fwd_col(c->U, c->cturn, c->zlist, c->Spart, c->W, c->H, 0, c->Nz, c->nchunks, c->st));
+  }
+  ProfScope ps(c, K_PLANE);
+  KL(launch_sum_chunks(c->Spart, c->nchunks, c->S, (long long)c->HW, c->st));
+  KL(launch_plane_col(1, c->S, c->pc1, c->W, c->H, 1.0f, c->st));
+  KL(launch_rows(1, ELEM_C32, c->pc1, ELEM_C32, c->pc2, c->W, c->H, 1.0f / (float)c->HW, c->st));
+  int nb = 0;
+  KL(launch_finish_forward(c->pc2, c->b, c->dnew, (long long)c->HW, c->partials, &nb, c->st));
+  return reduce_into(c, nb, SLOT_FWD);
+}
+
+ProxArgs prox_args(rihvr_ctx* c, double t) {
+  ProxArgs a;
+  a.P = c->vol[c->iCur];
+  a.Pprev = c->vol[c->iPrev];
+  a.G = c->G;
+  a.Pnew = c->vol[c->iNew];
+  a.W = c->W;
+  a.H = c->H;
+  a.Nz = c->Nz;
+  a.beta = (float)c->beta;
+  a.t = (float)t;
+  const double tv = (double)c->p.regularization_TV_param;
+  a.mu = (float)(t * tv);
+  a.s = tv > 0 ? (float)(1.0 / (4.0 * 3.0 * t * tv)) : 0.f;
+  a.thr = (float)(t * (double)c->p.regularization_param);
+  a.n_tv = c->p.num_tv_iterations;
+  a.faithful = c->p.faithful;
+  a.want_norms = c->p.record_objective;
+  a.partials = c->partials;
+  return a;
+}
+
+// P_{k+1} = prox(x_k - t G) for the active mode; sums into SLOT_PROX.
+int prox_volume(rihvr_ctx* c, double t) {
+  ProxArgs a = prox_args(c, t);
+  int nb = 0;
+  ProfScope ps(c, K_PROX);
+  if (c->mode == 7) {
+    // proximalFusedLasso2d (:3652-3732); block_soft_threshold only if l1 > 0 (:3715)
+    if (!(c->p.regularization_param > 0.f)) a.thr = 0.f;
+    KL(launch_prox_tv2d(c->storage, a, &nb, c->st));
+  } else if (c->mode == 5) {
+    KL(launch_prox_l1(c->storage, a, &nb, c->st));
+  } else {
+    KL(launch_prox6_init(c->storage, a, c->X1, c->st));
+    CK(cudaMemsetAsync(c->gx, 0, sizeof(float2) * c->V, c->st));
+    CK(cudaMemsetAsync(c->gy, 0, sizeof(float2) * c->V, c->st));
+    CK(cudaMemsetAsync(c->gz, 0, sizeof(float2) * c->V, c->st));
+    for (int i = 0; i < a.n_tv; ++i) {
+      KL(launch_tv3_estimate(c->X1, c->gx, c->gy, c->gz, c->Y, c->W, c->H, c->Nz, a.mu, c->st));
+      KL(launch_tv3_dual(c->Y, c->gx, c->gy, c->gz, c->W, c->H, c->Nz, a.s, c->st));
+    }
+    KL(launch_tv3_estimate(c->X1, c->gx, c->gy, c->gz, c->Y, c->W, c->H, c->Nz, a.mu, c->st));
+    KL(launch_prox6_finish(c->storage, a, c->Y, &nb, c->st));
+  }
+  return reduce_into(c, nb, SLOT_PROX);
+}
+
+int fetch_sums(rihvr_ctx* c) {
+  CK(cudaMemcpyAsync(c->sums_h, c->sums_d, sizeof(double) * kNumSums * NUM_SLOTS, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return RIHVR_OK;
+}
+
+double tv_weight(const rihvr_ctx* c) { return c->mode == 5 ? 0.0 : (double)c->p.regularization_TV_param; }
+
+int state_reset(rihvr_ctx* c) {
+  for (int i = 0; i < 3; ++i) CK(cudaMemsetAsync(c->vol[i], 0, c->esize * c->V, c->st));
+  CK(cudaMemsetAsync(c->dnew, 0, sizeof(float) * c->HW, c->st));
+  CK(cudaMemsetAsync(c->dY0, 0, sizeof(float) * c->HW, c->st));
+  c->iPrev = 0;
+  c->iCur = 1;
+  c->iNew = 2;
+  c->beta = 0;
+  c->alpha1 = 1;
+  c->t = c->p.initial_step > 0 ? c->p.initial_step : 1.0 / (double)c->p.num_planes;
+  c->it = 0;
+  c->log.clear();
+  c->pending_x = -1;
+  // x = 0: d = 0, r = -b (:273)
+  int nb = 0;
+  KL(launch_holo_momentum(c->dnew, c->dY0, c->dX, c->b, c->r, 0.f, (long long)c->HW, c->partials, &nb, c->st));
+  RC(reduce_into(c, nb, SLOT_MOM));
+  RC(residual_spectrum(c));
+  RC(fetch_sums(c));
+  c->prev_f_resid = 0.5 * c->sums_h[SLOT_MOM * kNumSums + SUM_RR];
+  return RIHVR_OK;
+}
+
+// Fill the momentum-point terms of the last record from the x-norm sums.
+void settle_x_terms(rihvr_ctx* c, const double* s) {
+  if (c->pending_x < 0) return;
+  rihvr_iter_record& rec = c->log[c->pending_x];
+  rec.l1_x = s[SUM_L1X];
+  rec.tv_x = s[SUM_TVX];
+  rec.f_x = rec.f_resid_x + (double)c->p.regularization_param * rec.l1_x + tv_weight(c) * rec.tv_x;
+  c->pending_x = -1;
+}
+
+int norms_at_x(rihvr_ctx* c, double* l1x, double* tvx) {
+  int nb = 0;
+  KL(launch_momentum_norms(c->storage, c->vol[c->iCur], c->vol[c->iPrev], (float)c->beta, c->W, c->H, c->Nz,
+                           c->mode, c->partials, &nb, c->st));
+  RC(reduce_into(c, nb, SLOT_NORM));
+  RC(fetch_sums(c));
+  *l1x = c->sums_h[SLOT_NORM * kNumSums + SUM_L1X];
+  *tvx = c->sums_h[SLOT_NORM * kNumSums + SUM_TVX];
+  return RIHVR_OK;
+}
+
+// One FISTA iteration (:299-611).
+int one_iteration(rihvr_ctx* c) {
+  double alpha0 = c->alpha1;
+  RC(adjoint_volume(c));
+  int bt = 0;
+  double f_resid = 0, lim = 0, ratio = 0;
+  const double* sp = c->sums_h + SLOT_PROX * kNumSums;
+  for (;;) {
+    RC(prox_volume(c, c->t));
+    RC(forward_volume(c, elem_kind(c->storage), c->vol[c->iNew]));
+    RC(fetch_sums(c));
+    if (bt == 0 && c->p.record_objective) settle_x_terms(c, sp);
+    f_resid = 0.5 * c->sums_h[SLOT_FWD * kNumSums + SUM_RR];
+    lim = sp[SUM_LIM1] + sp[SUM_LIM2] / (2.0 * c->t);
+    ratio = f_resid / (c->prev_f_resid + lim);
+    if (((ratio > 1.0) || (ratio < 0.0)) && bt < c->p.max_backtracks) {
+      c->t *= 0.5;  // stepsize_shrinkage (:63)
+      ++bt;
+      continue;
+    }
+    break;
+  }
+  rihvr_iter_record rec{};
+  rec.f_resid_prox = f_resid;
+  rec.lim = lim;
+  rec.ratio = ratio;
+  rec.t = c->t;
+  rec.backtracks = bt;
+  rec.restart_sum = sp[SUM_RS];
+  rec.f_prox = f_resid + (double)c->p.regularization_param * sp[SUM_L1P] + tv_weight(c) * sp[SUM_TVP];
+  // fistaRestart (:471-475) and the alpha/beta update (:476-481)
+  const bool restarted = sp[SUM_RS] > 0.0;
+  if (restarted) alpha0 = 1.0;
+  c->alpha1 = (1.0 + std::sqrt(1.0 + 4.0 * alpha0 * alpha0)) / 2.0;
+  const double beta = (alpha0 - 1.0) / c->alpha1;
+  rec.beta = beta;
+  rec.restarted = restarted ? 1 : 0;
+  // hologram momentum, residual at the new momentum point and its spectrum
+  int nb = 0;
+  KL(launch_holo_momentum(c->dnew, c->dY0, c->dX, c->b, c->r, (float)beta, (long long)c->HW, c->partials, &nb,
+                          c->st));
+  RC(reduce_into(c, nb, SLOT_MOM));
+  RC(residual_spectrum(c));
+  // rotate: P_{k-1} <- P_k, P_k <- P_{k+1}
+  const int old_prev = c->iPrev;
+  c->iPrev = c->iCur;
+  c->iCur = c->iNew;
+  c->iNew = old_prev;
+  c->beta = beta;
+  RC(fetch_sums(c));
+  c->prev_f_resid = 0.5 * c->sums_h[SLOT_MOM * kNumSums + SUM_RR];
+  rec.f_resid_x = c->prev_f_resid;
+  rec.f_x = rec.f_resid_x;
+  c->log.push_back(rec);
+  c->pending_x = (int)c->log.size() - 1;
+  c->it++;
+  return RIHVR_OK;
+}
+
+int run_iterations(rihvr_ctx* c, int n) {
+  if (!c->have_holo) return fail(RIHVR_ERR_MISSING_DATA, "no hologram set");
+  for (int i = 0; i < n; ++i) RC(one_iteration(c));
+  if (c->p.record_objective && c->pending_x >= 0) {
+    double l1x, tvx;
+    RC(norms_at_x(c, &l1x, &tvx));
+    double s[kNumSums] = {0};
+    s[SUM_L1X] = l1x;
+    s[SUM_TVX] = tvx;
+    settle_x_terms(c, s);
+  }
+  return RIHVR_OK;
+}
+
+int copy_out(rihvr_ctx* c, void* dst, const void* src, size_t bytes, int is_device) {
+  CK(cudaMemcpyAsync(dst, src, bytes, is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return RIHVR_OK;
+}
+
+int copy_in(rihvr_ctx* c, void* dst, const void* src, size_t bytes, int is_device) {
+  CK(cudaMemcpyAsync(dst, src, bytes, is_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, c->st));
+  return RIHVR_OK;
+}
+
+int validate(const rihvr_params* p, int W, int H) {
+  if (!p) return fail(RIHVR_ERR_INVALID_ARGUMENT, "params is NULL");
+  if (W <= 0 || H <= 0) return fail(RIHVR_ERR_INVALID_ARGUMENT, "width and height must be positive");
+  if (W != H)
+    return fail(RIHVR_ERR_UNSUPPORTED_SIZE, "planes must be square (the reference zero-pads to square planes)");
+  if (!line_size_supported(W))
+    return fail(RIHVR_ERR_UNSUPPORTED_SIZE,
+                "unsupported plane side " + std::to_string(W) + " (supported: 32 48 64 128 256 384 512 768 1024)");
+  if (p->num_planes < 1) return fail(RIHVR_ERR_INVALID_ARGUMENT, "num_planes must be >= 1");
+  if (p->mode != 5 && p->mode != 6 && p->mode != 7)
+    return fail(RIHVR_ERR_UNKNOWN_MODE, "mode must be 5, 6 or 7 (unsupported mode)");
+  if (p->storage < 0 || p->storage > 2) return fail(RIHVR_ERR_INVALID_ARGUMENT, "storage must be 0, 1 or 2");
+  if (p->num_tv_iterations < 0 || p->num_tv_iterations > 20)
+    return fail(RIHVR_ERR_INVALID_ARGUMENT, "num_tv_iterations must be in 0..20");
+  if (!(p->wavelength > 0.f) || !(p->resolution > 0.f))
+    return fail(RIHVR_ERR_INVALID_ARGUMENT, "wavelength and resolution must be positive");
+  if (p->regularization_param < 0.f || p->regularization_TV_param < 0.f)
+    return fail(RIHVR_ERR_INVALID_ARGUMENT, "regularization weights must be non-negative");
+  if (p->max_backtracks < 0) return fail(RIHVR_ERR_INVALID_ARGUMENT, "max_backtracks must be >= 0");
+  return RIHVR_OK;
+}
+
+// c(f)/(2 pi) per frequency, in turns per unit z (sparse_rs_exponent_kernel,
+// :38-56, combined with the carrier phase of sparse_phase_scale_kernel).
+void phase_turns(int H, int W, double dx, double lambda, std::vector<double>& out) {
+  out.resize((size_t)H * W);
+  const double q = (lambda / dx) * (lambda / dx);
+  for (int y = 0; y < H; ++y) {
+    const double fy = (double)(((y + H / 2) % H) - (H / 2)) / (double)H;
+    for (int x = 0; x < W; ++x) {
+      const double fx = (double)(((x + W / 2) % W) - (W / 2)) / (double)W;
+      const double a = q * (fx * fx + fy * fy);
+      const double sm1 = (a >= 1.0) ? -1.0 : -a / (std::sqrt(1.0 - a) + 1.0);
+      out[(size_t)y * W + x] = sm1 / lambda;  // (2 pi / lambda)(s - 1) / (2 pi)
+    }
+  }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+const char* rihvr_last_error(void) { return g_last_error.c_str(); }
+
+const char* rihvr_status_string(int s) {
+  switch (s) {
+    case RIHVR_OK: return "ok";
+    case RIHVR_ERR_UNKNOWN_TYPE: return "unknown type";
+    case RIHVR_ERR_BAD_FILENAME: return "bad filename";
+    case RIHVR_ERR_MISSING_DATA: return "missing data";
+    case RIHVR_ERR_INVALID_STATE: return "invalid state";
+    case RIHVR_ERR_OUT_OF_MEMORY: return "out of memory";
+    case RIHVR_ERR_UNKNOWN_MODE: return "unknown mode";
+    case RIHVR_ERR_INVALID_ARGUMENT: return "invalid argument";
+    case RIHVR_ERR_UNKNOWN_ERROR: return "unknown error";
+    case RIHVR_ERR_INVALID_FILE: return "invalid file";
+    case RIHVR_ERR_INVALID_DATA: return "invalid data";
+    case RIHVR_ERR_CRITICAL_ASSUMPTION: return "critical assumption";
+    case RIHVR_ERR_INFINITE_LOOP: return "infinite loop";
+    case RIHVR_ERR_CUDA: return "CUDA error";
+    case RIHVR_ERR_NO_DEVICE: return "no CUDA device";
+    case RIHVR_ERR_UNSUPPORTED_SIZE: return "unsupported size";
+    default: return "unrecognised status";
+  }
+}
+
+int rihvr_create(const rihvr_params* params, int width, int height, rihvr_ctx** out) {
+  if (!out) return fail(RIHVR_ERR_INVALID_ARGUMENT, "out is NULL");
+  *out = nullptr;
+  RC(validate(params, width, height));
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return fail(RIHVR_ERR_NO_DEVICE, "no CUDA device is visible");
+  }
+  rihvr_ctx* c = new (std::nothrow) rihvr_ctx();
+  if (!c) return fail(RIHVR_ERR_OUT_OF_MEMORY, "host allocation failed");
+  c->p = *params;
+  c->W = width;
+  c->H = height;
+  c->Nz = params->num_planes;
+  c->HW = (size_t)width * height;
+  c->V = c->HW * c->Nz;
+  // No TV regularisation means the L1 prox (:187-195)
+  c->mode = params->regularization_TV_param == 0.f ? 5 : params->mode;
+  c->storage = params->storage;
+  c->esize = params->storage == STORE_F32 ? 8 : 4;
+  cudaGetDevice(&c->device);
+  auto cleanup = [&](int rc) {
+    rihvr_destroy(c);
+    return rc;
+  };
+  if (cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess)
+    return cleanup(fail(RIHVR_ERR_CUDA, "cudaStreamCreate failed"));
+  int rc = RIHVR_OK;
+  for (int i = 0; i < 3 && rc == RIHVR_OK; ++i) rc = dalloc(c, &c->vol[i], c->esize * c->V);
+  if (rc == RIHVR_OK) rc = dalloc_t(c, &c->G, c->V);
+  if (rc == RIHVR_OK) rc = dalloc_t(c, &c->U, c->V);
+  c->nchunks = fwd_col_chunks(width, height, c->Nz);
+  if (rc == RIHVR_OK) rc = dalloc_t(c, &c->Spart, c->HW * c->nchunks);
+  if (rc == RIHVR_OK) rc = dalloc_t(c, &c->S, c->HW);
+  if (rc == RIHVR_OK) rc = dalloc_t(c, &c->pc1, c->HW);
+  if (rc == RIHVR_OK) rc = dalloc_t(c, &c->pc2, c->HW);
+  if (rc == RIHVR_OK) rc = dalloc_t(c, &c->Rs, c->HW);
+  if (rc == RIHVR_OK) rc = dalloc_t(c, &c->b, c->HW);
+  if (rc == RIHVR_OK) rc = dalloc_t(c, &c->dnew, c->HW);
+  if (rc == RIHVR_OK) rc = dalloc_t(c, &c->dY0, c->HW);
+  if (rc == RIHVR_OK) rc = dalloc_t(c, &c->dX, c->HW);
+  if (rc == RIHVR_OK) rc = dalloc_t(c, &c->r, c->HW);
+  if (rc == RIHVR_OK) rc = dalloc_t(c, &c->cturn, c->HW);
+  if (rc == RIHVR_OK) rc = dalloc_t(c, &c->zlist, (size_t)c->Nz);
+  if (c->mode == 6) {
+    if (rc == RIHVR_OK) rc = dalloc_t(c, &c->X1, c->V);
+    if (rc == RIHVR_OK) rc = dalloc_t(c, &c->gx, c->V);
+    if (rc == RIHVR_OK) rc = dalloc_t(c, &c->gy, c->V);
+    if (rc == RIHVR_OK) rc = dalloc_t(c, &c->gz, c->V);
+    if (rc == RIHVR_OK) rc = dalloc_t(c, &c->Y, c->V);
+  }
+  c->partial_cap = max_partial_blocks(width, height, c->Nz);
+  if (rc == RIHVR_OK) rc = dalloc_t(c, &c->partials, c->partial_cap * kNumSums);
+  if (rc == RIHVR_OK) rc = dalloc_t(c, &c->sums_d, (size_t)kNumSums * NUM_SLOTS);
+  if (rc != RIHVR_OK) return cleanup(rc);
+  if (cudaMallocHost(&c->sums_h, sizeof(double) * kNumSums * NUM_SLOTS) != cudaSuccess)
+    return cleanup(fail(RIHVR_ERR_OUT_OF_MEMORY, "cudaMallocHost failed"));
+  std::vector<double> ct;
+  phase_turns(height, width, (double)params->resolution, (double)params->wavelength, ct);
+  std::vector<double> zl((size_t)c->Nz);
+  rihvr_plane_list(params, zl.data());
+  if (cudaMemcpy(c->cturn, ct.data(), sizeof(double) * ct.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemcpy(c->zlist, zl.data(), sizeof(double) * zl.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+      cudaMemsetAsync(c->b, 0, sizeof(float) * c->HW, c->st) != cudaSuccess)
+    return cleanup(fail(RIHVR_ERR_CUDA, "initial copies failed"));
+  *out = c;
+  return RIHVR_OK;
+}
+
+void rihvr_destroy(rihvr_ctx* c) {
+  if (!c) return;
+  if (c->st) cudaStreamSynchronize(c->st);
+  for (void* p : c->allocs) cudaFree(p);
+  if (c->sums_h) cudaFreeHost(c->sums_h);
+  for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
+  if (c->st) cudaStreamDestroy(c->st);
+  delete c;
+}
+
+int rihvr_set_hologram(rihvr_ctx* c, const float* b, int is_device) {
+  if (!c || !b) return fail(RIHVR_ERR_INVALID_ARGUMENT, "NULL argument");
+  RC(copy_in(c, c->b, b, sizeof(float) * c->HW, is_device));
+  c->have_holo = true;
+  return state_reset(c);
+}
+
+int rihvr_reset(rihvr_ctx* c) {
+  if (!c) return fail(RIHVR_ERR_INVALID_ARGUMENT, "NULL context");
+  if (!c->have_holo) return fail(RIHVR_ERR_MISSING_DATA, "no hologram set");
+  return state_reset(c);
+}
+
+int rihvr_iterate(rihvr_ctx* c, int n) {
+  if (!c || n < 0) return fail(RIHVR_ERR_INVALID_ARGUMENT, "bad argument");
+  return run_iterations(c, n);
+}
+
+int rihvr_iterate_timed(rihvr_ctx* c, int n, float* ms) {
+  if (!c || n < 0 || !ms) return fail(RIHVR_ERR_INVALID_ARGUMENT, "bad argument");
+  cudaEvent_t a, b;
+  CK(cudaEventCreate(&a));
+  CK(cudaEventCreate(&b));
+  CK(cudaEventRecord(a, c->st));
+  int rc = run_iterations(c, n);
+  cudaEventRecord(b, c->st);
+  cudaEventSynchronize(b);
+  cudaEventElapsedTime(ms, a, b);
+  cudaEventDestroy(a);
+  cudaEventDestroy(b);
+  return rc;
+}
+
+int rihvr_reconstruct(rihvr_ctx* c, double* final_objective) {
+  if (!c) return fail(RIHVR_ERR_INVALID_ARGUMENT, "NULL context");
+  if (!c->have_holo) return fail(RIHVR_ERR_MISSING_DATA, "no hologram set");
+  RC(state_reset(c));
+  RC(run_iterations(c, c->p.num_inverse_iterations));
+  if (final_objective) RC(rihvr_objective(c, final_objective, nullptr));
+  return RIHVR_OK;
+}
+
+int rihvr_iteration_count(const rihvr_ctx* c) { return c ? c->it : -1; }
+
+int rihvr_objective(rihvr_ctx* c, double* f, double* terms3) {
+  if (!c || !f) return fail(RIHVR_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (!c->have_holo) return fail(RIHVR_ERR_MISSING_DATA, "no hologram set");
+  double l1x, tvx;
+  RC(norms_at_x(c, &l1x, &tvx));
+  const double fr = c->prev_f_resid;
+  *f = fr + (double)c->p.regularization_param * l1x + tv_weight(c) * tvx;
+  if (terms3) {
+    terms3[0] = fr;
+    terms3[1] = l1x;
+    terms3[2] = c->mode == 5 ? 0.0 : tvx;
+  }
+  return RIHVR_OK;
+}
+
+int rihvr_get_iterations(const rihvr_ctx* c, rihvr_iter_record* out, int max_records, int* n_out) {
+  if (!c || !n_out) return fail(RIHVR_ERR_INVALID_ARGUMENT, "NULL argument");
+  const int n = (int)c->log.size();
+  *n_out = n;
+  if (out)
+    for (int i = 0; i < n && i < max_records; ++i) out[i] = c->log[i];
+  return RIHVR_OK;
+}
+
+int rihvr_get_volume(rihvr_ctx* c, float* out, int is_device) {
+  if (!c || !out) return fail(RIHVR_ERR_INVALID_ARGUMENT, "NULL argument");
+  // materialise x = P + beta (P - Pprev) into the intermediate buffer
+  KL(launch_materialize_x(c->storage, c->vol[c->iCur], c->vol[c->iPrev], (float)c->beta, c->U, (long long)c->V,
+                          c->st));
+  return copy_out(c, out, c->U, sizeof(float2) * c->V, is_device);
+}
+
+int rihvr_get_plane(rihvr_ctx* c, int z, float* out, int is_device) {
+  if (!c || !out) return fail(RIHVR_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (z < 0 || z >= c->Nz) return fail(RIHVR_ERR_INVALID_ARGUMENT, "plane out of bounds");  // :950-954
+  const size_t off = (size_t)z * c->HW;
+  const char* P = static_cast<const char*>(c->vol[c->iCur]) + off * c->esize;
+  const char* Pp = static_cast<const char*>(c->vol[c->iPrev]) + off * c->esize;
+  KL(launch_materialize_x(c->storage, P, Pp, (float)c->beta, c->pc1, (long long)c->HW, c->st));
+  return copy_out(c, out, c->pc1, sizeof(float2) * c->HW, is_device);
+}
+
+int rihvr_get_estimate(rihvr_ctx* c, float* out, int is_device) {
+  if (!c || !out) return fail(RIHVR_ERR_INVALID_ARGUMENT, "NULL argument");
+  return copy_out(c, out, c->dX, sizeof(float) * c->HW, is_device);
+}
+
+int rihvr_get_residual(rihvr_ctx* c, float* out, int is_device) {
+  if (!c || !out) return fail(RIHVR_ERR_INVALID_ARGUMENT, "NULL argument");
+  return copy_out(c, out, c->r, sizeof(float) * c->HW, is_device);
+}
+
+int rihvr_forward(rihvr_ctx* c, const float* volume, float* holo_out, int is_device) {
+  if (!c || !volume || !holo_out) return fail(RIHVR_ERR_INVALID_ARGUMENT, "NULL argument");
+  RC(copy_in(c, c->G, volume, sizeof(float2) * c->V, is_device));
+  RC(forward_volume(c, ELEM_C32, c->G));
+  return copy_out(c, holo_out, c->dnew, sizeof(float) * c->HW, is_device);
+}
+
+int rihvr_adjoint(rihvr_ctx* c, const float* residual, float* volume_out, int is_device) {
+  if (!c || !residual || !volume_out) return fail(RIHVR_ERR_INVALID_ARGUMENT, "NULL argument");
+  RC(copy_in(c, c->r, residual, sizeof(float) * c->HW, is_device));
+  RC(residual_spectrum(c));
+  RC(adjoint_volume(c));
+  return copy_out(c, volume_out, c->G, sizeof(float2) * c->V, is_device);
+}
+
+int rihvr_prox_step(rihvr_ctx* c, const float* x, const float* residual, double t, float* p_out, double* sums3,
+                    int is_device) {
+  if (!c || !x || !residual || !p_out) return fail(RIHVR_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (!(t > 0)) return fail(RIHVR_ERR_INVALID_ARGUMENT, "t must be positive");
+  // x into the P_k slot (storage type) and P_{k-1} = P_k with beta = 0
+  RC(copy_in(c, c->U, x, sizeof(float2) * c->V, is_device));
+  KL(launch_store_volume(c->storage, c->U, c->vol[c->iCur], (long long)c->V, c->st));
+  CK(cudaMemcpyAsync(c->vol[c->iPrev], c->vol[c->iCur], c->esize * c->V, cudaMemcpyDeviceToDevice, c->st));
+  const double saved_beta = c->beta;
+  c->beta = 0;
+  RC(copy_in(c, c->r, residual, sizeof(float) * c->HW, is_device));
+  RC(residual_spectrum(c));
+  RC(adjoint_volume(c));
+  int rc = prox_volume(c, t);
+  c->beta = saved_beta;
+  if (rc != RIHVR_OK) return rc;
+  RC(fetch_sums(c));
+  if (sums3) {
+    sums3[0] = c->sums_h[SLOT_PROX * kNumSums + SUM_LIM1];
+    sums3[1] = c->sums_h[SLOT_PROX * kNumSums + SUM_LIM2];
+    sums3[2] = c->sums_h[SLOT_PROX * kNumSums + SUM_RS];
+  }
+  KL(launch_materialize_x(c->storage, c->vol[c->iNew], c->vol[c->iNew], 0.f, c->U, (long long)c->V, c->st));
+  // the context's solve state is no longer meaningful after this call
+  c->have_holo = false;
+  return copy_out(c, p_out, c->U, sizeof(float2) * c->V, is_device);
+}
+
+int rihvr_set_profiling(rihvr_ctx* c, int enable) {
+  if (!c) return fail(RIHVR_ERR_INVALID_ARGUMENT, "NULL context");
+  CK(cudaStreamSynchronize(c->st));
+  c->profiling = enable != 0;
+  c->evs.clear();
+  c->ev_used = 0;
+  return RIHVR_OK;
+}
+
+int rihvr_kernel_times(rihvr_ctx* c, const char** names, double* total_ms, int* launches, int max, int* n_out) {
+  if (!c || !n_out) return fail(RIHVR_ERR_INVALID_ARGUMENT, "NULL argument");
+  CK(cudaStreamSynchronize(c->st));
+  double tot[K_NUM] = {0};
+  int cnt[K_NUM] = {0};
+  for (const auto& e : c->evs) {
+    float ms = 0;
+    if (cudaEventElapsedTime(&ms, e.a, e.b) == cudaSuccess) {
+      tot[e.cls] += ms;
+      cnt[e.cls]++;
+    }
+  }
+  *n_out = K_NUM;
+  for (int k = 0; k < K_NUM && k < max; ++k) {
+    if (names) names[k] = kClassNames[k];
+    if (total_ms) total_ms[k] = tot[k];
+    if (launches) launches[k] = cnt[k];
+  }
+  return RIHVR_OK;
+}
+
+size_t rihvr_device_bytes(const rihvr_ctx* c) { return c ? c->bytes : 0; }
+
+long long rihvr_launch_count(const rihvr_ctx* c) { return c ? c->launches : -1; }
+
+void* rihvr_get_stream(rihvr_ctx* c) { return c ? (void*)c->st : nullptr; }
+
+}  // extern "C"

@@ -1,0 +1,183 @@
+"""GPU parity of the sm_100a path against the FP64 oracle, through the C ABI.
+
+Tolerances (relative L2 error / relative objective gap): 1e-4 for FP32 volume
+storage and 1e-2 for BF16/FP16 storage.  Operators are compared elementwise on
+random inputs; solves are compared iteration by iteration (same backtracking
+and restart decisions, objective within tolerance) and on the final volume.
+"""
+import hashlib
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+TOL_F32 = 1e-4
+TOL_LOW = 1e-2
+GOLD_C1 = os.path.join(os.path.dirname(__file__), "golden", "oracle_c1_384x384x40.npz")
+
+
+def rel(a, b):
+    a = np.asarray(a, np.complex128)
+    b = np.asarray(b, np.complex128)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def make(rihvr, side, nz, **kw):
+    p = rihvr.default_params()
+    p.start_plane, p.plane_stepsize, p.num_planes = 100.0, 40.0, nz
+    p.wavelength, p.resolution = 0.632, 2.0
+    p.regularization_param, p.regularization_TV_param, p.num_tv_iterations = 0.01, 0.02, 5
+    p.zero_padding = 0
+    for k, v in kw.items():
+        setattr(p, k, v)
+    return p
+
+
+def oparams(rihvr, p, side, **kw):
+    d = dict(W=side, H=side, z=rihvr.plane_list(p), dx=float(np.float32(p.resolution)),
+             lam=float(np.float32(p.wavelength)), l1=float(np.float32(p.regularization_param)),
+             tv=float(np.float32(p.regularization_TV_param)), n_tv=p.num_tv_iterations, mode=p.mode,
+             faithful=p.faithful, t0=p.initial_step)
+    d.update(kw)
+    return O.OracleParams(**d)
+
+
+def rand_volume(rng, nz, side, scale=0.05):
+    return (scale * (rng.standard_normal((nz, side, side)) + 1j * rng.standard_normal((nz, side, side)))).astype(
+        np.complex64)
+
+
+@pytest.mark.parametrize("side,nz", [(32, 3), (64, 5), (128, 4), (384, 3), (1024, 2)])
+def test_forward_matches_oracle(rihvr, side, nz):
+    p = make(rihvr, side, nz)
+    rng = np.random.default_rng(side + nz)
+    vol = rand_volume(rng, nz, side)
+    with rihvr.SparseCompressiveHolo(p, side, side) as s:
+        d = s.forward(vol)
+    ref = O.forward(oparams(rihvr, p, side), vol.astype(np.complex128))
+    assert rel(d, ref) < TOL_F32
+
+
+@pytest.mark.parametrize("side,nz", [(32, 3), (64, 5), (384, 3), (1024, 2)])
+def test_adjoint_matches_oracle(rihvr, side, nz):
+    p = make(rihvr, side, nz)
+    rng = np.random.default_rng(7 * side + nz)
+    r = rng.standard_normal((side, side)).astype(np.float32)
+    with rihvr.SparseCompressiveHolo(p, side, side) as s:
+        g = s.adjoint(r)
+    ref = O.adjoint(oparams(rihvr, p, side), r.astype(np.float64))
+    assert rel(g, ref) < TOL_F32
+
+
+def test_adjoint_identity_on_gpu(rihvr):
+    """<A x, r> = <x, A^H r> in FP32 (testAdjoint, sparse_compressive_holo.cu:2533-2652)."""
+    side, nz = 128, 6
+    p = make(rihvr, side, nz)
+    rng = np.random.default_rng(5)
+    x = rand_volume(rng, nz, side, 1.0)
+    r = rng.standard_normal((side, side)).astype(np.float32)
+    with rihvr.SparseCompressiveHolo(p, side, side) as s:
+        lhs = float(np.sum(s.forward(x).astype(np.float64) * r))
+        g = s.adjoint(r).astype(np.complex128)
+    rhs = float(np.sum(x.real * g.real + x.imag * g.imag))
+    assert abs(lhs - rhs) < 1e-5 * max(abs(lhs), abs(rhs))
+
+
+@pytest.mark.parametrize("mode", [5, 6, 7])
+@pytest.mark.parametrize("faithful", [1, 0])
+def test_prox_step_matches_oracle(rihvr, mode, faithful):
+    side, nz = 64, 4
+    p = make(rihvr, side, nz, mode=mode, faithful=faithful)
+    rng = np.random.default_rng(mode * 10 + faithful)
+    x = rand_volume(rng, nz, side, 0.05)
+    r = rng.standard_normal((side, side)).astype(np.float32)
+    t = 0.2
+    with rihvr.SparseCompressiveHolo(p, side, side) as s:
+        out, sums = s.prox_step(x, r, t)
+    op = oparams(rihvr, p, side)
+    ref, rsums = O.prox_from(op, x.astype(np.complex128), x.astype(np.complex128), r.astype(np.float64), t)
+    assert rel(out, ref) < TOL_F32
+    assert abs(sums[0] - rsums[0]) < 1e-4 * max(abs(rsums[0]), 1e-6 * abs(rsums[1]) + 1e-12)
+    assert abs(sums[1] - rsums[1]) < 1e-4 * abs(rsums[1])
+
+
+def run_gpu(rihvr, p, side, b, n):
+    with rihvr.SparseCompressiveHolo(p, side, side) as s:
+        s.setHologram(b)
+        s.iterate(n)
+        log = s.iterations()
+        X = s.getVolume()
+        f, terms = s.calcObjectiveFunction()
+        est = s.getEstimate()
+    return log, X, f, terms, est
+
+
+@pytest.mark.parametrize("mode,faithful,t0", [(7, 1, 0.0), (7, 0, 0.0), (7, 1, 3.0), (5, 1, 3.0), (6, 1, 2.0)])
+def test_solve_matches_oracle(rihvr, synthmod, cache_dir, mode, faithful, t0):
+    side, nz, n = 64, 6, 20
+    cfg = synthmod.small_config(W=side, H=side, Nz=nz, seed=2)
+    _, b = synthmod.make_hologram(cfg, cache_dir=cache_dir)
+    p = rihvr.params_from_config(cfg, mode=mode, faithful=faithful, initial_step=t0 / nz if t0 else 0.0)
+    log, X, f, terms, est = run_gpu(rihvr, p, side, b, n)
+    op = oparams(rihvr, p, side)
+    # replay the GPU's decisions so that the trajectories are comparable even
+    # if a ratio lands within rounding of a threshold
+    olog, OX, OP, oest, f0 = O.solve(op, b.astype(np.float64), n, forced_bt=log["backtracks"],
+                                     forced_rs=log["restarted"])
+    free, _, _, _, _ = O.solve(op, b.astype(np.float64), n, want_volumes=False)
+    agree = np.mean((free["backtracks"] == log["backtracks"]) & (free["restarted"] == log["restarted"]))
+    assert agree >= 0.9, (free["backtracks"], log["backtracks"], free["restarted"], log["restarted"])
+    gap = np.abs(log["f_x"] - olog["f_x"]) / np.abs(olog["f_x"])
+    assert gap.max() < TOL_F32, gap
+    assert rel(X, OX) < TOL_F32 * 10
+    assert abs(f - olog["f_x"][-1]) / abs(olog["f_x"][-1]) < TOL_F32
+    assert rel(est, oest) < TOL_F32
+
+
+@pytest.mark.parametrize("storage", [1, 2])
+def test_reduced_precision_storage(rihvr, synthmod, cache_dir, storage):
+    side, nz, n = 64, 6, 20
+    cfg = synthmod.small_config(W=side, H=side, Nz=nz, seed=4)
+    _, b = synthmod.make_hologram(cfg, cache_dir=cache_dir)
+    p = rihvr.params_from_config(cfg, storage=storage)
+    log, X, f, terms, est = run_gpu(rihvr, p, side, b, n)
+    olog, OX, _, _, _ = O.solve(oparams(rihvr, p, side), b.astype(np.float64), n)
+    assert abs(f - olog["f_x"][-1]) / abs(olog["f_x"][-1]) < TOL_LOW
+    assert rel(X, OX) < 10 * TOL_LOW
+
+
+def test_c1_workload_matches_oracle_fixture(rihvr, synthmod):
+    """384x384x40, 100 FISTA / 5 TV iterations against the committed oracle run."""
+    g = np.load(GOLD_C1)
+    cfg = synthmod.config1()
+    _, b = synthmod.make_hologram(cfg)
+    assert hashlib.sha1(b.tobytes()).digest() == bytes(g["b_sha1"]), "synthetic hologram differs from the fixture's"
+    p = rihvr.params_from_config(cfg)
+    log, X, f, terms, est = run_gpu(rihvr, p, cfg.W, b, cfg.num_inverse_iterations)
+    assert np.array_equal(log["backtracks"], g["backtracks"])
+    assert np.mean(log["restarted"] == g["restarted"]) >= 0.95
+    gap = np.abs(log["f_x"] - g["f_x"]) / np.abs(g["f_x"])
+    assert gap[-1] < TOL_F32, gap[-1]
+    assert gap.max() < 10 * TOL_F32, gap.max()
+    l1 = np.abs(X).sum(axis=(1, 2))
+    assert np.abs(l1 - g["plane_l1"]).sum() / g["plane_l1"].sum() < 1e-3
+    crops = X[list(g["crop_planes"])][..., 160:224, 160:224]
+    assert rel(crops, g["crops"]) < 1e-2
+
+
+def test_errors_are_status_codes(rihvr):
+    p = make(rihvr, 64, 2)
+    with rihvr.SparseCompressiveHolo(p, 64, 64) as s:
+        with pytest.raises(rihvr.RihvrError) as e:
+            s.iterate(1)  # no hologram yet
+        assert e.value.code == rihvr.ERR_MISSING_DATA
+        with pytest.raises(rihvr.RihvrError) as e:
+            s.getPlane(5)
+        assert e.value.code == rihvr.ERR_INVALID_ARGUMENT
+        s.setHologram(np.zeros((64, 64), np.float32))
+        s.iterate(2)  # a zero hologram is a valid (trivial) problem
+        assert np.all(s.getVolume() == 0)
