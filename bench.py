@@ -181,6 +181,10 @@ def run_ours(args):
     base = workload(args.config)
     # independent frames: each rank reconstructs its own hologram
     cfg = (synth.config2 if args.config == "c2" else synth.config1)(seed=base.seed + rank)
+    if args.nz:
+        # smaller profiling case: same planes and physics, fewer of them
+        cfg.num_planes = args.nz
+        cfg.name = f"{cfg.name}_nz{args.nz}"
     _, b = synth.make_hologram(cfg)
     storage = {"f32": 0, "bf16": 1, "f16": 2}[args.storage]
     p = rihvr.params_from_config(cfg, record_objective=0, storage=storage)
@@ -199,6 +203,7 @@ def run_ours(args):
     launches0 = s.launch_count()
     barrier()
     with ClockSampler(local) as clk:
+        time.sleep(0.5)  # let the sampler start before the timed region
         ms = s.iterate_timed(args.steps)
     barrier()
     launches = s.launch_count() - launches0
@@ -291,6 +296,7 @@ def main():
     ap.add_argument("--config", default="c2", choices=["c2", "c1"])
     ap.add_argument("--storage", default="f32", choices=["f32", "bf16", "f16"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--nz", type=int, default=0, help="override the plane count (profiling cases)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

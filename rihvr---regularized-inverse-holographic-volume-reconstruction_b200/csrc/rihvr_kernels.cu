@@ -584,126 +584,231 @@ __device__ __forceinline__ float cabs2(float2 a) { return a.x * a.x + a.y * a.y;
 //   x = P + beta (P - Pprev);  xh = x - t g
 //   gx = gy = 0; n_tv times: y = xh - mu div(g);  g = (g + s grad y)/max(1, |.|)
 //   y = xh - mu div(g);  p = shrink(y, thr)
-// div uses forward periodic differences, grad backward periodic differences, the
-// projection norm is taken over the four real components.  Tiles are 64x64 with
-// a recomputed halo of n_tv + 1 pixels, which makes the interior exact.
-// The same sweep accumulates the line-search sums, the restart statistic and
-// (optionally) the L1/TV norms of p and x.
+// div uses forward periodic differences, grad backward periodic differences and
+// the projection norm is taken over the four real components (Jacobi updates,
+// as the reference's two kernels per iteration).
+//
+// Layout: a block holds a 64 x 128 tile (columns x rows) with a recomputed halo
+// of n_tv + 1 pixels on every side, which makes the interior exact.  Warp w owns
+// rows [8w, 8w+8); lane l owns columns 2l and 2l+1.  The Chambolle state (xh, gx,
+// gy) stays in registers; each TV iteration sweeps a thread's 8 rows top to
+// bottom so that y is only ever live for one row, right neighbours of gx and
+// left neighbours of y move by warp shuffles, and only the first/last row of
+// each warp's run crosses warps, through double-buffered shared memory (one
+// barrier per iteration).  The row above a run is recomputed from the published
+// last row of the warp above instead of being waited for.
+// The final sweep also accumulates the line-search sums, the restart statistic
+// and (optionally) the L1/TV norms of p and x.
 // ---------------------------------------------------------------------------
-constexpr int TV_EXT = 64, TV_RUN = 16, TV_RUNS = TV_EXT / TV_RUN, TV_THREADS = TV_EXT * TV_RUNS;
-constexpr size_t TV_SMEM = sizeof(float2) * (5 * TV_EXT * TV_EXT + TV_RUNS * TV_EXT);
+constexpr int TV_CPL = 2;                  // columns per lane
+constexpr int TV_EW = 32 * TV_CPL;         // tile width incl. halo
+constexpr int TV_R = 8;                    // rows per thread
+constexpr int TV_NW = 16;                  // warps, stacked vertically
+constexpr int TV_EH = TV_NW * TV_R;        // tile height incl. halo
+constexpr int TV_THREADS = 32 * TV_NW;
+constexpr int TV_BND = TV_NW * TV_EW;      // one boundary row per warp
+constexpr size_t TV_SMEM = sizeof(float2) * (2 * TV_EH * TV_EW + 3 * 2 * TV_BND + TV_BND);
+
+__device__ __forceinline__ float2 shfl_down2(float2 v) {
+  return make_float2(__shfl_down_sync(0xffffffffu, v.x, 1), __shfl_down_sync(0xffffffffu, v.y, 1));
+}
+__device__ __forceinline__ float2 shfl_up2(float2 v) {
+  return make_float2(__shfl_up_sync(0xffffffffu, v.x, 1), __shfl_up_sync(0xffffffffu, v.y, 1));
+}
+
+// y = xh - mu ((gxr - gx) + (gyd - gy))
+__device__ __forceinline__ float2 tv_estimate(float2 xh, float2 gx, float2 gxr, float2 gy, float2 gyd, float mu) {
+  const float dvx = (gxr.x - gx.x) + (gyd.x - gy.x);
+  const float dvy = (gxr.y - gx.y) + (gyd.y - gy.y);
+  return make_float2(fmaf(-mu, dvx, xh.x), fmaf(-mu, dvy, xh.y));
+}
 
 template <typename ST>
 __global__ void __launch_bounds__(TV_THREADS, 1) k_prox_tv2d(ProxArgs a) {
   extern __shared__ float2 smem[];
-  float2* s_y = smem;
-  float2* s_gx = s_y + TV_EXT * TV_EXT;
-  float2* s_X = s_gx + TV_EXT * TV_EXT;
-  float2* s_g = s_X + TV_EXT * TV_EXT;
-  float2* s_P = s_g + TV_EXT * TV_EXT;
-  float2* s_gyb = s_P + TV_EXT * TV_EXT;
+  float2* s_g = smem;                      // [EH][EW] gradient at load
+  float2* s_P = s_g + TV_EH * TV_EW;       // [EH][EW] P at load
+  float2* s_gyf = s_P + TV_EH * TV_EW;     // [2][NW][EW] first-row gy of each run
+  float2* s_gxl = s_gyf + 2 * TV_BND;      // [2][NW][EW] last-row gx
+  float2* s_gyl = s_gxl + 2 * TV_BND;      // [2][NW][EW] last-row gy
+  float2* s_xhl = s_gyl + 2 * TV_BND;      // [NW][EW]   last-row xh
   const int W = a.W, H = a.H;
-  const int ex = threadIdx.x % TV_EXT, run = threadIdx.x / TV_EXT;
-  const int h = a.n_tv + 1, inner = TV_EXT - 2 * h;
-  const int ox = blockIdx.x * inner - h, oy = blockIdx.y * inner - h;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int h = a.n_tv + 1, VW = TV_EW - 2 * h, VH = TV_EH - 2 * h;
+  const int ox = blockIdx.x * VW - h, oy = blockIdx.y * VH - h;
   const size_t plane = (size_t)blockIdx.z * W * H;
   const ST* P = static_cast<const ST*>(a.P) + plane;
   const ST* Pp = static_cast<const ST*>(a.Pprev) + plane;
   const float2* G = a.G + plane;
-  const int gcol = ((ox + ex) % W + W) % W;
-  float2 xh[TV_RUN], gx[TV_RUN], gy[TV_RUN], y[TV_RUN];
+  const float mu = a.mu, s = a.s, t = a.t, beta = a.beta;
+  const int col0 = lane * TV_CPL;
+
+  float2 xh[TV_R][TV_CPL], gx[TV_R][TV_CPL], gy[TV_R][TV_CPL];
+  int gcol[TV_CPL];
 #pragma unroll
-  for (int i = 0; i < TV_RUN; ++i) {
-    const int row = run * TV_RUN + i;
-    const int grow = ((oy + row) % H + H) % H;
-    const size_t idx = (size_t)grow * W + gcol;
-    const float2 p = Store<ST>::ld(P + idx), pp = Store<ST>::ld(Pp + idx), g = G[idx];
-    const float2 x = make_float2(fmaf(a.beta, p.x - pp.x, p.x), fmaf(a.beta, p.y - pp.y, p.y));
-    xh[i] = make_float2(fmaf(-a.t, g.x, x.x), fmaf(-a.t, g.y, x.y));
-    s_X[row * TV_EXT + ex] = x;
-    s_g[row * TV_EXT + ex] = g;
-    s_P[row * TV_EXT + ex] = p;
-    s_gx[row * TV_EXT + ex] = make_float2(0.f, 0.f);
-    gx[i] = make_float2(0.f, 0.f);
-    gy[i] = make_float2(0.f, 0.f);
-  }
-  s_gyb[run * TV_EXT + ex] = make_float2(0.f, 0.f);
-  __syncthreads();
-  const float mu = a.mu, s = a.s;
-  for (int it = 0;; ++it) {
-    // y = xh - mu div(g)
+  for (int c = 0; c < TV_CPL; ++c) gcol[c] = ((ox + col0 + c) % W + W) % W;
 #pragma unroll
-    for (int i = 0; i < TV_RUN; ++i) {
-      const int row = run * TV_RUN + i;
-      const float2 gxr = (ex < TV_EXT - 1) ? s_gx[row * TV_EXT + ex + 1] : gx[i];
-      float2 gyd;
-      if (i < TV_RUN - 1) gyd = gy[i + 1];
-      else gyd = (run < TV_RUNS - 1) ? s_gyb[(run + 1) * TV_EXT + ex] : gy[i];
-      const float dvx = (gxr.x - gx[i].x) + (gyd.x - gy[i].x);
-      const float dvy = (gxr.y - gx[i].y) + (gyd.y - gy[i].y);
-      y[i] = make_float2(fmaf(-mu, dvx, xh[i].x), fmaf(-mu, dvy, xh[i].y));
+  for (int i = 0; i < TV_R; ++i) {
+    const int row = w * TV_R + i;
+    const size_t rbase = (size_t)(((oy + row) % H + H) % H) * W;
+#pragma unroll
+    for (int c = 0; c < TV_CPL; ++c) {
+      const size_t idx = rbase + gcol[c];
+      const float2 p = Store<ST>::ld(P + idx), pp = Store<ST>::ld(Pp + idx), g = G[idx];
+      const float2 x = make_float2(fmaf(beta, p.x - pp.x, p.x), fmaf(beta, p.y - pp.y, p.y));
+      xh[i][c] = make_float2(fmaf(-t, g.x, x.x), fmaf(-t, g.y, x.y));
+      s_g[row * TV_EW + col0 + c] = g;
+      s_P[row * TV_EW + col0 + c] = p;
+      gx[i][c] = make_float2(0.f, 0.f);
+      gy[i][c] = make_float2(0.f, 0.f);
     }
-    if (it == a.n_tv) break;
+  }
 #pragma unroll
-    for (int i = 0; i < TV_RUN; ++i) s_y[(run * TV_RUN + i) * TV_EXT + ex] = y[i];
-    __syncthreads();
-    // g = P(g + s grad y)
+  for (int c = 0; c < TV_CPL; ++c) s_xhl[w * TV_EW + col0 + c] = xh[TV_R - 1][c];
+
+  for (int k = 0; k < a.n_tv; ++k) {
+    float2* gyf = s_gyf + (k & 1) * TV_BND;
+    float2* gxl = s_gxl + (k & 1) * TV_BND;
+    float2* gyl = s_gyl + (k & 1) * TV_BND;
 #pragma unroll
-    for (int i = 0; i < TV_RUN; ++i) {
-      const int row = run * TV_RUN + i;
-      const float2 yl = (ex > 0) ? s_y[row * TV_EXT + ex - 1] : y[i];
-      float2 yu;
-      if (i > 0) yu = y[i - 1];
-      else yu = (run > 0) ? s_y[(row - 1) * TV_EXT + ex] : y[i];
-      const float2 px = make_float2(fmaf(s, yl.x - y[i].x, gx[i].x), fmaf(s, yl.y - y[i].y, gx[i].y));
-      const float2 py = make_float2(fmaf(s, yu.x - y[i].x, gy[i].x), fmaf(s, yu.y - y[i].y, gy[i].y));
-      const float n2 = cabs2(px) + cabs2(py);
-      const float sc = (n2 > 1.f) ? rsqrtf(n2) : 1.f;
-      gx[i] = cscale(px, sc);
-      gy[i] = cscale(py, sc);
-      s_gx[row * TV_EXT + ex] = gx[i];
+    for (int c = 0; c < TV_CPL; ++c) {
+      gyf[w * TV_EW + col0 + c] = gy[0][c];
+      gxl[w * TV_EW + col0 + c] = gx[TV_R - 1][c];
+      gyl[w * TV_EW + col0 + c] = gy[TV_R - 1][c];
     }
-    s_gyb[run * TV_EXT + ex] = gy[0];
     __syncthreads();
-  }
-  // shrink, publish p for the TV-norm neighbours
+    // y of the row above this run, recomputed from the published last row of warp w-1
+    float2 yu[TV_CPL];
 #pragma unroll
-  for (int i = 0; i < TV_RUN; ++i) {
-    y[i] = shrink(y[i], a.thr, a.faithful);
+    for (int c = 0; c < TV_CPL; ++c) {
+      yu[c] = make_float2(0.f, 0.f);  // top halo rows: value irrelevant
+      if (w > 0) {
+        const int col = col0 + c, b = (w - 1) * TV_EW;
+        const float2 gxu = gxl[b + col], gyu = gyl[b + col];
+        const float2 gxru = (col + 1 < TV_EW) ? gxl[b + col + 1] : gxu;
+        yu[c] = tv_estimate(s_xhl[b + col], gxu, gxru, gyu, gy[0][c], mu);
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < TV_R; ++i) {
+      float2 gxr[TV_CPL], gyd[TV_CPL], y[TV_CPL], yl[TV_CPL];
+#pragma unroll
+      for (int c = 0; c < TV_CPL - 1; ++c) gxr[c] = gx[i][c + 1];
+      gxr[TV_CPL - 1] = shfl_down2(gx[i][0]);  // lane 31 gets its own (halo column)
+#pragma unroll
+      for (int c = 0; c < TV_CPL; ++c) {
+        if (i < TV_R - 1) gyd[c] = gy[i + 1][c];
+        else gyd[c] = (w < TV_NW - 1) ? gyf[(w + 1) * TV_EW + col0 + c] : gy[i][c];
+        y[c] = tv_estimate(xh[i][c], gx[i][c], gxr[c], gy[i][c], gyd[c], mu);
+      }
+      yl[0] = shfl_up2(y[TV_CPL - 1]);  // lane 0 gets its own (halo column)
+#pragma unroll
+      for (int c = 1; c < TV_CPL; ++c) yl[c] = y[c - 1];
+#pragma unroll
+      for (int c = 0; c < TV_CPL; ++c) {
+        const float2 px = make_float2(fmaf(s, yl[c].x - y[c].x, gx[i][c].x), fmaf(s, yl[c].y - y[c].y, gx[i][c].y));
+        const float2 py = make_float2(fmaf(s, yu[c].x - y[c].x, gy[i][c].x), fmaf(s, yu[c].y - y[c].y, gy[i][c].y));
+        const float n2 = cabs2(px) + cabs2(py);
+        const float sc = (n2 > 1.f) ? rsqrtf(n2) : 1.f;
+        gx[i][c] = cscale(px, sc);
+        gy[i][c] = cscale(py, sc);
+        yu[c] = y[c];
+      }
+    }
+  }
+
+  // final estimate and shrink: p replaces gx in registers
+  {
+    float2* gyf = s_gyf + (a.n_tv & 1) * TV_BND;
+#pragma unroll
+    for (int c = 0; c < TV_CPL; ++c) gyf[w * TV_EW + col0 + c] = gy[0][c];
+    __syncthreads();
+#pragma unroll
+    for (int i = 0; i < TV_R; ++i) {
+      float2 gxr[TV_CPL];
+#pragma unroll
+      for (int c = 0; c < TV_CPL - 1; ++c) gxr[c] = gx[i][c + 1];
+      gxr[TV_CPL - 1] = shfl_down2(gx[i][0]);
+#pragma unroll
+      for (int c = 0; c < TV_CPL; ++c) {
+        float2 gyd;
+        if (i < TV_R - 1) gyd = gy[i + 1][c];
+        else gyd = (w < TV_NW - 1) ? gyf[(w + 1) * TV_EW + col0 + c] : gy[i][c];
+        const float2 y = tv_estimate(xh[i][c], gx[i][c], gxr[c], gy[i][c], gyd, mu);
+        gx[i][c] = shrink(y, a.thr, a.faithful);
+      }
+    }
+  }
+  // last-row p and x of each run for the TV norms of the run below
+  float2* pl_last = s_gxl;  // reused: no TV reads remain
+  float2* xl_last = s_gyl;
+  if (a.want_norms) {
+#pragma unroll
+    for (int c = 0; c < TV_CPL; ++c) {
+      const int col = col0 + c;
+      const float2 g = s_g[(w * TV_R + TV_R - 1) * TV_EW + col];
+      pl_last[w * TV_EW + col] = gx[TV_R - 1][c];
+      xl_last[w * TV_EW + col] = make_float2(fmaf(t, g.x, xh[TV_R - 1][c].x), fmaf(t, g.y, xh[TV_R - 1][c].y));
+    }
   }
   __syncthreads();
-#pragma unroll
-  for (int i = 0; i < TV_RUN; ++i) s_y[(run * TV_RUN + i) * TV_EXT + ex] = y[i];
-  __syncthreads();
+
   double acc[kNumSums];
 #pragma unroll
   for (int k = 0; k < kNumSums; ++k) acc[k] = 0.0;
-  const int gx0 = ox + ex;  // unwrapped column of this thread
-  const bool col_in = (ex >= h) && (ex < h + inner) && (gx0 < W);
   ST* Pn = static_cast<ST*>(a.Pnew) + plane;
+  float2 pu[TV_CPL], xu[TV_CPL];
 #pragma unroll
-  for (int i = 0; i < TV_RUN; ++i) {
-    const int row = run * TV_RUN + i;
-    const int gy0 = oy + row;
-    if (!(col_in && row >= h && row < h + inner && gy0 < H)) continue;
-    const size_t e = (size_t)gy0 * W + gx0;
-    const float2 p = y[i];
-    Store<ST>::st(Pn + e, p);
-    const float2 x = s_X[row * TV_EXT + ex], g = s_g[row * TV_EXT + ex], y0 = s_P[row * TV_EXT + ex];
-    const float2 d = csub(p, x);
-    acc[SUM_LIM1] += (double)(d.x * g.x) + (double)(d.y * g.y);
-    acc[SUM_LIM2] += (double)cabs2(d);
-    float wr, wi;
-    restart_w(e, a.faithful, &wr, &wi);
-    const float2 u = csub(x, p), v = csub(p, y0);
-    acc[SUM_RS] += (double)(wr * u.x * v.x) + (double)(wi * u.y * v.y);
-    if (a.want_norms) {
-      const float2 pl = s_y[row * TV_EXT + ex - 1], pu = s_y[(row - 1) * TV_EXT + ex];
-      const float2 xl = s_X[row * TV_EXT + ex - 1], xu = s_X[(row - 1) * TV_EXT + ex];
-      acc[SUM_L1P] += (double)sqrtf(cabs2(p));
-      acc[SUM_TVP] += (double)sqrtf(cabs2(csub(pl, p)) + cabs2(csub(pu, p)));
-      acc[SUM_L1X] += (double)sqrtf(cabs2(x));
-      acc[SUM_TVX] += (double)sqrtf(cabs2(csub(xl, x)) + cabs2(csub(xu, x)));
+  for (int c = 0; c < TV_CPL; ++c) {
+    pu[c] = make_float2(0.f, 0.f);
+    xu[c] = make_float2(0.f, 0.f);
+    if (w > 0 && a.want_norms) {
+      pu[c] = pl_last[(w - 1) * TV_EW + col0 + c];
+      xu[c] = xl_last[(w - 1) * TV_EW + col0 + c];
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < TV_R; ++i) {
+    const int row = w * TV_R + i;
+    const int grow = oy + row;
+    const bool row_ok = row >= h && row < h + VH && grow < H;
+    float2 x[TV_CPL], pl[TV_CPL], xl[TV_CPL];
+#pragma unroll
+    for (int c = 0; c < TV_CPL; ++c) {
+      const float2 g = s_g[row * TV_EW + col0 + c];
+      x[c] = make_float2(fmaf(t, g.x, xh[i][c].x), fmaf(t, g.y, xh[i][c].y));
+    }
+    pl[0] = shfl_up2(gx[i][TV_CPL - 1]);
+    xl[0] = shfl_up2(x[TV_CPL - 1]);
+#pragma unroll
+    for (int c = 1; c < TV_CPL; ++c) {
+      pl[c] = gx[i][c - 1];
+      xl[c] = x[c - 1];
+    }
+#pragma unroll
+    for (int c = 0; c < TV_CPL; ++c) {
+      const int col = col0 + c, gcl = ox + col;
+      const float2 p = gx[i][c];
+      if (row_ok && col >= h && col < h + VW && gcl < W) {
+        const size_t e = (size_t)grow * W + gcl;
+        Store<ST>::st(Pn + e, p);
+        const float2 g = s_g[row * TV_EW + col], y0 = s_P[row * TV_EW + col];
+        const float2 d = csub(p, x[c]);
+        acc[SUM_LIM1] += (double)(d.x * g.x) + (double)(d.y * g.y);
+        acc[SUM_LIM2] += (double)cabs2(d);
+        float wr, wi;
+        restart_w(e, a.faithful, &wr, &wi);
+        const float2 u = csub(x[c], p), v = csub(p, y0);
+        acc[SUM_RS] += (double)(wr * u.x * v.x) + (double)(wi * u.y * v.y);
+        if (a.want_norms) {
+          acc[SUM_L1P] += (double)sqrtf(cabs2(p));
+          acc[SUM_TVP] += (double)sqrtf(cabs2(csub(pl[c], p)) + cabs2(csub(pu[c], p)));
+          acc[SUM_L1X] += (double)sqrtf(cabs2(x[c]));
+          acc[SUM_TVX] += (double)sqrtf(cabs2(csub(xl[c], x[c])) + cabs2(csub(xu[c], x[c])));
+        }
+      }
+      pu[c] = p;
+      xu[c] = x[c];
     }
   }
   const int blk = (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
@@ -711,14 +816,15 @@ __global__ void __launch_bounds__(TV_THREADS, 1) k_prox_tv2d(ProxArgs a) {
 }
 
 static void tv_grid(const ProxArgs& a, dim3* g) {
-  const int inner = TV_EXT - 2 * (a.n_tv + 1);
-  *g = dim3((a.W + inner - 1) / inner, (a.H + inner - 1) / inner, a.Nz);
+  const int h = a.n_tv + 1;
+  const int VW = TV_EW - 2 * h, VH = TV_EH - 2 * h;
+  *g = dim3((a.W + VW - 1) / VW, (a.H + VH - 1) / VH, a.Nz);
 }
 
 size_t max_partial_blocks(int W, int H, int Nz) {
   // the TV prox with the largest halo it accepts (n_tv <= 20) bounds all grids
-  const int inner = TV_EXT - 2 * 21;
-  size_t tv = (size_t)((W + inner - 1) / inner) * ((H + inner - 1) / inner) * Nz;
+  const int h = 21, VW = TV_EW - 2 * h, VH = TV_EH - 2 * h;
+  size_t tv = (size_t)((W + VW - 1) / VW) * ((H + VH - 1) / VH) * Nz;
   size_t flat = 4096;
   return tv > flat ? tv : flat;
 }
@@ -807,28 +913,48 @@ cudaError_t launch_prox_l1(int storage, const ProxArgs& a, int* nblocks_out, cud
 }
 
 // ---------------------------------------------------------------------------
-// final reduction of block partials (single block, fixed order)
+// reduction of block partials in two fixed-shape stages (deterministic):
+// stage 1 sums contiguous slices of the partials, stage 2 sums the slices.
 // ---------------------------------------------------------------------------
-__global__ void k_reduce_partials(const double* __restrict__ partials, int nblocks, double* __restrict__ out) {
-  __shared__ double red[256];
-  for (int k = 0; k < kNumSums; ++k) {
-    double s = 0;
-    for (int b = threadIdx.x; b < nblocks; b += blockDim.x) s += partials[(size_t)b * kNumSums + k];
-    red[threadIdx.x] = s;
-    __syncthreads();
-    for (int w = blockDim.x / 2; w > 0; w >>= 1) {
-      if (threadIdx.x < w) red[threadIdx.x] += red[threadIdx.x + w];
-      __syncthreads();
-    }
-    if (threadIdx.x == 0) out[k] = red[0];
-    __syncthreads();
+constexpr int RED_THREADS = 256;
+constexpr int RED_SLICES = 512;
+
+__global__ void __launch_bounds__(RED_THREADS) k_reduce_stage(const double* __restrict__ in, int n, int per_block,
+                                                              double* __restrict__ out) {
+  __shared__ double red[RED_THREADS / 32][kNumSums];
+  const int b0 = blockIdx.x * per_block, b1 = min(n, b0 + per_block);
+  // thread j handles slot j % kNumSums of rows b0 + j / kNumSums, strided
+  const int slot = threadIdx.x % kNumSums, lane_row = threadIdx.x / kNumSums;
+  constexpr int ROWS_PER_PASS = RED_THREADS / kNumSums;
+  double v = 0.0;
+  for (int b = b0 + lane_row; b < b1; b += ROWS_PER_PASS) v += in[(size_t)b * kNumSums + slot];
+  // gather per-slot sums: rows of the same slot are kNumSums lanes apart
+#pragma unroll
+  for (int o = 16; o >= kNumSums; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane < kNumSums) red[wid][lane] = v;
+  __syncthreads();
+  if (threadIdx.x < kNumSums) {
+    double s = 0.0;
+    for (int w = 0; w < RED_THREADS / 32; ++w) s += red[w][threadIdx.x];
+    out[(size_t)blockIdx.x * kNumSums + threadIdx.x] = s;
   }
 }
 
-cudaError_t launch_reduce_partials(const double* partials, int nblocks, double* out, cudaStream_t st) {
-  k_reduce_partials<<<1, 256, 0, st>>>(partials, nblocks, out);
+cudaError_t launch_reduce_partials(const double* partials, int nblocks, double* scratch, double* out,
+                                   cudaStream_t st) {
+  if (nblocks <= RED_THREADS) {
+    k_reduce_stage<<<1, RED_THREADS, 0, st>>>(partials, nblocks, nblocks, out);
+    return cudaGetLastError();
+  }
+  const int per = (nblocks + RED_SLICES - 1) / RED_SLICES;
+  const int slices = (nblocks + per - 1) / per;
+  k_reduce_stage<<<slices, RED_THREADS, 0, st>>>(partials, nblocks, per, scratch);
+  k_reduce_stage<<<1, RED_THREADS, 0, st>>>(scratch, slices, slices, out);
   return cudaGetLastError();
 }
+
+size_t reduce_scratch_doubles() { return (size_t)RED_SLICES * kNumSums; }
 
 // ---------------------------------------------------------------------------
 // plane-level kernels

@@ -53,7 +53,9 @@ cudaError_t launch_plane_col(int inverse, const float2* in, float2* out, int W, 
 cudaError_t launch_sum_chunks(const float2* Spart, int nchunks, float2* S, long long n, cudaStream_t st);
 cudaError_t launch_prox_tv2d(int storage, const ProxArgs& a, int* nblocks_out, cudaStream_t st);
 cudaError_t launch_prox_l1(int storage, const ProxArgs& a, int* nblocks_out, cudaStream_t st);
-cudaError_t launch_reduce_partials(const double* partials, int nblocks, double* out, cudaStream_t st);
+cudaError_t launch_reduce_partials(const double* partials, int nblocks, double* scratch, double* out,
+                                   cudaStream_t st);
+size_t reduce_scratch_doubles();
 cudaError_t launch_finish_forward(const float2* c, const float* b, float* dnew, long long n, double* partials,
                                   int* nblocks_out, cudaStream_t st);
 cudaError_t launch_holo_momentum(const float* dnew, float* dY0, float* dX, const float* b, float* r,

@@ -91,6 +91,7 @@ struct rihvr_ctx {
   double* partials = nullptr;
   size_t partial_cap = 0;
   double* sums_d = nullptr;
+  double* red_scratch = nullptr;
   double* sums_h = nullptr;  // pinned
   int nchunks = 1;
   float2 *X1 = nullptr, *gx = nullptr, *gy = nullptr, *gz = nullptr, *Y = nullptr;  // mode 6
@@ -177,7 +178,8 @@ int residual_spectrum(rihvr_ctx* c) {
 }
 
 int reduce_into(rihvr_ctx* c, int nblocks, int slot) {
-  KL(launch_reduce_partials(c->partials, nblocks, c->sums_d + slot * kNumSums, c->st));
+  KL(launch_reduce_partials(c->partials, nblocks, c->red_scratch, c->sums_d + slot * kNumSums, c->st));
+  if (nblocks > 256) ++c->launches;  // two-stage reduction
   return RIHVR_OK;
 }
 
@@ -521,6 +523,7 @@ int rihvr_create(const rihvr_params* params, int width, int height, rihvr_ctx** 
   c->partial_cap = max_partial_blocks(width, height, c->Nz);
   if (rc == RIHVR_OK) rc = dalloc_t(c, &c->partials, c->partial_cap * kNumSums);
   if (rc == RIHVR_OK) rc = dalloc_t(c, &c->sums_d, (size_t)kNumSums * NUM_SLOTS);
+  if (rc == RIHVR_OK) rc = dalloc_t(c, &c->red_scratch, reduce_scratch_doubles());
   if (rc != RIHVR_OK) return cleanup(rc);
   if (cudaMallocHost(&c->sums_h, sizeof(double) * kNumSums * NUM_SLOTS) != cudaSuccess)
     return cleanup(fail(RIHVR_ERR_OUT_OF_MEMORY, "cudaMallocHost failed"));
