@@ -189,6 +189,23 @@ int rihvr_adjoint(rihvr_ctx* ctx, const float* residual, float* volume_out, int 
 int rihvr_prox_step(rihvr_ctx* ctx, const float* x, const float* residual, double t, float* p_out,
                     double* sums3, int is_device);
 
+/* Allocation-free adjoint.  No counterpart in the reference: for callers that
+ * cannot allocate device memory - code running while a CUDA graph is captured,
+ * plugin hosts that hand out all device memory from their own pool, real-time
+ * loops that cannot take an allocation's latency.  Computes what rihvr_adjoint
+ * computes (g_z = IFFT(conj(H'_z) FFT(r)) for every plane) without a context:
+ * `residual` (height x width floats) and `volume_out` (Nz x height x width
+ * complex interleaved) are device memory owned by the caller; `stream` is a
+ * cudaStream_t (NULL = legacy default stream); the call is asynchronous on it.
+ * Scratch lives in one fixed 24 MiB + 32 KiB device array that every GPU
+ * loading the library holds until exit: planes must be square with a supported
+ * side of at most 1024 and num_planes at most 4096, otherwise
+ * RIHVR_ERR_UNSUPPORTED_SIZE is returned.  The first call on a device looks the
+ * array up (and may load the module), so make it before any stream capture.
+ * Calls share the array and race if they overlap on the GPU; serialise them. */
+int rihvr_adjoint_noalloc(const rihvr_params* params, int width, int height, const float* residual,
+                          float* volume_out, void* stream);
+
 /* Device time per kernel class of the iterations run with profiling on
  * (names "adj_col", "adj_row", "prox", "fwd_row", "fwd_col", "plane").
  * Enabling records a pair of CUDA events around each launch. */

@@ -95,6 +95,7 @@ EXPORTED = (
     "rihvr_set_hologram", "rihvr_reconstruct", "rihvr_reset", "rihvr_iterate", "rihvr_iterate_timed",
     "rihvr_iteration_count", "rihvr_objective", "rihvr_get_iterations", "rihvr_get_plane", "rihvr_get_volume",
     "rihvr_get_estimate", "rihvr_get_residual", "rihvr_forward", "rihvr_adjoint", "rihvr_prox_step",
+    "rihvr_adjoint_noalloc",
     "rihvr_set_profiling", "rihvr_kernel_times", "rihvr_get_stream", "rihvr_launch_count", "rihvr_device_bytes",
     "rihvr_status_string", "rihvr_last_error",
 )
@@ -146,6 +147,7 @@ def load_library(path: str = LIB_PATH):
     L.rihvr_forward.argtypes = [vp, vp, vp, ip]
     L.rihvr_adjoint.argtypes = [vp, vp, vp, ip]
     L.rihvr_prox_step.argtypes = [vp, vp, vp, dp, vp, P(ctypes.c_double), ip]
+    L.rihvr_adjoint_noalloc.argtypes = [P(RihvrParams), ip, ip, vp, vp, vp]
     L.rihvr_set_profiling.argtypes = [vp, ip]
     L.rihvr_kernel_times.argtypes = [vp, P(ctypes.c_char_p), P(ctypes.c_double), P(ctypes.c_int), ip,
                                      P(ctypes.c_int)]
@@ -188,6 +190,15 @@ def plane_list(p: RihvrParams) -> np.ndarray:
     _check(load_library().rihvr_plane_list(ctypes.byref(p), z.ctypes.data_as(ctypes.POINTER(ctypes.c_double))),
            "rihvr_plane_list")
     return z
+
+
+def adjoint_noalloc(params: RihvrParams, width: int, height: int, residual_dev: int, volume_dev: int,
+                    stream: int = 0):
+    """Allocation-free adjoint over caller-owned device buffers (raw pointers):
+    for callers that cannot allocate device memory.  Asynchronous on `stream`."""
+    _check(load_library().rihvr_adjoint_noalloc(ctypes.byref(params), int(width), int(height),
+                                                 ctypes.c_void_p(residual_dev), ctypes.c_void_p(volume_dev),
+                                                 ctypes.c_void_p(stream)), "rihvr_adjoint_noalloc")
 
 
 def params_from_config(cfg, **overrides) -> RihvrParams:

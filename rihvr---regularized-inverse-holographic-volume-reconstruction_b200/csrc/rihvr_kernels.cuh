@@ -39,6 +39,8 @@ struct ProxArgs {
 };
 
 bool line_size_supported(int n);
+// message returned by rihvr_last_error on this thread
+void set_last_error(const char* msg);
 size_t max_partial_blocks(int W, int H, int Nz);
 
 cudaError_t launch_adj_col(const float2* Rs, const double* cturn, const double* zlist, float2* U, int W,

@@ -33,6 +33,12 @@ int fail(int code, const std::string& msg) {
   return code;
 }
 
+}  // namespace
+
+void rihvr::set_last_error(const char* msg) { g_last_error = msg ? msg : ""; }
+
+namespace {
+
 #define CK(call)                                                                                   \
   do {                                                                                             \
     cudaError_t e_ = (call);                                                                       \
