@@ -588,7 +588,7 @@ __device__ __forceinline__ float cabs2(float2 a) { return a.x * a.x + a.y * a.y;
 // the projection norm is taken over the four real components (Jacobi updates,
 // as the reference's two kernels per iteration).
 //
-// Layout: a block holds a 64 x 128 tile (columns x rows) with a recomputed halo
+// Layout: a block holds a 64 x 64 tile (columns x rows) with a recomputed halo
 // of n_tv + 1 pixels on every side, which makes the interior exact.  Warp w owns
 // rows [8w, 8w+8); lane l owns columns 2l and 2l+1.  The Chambolle state (xh, gx,
 // gy) stays in registers; each TV iteration sweeps a thread's 8 rows top to
@@ -603,7 +603,7 @@ __device__ __forceinline__ float cabs2(float2 a) { return a.x * a.x + a.y * a.y;
 constexpr int TV_CPL = 2;                  // columns per lane
 constexpr int TV_EW = 32 * TV_CPL;         // tile width incl. halo
 constexpr int TV_R = 8;                    // rows per thread
-constexpr int TV_NW = 16;                  // warps, stacked vertically
+constexpr int TV_NW = 8;                   // warps, stacked vertically
 constexpr int TV_EH = TV_NW * TV_R;        // tile height incl. halo
 constexpr int TV_THREADS = 32 * TV_NW;
 constexpr int TV_BND = TV_NW * TV_EW;      // one boundary row per warp
@@ -616,15 +616,58 @@ __device__ __forceinline__ float2 shfl_up2(float2 v) {
   return make_float2(__shfl_up_sync(0xffffffffu, v.x, 1), __shfl_up_sync(0xffffffffu, v.y, 1));
 }
 
-// y = xh - mu ((gxr - gx) + (gyd - gy))
-__device__ __forceinline__ float2 tv_estimate(float2 xh, float2 gx, float2 gxr, float2 gy, float2 gyd, float mu) {
-  const float dvx = (gxr.x - gx.x) + (gyd.x - gy.x);
-  const float dvy = (gxr.y - gx.y) + (gyd.y - gy.y);
-  return make_float2(fmaf(-mu, dvx, xh.x), fmaf(-mu, dvy, xh.y));
+// y = xh - mu ((gxr - gx) + (gyd - gy)), packed: nmu = (-mu, -mu)
+__device__ __forceinline__ float2 tv_estimate(float2 xh, float2 gx, float2 gxr, float2 gy, float2 gyd, float2 nmu) {
+  return f2fma(nmu, f2add(f2sub(gxr, gx), f2sub(gyd, gy)), xh);
 }
 
+// g = P(g + s grad y) for one pixel: px = gx + s (yl - y), py = gy + s (yu - y),
+// divided by max(1, |(px, py)|) over the four real components.
+__device__ __forceinline__ void tv_dual(float2& gx, float2& gy, float2 y, float2 yl, float2 yu, float2 s2) {
+  const float2 px = f2fma(s2, f2sub(yl, y), gx);
+  const float2 py = f2fma(s2, f2sub(yu, y), gy);
+  const float2 q = f2fma(py, py, f2mul(px, px));
+  const float n2 = q.x + q.y;
+  const float sc = (n2 > 1.f) ? rsqrtf(n2) : 1.f;
+  const float2 sc2 = make_float2(sc, sc);
+  gx = f2mul(px, sc2);
+  gy = f2mul(py, sc2);
+}
+
+// wrap an index that lies within one period of [0, n)
+__device__ __forceinline__ int wrap1(int i, int n) { return i < 0 ? i + n : (i >= n ? i - n : i); }
+
 template <typename ST>
-__global__ void __launch_bounds__(TV_THREADS, 1) k_prox_tv2d(ProxArgs a) {
+struct Pair;  // two adjacent complex values in storage layout
+template <>
+struct Pair<float2> {
+  using T = float4;
+  static __device__ __forceinline__ void ld(const float2* p, float2& a, float2& b) {
+    const float4 v = *reinterpret_cast<const float4*>(p);
+    a = make_float2(v.x, v.y);
+    b = make_float2(v.z, v.w);
+  }
+};
+template <>
+struct Pair<__nv_bfloat162> {
+  static __device__ __forceinline__ void ld(const __nv_bfloat162* p, float2& a, float2& b) {
+    const uint2 v = *reinterpret_cast<const uint2*>(p);
+    a = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&v.x));
+    b = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&v.y));
+  }
+};
+template <>
+struct Pair<__half2> {
+  static __device__ __forceinline__ void ld(const __half2* p, float2& a, float2& b) {
+    const uint2 v = *reinterpret_cast<const uint2*>(p);
+    a = __half22float2(*reinterpret_cast<const __half2*>(&v.x));
+    b = __half22float2(*reinterpret_cast<const __half2*>(&v.y));
+  }
+};
+
+template <typename ST>
+__global__ void __launch_bounds__(TV_THREADS, 2) k_prox_tv2d(ProxArgs a) {
+  static_assert(TV_CPL == 2, "paired loads assume two columns per lane");
   extern __shared__ float2 smem[];
   float2* s_g = smem;                      // [EH][EW] gradient at load
   float2* s_P = s_g + TV_EH * TV_EW;       // [EH][EW] P at load
@@ -640,28 +683,47 @@ __global__ void __launch_bounds__(TV_THREADS, 1) k_prox_tv2d(ProxArgs a) {
   const ST* P = static_cast<const ST*>(a.P) + plane;
   const ST* Pp = static_cast<const ST*>(a.Pprev) + plane;
   const float2* G = a.G + plane;
-  const float mu = a.mu, s = a.s, t = a.t, beta = a.beta;
+  const float t = a.t, beta = a.beta;
+  const float2 nmu = make_float2(-a.mu, -a.mu), s2 = make_float2(a.s, a.s);
   const int col0 = lane * TV_CPL;
+  // tiles are at most one period outside the plane when it is at least as
+  // large as a tile; smaller planes wrap several times
+  const bool small = (W < TV_EW) || (H < TV_EH);
+  // adjacent column pairs are contiguous and 16-byte aligned when the tile
+  // origin is even (the plane side is even)
+  const bool paired = !small && ((ox & 1) == 0);
 
   float2 xh[TV_R][TV_CPL], gx[TV_R][TV_CPL], gy[TV_R][TV_CPL];
-  int gcol[TV_CPL];
+  int gc[TV_CPL];
 #pragma unroll
-  for (int c = 0; c < TV_CPL; ++c) gcol[c] = ((ox + col0 + c) % W + W) % W;
+  for (int c = 0; c < TV_CPL; ++c) gc[c] = small ? ((ox + col0 + c) % W + W) % W : wrap1(ox + col0 + c, W);
 #pragma unroll
   for (int i = 0; i < TV_R; ++i) {
     const int row = w * TV_R + i;
-    const size_t rbase = (size_t)(((oy + row) % H + H) % H) * W;
+    const int gr = small ? ((oy + row) % H + H) % H : wrap1(oy + row, H);
+    const size_t rbase = (size_t)gr * W;
+    float2 p[TV_CPL], pp[TV_CPL], g[TV_CPL];
+    if (paired) {
+      Pair<ST>::ld(P + rbase + gc[0], p[0], p[1]);
+      Pair<ST>::ld(Pp + rbase + gc[0], pp[0], pp[1]);
+      Pair<float2>::ld(G + rbase + gc[0], g[0], g[1]);
+    } else {
+#pragma unroll
+      for (int c = 0; c < TV_CPL; ++c) {
+        p[c] = Store<ST>::ld(P + rbase + gc[c]);
+        pp[c] = Store<ST>::ld(Pp + rbase + gc[c]);
+        g[c] = G[rbase + gc[c]];
+      }
+    }
 #pragma unroll
     for (int c = 0; c < TV_CPL; ++c) {
-      const size_t idx = rbase + gcol[c];
-      const float2 p = Store<ST>::ld(P + idx), pp = Store<ST>::ld(Pp + idx), g = G[idx];
-      const float2 x = make_float2(fmaf(beta, p.x - pp.x, p.x), fmaf(beta, p.y - pp.y, p.y));
-      xh[i][c] = make_float2(fmaf(-t, g.x, x.x), fmaf(-t, g.y, x.y));
-      s_g[row * TV_EW + col0 + c] = g;
-      s_P[row * TV_EW + col0 + c] = p;
+      const float2 x = f2fma(make_float2(beta, beta), f2sub(p[c], pp[c]), p[c]);
+      xh[i][c] = f2fma(make_float2(-t, -t), g[c], x);
       gx[i][c] = make_float2(0.f, 0.f);
       gy[i][c] = make_float2(0.f, 0.f);
     }
+    *reinterpret_cast<float4*>(s_g + row * TV_EW + col0) = make_float4(g[0].x, g[0].y, g[1].x, g[1].y);
+    *reinterpret_cast<float4*>(s_P + row * TV_EW + col0) = make_float4(p[0].x, p[0].y, p[1].x, p[1].y);
   }
 #pragma unroll
   for (int c = 0; c < TV_CPL; ++c) s_xhl[w * TV_EW + col0 + c] = xh[TV_R - 1][c];
@@ -686,7 +748,7 @@ __global__ void __launch_bounds__(TV_THREADS, 1) k_prox_tv2d(ProxArgs a) {
         const int col = col0 + c, b = (w - 1) * TV_EW;
         const float2 gxu = gxl[b + col], gyu = gyl[b + col];
         const float2 gxru = (col + 1 < TV_EW) ? gxl[b + col + 1] : gxu;
-        yu[c] = tv_estimate(s_xhl[b + col], gxu, gxru, gyu, gy[0][c], mu);
+        yu[c] = tv_estimate(s_xhl[b + col], gxu, gxru, gyu, gy[0][c], nmu);
       }
     }
 #pragma unroll
@@ -699,19 +761,14 @@ __global__ void __launch_bounds__(TV_THREADS, 1) k_prox_tv2d(ProxArgs a) {
       for (int c = 0; c < TV_CPL; ++c) {
         if (i < TV_R - 1) gyd[c] = gy[i + 1][c];
         else gyd[c] = (w < TV_NW - 1) ? gyf[(w + 1) * TV_EW + col0 + c] : gy[i][c];
-        y[c] = tv_estimate(xh[i][c], gx[i][c], gxr[c], gy[i][c], gyd[c], mu);
+        y[c] = tv_estimate(xh[i][c], gx[i][c], gxr[c], gy[i][c], gyd[c], nmu);
       }
       yl[0] = shfl_up2(y[TV_CPL - 1]);  // lane 0 gets its own (halo column)
 #pragma unroll
       for (int c = 1; c < TV_CPL; ++c) yl[c] = y[c - 1];
 #pragma unroll
       for (int c = 0; c < TV_CPL; ++c) {
-        const float2 px = make_float2(fmaf(s, yl[c].x - y[c].x, gx[i][c].x), fmaf(s, yl[c].y - y[c].y, gx[i][c].y));
-        const float2 py = make_float2(fmaf(s, yu[c].x - y[c].x, gy[i][c].x), fmaf(s, yu[c].y - y[c].y, gy[i][c].y));
-        const float n2 = cabs2(px) + cabs2(py);
-        const float sc = (n2 > 1.f) ? rsqrtf(n2) : 1.f;
-        gx[i][c] = cscale(px, sc);
-        gy[i][c] = cscale(py, sc);
+        tv_dual(gx[i][c], gy[i][c], y[c], yl[c], yu[c], s2);
         yu[c] = y[c];
       }
     }
@@ -734,7 +791,7 @@ __global__ void __launch_bounds__(TV_THREADS, 1) k_prox_tv2d(ProxArgs a) {
         float2 gyd;
         if (i < TV_R - 1) gyd = gy[i + 1][c];
         else gyd = (w < TV_NW - 1) ? gyf[(w + 1) * TV_EW + col0 + c] : gy[i][c];
-        const float2 y = tv_estimate(xh[i][c], gx[i][c], gxr[c], gy[i][c], gyd, mu);
+        const float2 y = tv_estimate(xh[i][c], gx[i][c], gxr[c], gy[i][c], gyd, nmu);
         gx[i][c] = shrink(y, a.thr, a.faithful);
       }
     }
@@ -742,20 +799,22 @@ __global__ void __launch_bounds__(TV_THREADS, 1) k_prox_tv2d(ProxArgs a) {
   // last-row p and x of each run for the TV norms of the run below
   float2* pl_last = s_gxl;  // reused: no TV reads remain
   float2* xl_last = s_gyl;
+  const float2 t2 = make_float2(t, t);
   if (a.want_norms) {
 #pragma unroll
     for (int c = 0; c < TV_CPL; ++c) {
       const int col = col0 + c;
       const float2 g = s_g[(w * TV_R + TV_R - 1) * TV_EW + col];
       pl_last[w * TV_EW + col] = gx[TV_R - 1][c];
-      xl_last[w * TV_EW + col] = make_float2(fmaf(t, g.x, xh[TV_R - 1][c].x), fmaf(t, g.y, xh[TV_R - 1][c].y));
+      xl_last[w * TV_EW + col] = f2fma(t2, g, xh[TV_R - 1][c]);
     }
   }
   __syncthreads();
 
-  double acc[kNumSums];
+  // per-thread FP32 partials over at most 16 pixels, FP64 from there on
+  float acc[kNumSums];
 #pragma unroll
-  for (int k = 0; k < kNumSums; ++k) acc[k] = 0.0;
+  for (int k = 0; k < kNumSums; ++k) acc[k] = 0.f;
   ST* Pn = static_cast<ST*>(a.Pnew) + plane;
   float2 pu[TV_CPL], xu[TV_CPL];
 #pragma unroll
@@ -772,12 +831,17 @@ __global__ void __launch_bounds__(TV_THREADS, 1) k_prox_tv2d(ProxArgs a) {
     const int row = w * TV_R + i;
     const int grow = oy + row;
     const bool row_ok = row >= h && row < h + VH && grow < H;
-    float2 x[TV_CPL], pl[TV_CPL], xl[TV_CPL];
-#pragma unroll
-    for (int c = 0; c < TV_CPL; ++c) {
-      const float2 g = s_g[row * TV_EW + col0 + c];
-      x[c] = make_float2(fmaf(t, g.x, xh[i][c].x), fmaf(t, g.y, xh[i][c].y));
+    float2 x[TV_CPL], pl[TV_CPL], xl[TV_CPL], g[TV_CPL], y0[TV_CPL];
+    {
+      const float4 gv = *reinterpret_cast<const float4*>(s_g + row * TV_EW + col0);
+      const float4 pv = *reinterpret_cast<const float4*>(s_P + row * TV_EW + col0);
+      g[0] = make_float2(gv.x, gv.y);
+      g[1] = make_float2(gv.z, gv.w);
+      y0[0] = make_float2(pv.x, pv.y);
+      y0[1] = make_float2(pv.z, pv.w);
     }
+#pragma unroll
+    for (int c = 0; c < TV_CPL; ++c) x[c] = f2fma(t2, g[c], xh[i][c]);
     pl[0] = shfl_up2(gx[i][TV_CPL - 1]);
     xl[0] = shfl_up2(x[TV_CPL - 1]);
 #pragma unroll
@@ -792,27 +856,30 @@ __global__ void __launch_bounds__(TV_THREADS, 1) k_prox_tv2d(ProxArgs a) {
       if (row_ok && col >= h && col < h + VW && gcl < W) {
         const size_t e = (size_t)grow * W + gcl;
         Store<ST>::st(Pn + e, p);
-        const float2 g = s_g[row * TV_EW + col], y0 = s_P[row * TV_EW + col];
-        const float2 d = csub(p, x[c]);
-        acc[SUM_LIM1] += (double)(d.x * g.x) + (double)(d.y * g.y);
-        acc[SUM_LIM2] += (double)cabs2(d);
+        const float2 d = f2sub(p, x[c]);
+        const float2 dg = f2mul(d, g[c]);
+        acc[SUM_LIM1] += dg.x + dg.y;
+        acc[SUM_LIM2] += cabs2(d);
         float wr, wi;
         restart_w(e, a.faithful, &wr, &wi);
-        const float2 u = csub(x[c], p), v = csub(p, y0);
-        acc[SUM_RS] += (double)(wr * u.x * v.x) + (double)(wi * u.y * v.y);
+        const float2 uv = f2mul(f2sub(x[c], p), f2sub(p, y0[c]));
+        acc[SUM_RS] += fmaf(wr, uv.x, wi * uv.y);
         if (a.want_norms) {
-          acc[SUM_L1P] += (double)sqrtf(cabs2(p));
-          acc[SUM_TVP] += (double)sqrtf(cabs2(csub(pl[c], p)) + cabs2(csub(pu[c], p)));
-          acc[SUM_L1X] += (double)sqrtf(cabs2(x[c]));
-          acc[SUM_TVX] += (double)sqrtf(cabs2(csub(xl[c], x[c])) + cabs2(csub(xu[c], x[c])));
+          acc[SUM_L1P] += sqrtf(cabs2(p));
+          acc[SUM_TVP] += sqrtf(cabs2(f2sub(pl[c], p)) + cabs2(f2sub(pu[c], p)));
+          acc[SUM_L1X] += sqrtf(cabs2(x[c]));
+          acc[SUM_TVX] += sqrtf(cabs2(f2sub(xl[c], x[c])) + cabs2(f2sub(xu[c], x[c])));
         }
       }
       pu[c] = p;
       xu[c] = x[c];
     }
   }
+  double dacc[kNumSums];
+#pragma unroll
+  for (int k = 0; k < kNumSums; ++k) dacc[k] = (double)acc[k];
   const int blk = (blockIdx.z * gridDim.y + blockIdx.y) * gridDim.x + blockIdx.x;
-  block_write_sums<TV_THREADS>(acc, a.partials, blk);
+  block_write_sums<TV_THREADS>(dacc, a.partials, blk);
 }
 
 static void tv_grid(const ProxArgs& a, dim3* g) {
