@@ -176,6 +176,15 @@ int rihvr_get_volume(rihvr_ctx* ctx, float* out, int is_device);
 int rihvr_get_estimate(rihvr_ctx* ctx, float* out, int is_device);
 int rihvr_get_residual(rihvr_ctx* ctx, float* out, int is_device);
 
+/* Fraction of non-zero voxels of the current momentum point
+ * (SparseVolume::getSparsity, as printed per iteration at :561-565). */
+int rihvr_sparsity(rihvr_ctx* ctx, double* fraction);
+
+/* backPropagateInitial + calcInitialResidual (:2079-2133, :2725-2771): the
+ * hologram estimated from t A^H b with t = 1/num_planes, written by the
+ * reference as estimate_initial.tif.  Leaves the solve reset to x = 0. */
+int rihvr_initial_estimate(rihvr_ctx* ctx, float* estimate_out, int is_device);
+
 /* Operator entry points. */
 /* backPropagate (:1935-2077): d = Re(IFFT(sum_z H'_z FFT(x_z))), x complex
  * interleaved Nz x height x width, d height x width floats. */
@@ -188,6 +197,25 @@ int rihvr_adjoint(rihvr_ctx* ctx, const float* residual, float* volume_out, int 
  * sum (p - x).g, sum |p - x|^2 and the restart statistic against y0 = x. */
 int rihvr_prox_step(rihvr_ctx* ctx, const float* x, const float* residual, double t, float* p_out,
                     double* sums3, int is_device);
+
+/* Image I/O and preprocessing of the hologram frame (the OpenCV parts of
+ * Hologram on the reconstruction path).
+ * rihvr_read_image: Hologram::read (hologram.cu:139-199) - 8/16-bit grayscale
+ * or RGB TIFF (uncompressed, PackBits, LZW, horizontal predictor) or binary
+ * PGM; values as stored.  Call with pixels == NULL to get the size, then with
+ * a width*height buffer and the same width/height. */
+int rihvr_read_image(const char* path, float* pixels, int* width, int* height, int* bits);
+/* cv::imwrite of an 8-bit grayscale image: baseline uncompressed TIFF. */
+int rihvr_write_tiff8(const char* path, const unsigned char* pixels, int width, int height);
+/* The preprocessing of main_sparse_inverse.cu:106-124: /255 (hologram.cu:
+ * 401-439); I/mean - 1 (:332-358) or, when files->remove_background, (I - B) /
+ * max(sqrt(B), 0.1) (:1365-1432); crop to files' ROI (:768-887); zero padding
+ * (:889-945).  `files` may be NULL (whole frame, no background).  Size query
+ * and call protocol as rihvr_read_image. */
+int rihvr_preprocess(const float* holo, int width, int height, const float* background,
+                     const rihvr_file_params* files, int zero_padding, float* out, int* out_width, int* out_height);
+/* Message of the last failed image call on this thread. */
+const char* rihvr_io_error(void);
 
 /* Allocation-free adjoint.  No counterpart in the reference: for callers that
  * cannot allocate device memory - code running while a CUDA graph is captured,

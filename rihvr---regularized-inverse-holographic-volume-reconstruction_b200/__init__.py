@@ -95,7 +95,8 @@ EXPORTED = (
     "rihvr_set_hologram", "rihvr_reconstruct", "rihvr_reset", "rihvr_iterate", "rihvr_iterate_timed",
     "rihvr_iteration_count", "rihvr_objective", "rihvr_get_iterations", "rihvr_get_plane", "rihvr_get_volume",
     "rihvr_get_estimate", "rihvr_get_residual", "rihvr_forward", "rihvr_adjoint", "rihvr_prox_step",
-    "rihvr_adjoint_noalloc",
+    "rihvr_adjoint_noalloc", "rihvr_sparsity", "rihvr_initial_estimate",
+    "rihvr_read_image", "rihvr_write_tiff8", "rihvr_preprocess", "rihvr_io_error",
     "rihvr_set_profiling", "rihvr_kernel_times", "rihvr_get_stream", "rihvr_launch_count", "rihvr_device_bytes",
     "rihvr_status_string", "rihvr_last_error",
 )
@@ -148,6 +149,12 @@ def load_library(path: str = LIB_PATH):
     L.rihvr_adjoint.argtypes = [vp, vp, vp, ip]
     L.rihvr_prox_step.argtypes = [vp, vp, vp, dp, vp, P(ctypes.c_double), ip]
     L.rihvr_adjoint_noalloc.argtypes = [P(RihvrParams), ip, ip, vp, vp, vp]
+    L.rihvr_sparsity.argtypes = [vp, P(ctypes.c_double)]
+    L.rihvr_read_image.argtypes = [ctypes.c_char_p, vp, P(ctypes.c_int), P(ctypes.c_int), P(ctypes.c_int)]
+    L.rihvr_write_tiff8.argtypes = [ctypes.c_char_p, vp, ip, ip]
+    L.rihvr_preprocess.argtypes = [vp, ip, ip, vp, P(FileParams), ip, vp, P(ctypes.c_int), P(ctypes.c_int)]
+    L.rihvr_io_error.restype = ctypes.c_char_p
+    L.rihvr_initial_estimate.argtypes = [vp, vp, ip]
     L.rihvr_set_profiling.argtypes = [vp, ip]
     L.rihvr_kernel_times.argtypes = [vp, P(ctypes.c_char_p), P(ctypes.c_double), P(ctypes.c_int), ip,
                                      P(ctypes.c_int)]
@@ -199,6 +206,50 @@ def adjoint_noalloc(params: RihvrParams, width: int, height: int, residual_dev: 
     _check(load_library().rihvr_adjoint_noalloc(ctypes.byref(params), int(width), int(height),
                                                  ctypes.c_void_p(residual_dev), ctypes.c_void_p(volume_dev),
                                                  ctypes.c_void_p(stream)), "rihvr_adjoint_noalloc")
+
+
+def _io_check(rc: int, where: str):
+    if rc != OK:
+        msg = (load_library().rihvr_io_error() or b"").decode(errors="replace")
+        raise RihvrError(rc, f"{where}: {msg}")
+
+
+def read_image(path: str):
+    """Hologram::read: (pixels float32 [H, W] as stored, bits per sample)."""
+    L = load_library()
+    w, h, bits = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+    _io_check(L.rihvr_read_image(path.encode(), None, ctypes.byref(w), ctypes.byref(h), ctypes.byref(bits)),
+              "rihvr_read_image")
+    out = np.empty((h.value, w.value), np.float32)
+    _io_check(L.rihvr_read_image(path.encode(), _ptr(out), ctypes.byref(w), ctypes.byref(h), None),
+              "rihvr_read_image")
+    return out, bits.value
+
+
+def write_tiff8(path: str, img: np.ndarray):
+    img = np.ascontiguousarray(img, dtype=np.uint8)
+    _io_check(load_library().rihvr_write_tiff8(path.encode(), _ptr(img), img.shape[1], img.shape[0]),
+              "rihvr_write_tiff8")
+
+
+def preprocess(holo: np.ndarray, zero_padding: int, background: np.ndarray | None = None,
+               files: FileParams | None = None) -> np.ndarray:
+    """The reference preprocessing (rescale, normalise or background divide,
+    crop, zero pad) of a raw frame; returns the measured hologram b."""
+    L = load_library()
+    holo = np.ascontiguousarray(holo, dtype=np.float32)
+    bg = None if background is None else np.ascontiguousarray(background, dtype=np.float32)
+    if bg is not None and files is None:
+        files = FileParams()
+        files.remove_background = 1
+        files.roi_size = -1
+    fp = ctypes.byref(files) if files is not None else None
+    w, h = ctypes.c_int(), ctypes.c_int()
+    args = (_ptr(holo), holo.shape[1], holo.shape[0], _ptr(bg) if bg is not None else None, fp, int(zero_padding))
+    _io_check(L.rihvr_preprocess(*args, None, ctypes.byref(w), ctypes.byref(h)), "rihvr_preprocess")
+    out = np.empty((h.value, w.value), np.float32)
+    _io_check(L.rihvr_preprocess(*args, _ptr(out), ctypes.byref(w), ctypes.byref(h)), "rihvr_preprocess")
+    return out
 
 
 def params_from_config(cfg, **overrides) -> RihvrParams:
@@ -289,6 +340,16 @@ class SparseCompressiveHolo:
         out = np.zeros(n.value, ITER_DTYPE)
         if n.value:
             _check(self._L.rihvr_get_iterations(self._h, _ptr(out), n.value, ctypes.byref(n)), "rihvr_get_iterations")
+        return out
+
+    def getSparsity(self) -> float:
+        v = ctypes.c_double()
+        _check(self._L.rihvr_sparsity(self._h, ctypes.byref(v)), "rihvr_sparsity")
+        return v.value
+
+    def initialEstimate(self) -> np.ndarray:
+        out = np.empty((self.height, self.width), np.float32)
+        _check(self._L.rihvr_initial_estimate(self._h, _ptr(out), 0), "rihvr_initial_estimate")
         return out
 
     def getPlane(self, z: int) -> np.ndarray:

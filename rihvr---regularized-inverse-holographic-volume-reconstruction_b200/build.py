@@ -28,8 +28,8 @@ CUDA_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr
 # nvcc and the host objects use the system g++.
 HOST_CXX = shutil.which("g++") or "g++"
 
-LIB_SOURCES = ["rihvr_kernels.cu", "rihvr_solver.cu", "rihvr_params.cpp", "rihvr_noalloc.cu"]
-CLI_SOURCES = ["sparse_inverse_recon.cpp", "rihvr_image.cpp"]
+LIB_SOURCES = ["rihvr_kernels.cu", "rihvr_solver.cu", "rihvr_params.cpp", "rihvr_noalloc.cu", "rihvr_image.cpp"]
+CLI_SOURCES = ["sparse_inverse_recon.cpp"]
 HEADERS = ["rihvr_device.cuh", "rihvr_kernels.cuh", "rihvr_image.h"]
 
 

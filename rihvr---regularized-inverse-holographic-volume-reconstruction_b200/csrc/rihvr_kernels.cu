@@ -1104,6 +1104,7 @@ __global__ void __launch_bounds__(FLAT_THREADS) k_momentum_norms(const ST* __res
     const int yy = (int)(e / W), xx = (int)(e - (size_t)yy * W);
     const float2 x = xval(P, Pp, beta, i);
     acc[SUM_L1X] += (double)sqrtf(cabs2(x));
+    acc[SUM_LIM1] += (x.x != 0.f || x.y != 0.f) ? 1.0 : 0.0;  // non-zero voxels
     if (mode == 7 || mode == 6) {
       const int xm = xx > 0 ? xx - 1 : W - 1, ym = yy > 0 ? yy - 1 : H - 1;
       const float2 xl = xval(P, Pp, beta, (size_t)z * HW + (size_t)yy * W + xm);

@@ -310,7 +310,7 @@ void settle_x_terms(rihvr_ctx* c, const double* s) {
   c->pending_x = -1;
 }
 
-int norms_at_x(rihvr_ctx* c, double* l1x, double* tvx) {
+int norms_at_x(rihvr_ctx* c, double* l1x, double* tvx, double* nnz = nullptr) {
   int nb = 0;
   KL(launch_momentum_norms(c->storage, c->vol[c->iCur], c->vol[c->iPrev], (float)c->beta, c->W, c->H, c->Nz,
                            c->mode, c->partials, &nb, c->st));
@@ -318,6 +318,7 @@ int norms_at_x(rihvr_ctx* c, double* l1x, double* tvx) {
   RC(fetch_sums(c));
   *l1x = c->sums_h[SLOT_NORM * kNumSums + SUM_L1X];
   *tvx = c->sums_h[SLOT_NORM * kNumSums + SUM_TVX];
+  if (nnz) *nnz = c->sums_h[SLOT_NORM * kNumSums + SUM_LIM1];
   return RIHVR_OK;
 }
 
@@ -612,6 +613,31 @@ int rihvr_objective(rihvr_ctx* c, double* f, double* terms3) {
     terms3[2] = c->mode == 5 ? 0.0 : tvx;
   }
   return RIHVR_OK;
+}
+
+int rihvr_sparsity(rihvr_ctx* c, double* fraction) {
+  if (!c || !fraction) return fail(RIHVR_ERR_INVALID_ARGUMENT, "NULL argument");
+  double l1x, tvx, nnz;
+  RC(norms_at_x(c, &l1x, &tvx, &nnz));
+  *fraction = nnz / (double)c->V;
+  return RIHVR_OK;
+}
+
+int rihvr_initial_estimate(rihvr_ctx* c, float* out, int is_device) {
+  if (!c || !out) return fail(RIHVR_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (!c->have_holo) return fail(RIHVR_ERR_MISSING_DATA, "no hologram set");
+  // gradient.reconstruct(measured) then backPropagateInitial: A (t A^H b), t = 1/Nz
+  CK(cudaMemcpyAsync(c->r, c->b, sizeof(float) * c->HW, cudaMemcpyDeviceToDevice, c->st));
+  RC(residual_spectrum(c));
+  RC(adjoint_volume(c));
+  RC(forward_volume(c, ELEM_C32, c->G));
+  std::vector<float> d(c->HW);
+  CK(cudaMemcpyAsync(d.data(), c->dnew, sizeof(float) * c->HW, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  const float t = (float)(1.0 / (double)c->p.num_planes);
+  for (float& v : d) v *= t;
+  CK(cudaMemcpy(out, d.data(), sizeof(float) * c->HW, is_device ? cudaMemcpyHostToDevice : cudaMemcpyHostToHost));
+  return state_reset(c);
 }
 
 int rihvr_get_iterations(const rihvr_ctx* c, rihvr_iter_record* out, int max_records, int* n_out) {
