@@ -178,9 +178,11 @@ def run_ours(args):
         pg = dist
     rihvr = importlib.import_module(PKG)
     synth = importlib.import_module(PKG + ".synth")
+    frames = importlib.import_module(PKG + ".frames")
     base = workload(args.config)
-    # independent frames: each rank reconstructs its own hologram
-    cfg = (synth.config2 if args.config == "c2" else synth.config1)(seed=base.seed + rank)
+    # independent frames of a series: each rank reconstructs its own hologram
+    (frame,) = frames.rank_frames(ws, ws, rank)
+    cfg = (synth.config2 if args.config == "c2" else synth.config1)(seed=frames.frame_seed(base.seed, frame))
     if args.nz:
         # smaller profiling case: same planes and physics, fewer of them
         cfg.num_planes = args.nz
@@ -210,12 +212,8 @@ def run_ours(args):
     ktimes = s.kernel_times()
     s.set_profiling(False)
     log = s.iterations()
-    max_ms = ms
-    if pg is not None:
-        t = torch.tensor([ms], device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        max_ms = float(t.item())
-    value = ws * V * args.steps / (max_ms / 1e3)
+    max_ms = frames.reduce_max(ms, device="cuda")
+    value = frames.weak_throughput(ws * V * args.steps, max_ms)
 
     # end to end through the C ABI: host hologram in, host estimate + objective out
     stream = torch.cuda.ExternalStream(s.stream())
@@ -235,11 +233,8 @@ def run_ours(args):
     e1.synchronize()
     e2e_ms = e0.elapsed_time(e1)
     barrier()
-    if pg is not None:
-        t = torch.tensor([e2e_ms], device="cuda")
-        pg.all_reduce(t, op=pg.ReduceOp.MAX)
-        e2e_ms = float(t.item())
-    e2e = {"value": ws * V * args.steps / (e2e_ms / 1e3), "unit": "voxel-iters/s",
+    e2e_ms = frames.reduce_max(e2e_ms, device="cuda")
+    e2e = {"value": frames.weak_throughput(ws * V * args.steps, e2e_ms), "unit": "voxel-iters/s",
            "h2d_bytes_per_step": int(b.nbytes) / args.steps, "d2h_bytes_per_step": (int(hout.numel() * 4) + 8) / args.steps,
            "ms": e2e_ms, "what": "set_hologram (H2D from pinned) + K iterations + estimate and objective (D2H)"}
 
