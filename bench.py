@@ -182,12 +182,13 @@ def run_ours(args):
     base = workload(args.config)
     # independent frames of a series: each rank reconstructs its own hologram
     (frame,) = frames.rank_frames(ws, ws, rank)
-    cfg = (synth.config2 if args.config == "c2" else synth.config1)(seed=frames.frame_seed(base.seed, frame))
+    cfg = base
     if args.nz:
         # smaller profiling case: same planes and physics, fewer of them
         cfg.num_planes = args.nz
         cfg.name = f"{cfg.name}_nz{args.nz}"
-    _, b = synth.make_hologram(cfg)
+    _, b0 = synth.make_hologram(cfg)
+    b = synth.translated_frame(b0, frame)
     storage = {"f32": 0, "bf16": 1, "f16": 2}[args.storage]
     p = rihvr.params_from_config(cfg, record_objective=0, storage=storage)
     s = rihvr.SparseCompressiveHolo(p, cfg.W, cfg.H)

@@ -192,6 +192,16 @@ def propagate_objects(cfg: HoloConfig, masks: dict) -> np.ndarray:
     return 1.0 + _ifft2(S)
 
 
+def translated_frame(b: np.ndarray, k: int) -> np.ndarray:
+    """Frame k of a series made by translating frame 0's particle field: the
+    hologram of a translated field is the circularly shifted hologram (the
+    transfer function is shift invariant and the planes are periodic)."""
+    if k == 0:
+        return b
+    H, W = b.shape
+    return np.roll(b, ((37 * k) % H, (53 * k) % W), axis=(0, 1)).copy()
+
+
 def camera_image(cfg: HoloConfig, field_: np.ndarray) -> np.ndarray:
     """uint8 camera frame of the unpadded hologram area."""
     rng = np.random.Generator(np.random.PCG64(cfg.seed + 7919))
