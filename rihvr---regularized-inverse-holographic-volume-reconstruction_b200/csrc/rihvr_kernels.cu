@@ -209,7 +209,41 @@ struct ColLayout {
   static constexpr int THREADS = CC * C::N1;
   static constexpr int SMEM_ELEMS = C::N2 * C::LD * CC;
   static constexpr size_t SMEM_BYTES = sizeof(float2) * SMEM_ELEMS;
+  // one plane's column strip (N rows x CC columns) of complex values
+  static constexpr size_t STRIP_ELEMS = (size_t)N * CC;
+  // staging strips in shared memory next to the exchange buffer: two for the
+  // forward pass (double-buffered prefetch), one complex + one FP64 strip for
+  // the adjoint (spectrum and phase table, constant over z)
+  static constexpr bool STAGE = (N % CC == 0) && (SMEM_BYTES + 2 * sizeof(float2) * STRIP_ELEMS <= 220 * 1024);
+  static constexpr size_t STAGE_BYTES = SMEM_BYTES + (STAGE ? 2 * sizeof(float2) * STRIP_ELEMS : 0);
 };
+
+// 16-byte asynchronous global -> shared copies (Ampere+ cp.async, L2 only)
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N_>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N_) : "memory");
+}
+
+// Copy the CC-column strip starting at column x0 of an N x N plane into a
+// dense [row][CC] shared buffer (16-byte pieces spread over the block).
+template <int N, typename T>
+__device__ __forceinline__ void strip_async(T* dst, const T* plane, int x0) {
+  using Lay = ColLayout<N>;
+  constexpr int CC = Lay::CC;
+  constexpr int PER_ROW = CC * (int)sizeof(T) / 16;  // 16-byte pieces per strip row
+  constexpr int PIECES = N * PER_ROW;
+  const char* src = reinterpret_cast<const char*>(plane + x0);
+  char* d = reinterpret_cast<char*>(dst);
+  for (int k = threadIdx.x; k < PIECES; k += Lay::THREADS) {
+    const int row = k / PER_ROW, piece = k - row * PER_ROW;
+    cp_async16(d + ((size_t)row * CC * sizeof(T) + piece * 16), src + ((size_t)row * N * sizeof(T) + piece * 16));
+  }
+}
 
 // Phase-table reads are issued in groups separated by a compiler scheduling
 // fence so that the FP64 table values of a whole line are not all live at once.
@@ -252,6 +286,8 @@ __device__ __forceinline__ void col_exchange(float2 (&v)[LineCfg<N>::N2], float2
 // Adjoint column pass: U_z(:, x) = IDFT_y( conj(H'_z(:, x)) * Rs(:, x) ), z in [zb, ze).
 // Square planes: the row pitch equals the line length N, so every element
 // offset below is a compile-time multiple of N.  Rs already carries 1/(W H).
+// The spectrum and phase-table strips are the same for every plane: they are
+// staged in shared memory once per block when they fit.
 template <int N>
 __global__ void __launch_bounds__(ColLayout<N>::THREADS) k_adj_col(const float2* __restrict__ Rs,
                                                                    const double* __restrict__ cturn,
@@ -262,29 +298,46 @@ __global__ void __launch_bounds__(ColLayout<N>::THREADS) k_adj_col(const float2*
   using Lay = ColLayout<N>;
   constexpr int N1 = C::N1, N2 = C::N2, M = C::M, CC = Lay::CC;
   constexpr int W = N;
-  extern __shared__ float2 sm[];
+  extern __shared__ __align__(16) float2 sm[];
   const int c = threadIdx.x % CC, t = threadIdx.x / CC;
   const int xr = blockIdx.x * CC + c;
   const bool col_ok = xr < W;
   const int x = col_ok ? xr : W - 1;
   const int zb = z0 + blockIdx.y * zpb, ze = min(zb + zpb, z1);
   constexpr size_t HW = (size_t)N * W;
+  float2* s_rs = sm + Lay::SMEM_ELEMS;
+  double* s_ct = reinterpret_cast<double*>(s_rs + Lay::STRIP_ELEMS);
+  if constexpr (Lay::STAGE) {
+    strip_async<N>(s_rs, Rs, blockIdx.x * CC);
+    strip_async<N>(s_ct, cturn, blockIdx.x * CC);
+    cp_async_commit();
+    cp_async_wait<0>();
+    __syncthreads();
+  }
   const float2* rs = Rs + (size_t)t * W + x;
   const double* ct = cturn + (size_t)t * W + x;
 #pragma unroll 1
   for (int z = zb; z < ze; ++z) {
     const double zz = zlist[z];
-    const float2* rsz = launder(rs);
-    const double* ctz = launder(ct);
     float2 v[N2];
+    if constexpr (Lay::STAGE) {
 #pragma unroll
-    for (int g = 0; g < N2; g += kPhaseGroup) {
-#pragma unroll
-      for (int q = 0; q < kPhaseGroup; ++q) {
-        const int n2 = g + q;
-        v[n2] = cmul(__ldg(rsz + (size_t)n2 * N1 * W), transfer(zz, __ldg(ctz + (size_t)n2 * N1 * W), true));
+      for (int n2 = 0; n2 < N2; ++n2) {
+        const int i = (t + N1 * n2) * CC + c;
+        v[n2] = cmul(s_rs[i], transfer(zz, s_ct[i], true));
       }
-      sched_fence();
+    } else {
+      const float2* rsz = launder(rs);
+      const double* ctz = launder(ct);
+#pragma unroll
+      for (int g = 0; g < N2; g += kPhaseGroup) {
+#pragma unroll
+        for (int q = 0; q < kPhaseGroup; ++q) {
+          const int n2 = g + q;
+          v[n2] = cmul(__ldg(rsz + (size_t)n2 * N1 * W), transfer(zz, __ldg(ctz + (size_t)n2 * N1 * W), true));
+        }
+        sched_fence();
+      }
     }
     reg_fft<N2, true>(v);
     line_twiddle<N, N2, true>(v, launder_i(t));
@@ -300,6 +353,8 @@ __global__ void __launch_bounds__(ColLayout<N>::THREADS) k_adj_col(const float2*
 }
 
 // Forward column pass with the z-sum: Spart[chunk](:, x) = sum_z H'_z(:, x) DFT_y(T_z(:, x)).
+// When two column strips fit in shared memory next to the exchange buffer,
+// plane z+1's strip is fetched asynchronously while plane z is transformed.
 template <int N>
 __global__ void __launch_bounds__(ColLayout<N>::THREADS) k_fwd_col(const float2* __restrict__ T,
                                                                    const double* __restrict__ cturn,
@@ -310,7 +365,7 @@ __global__ void __launch_bounds__(ColLayout<N>::THREADS) k_fwd_col(const float2*
   using Lay = ColLayout<N>;
   constexpr int N1 = C::N1, N2 = C::N2, M = C::M, CC = Lay::CC;
   constexpr int W = N;
-  extern __shared__ float2 sm[];
+  extern __shared__ __align__(16) float2 sm[];
   const int c = threadIdx.x % CC, t = threadIdx.x / CC;
   const int xr = blockIdx.x * CC + c;
   const bool col_ok = xr < W;
@@ -318,16 +373,34 @@ __global__ void __launch_bounds__(ColLayout<N>::THREADS) k_fwd_col(const float2*
   const int zb = z0 + blockIdx.y * zpb, ze = min(zb + zpb, z1);
   constexpr size_t HW = (size_t)N * W;
   const double* ct = cturn + (size_t)t * W + x;
+  float2* const stage0 = sm + Lay::SMEM_ELEMS;  // two strips: stage0 and stage0 + STRIP_ELEMS
+  if constexpr (Lay::STAGE) {
+    if (zb < ze) strip_async<N>(stage0, T + (size_t)zb * HW, blockIdx.x * CC);
+    cp_async_commit();
+  }
   float2 acc[N2];
 #pragma unroll
   for (int i = 0; i < N2; ++i) acc[i] = make_float2(0.f, 0.f);
 #pragma unroll 1
   for (int z = zb; z < ze; ++z) {
     const double zz = zlist[z];
-    const float2* Tz = T + (size_t)z * HW + (size_t)t * W + x;
     float2 v[N2];
+    if constexpr (Lay::STAGE) {
+      // the buffer refilled here was last read before the previous plane's
+      // exchange barrier, so every thread is done with it
+      if (z + 1 < ze)
+        strip_async<N>(stage0 + ((z + 1 - zb) & 1) * Lay::STRIP_ELEMS, T + (size_t)(z + 1) * HW, blockIdx.x * CC);
+      cp_async_commit();
+      cp_async_wait<1>();
+      __syncthreads();
+      const float2* sb = stage0 + ((z - zb) & 1) * Lay::STRIP_ELEMS;
 #pragma unroll
-    for (int n2 = 0; n2 < N2; ++n2) v[n2] = Tz[(size_t)n2 * N1 * W];
+      for (int n2 = 0; n2 < N2; ++n2) v[n2] = sb[(t + N1 * n2) * CC + c];
+    } else {
+      const float2* Tz = T + (size_t)z * HW + (size_t)t * W + x;
+#pragma unroll
+      for (int n2 = 0; n2 < N2; ++n2) v[n2] = Tz[(size_t)n2 * N1 * W];
+    }
     reg_fft<N2, false>(v);
     line_twiddle<N, N2, false>(v, launder_i(t));
     col_exchange<N, false>(v, sm, c, t);
@@ -343,6 +416,7 @@ __global__ void __launch_bounds__(ColLayout<N>::THREADS) k_fwd_col(const float2*
       sched_fence();
     }
   }
+  if constexpr (Lay::STAGE) cp_async_wait<0>();
   if (col_ok) {
     float2* Sp = Spart + (size_t)blockIdx.y * HW + (size_t)t * W + x;
 #pragma unroll
@@ -399,9 +473,9 @@ static cudaError_t adj_col_n(const float2* Rs, const double* cturn, const double
   if (chunks < 1) chunks = 1;
   const int zpb = (nz + chunks - 1) / chunks;
   chunks = (nz + zpb - 1) / zpb;
-  cudaError_t e = allow_smem(k_adj_col<N>, Lay::SMEM_BYTES);
+  cudaError_t e = allow_smem(k_adj_col<N>, Lay::STAGE_BYTES);
   if (e != cudaSuccess) return e;
-  k_adj_col<N><<<dim3(strips, chunks), Lay::THREADS, Lay::SMEM_BYTES, st>>>(Rs, cturn, zlist, U, z0, z1, zpb);
+  k_adj_col<N><<<dim3(strips, chunks), Lay::THREADS, Lay::STAGE_BYTES, st>>>(Rs, cturn, zlist, U, z0, z1, zpb);
   return cudaGetLastError();
 }
 
@@ -449,13 +523,13 @@ static cudaError_t fwd_col_n(const float2* T, const double* cturn, const double*
   const int strips = col_strips<N>(W);
   const int zpb = (nz + nchunks - 1) / nchunks;
   const int chunks = (nz + zpb - 1) / zpb;
-  cudaError_t e = allow_smem(k_fwd_col<N>, Lay::SMEM_BYTES);
+  cudaError_t e = allow_smem(k_fwd_col<N>, Lay::STAGE_BYTES);
   if (e != cudaSuccess) return e;
   if (chunks < nchunks) {  // unused chunk slots must read as zero
     e = cudaMemsetAsync(Spart + (size_t)chunks * N * W, 0, sizeof(float2) * (size_t)(nchunks - chunks) * N * W, st);
     if (e != cudaSuccess) return e;
   }
-  k_fwd_col<N><<<dim3(strips, chunks), Lay::THREADS, Lay::SMEM_BYTES, st>>>(T, cturn, zlist, Spart, z0, z1, zpb);
+  k_fwd_col<N><<<dim3(strips, chunks), Lay::THREADS, Lay::STAGE_BYTES, st>>>(T, cturn, zlist, Spart, z0, z1, zpb);
   return cudaGetLastError();
 }
 
