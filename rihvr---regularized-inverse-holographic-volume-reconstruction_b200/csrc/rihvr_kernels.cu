@@ -10,6 +10,10 @@
 // passes carry the transfer-function multiply (regenerated from an FP64 table of
 // c/(2 pi) per frequency, phase reduced mod 1 turn in FP64) and, for the forward
 // operator, the sum over z, so the Nz transformed planes never go back to memory.
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+
 #include "rihvr_device.cuh"
 #include "rihvr_kernels.cuh"
 
@@ -64,7 +68,8 @@ static int num_sms() {
 
 template <typename K>
 static cudaError_t allow_smem(K kernel, size_t bytes) {
-  if (bytes <= 48 * 1024) return cudaSuccess;
+  // dynamic plus static shared memory above 48 KB needs the opt-in
+  if (bytes + 4096 <= 48 * 1024) return cudaSuccess;
   return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
@@ -695,6 +700,14 @@ __device__ __forceinline__ float2 tv_estimate(float2 xh, float2 gx, float2 gxr, 
   return f2fma(nmu, f2add(f2sub(gxr, gx), f2sub(gyd, gy)), xh);
 }
 
+// hardware reciprocal square root (PTX rsqrt.approx.f32), one instruction
+// wherever it is inlined
+__device__ __forceinline__ float rsqrt_approx(float x) {
+  float r;
+  asm("rsqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(x));
+  return r;
+}
+
 // g = P(g + s grad y) for one pixel: px = gx + s (yl - y), py = gy + s (yu - y),
 // divided by max(1, |(px, py)|) over the four real components.
 __device__ __forceinline__ void tv_dual(float2& gx, float2& gy, float2 y, float2 yl, float2 yu, float2 s2) {
@@ -702,7 +715,7 @@ __device__ __forceinline__ void tv_dual(float2& gx, float2& gy, float2 y, float2
   const float2 py = f2fma(s2, f2sub(yu, y), gy);
   const float2 q = f2fma(py, py, f2mul(px, px));
   const float n2 = q.x + q.y;
-  const float sc = (n2 > 1.f) ? rsqrtf(n2) : 1.f;
+  const float sc = (n2 > 1.f) ? rsqrt_approx(n2) : 1.f;
   const float2 sc2 = make_float2(sc, sc);
   gx = f2mul(px, sc2);
   gy = f2mul(py, sc2);
@@ -956,6 +969,411 @@ __global__ void __launch_bounds__(TV_THREADS, 2) k_prox_tv2d(ProxArgs a) {
   block_write_sums<TV_THREADS>(dacc, a.partials, blk);
 }
 
+template <typename ST>
+struct Raw2;  // two adjacent complex values as loaded from storage
+template <>
+struct Raw2<float2> {
+  using T = float4;
+  static __device__ __forceinline__ T ld(const float2* p) { return *reinterpret_cast<const float4*>(p); }
+  static __device__ __forceinline__ void cvt(T v, float2& a, float2& b) {
+    a = make_float2(v.x, v.y);
+    b = make_float2(v.z, v.w);
+  }
+  static __device__ __forceinline__ void st(float2* p, float2 a, float2 b) {
+    *reinterpret_cast<float4*>(p) = make_float4(a.x, a.y, b.x, b.y);
+  }
+};
+template <>
+struct Raw2<__nv_bfloat162> {
+  using T = uint2;
+  static __device__ __forceinline__ T ld(const __nv_bfloat162* p) { return *reinterpret_cast<const uint2*>(p); }
+  static __device__ __forceinline__ void cvt(T v, float2& a, float2& b) {
+    a = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&v.x));
+    b = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&v.y));
+  }
+  static __device__ __forceinline__ void st(__nv_bfloat162* p, float2 a, float2 b) {
+    const __nv_bfloat162 u = __float22bfloat162_rn(a), v = __float22bfloat162_rn(b);
+    *reinterpret_cast<uint2*>(p) =
+        make_uint2(*reinterpret_cast<const unsigned*>(&u), *reinterpret_cast<const unsigned*>(&v));
+  }
+};
+template <>
+struct Raw2<__half2> {
+  using T = uint2;
+  static __device__ __forceinline__ T ld(const __half2* p) { return *reinterpret_cast<const uint2*>(p); }
+  static __device__ __forceinline__ void cvt(T v, float2& a, float2& b) {
+    a = __half22float2(*reinterpret_cast<const __half2*>(&v.x));
+    b = __half22float2(*reinterpret_cast<const __half2*>(&v.y));
+  }
+  static __device__ __forceinline__ void st(__half2* p, float2 a, float2 b) {
+    const __half2 u = __float22half2_rn(a), v = __float22half2_rn(b);
+    *reinterpret_cast<uint2*>(p) =
+        make_uint2(*reinterpret_cast<const unsigned*>(&u), *reinterpret_cast<const unsigned*>(&v));
+  }
+};
+
+struct TvsGrid {
+  int nstrips, nseg, seg_len;
+};
+
+// ---------------------------------------------------------------------------
+// Streaming form of the same prox (1 <= n_tv <= 6), the default.  The tiled
+// kernel above recomputes a halo of n_tv + 1 rows and columns around every
+// 64 x 64 tile, so a third of its work is thrown away, and it needs a block
+// barrier per TV iteration.  Here a lane owns CPL adjacent columns and a warp a
+// strip of 32 CPL columns with an x halo of HX (n_tv + 1 rounded up to a
+// multiple of CPL) on each side; the warp walks a run of rows with the n_tv
+// Chambolle iterations pipelined one row apart: at the step that loads row j,
+// iteration k updates row j - k from iteration k-1's rows j-k (kept from the
+// previous step) and j-k+1 (produced this step), and the final estimate and
+// shrink produce row j - n_tv - 1.  A run starts 2 (n_tv + 1) rows early
+// (periodic wrap) so that its first output row is exact, which removes the y
+// halo.  Warps are independent and exchange x neighbours by shuffles only.
+//
+// Per lane, the state is one row of (gx, gy) and one row of y per iteration in
+// registers.  Rows arrive one step ahead by cp.async into a per-lane ring of D
+// rows in shared memory holding (raw Pprev, overwritten by xh), G and raw P;
+// each lane reads back only what it copied, so no barrier is involved.
+// Iteration 1 starts from g = 0, where the estimate is xh itself.  The
+// arithmetic is the tiled kernel's operation for operation, so P_new has the
+// same bits; the sums differ only in summation order.
+//
+// The step loop is unrolled by two.  With an odd number of steps that build
+// gave last rows of a run 1 ulp away from the tiled kernel, so runs of odd
+// length start one row earlier and every run has an even number of steps.
+// ---------------------------------------------------------------------------
+template <int NTV, int CPL>
+struct TvwShape {
+  static constexpr int h = NTV + 1;
+  static constexpr int AL = CPL < 2 ? 2 : CPL;
+  static constexpr int HX = (h + AL - 1) / AL * AL;   // keeps each lane's columns aligned
+  static constexpr int SW = 32 * CPL;                 // strip width
+  static constexpr int VW = SW - 2 * HX;              // valid columns per strip
+  static constexpr int D = (h + 2 <= 8) ? 8 : 16;     // rows in use: h + 1, plus one landing
+  static constexpr int F4 = CPL / 2;                  // float4 per array per lane row (FP32)
+  static constexpr int SLOT = 3 * F4 * 32;            // float4 per ring slot, whole warp
+  static constexpr int NW = 4;                        // warps per block
+  static constexpr size_t SMEM = sizeof(float4) * (size_t)SLOT * D * NW;
+  static constexpr int MINB = (3 * (SMEM + 1024) <= 228 * 1024) ? 3 : 2;  // blocks per SM
+  static_assert(CPL == 2 || CPL == 4, "columns per lane");
+  static_assert(VW > 0, "halo wider than the strip");
+};
+
+// copy CPL complex values in storage type (16-byte aligned source for
+// CPL * sizeof(ST) >= 16, else 8-byte aligned) to shared memory
+template <typename ST, int CPL>
+__device__ __forceinline__ void cp_async_run(float4* smem, const ST* gmem) {
+  constexpr int BYTES = CPL * (int)sizeof(ST);
+  if constexpr (BYTES >= 16) {
+#pragma unroll
+    for (int k = 0; k < BYTES / 16; ++k) {
+      const unsigned d = (unsigned)__cvta_generic_to_shared(smem + k * 32);
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d),
+                   "l"(reinterpret_cast<const char*>(gmem) + 16 * k)
+                   : "memory");
+    }
+  } else {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(gmem) : "memory");
+  }
+}
+
+// CPL complex values of storage type ST from their ring copy (16-byte pieces
+// 32 float4 apart)
+template <typename ST, int CPL>
+__device__ __forceinline__ void ring_vals(const float4* e, float2 (&v)[CPL]) {
+  if constexpr (sizeof(ST) == 8) {
+#pragma unroll
+    for (int k = 0; k < CPL / 2; ++k) {
+      const float4 f = e[k * 32];
+      v[2 * k] = make_float2(f.x, f.y);
+      v[2 * k + 1] = make_float2(f.z, f.w);
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < (CPL + 3) / 4; ++k) {
+      const float4 f = e[k * 32];
+      const unsigned u[4] = {__float_as_uint(f.x), __float_as_uint(f.y), __float_as_uint(f.z), __float_as_uint(f.w)};
+#pragma unroll
+      for (int j = 0; j < 4 && 4 * k + j < CPL; ++j) {
+        float2 a, b;
+        Raw2<ST>::cvt(make_uint2(u[j], 0u), a, b);
+        v[4 * k + j] = a;
+      }
+    }
+  }
+}
+
+template <typename ST, int CPL>
+__device__ __forceinline__ void store_run(ST* p, const float2 (&v)[CPL]) {
+#pragma unroll
+  for (int c = 0; c < CPL; c += 2) Raw2<ST>::st(p + c, v[c], v[c + 1]);
+}
+
+template <typename ST, int NTV, int CPL = 2, int NW = TvwShape<NTV, CPL>::NW, int MINB = TvwShape<NTV, CPL>::MINB,
+          int UNR = 2, int EVEN = 1>
+__global__ void __launch_bounds__(32 * NW, MINB) k_prox_tv2d_strip(ProxArgs a, TvsGrid gr) {
+  using Sh = TvwShape<NTV, CPL>;
+  constexpr int h = Sh::h, HX = Sh::HX, VW = Sh::VW, D = Sh::D, RM = D - 1, F4 = Sh::F4;
+  constexpr int QS = F4 * 32;     // float4 between the arrays of a slot
+  constexpr int SL = 3 * QS;      // float4 per slot
+  extern __shared__ float4 tvw_ring[];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  float4* ring = tvw_ring + (size_t)w * SL * D + lane;
+  const int W = a.W, H = a.H;
+  const long long work = (long long)blockIdx.x * NW + w;
+  const long long nwork = (long long)gr.nstrips * gr.nseg * a.Nz;
+
+  double dacc[kNumSums];
+#pragma unroll
+  for (int k = 0; k < kNumSums; ++k) dacc[k] = 0.0;
+
+  if (work < nwork) {
+    const int strip = (int)(work % gr.nstrips);
+    const long long rest = work / gr.nstrips;
+    const int seg = (int)(rest % gr.nseg);
+    const size_t plane = (size_t)(rest / gr.nseg) * W * H;
+    const ST* P = static_cast<const ST*>(a.P) + plane;
+    const ST* Pp = static_cast<const ST*>(a.Pprev) + plane;
+    const float2* G = a.G + plane;
+    ST* Pn = static_cast<ST*>(a.Pnew) + plane;
+    const float t = a.t, beta = a.beta;
+    const float2 nmu = make_float2(-a.mu, -a.mu), s2 = make_float2(a.s, a.s);
+    const float2 bb = make_float2(beta, beta), nt2 = make_float2(-t, -t), t2 = make_float2(t, t);
+    const float2 z2 = make_float2(0.f, 0.f);
+    const float thr = a.thr;
+    const int faithful = a.faithful, want_norms = a.want_norms;
+
+    const int cu = strip * VW - HX + CPL * lane;   // first column of this lane, unwrapped
+    const int gc = ((cu % W) + W) % W;             // a multiple of CPL; W is one too
+    const bool lane_ok = (CPL * lane >= HX) && (CPL * lane < HX + VW) && (cu < W);
+    const int r0 = seg * gr.seg_len;
+    const int r1 = min(H, r0 + gr.seg_len);
+    // with EVEN, runs of odd length start one row earlier
+    const int pad = EVEN ? ((r1 - r0) & 1) : 0;
+    const int nsteps = (r1 - r0) + 2 * h + pad;
+    int lrow = r0 - h - pad;
+    if (lrow < 0) lrow += H;
+    int orow = r0 - 2 * h - pad;
+    if (orow < 0) orow += H;
+
+    // Ring slots are read as rows above r0 - h before any copy lands there;
+    // those rows only feed rows above r0, which are not written.
+    auto request = [&](int slot) {
+      const size_t off = (size_t)lrow * W + gc;
+      float4* e = ring + slot * SL;
+      cp_async_run<ST, CPL>(e, Pp + off);
+      cp_async_run<float2, CPL>(e + QS, G + off);
+      cp_async_run<ST, CPL>(e + 2 * QS, P + off);
+      cp_async_commit();
+      lrow = (lrow + 1 == H) ? 0 : lrow + 1;
+    };
+    request(0);
+
+    float2 gX[NTV][CPL], gY[NTV][CPL], yU[NTV][CPL];
+#pragma unroll
+    for (int k = 0; k < NTV; ++k)
+#pragma unroll
+      for (int c = 0; c < CPL; ++c) gX[k][c] = gY[k][c] = yU[k][c] = z2;
+    float2 pu[CPL], xu[CPL];
+#pragma unroll
+    for (int c = 0; c < CPL; ++c) pu[c] = xu[c] = z2;
+    float acc[kNumSums];
+#pragma unroll
+    for (int k = 0; k < kNumSums; ++k) acc[k] = 0.f;
+
+#pragma unroll UNR
+    for (int i = 0; i < nsteps; ++i) {
+      cp_async_wait<0>();
+      // stage 0: xh = P + beta (P - Pprev) - t G replaces Pprev in the slot
+      {
+        float4* e = ring + (i & RM) * SL;
+        float2 p[CPL], q[CPL], g[CPL];
+        ring_vals<ST, CPL>(e + 2 * QS, p);
+        ring_vals<ST, CPL>(e, q);
+        ring_vals<float2, CPL>(e + QS, g);
+#pragma unroll
+        for (int k = 0; k < F4; ++k) {
+          const float2 xa = f2fma(nt2, g[2 * k], f2fma(bb, f2sub(p[2 * k], q[2 * k]), p[2 * k]));
+          const float2 xb = f2fma(nt2, g[2 * k + 1], f2fma(bb, f2sub(p[2 * k + 1], q[2 * k + 1]), p[2 * k + 1]));
+          e[k * 32] = make_float4(xa.x, xa.y, xb.x, xb.y);
+        }
+      }
+      if (i + 1 < nsteps) request((i + 1) & RM);
+
+      float2 ny[CPL];   // gy of the iteration before, on the row below
+      // iteration 1 on row j-1: g^0 = 0, so the estimate is xh itself
+      {
+        float2 y[CPL], yl[CPL];
+        ring_vals<float2, CPL>(ring + ((i - 1) & RM) * SL, y);
+        yl[0] = shfl_up2(y[CPL - 1]);
+#pragma unroll
+        for (int c = 1; c < CPL; ++c) yl[c] = y[c - 1];
+#pragma unroll
+        for (int c = 0; c < CPL; ++c) {
+          float2 gx = z2, gy = z2;
+          tv_dual(gx, gy, y[c], yl[c], yU[0][c], s2);
+          yU[0][c] = y[c];
+          ny[c] = gy;
+          // the new row replaces the one above it, which moves to (y, yl)
+          const float2 ogx = gX[0][c], ogy = gY[0][c];
+          gX[0][c] = gx;
+          gY[0][c] = gy;
+          y[c] = ogx;
+          yl[c] = ogy;
+        }
+        // from here (y, yl) carry the previous iteration's (gx, gy) on the
+        // row the next stage works on
+#pragma unroll
+        for (int L = 1; L <= NTV; ++L) {
+          // stage L+1 (iteration L+1, or the final stage when L == NTV) on row j-1-L
+          const float4* e = ring + ((i - 1 - L) & RM) * SL;
+          float2 xh[CPL];
+          ring_vals<float2, CPL>(e, xh);
+          float2 gxr[CPL], yy[CPL];
+#pragma unroll
+          for (int c = 0; c < CPL - 1; ++c) gxr[c] = y[c + 1];
+          gxr[CPL - 1] = shfl_down2(y[0]);
+#pragma unroll
+          for (int c = 0; c < CPL; ++c) yy[c] = tv_estimate(xh[c], y[c], gxr[c], yl[c], ny[c], nmu);
+          if (L < NTV) {
+            float2 yls[CPL];
+            yls[0] = shfl_up2(yy[CPL - 1]);
+#pragma unroll
+            for (int c = 1; c < CPL; ++c) yls[c] = yy[c - 1];
+#pragma unroll
+            for (int c = 0; c < CPL; ++c) {
+              float2 gx = y[c], gy = yl[c];
+              tv_dual(gx, gy, yy[c], yls[c], yU[L][c], s2);
+              yU[L][c] = yy[c];
+              ny[c] = gy;
+              const float2 ogx = gX[L][c], ogy = gY[L][c];
+              gX[L][c] = gx;
+              gY[L][c] = gy;
+              y[c] = ogx;
+              yl[c] = ogy;
+            }
+          } else {
+            // final stage: p = shrink(estimate) on row j - h, then the sums
+            float2 p[CPL], x[CPL], g[CPL], y0[CPL];
+            ring_vals<float2, CPL>(e + QS, g);
+            ring_vals<ST, CPL>(e + 2 * QS, y0);
+#pragma unroll
+            for (int c = 0; c < CPL; ++c) {
+              p[c] = shrink(yy[c], thr, faithful);
+              x[c] = f2fma(t2, g[c], xh[c]);
+            }
+            if (i >= 2 * h + pad) {  // row orow is exact
+              float2 pl0 = shfl_up2(p[CPL - 1]), xl0 = shfl_up2(x[CPL - 1]);
+              if (lane_ok) {
+                const size_t eo = (size_t)orow * W + gc;
+                store_run<ST, CPL>(Pn + eo, p);
+                float wr, wi;
+                restart_w(eo, faithful, &wr, &wi);
+#pragma unroll
+                for (int c = 0; c < CPL; ++c) {
+                  const float2 d = f2sub(p[c], x[c]);
+                  const float2 dg = f2mul(d, g[c]);
+                  acc[SUM_LIM1] += dg.x + dg.y;
+                  acc[SUM_LIM2] += cabs2(d);
+                  const float2 uv = f2mul(f2sub(x[c], p[c]), f2sub(p[c], y0[c]));
+                  acc[SUM_RS] += fmaf(wr, uv.x, wi * uv.y);
+                  if (want_norms) {
+                    const float2 pl = c ? p[c - 1] : pl0, xl = c ? x[c - 1] : xl0;
+                    acc[SUM_L1P] += sqrtf(cabs2(p[c]));
+                    acc[SUM_TVP] += sqrtf(cabs2(f2sub(pl, p[c])) + cabs2(f2sub(pu[c], p[c])));
+                    acc[SUM_L1X] += sqrtf(cabs2(x[c]));
+                    acc[SUM_TVX] += sqrtf(cabs2(f2sub(xl, x[c])) + cabs2(f2sub(xu[c], x[c])));
+                  }
+                }
+              }
+              if (((i - 2 * h - pad) & 7) == 7) {  // FP32 partials over at most 8 rows
+#pragma unroll
+                for (int k = 0; k < kNumSums; ++k) {
+                  dacc[k] += (double)acc[k];
+                  acc[k] = 0.f;
+                }
+              }
+            }
+#pragma unroll
+            for (int c = 0; c < CPL; ++c) {
+              pu[c] = p[c];
+              xu[c] = x[c];
+            }
+          }
+        }
+      }
+      orow = (orow + 1 == H) ? 0 : orow + 1;
+    }
+    cp_async_wait<0>();
+#pragma unroll
+    for (int k = 0; k < kNumSums; ++k) dacc[k] += (double)acc[k];
+  }
+  block_write_sums<32 * NW>(dacc, a.partials, blockIdx.x);
+}
+
+// Runs per plane: enough warps for several full waves, while keeping the
+// warm-up rows of each run small against the run length.
+static TvsGrid tvs_grid(int W, int H, int Nz, int VW, int warps_per_sm, int warm) {
+  TvsGrid g;
+  g.nstrips = (W + VW - 1) / VW;
+  const double slots = (double)num_sms() * warps_per_sm;  // resident warps
+  double best = 1e300;
+  g.nseg = 1;
+  for (int ns = 1; ns <= 64 && ns <= H; ++ns) {
+    const int len = (H + ns - 1) / ns;
+    if (ns > 1 && len < 2 * warm) break;
+    const double runs = (double)g.nstrips * ns * Nz;
+    const double waves = std::ceil(runs / slots);
+    const double cost = waves * (len + warm);  // steps on the critical path
+    if (cost < best * 0.999) {
+      best = cost;
+      g.nseg = ns;
+    }
+  }
+  g.seg_len = (H + g.nseg - 1) / g.nseg;
+  g.nseg = (H + g.seg_len - 1) / g.seg_len;
+  return g;
+}
+
+template <typename ST, int NTV>
+static cudaError_t strip_launch(const ProxArgs& a, int* nblocks_out, cudaStream_t st) {
+  using Sh = TvwShape<NTV, 2>;
+  const TvsGrid g = tvs_grid(a.W, a.H, a.Nz, Sh::VW, Sh::NW * Sh::MINB, 2 * Sh::h + 1);
+  const long long runs = (long long)g.nstrips * g.nseg * a.Nz;
+  const long long blocks = (runs + Sh::NW - 1) / Sh::NW;
+  if (blocks > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
+  *nblocks_out = (int)blocks;
+  cudaError_t e = allow_smem(k_prox_tv2d_strip<ST, NTV>, Sh::SMEM);
+  if (e != cudaSuccess) return e;
+  k_prox_tv2d_strip<ST, NTV><<<(unsigned)blocks, 32 * Sh::NW, Sh::SMEM, st>>>(a, g);
+  return cudaGetLastError();
+}
+
+template <typename ST>
+static cudaError_t strip_dispatch(const ProxArgs& a, int* nb, cudaStream_t st) {
+  switch (a.n_tv) {
+    case 1: return strip_launch<ST, 1>(a, nb, st);
+    case 2: return strip_launch<ST, 2>(a, nb, st);
+    case 3: return strip_launch<ST, 3>(a, nb, st);
+    case 4: return strip_launch<ST, 4>(a, nb, st);
+    case 5: return strip_launch<ST, 5>(a, nb, st);
+    case 6: return strip_launch<ST, 6>(a, nb, st);
+    default: return cudaErrorInvalidValue;
+  }
+}
+constexpr int kStripNtvMax = 6;
+
+// RIHVR_TV_KERNEL=tiles forces the tiled kernel (comparison and fallback);
+// read once per process.
+static bool tv_stream_enabled() {
+  static const bool on = [] {
+    const char* v = std::getenv("RIHVR_TV_KERNEL");
+    return !(v && std::strcmp(v, "tiles") == 0);
+  }();
+  return on;
+}
+
 static void tv_grid(const ProxArgs& a, dim3* g) {
   const int h = a.n_tv + 1;
   const int VW = TV_EW - 2 * h, VH = TV_EH - 2 * h;
@@ -972,6 +1390,13 @@ size_t max_partial_blocks(int W, int H, int Nz) {
 
 cudaError_t launch_prox_tv2d(int storage, const ProxArgs& a, int* nblocks_out, cudaStream_t st) {
   if (a.n_tv < 0 || a.n_tv > 20) return cudaErrorInvalidValue;
+  if (a.n_tv >= 1 && a.n_tv <= kStripNtvMax && tv_stream_enabled()) {
+    switch (storage) {
+      case STORE_BF16: return strip_dispatch<__nv_bfloat162>(a, nblocks_out, st);
+      case STORE_F16: return strip_dispatch<__half2>(a, nblocks_out, st);
+      default: return strip_dispatch<float2>(a, nblocks_out, st);
+    }
+  }
   dim3 g;
   tv_grid(a, &g);
   *nblocks_out = (int)(g.x * g.y * g.z);

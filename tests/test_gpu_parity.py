@@ -105,6 +105,69 @@ def test_prox_step_matches_oracle(rihvr, mode, faithful):
     assert abs(sums[1] - rsums[1]) < 1e-4 * abs(rsums[1])
 
 
+@pytest.mark.parametrize("side,nz,n_tv", [(32, 3, 5), (128, 3, 1), (128, 2, 2), (384, 2, 3), (256, 2, 6),
+                                         (128, 2, 7), (64, 3, 0)])
+def test_tv_prox_iteration_counts(rihvr, side, nz, n_tv):
+    """Streaming TV prox (1..6 Chambolle iterations) and the tiled one (other
+    counts) against the oracle, on planes with several strips and runs."""
+    p = make(rihvr, side, nz, mode=7, faithful=1, num_tv_iterations=n_tv)
+    rng = np.random.default_rng(side * 10 + n_tv)
+    x = rand_volume(rng, nz, side, 0.05)
+    r = rng.standard_normal((side, side)).astype(np.float32)
+    t = 0.3
+    with rihvr.SparseCompressiveHolo(p, side, side) as s:
+        out, sums = s.prox_step(x, r, t)
+    ref, rsums = O.prox_from(oparams(rihvr, p, side), x.astype(np.complex128), x.astype(np.complex128),
+                             r.astype(np.float64), t)
+    assert rel(out, ref) < TOL_F32
+    assert abs(sums[1] - rsums[1]) < 1e-4 * abs(rsums[1])
+
+
+_TILES_SCRIPT = """
+import sys, numpy as np
+sys.path.insert(0, sys.argv[1])
+import importlib
+R = importlib.import_module(sys.argv[2])
+side, nz, ntv, st = (int(v) for v in sys.argv[3:7])
+p = R.default_params()
+p.start_plane, p.plane_stepsize, p.num_planes = 100.0, 40.0, nz
+p.wavelength, p.resolution, p.zero_padding = 0.632, 2.0, 0
+p.regularization_param, p.regularization_TV_param, p.num_tv_iterations = 0.01, 0.02, ntv
+p.storage = st
+rng = np.random.default_rng(11)
+x = (0.05 * (rng.standard_normal((nz, side, side)) + 1j * rng.standard_normal((nz, side, side)))).astype(np.complex64)
+r = rng.standard_normal((side, side)).astype(np.float32)
+with R.SparseCompressiveHolo(p, side, side) as s:
+    out, sums = s.prox_step(x, r, 0.3)
+np.save(sys.argv[7], out)
+"""
+
+
+@pytest.mark.parametrize("side,nz,ntv,storage", [(1024, 3, 5, 0), (384, 4, 3, 0), (768, 2, 6, 1), (256, 3, 4, 2)])
+def test_streaming_prox_bits_equal_tiled(rihvr, tmp_path, side, nz, ntv, storage):
+    """The streaming TV prox reproduces the tiled kernel's P_new bit for bit
+    (run lengths odd and even, every storage type)."""
+    import subprocess
+    import sys
+
+    from conftest import PKG_NAME, ROOT
+
+    script = tmp_path / "prox.py"
+    script.write_text(_TILES_SCRIPT)
+    outs = {}
+    for kern in ("tiles", "strip"):
+        env = dict(os.environ)
+        env.pop("RIHVR_TV_KERNEL", None)
+        if kern == "tiles":
+            env["RIHVR_TV_KERNEL"] = "tiles"
+        f = tmp_path / f"{kern}.npy"
+        r = subprocess.run([sys.executable, str(script), ROOT, PKG_NAME, str(side), str(nz), str(ntv), str(storage),
+                            str(f)], env=env, capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0, r.stderr[-2000:]
+        outs[kern] = np.load(f)
+    assert np.array_equal(outs["tiles"].view(np.uint32), outs["strip"].view(np.uint32))
+
+
 def run_gpu(rihvr, p, side, b, n):
     with rihvr.SparseCompressiveHolo(p, side, side) as s:
         s.setHologram(b)
