@@ -120,6 +120,19 @@ def class_bytes(s: int) -> dict:
     }
 
 
+# DRAM bytes per voxel that ncu measured for one launch of a kernel class
+# (dram__bytes_read.sum + dram__bytes_write.sum of a 1024 x 1024 x 16-plane
+# capture of `bench.py --nz 16`, divided by its voxels), keyed by (class,
+# stored bytes per voxel).  Scaled by the voxels of a launch, since traffic
+# grows with the planes processed.
+MEASURED_TRAFFIC_PER_VOXEL = {
+    ("prox", 8): (454.7e6 + 116.2e6) / (1024 * 1024 * 16),
+    ("fwd_col", 8): (143.7e6 + 18.5e6) / (1024 * 1024 * 16),
+    ("fwd_row", 8): (134.3e6 + 86.4e6) / (1024 * 1024 * 16),
+    ("adj_row", 8): (134.3e6 + 86.7e6) / (1024 * 1024 * 16),
+}
+
+
 def cpu_sample(cfg, b, steps: int, warmup: int):
     """Time the FP64 oracle on a bounded sample of the workload: the first 16
     planes of the volume, full plane size, one FISTA iteration per step."""
@@ -248,8 +261,10 @@ def run_ours(args):
     avg_ms = tot_ms / nl
     bytes_per_launch = cb[dom] * V
     achieved = bytes_per_launch / (avg_ms / 1e3) / 1e9
+    tpv = MEASURED_TRAFFIC_PER_VOXEL.get((dom, sbytes))
+    traffic = tpv * V if tpv is not None else None
     roofline = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "traffic": None, "peak_source": peak_kind,
+                "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
                 "bytes_per_launch": bytes_per_launch, "avg_launch_ms": avg_ms}
     iter_bytes = (32 + 4 * sbytes) * V  # per voxel-iteration, minimal two-pass data flow
     kernels = {k: {"ms_total": v[0], "launches": v[1]} for k, v in ktimes.items()}
