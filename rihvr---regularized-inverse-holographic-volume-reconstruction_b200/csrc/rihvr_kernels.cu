@@ -358,8 +358,10 @@ __global__ void __launch_bounds__(ColLayout<N>::THREADS) k_adj_col(const float2*
 }
 
 // Forward column pass with the z-sum: Spart[chunk](:, x) = sum_z H'_z(:, x) DFT_y(T_z(:, x)).
-// When two column strips fit in shared memory next to the exchange buffer,
-// plane z+1's strip is fetched asynchronously while plane z is transformed.
+// When they fit next to the exchange buffer, the block's strip of the phase
+// table (constant over z) and one strip of T are staged in shared memory:
+// plane z+1's strip is fetched asynchronously once the exchange of plane z has
+// consumed the buffer, and overlaps the transfer-function multiply and sum.
 template <int N>
 __global__ void __launch_bounds__(ColLayout<N>::THREADS) k_fwd_col(const float2* __restrict__ T,
                                                                    const double* __restrict__ cturn,
@@ -378,9 +380,11 @@ __global__ void __launch_bounds__(ColLayout<N>::THREADS) k_fwd_col(const float2*
   const int zb = z0 + blockIdx.y * zpb, ze = min(zb + zpb, z1);
   constexpr size_t HW = (size_t)N * W;
   const double* ct = cturn + (size_t)t * W + x;
-  float2* const stage0 = sm + Lay::SMEM_ELEMS;  // two strips: stage0 and stage0 + STRIP_ELEMS
+  float2* const s_t = sm + Lay::SMEM_ELEMS;                                  // one strip of T
+  const double* const s_ct = reinterpret_cast<const double*>(s_t + Lay::STRIP_ELEMS);  // phase-table strip
   if constexpr (Lay::STAGE) {
-    if (zb < ze) strip_async<N>(stage0, T + (size_t)zb * HW, blockIdx.x * CC);
+    strip_async<N>(const_cast<double*>(s_ct), cturn, blockIdx.x * CC);
+    if (zb < ze) strip_async<N>(s_t, T + (size_t)zb * HW, blockIdx.x * CC);
     cp_async_commit();
   }
   float2 acc[N2];
@@ -391,16 +395,10 @@ __global__ void __launch_bounds__(ColLayout<N>::THREADS) k_fwd_col(const float2*
     const double zz = zlist[z];
     float2 v[N2];
     if constexpr (Lay::STAGE) {
-      // the buffer refilled here was last read before the previous plane's
-      // exchange barrier, so every thread is done with it
-      if (z + 1 < ze)
-        strip_async<N>(stage0 + ((z + 1 - zb) & 1) * Lay::STRIP_ELEMS, T + (size_t)(z + 1) * HW, blockIdx.x * CC);
-      cp_async_commit();
-      cp_async_wait<1>();
+      cp_async_wait<0>();
       __syncthreads();
-      const float2* sb = stage0 + ((z - zb) & 1) * Lay::STRIP_ELEMS;
 #pragma unroll
-      for (int n2 = 0; n2 < N2; ++n2) v[n2] = sb[(t + N1 * n2) * CC + c];
+      for (int n2 = 0; n2 < N2; ++n2) v[n2] = s_t[(t + N1 * n2) * CC + c];
     } else {
       const float2* Tz = T + (size_t)z * HW + (size_t)t * W + x;
 #pragma unroll
@@ -408,17 +406,31 @@ __global__ void __launch_bounds__(ColLayout<N>::THREADS) k_fwd_col(const float2*
     }
     reg_fft<N2, false>(v);
     line_twiddle<N, N2, false>(v, launder_i(t));
+    // the exchange's first barrier also orders every thread's reads of s_t
+    // before the refill below
     col_exchange<N, false>(v, sm, c, t);
-    const double* ctz = launder(ct);
+    if constexpr (Lay::STAGE) {
+      if (z + 1 < ze) strip_async<N>(s_t, T + (size_t)(z + 1) * HW, blockIdx.x * CC);
+      cp_async_commit();
 #pragma unroll
-    for (int g = 0; g < N2; g += kPhaseGroup) {
+      for (int j = 0; j < M; ++j)
 #pragma unroll
-      for (int q = 0; q < kPhaseGroup; ++q) {
-        const int j = (g + q) / N1, k1 = (g + q) % N1;
-        const float2 h = transfer(zz, __ldg(ctz + (size_t)(N1 * j + N2 * k1) * W), false);
-        acc[j * N1 + k1] = cadd(acc[j * N1 + k1], cmul(v[j * N1 + k1], h));
+        for (int k1 = 0; k1 < N1; ++k1) {
+          const float2 h = transfer(zz, s_ct[(N1 * j + N2 * k1 + t) * CC + c], false);
+          acc[j * N1 + k1] = cadd(acc[j * N1 + k1], cmul(v[j * N1 + k1], h));
+        }
+    } else {
+      const double* ctz = launder(ct);
+#pragma unroll
+      for (int g = 0; g < N2; g += kPhaseGroup) {
+#pragma unroll
+        for (int q = 0; q < kPhaseGroup; ++q) {
+          const int j = (g + q) / N1, k1 = (g + q) % N1;
+          const float2 h = transfer(zz, __ldg(ctz + (size_t)(N1 * j + N2 * k1) * W), false);
+          acc[j * N1 + k1] = cadd(acc[j * N1 + k1], cmul(v[j * N1 + k1], h));
+        }
+        sched_fence();
       }
-      sched_fence();
     }
   }
   if constexpr (Lay::STAGE) cp_async_wait<0>();
