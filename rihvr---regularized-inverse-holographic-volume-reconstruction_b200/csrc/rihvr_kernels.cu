@@ -668,6 +668,15 @@ __device__ __forceinline__ float2 shrink(float2 v, float T, int faithful) {
 
 __device__ __forceinline__ float cabs2(float2 a) { return a.x * a.x + a.y * a.y; }
 
+// Square roots of the objective's norm terms (L1 and TV sums) use the
+// hardware approximation (PTX sqrt.approx.f32, one instruction): they only
+// feed the reported objective, summed over millions of voxels in FP64.
+__device__ __forceinline__ float norm_sqrt(float q) {
+  float r;
+  asm("sqrt.approx.f32 %0, %1;" : "=f"(r) : "f"(q));
+  return r;
+}
+
 // ---------------------------------------------------------------------------
 // Fused 2-D TV prox (mode 7): proximalFusedLasso2d, sparse_compressive_holo.cu:
 // 3652-3732 with kernels :3478-3597.  Per plane tile, with the momentum point
@@ -964,10 +973,10 @@ __global__ void __launch_bounds__(TV_THREADS, 2) k_prox_tv2d(ProxArgs a) {
         const float2 uv = f2mul(f2sub(x[c], p), f2sub(p, y0[c]));
         acc[SUM_RS] += fmaf(wr, uv.x, wi * uv.y);
         if (a.want_norms) {
-          acc[SUM_L1P] += sqrtf(cabs2(p));
-          acc[SUM_TVP] += sqrtf(cabs2(f2sub(pl[c], p)) + cabs2(f2sub(pu[c], p)));
-          acc[SUM_L1X] += sqrtf(cabs2(x[c]));
-          acc[SUM_TVX] += sqrtf(cabs2(f2sub(xl[c], x[c])) + cabs2(f2sub(xu[c], x[c])));
+          acc[SUM_L1P] += norm_sqrt(cabs2(p));
+          acc[SUM_TVP] += norm_sqrt(cabs2(f2sub(pl[c], p)) + cabs2(f2sub(pu[c], p)));
+          acc[SUM_L1X] += norm_sqrt(cabs2(x[c]));
+          acc[SUM_TVX] += norm_sqrt(cabs2(f2sub(xl[c], x[c])) + cabs2(f2sub(xu[c], x[c])));
         }
       }
       pu[c] = p;
@@ -1066,7 +1075,8 @@ struct TvwShape {
   static constexpr int SLOT = 3 * F4 * 32;            // float4 per ring slot, whole warp
   static constexpr int NW = 4;                        // warps per block
   static constexpr size_t SMEM = sizeof(float4) * (size_t)SLOT * D * NW;
-  static constexpr int MINB = (3 * (SMEM + 1024) <= 228 * 1024) ? 3 : 2;  // blocks per SM
+  // blocks per SM; a fourth block (128 registers) spills and runs far slower
+  static constexpr int MINB = (3 * (SMEM + 1024) <= 228 * 1024) ? 3 : 2;
   static_assert(CPL == 2 || CPL == 4, "columns per lane");
   static_assert(VW > 0, "halo wider than the strip");
 };
@@ -1122,8 +1132,8 @@ __device__ __forceinline__ void store_run(ST* p, const float2 (&v)[CPL]) {
   for (int c = 0; c < CPL; c += 2) Raw2<ST>::st(p + c, v[c], v[c + 1]);
 }
 
-template <typename ST, int NTV, int CPL = 2, int NW = TvwShape<NTV, CPL>::NW, int MINB = TvwShape<NTV, CPL>::MINB,
-          int UNR = 2, int EVEN = 1>
+template <typename ST, int NTV, bool NORMS, int CPL = 2, int NW = TvwShape<NTV, CPL>::NW,
+          int MINB = TvwShape<NTV, CPL>::MINB, int UNR = 2, int EVEN = 1>
 __global__ void __launch_bounds__(32 * NW, MINB) k_prox_tv2d_strip(ProxArgs a, TvsGrid gr) {
   using Sh = TvwShape<NTV, CPL>;
   constexpr int h = Sh::h, HX = Sh::HX, VW = Sh::VW, D = Sh::D, RM = D - 1, F4 = Sh::F4;
@@ -1154,7 +1164,8 @@ __global__ void __launch_bounds__(32 * NW, MINB) k_prox_tv2d_strip(ProxArgs a, T
     const float2 bb = make_float2(beta, beta), nt2 = make_float2(-t, -t), t2 = make_float2(t, t);
     const float2 z2 = make_float2(0.f, 0.f);
     const float thr = a.thr;
-    const int faithful = a.faithful, want_norms = a.want_norms;
+    const int faithful = a.faithful;
+    constexpr int NS = NORMS ? kNumSums : SUM_RS + 1;  // sums this kernel accumulates
 
     const int cu = strip * VW - HX + CPL * lane;   // first column of this lane, unwrapped
     const int gc = ((cu % W) + W) % W;             // a multiple of CPL; W is one too
@@ -1276,7 +1287,11 @@ __global__ void __launch_bounds__(32 * NW, MINB) k_prox_tv2d_strip(ProxArgs a, T
               x[c] = f2fma(t2, g[c], xh[c]);
             }
             if (i >= 2 * h + pad) {  // row orow is exact
-              float2 pl0 = shfl_up2(p[CPL - 1]), xl0 = shfl_up2(x[CPL - 1]);
+              float2 pl0 = z2, xl0 = z2;
+              if (NORMS) {
+                pl0 = shfl_up2(p[CPL - 1]);
+                xl0 = shfl_up2(x[CPL - 1]);
+              }
               if (lane_ok) {
                 const size_t eo = (size_t)orow * W + gc;
                 store_run<ST, CPL>(Pn + eo, p);
@@ -1290,27 +1305,29 @@ __global__ void __launch_bounds__(32 * NW, MINB) k_prox_tv2d_strip(ProxArgs a, T
                   acc[SUM_LIM2] += cabs2(d);
                   const float2 uv = f2mul(f2sub(x[c], p[c]), f2sub(p[c], y0[c]));
                   acc[SUM_RS] += fmaf(wr, uv.x, wi * uv.y);
-                  if (want_norms) {
+                  if (NORMS) {
                     const float2 pl = c ? p[c - 1] : pl0, xl = c ? x[c - 1] : xl0;
-                    acc[SUM_L1P] += sqrtf(cabs2(p[c]));
-                    acc[SUM_TVP] += sqrtf(cabs2(f2sub(pl, p[c])) + cabs2(f2sub(pu[c], p[c])));
-                    acc[SUM_L1X] += sqrtf(cabs2(x[c]));
-                    acc[SUM_TVX] += sqrtf(cabs2(f2sub(xl, x[c])) + cabs2(f2sub(xu[c], x[c])));
+                    acc[SUM_L1P] += norm_sqrt(cabs2(p[c]));
+                    acc[SUM_TVP] += norm_sqrt(cabs2(f2sub(pl, p[c])) + cabs2(f2sub(pu[c], p[c])));
+                    acc[SUM_L1X] += norm_sqrt(cabs2(x[c]));
+                    acc[SUM_TVX] += norm_sqrt(cabs2(f2sub(xl, x[c])) + cabs2(f2sub(xu[c], x[c])));
                   }
                 }
               }
               if (((i - 2 * h - pad) & 7) == 7) {  // FP32 partials over at most 8 rows
 #pragma unroll
-                for (int k = 0; k < kNumSums; ++k) {
+                for (int k = 0; k < NS; ++k) {
                   dacc[k] += (double)acc[k];
                   acc[k] = 0.f;
                 }
               }
             }
+            if (NORMS) {
 #pragma unroll
-            for (int c = 0; c < CPL; ++c) {
-              pu[c] = p[c];
-              xu[c] = x[c];
+              for (int c = 0; c < CPL; ++c) {
+                pu[c] = p[c];
+                xu[c] = x[c];
+              }
             }
           }
         }
@@ -1319,7 +1336,7 @@ __global__ void __launch_bounds__(32 * NW, MINB) k_prox_tv2d_strip(ProxArgs a, T
     }
     cp_async_wait<0>();
 #pragma unroll
-    for (int k = 0; k < kNumSums; ++k) dacc[k] += (double)acc[k];
+    for (int k = 0; k < NS; ++k) dacc[k] += (double)acc[k];
   }
   block_write_sums<32 * NW>(dacc, a.partials, blockIdx.x);
 }
@@ -1348,18 +1365,24 @@ static TvsGrid tvs_grid(int W, int H, int Nz, int VW, int warps_per_sm, int warm
   return g;
 }
 
-template <typename ST, int NTV>
-static cudaError_t strip_launch(const ProxArgs& a, int* nblocks_out, cudaStream_t st) {
+template <typename ST, int NTV, bool NORMS>
+static cudaError_t strip_launch_n(const ProxArgs& a, int* nblocks_out, cudaStream_t st) {
   using Sh = TvwShape<NTV, 2>;
   const TvsGrid g = tvs_grid(a.W, a.H, a.Nz, Sh::VW, Sh::NW * Sh::MINB, 2 * Sh::h + 1);
   const long long runs = (long long)g.nstrips * g.nseg * a.Nz;
   const long long blocks = (runs + Sh::NW - 1) / Sh::NW;
   if (blocks > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
   *nblocks_out = (int)blocks;
-  cudaError_t e = allow_smem(k_prox_tv2d_strip<ST, NTV>, Sh::SMEM);
+  cudaError_t e = allow_smem(k_prox_tv2d_strip<ST, NTV, NORMS>, Sh::SMEM);
   if (e != cudaSuccess) return e;
-  k_prox_tv2d_strip<ST, NTV><<<(unsigned)blocks, 32 * Sh::NW, Sh::SMEM, st>>>(a, g);
+  k_prox_tv2d_strip<ST, NTV, NORMS><<<(unsigned)blocks, 32 * Sh::NW, Sh::SMEM, st>>>(a, g);
   return cudaGetLastError();
+}
+
+template <typename ST, int NTV>
+static cudaError_t strip_launch(const ProxArgs& a, int* nblocks_out, cudaStream_t st) {
+  return a.want_norms ? strip_launch_n<ST, NTV, true>(a, nblocks_out, st)
+                      : strip_launch_n<ST, NTV, false>(a, nblocks_out, st);
 }
 
 template <typename ST>
@@ -1461,8 +1484,8 @@ __global__ void __launch_bounds__(FLAT_THREADS) k_prox_l1(ProxArgs a) {
     const float2 u = csub(x, p), v = csub(p, y0);
     acc[SUM_RS] += (double)(wr * u.x * v.x) + (double)(wi * u.y * v.y);
     if (a.want_norms) {
-      acc[SUM_L1P] += (double)sqrtf(cabs2(p));
-      acc[SUM_L1X] += (double)sqrtf(cabs2(x));
+      acc[SUM_L1P] += (double)norm_sqrt(cabs2(p));
+      acc[SUM_L1X] += (double)norm_sqrt(cabs2(x));
     }
   }
   block_write_sums<FLAT_THREADS>(acc, a.partials, blockIdx.x);
@@ -1614,7 +1637,7 @@ __global__ void __launch_bounds__(FLAT_THREADS) k_momentum_norms(const ST* __res
     const size_t e = i - (size_t)z * HW;
     const int yy = (int)(e / W), xx = (int)(e - (size_t)yy * W);
     const float2 x = xval(P, Pp, beta, i);
-    acc[SUM_L1X] += (double)sqrtf(cabs2(x));
+    acc[SUM_L1X] += (double)norm_sqrt(cabs2(x));
     acc[SUM_LIM1] += (x.x != 0.f || x.y != 0.f) ? 1.0 : 0.0;  // non-zero voxels
     if (mode == 7 || mode == 6) {
       const int xm = xx > 0 ? xx - 1 : W - 1, ym = yy > 0 ? yy - 1 : H - 1;
@@ -1625,7 +1648,7 @@ __global__ void __launch_bounds__(FLAT_THREADS) k_momentum_norms(const ST* __res
         const int zm = z > 0 ? z - 1 : Nz - 1;
         q += cabs2(csub(xval(P, Pp, beta, (size_t)zm * HW + e), x));
       }
-      acc[SUM_TVX] += (double)sqrtf(q);
+      acc[SUM_TVX] += (double)norm_sqrt(q);
     }
   }
   block_write_sums<FLAT_THREADS>(acc, partials, blockIdx.x);
@@ -1808,11 +1831,11 @@ __global__ void __launch_bounds__(FLAT_THREADS) k_prox6_finish(ProxArgs a, const
                    ib = (size_t)zm * HW + e;
       const float2 pl = shrink(Y[il], T, a.faithful), pu = shrink(Y[iu], T, a.faithful),
                    pb = shrink(Y[ib], T, a.faithful);
-      acc[SUM_L1P] += (double)sqrtf(cabs2(p));
-      acc[SUM_TVP] += (double)sqrtf(cabs2(csub(pl, p)) + cabs2(csub(pu, p)) + cabs2(csub(pb, p)));
+      acc[SUM_L1P] += (double)norm_sqrt(cabs2(p));
+      acc[SUM_TVP] += (double)norm_sqrt(cabs2(csub(pl, p)) + cabs2(csub(pu, p)) + cabs2(csub(pb, p)));
       const float2 xl = xval(P, Pp, a.beta, il), xu = xval(P, Pp, a.beta, iu), xb = xval(P, Pp, a.beta, ib);
-      acc[SUM_L1X] += (double)sqrtf(cabs2(x));
-      acc[SUM_TVX] += (double)sqrtf(cabs2(csub(xl, x)) + cabs2(csub(xu, x)) + cabs2(csub(xb, x)));
+      acc[SUM_L1X] += (double)norm_sqrt(cabs2(x));
+      acc[SUM_TVX] += (double)norm_sqrt(cabs2(csub(xl, x)) + cabs2(csub(xu, x)) + cabs2(csub(xb, x)));
     }
   }
   block_write_sums<FLAT_THREADS>(acc, a.partials, blockIdx.x);

@@ -201,6 +201,25 @@ def test_solve_matches_oracle(rihvr, synthmod, cache_dir, mode, faithful, t0):
     assert rel(est, oest) < TOL_F32
 
 
+def test_objective_recording_does_not_change_the_solve(rihvr, synthmod, cache_dir):
+    """record_objective = 0 runs the prox without the norm terms (another
+    kernel instantiation); the iterates must not change."""
+    side, nz, n = 128, 5, 12
+    cfg = synthmod.small_config(W=side, H=side, Nz=nz, seed=6)
+    _, b = synthmod.make_hologram(cfg, cache_dir=cache_dir)
+    out = {}
+    for rec in (1, 0):
+        p = rihvr.params_from_config(cfg, record_objective=rec)
+        with rihvr.SparseCompressiveHolo(p, side, side) as s:
+            s.setHologram(b)
+            s.iterate(n)
+            out[rec] = (s.getVolume(), s.iterations(), s.calcObjectiveFunction()[0])
+    assert np.array_equal(out[0][0], out[1][0])
+    assert np.array_equal(out[0][1]["backtracks"], out[1][1]["backtracks"])
+    assert np.array_equal(out[0][1]["restarted"], out[1][1]["restarted"])
+    assert out[0][2] == out[1][2]
+
+
 @pytest.mark.parametrize("storage", [1, 2])
 def test_reduced_precision_storage(rihvr, synthmod, cache_dir, storage):
     side, nz, n = 64, 6, 20
