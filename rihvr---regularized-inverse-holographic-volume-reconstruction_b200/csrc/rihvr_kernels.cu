@@ -10,6 +10,8 @@
 // passes carry the transfer-function multiply (regenerated from an FP64 table of
 // c/(2 pi) per frequency, phase reduced mod 1 turn in FP64) and, for the forward
 // operator, the sum over z, so the Nz transformed planes never go back to memory.
+#include <cuda.h>  // CUtensorMap and its enums; the encoder is resolved at run time
+
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -141,7 +143,7 @@ __global__ void __launch_bounds__(kRowThreads) k_rows(int in_kind, const void* _
   using Lay = RowLayout<N>;
   constexpr int N1 = C::N1, N2 = C::N2, M = C::M, LD = C::LD;
   static_assert(32 % N1 == 0, "a line must not straddle warps");
-  extern __shared__ float2 sm[];
+  extern __shared__ __align__(128) float2 sm[];
   const int li = threadIdx.x / N1, t = threadIdx.x % N1;
   long long L = (long long)blockIdx.x * Lay::LPB + li;
   const bool active = L < nlines;
@@ -270,6 +272,34 @@ __device__ __forceinline__ int launder_i(int v) {
   return v;
 }
 
+// Tensor-memory-accelerator (TMA) store of a dense shared-memory tile
+// [rows][CC] of 8-byte elements to a 3-D (x, row, plane) tensor.  Stores only,
+// no multicast.  The coordinates are non-negative and x * 8 bytes is a
+// multiple of 16.
+__device__ __forceinline__ void tma_store_3d(const CUtensorMap* map, const void* smem, int x, int y, int z) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.bulk.tensor.3d.global.shared::cta.bulk_group [%0, {%2, %3, %4}], [%1];" ::"l"(
+                   reinterpret_cast<unsigned long long>(map)),
+               "r"(s), "r"(x), "r"(y), "r"(z)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+// the source tiles of every committed store have been read
+__device__ __forceinline__ void bulk_wait_read_all() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+// every committed store has completed
+__device__ __forceinline__ void bulk_wait_all() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+// order this thread's shared-memory writes before later async-proxy reads
+__device__ __forceinline__ void fence_smem_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
+
+// rows per TMA box: the largest divisor of N not above 256 (the box limit)
+template <int N>
+constexpr int tma_rows() {
+  int r = 1;
+  for (int d = 1; d <= 256 && d <= N; ++d)
+    if (N % d == 0) r = d;
+  return r;
+}
+
 // Exchange + stage B shared by all column kernels.  On entry v holds the
 // twiddled stage-A output of this thread; on exit the stage-B output.
 template <int N, bool INV>
@@ -293,17 +323,17 @@ __device__ __forceinline__ void col_exchange(float2 (&v)[LineCfg<N>::N2], float2
 // offset below is a compile-time multiple of N.  Rs already carries 1/(W H).
 // The spectrum and phase-table strips are the same for every plane: they are
 // staged in shared memory once per block when they fit.
-template <int N>
+template <int N, bool TMA>
 __global__ void __launch_bounds__(ColLayout<N>::THREADS) k_adj_col(const float2* __restrict__ Rs,
                                                                    const double* __restrict__ cturn,
                                                                    const double* __restrict__ zlist,
                                                                    float2* __restrict__ U, int z0, int z1,
-                                                                   int zpb) {
+                                                                   int zpb, const __grid_constant__ CUtensorMap umap) {
   using C = LineCfg<N>;
   using Lay = ColLayout<N>;
   constexpr int N1 = C::N1, N2 = C::N2, M = C::M, CC = Lay::CC;
   constexpr int W = N;
-  extern __shared__ __align__(16) float2 sm[];
+  extern __shared__ __align__(128) float2 sm[];  // TMA sources need 128-byte alignment
   const int c = threadIdx.x % CC, t = threadIdx.x / CC;
   const int xr = blockIdx.x * CC + c;
   const bool col_ok = xr < W;
@@ -321,9 +351,11 @@ __global__ void __launch_bounds__(ColLayout<N>::THREADS) k_adj_col(const float2*
   }
   const float2* rs = Rs + (size_t)t * W + x;
   const double* ct = cturn + (size_t)t * W + x;
+  double znext = zb < ze ? zlist[zb] : 0.0;
 #pragma unroll 1
   for (int z = zb; z < ze; ++z) {
-    const double zz = zlist[z];
+    const double zz = znext;
+    if (z + 1 < ze) znext = zlist[z + 1];  // in flight during this plane
     float2 v[N2];
     if constexpr (Lay::STAGE) {
 #pragma unroll
@@ -346,8 +378,27 @@ __global__ void __launch_bounds__(ColLayout<N>::THREADS) k_adj_col(const float2*
     }
     reg_fft<N2, true>(v);
     line_twiddle<N, N2, true>(v, launder_i(t));
+    // the exchange buffer also holds the previous plane's output tile: its
+    // store must have read it (the exchange starts with a barrier)
+    if (TMA && threadIdx.x == 0) bulk_wait_read_all();
     col_exchange<N, true>(v, sm, c, t);
-    if (col_ok) {
+    if constexpr (TMA) {
+      // plane z's [N][CC] column strip goes out through the TMA from the
+      // exchange buffer, as a few bulk stores instead of N2 8-byte stores a thread
+      __syncthreads();  // every thread is done reading the exchange
+#pragma unroll
+      for (int j = 0; j < M; ++j)
+#pragma unroll
+        for (int k1 = 0; k1 < N1; ++k1) sm[(N1 * j + N2 * k1 + t) * CC + c] = v[j * N1 + k1];
+      fence_smem_async();
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        constexpr int R = tma_rows<N>();
+#pragma unroll 1
+        for (int b = 0; b < N; b += R) tma_store_3d(&umap, sm + b * CC, blockIdx.x * CC, b, z);
+        bulk_commit();
+      }
+    } else if (col_ok) {
       float2* Uz = U + (size_t)z * HW + (size_t)t * W + x;
 #pragma unroll
       for (int j = 0; j < M; ++j)
@@ -355,6 +406,7 @@ __global__ void __launch_bounds__(ColLayout<N>::THREADS) k_adj_col(const float2*
         for (int k1 = 0; k1 < N1; ++k1) Uz[(size_t)(N1 * j + N2 * k1) * W] = v[j * N1 + k1];
     }
   }
+  if (TMA && threadIdx.x == 0) bulk_wait_all();
 }
 
 // Forward column pass with the z-sum: Spart[chunk](:, x) = sum_z H'_z(:, x) DFT_y(T_z(:, x)).
@@ -372,7 +424,7 @@ __global__ void __launch_bounds__(ColLayout<N>::THREADS) k_fwd_col(const float2*
   using Lay = ColLayout<N>;
   constexpr int N1 = C::N1, N2 = C::N2, M = C::M, CC = Lay::CC;
   constexpr int W = N;
-  extern __shared__ __align__(16) float2 sm[];
+  extern __shared__ __align__(128) float2 sm[];
   const int c = threadIdx.x % CC, t = threadIdx.x / CC;
   const int xr = blockIdx.x * CC + c;
   const bool col_ok = xr < W;
@@ -390,9 +442,11 @@ __global__ void __launch_bounds__(ColLayout<N>::THREADS) k_fwd_col(const float2*
   float2 acc[N2];
 #pragma unroll
   for (int i = 0; i < N2; ++i) acc[i] = make_float2(0.f, 0.f);
+  double znext = zb < ze ? zlist[zb] : 0.0;
 #pragma unroll 1
   for (int z = zb; z < ze; ++z) {
-    const double zz = zlist[z];
+    const double zz = znext;
+    if (z + 1 < ze) znext = zlist[z + 1];  // in flight during this plane
     float2 v[N2];
     if constexpr (Lay::STAGE) {
       cp_async_wait<0>();
@@ -451,7 +505,7 @@ __global__ void __launch_bounds__(ColLayout<N>::THREADS) k_plane_col(const float
   using Lay = ColLayout<N>;
   constexpr int N1 = C::N1, N2 = C::N2, M = C::M, CC = Lay::CC;
   constexpr int W = N;
-  extern __shared__ float2 sm[];
+  extern __shared__ __align__(128) float2 sm[];
   const int c = threadIdx.x % CC, t = threadIdx.x / CC;
   const int xr = blockIdx.x * CC + c;
   const bool col_ok = xr < W;
@@ -477,6 +531,37 @@ static int col_strips(int W) {
   return (W + ColLayout<N>::CC - 1) / ColLayout<N>::CC;
 }
 
+// cuTensorMapEncodeTiled, resolved once through the runtime (no link-time
+// dependence on the driver library); null when unavailable
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+static EncodeTiledFn encode_tiled() {
+  static const EncodeTiledFn fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      p = nullptr;
+    return reinterpret_cast<EncodeTiledFn>(p);
+  }();
+  return fn;
+}
+
+// 3-D map (column, row, plane) of nz square N x N planes of 8-byte elements
+// with a box of CC columns x rows rows x 1 plane
+static bool plane_stack_map(CUtensorMap* m, void* base, int n, int nz, int cc, int rows) {
+  const EncodeTiledFn enc = encode_tiled();
+  if (!enc || (reinterpret_cast<uintptr_t>(base) & 15) != 0) return false;
+  const cuuint64_t dims[3] = {(cuuint64_t)n, (cuuint64_t)n, (cuuint64_t)nz};
+  const cuuint64_t strides[2] = {(cuuint64_t)n * 8, (cuuint64_t)n * n * 8};
+  const cuuint32_t box[3] = {(cuuint32_t)cc, (cuuint32_t)rows, 1};
+  const cuuint32_t estr[3] = {1, 1, 1};
+  return enc(m, CU_TENSOR_MAP_DATA_TYPE_INT64, 3, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+             CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) ==
+         CUDA_SUCCESS;
+}
+
 template <int N>
 static cudaError_t adj_col_n(const float2* Rs, const double* cturn, const double* zlist, float2* U, int W,
                              int z0, int z1, cudaStream_t st) {
@@ -490,9 +575,21 @@ static cudaError_t adj_col_n(const float2* Rs, const double* cturn, const double
   if (chunks < 1) chunks = 1;
   const int zpb = (nz + chunks - 1) / chunks;
   chunks = (nz + zpb - 1) / zpb;
-  cudaError_t e = allow_smem(k_adj_col<N>, Lay::STAGE_BYTES);
-  if (e != cudaSuccess) return e;
-  k_adj_col<N><<<dim3(strips, chunks), Lay::THREADS, Lay::STAGE_BYTES, st>>>(Rs, cturn, zlist, U, z0, z1, zpb);
+  CUtensorMap umap;
+  std::memset(&umap, 0, sizeof(umap));
+  const bool tma = (W == N) && (N % Lay::CC == 0) && plane_stack_map(&umap, U, N, z1, Lay::CC, tma_rows<N>());
+  cudaError_t e;
+  if (tma) {
+    e = allow_smem(k_adj_col<N, true>, Lay::STAGE_BYTES);
+    if (e != cudaSuccess) return e;
+    k_adj_col<N, true><<<dim3(strips, chunks), Lay::THREADS, Lay::STAGE_BYTES, st>>>(Rs, cturn, zlist, U, z0, z1,
+                                                                                        zpb, umap);
+  } else {
+    e = allow_smem(k_adj_col<N, false>, Lay::STAGE_BYTES);
+    if (e != cudaSuccess) return e;
+    k_adj_col<N, false><<<dim3(strips, chunks), Lay::THREADS, Lay::STAGE_BYTES, st>>>(Rs, cturn, zlist, U, z0, z1,
+                                                                                         zpb, umap);
+  }
   return cudaGetLastError();
 }
 
