@@ -145,6 +145,19 @@ int rihvr_set_hologram(rihvr_ctx* ctx, const float* b, int is_device);
  * the objective at the final momentum point. */
 int rihvr_reconstruct(rihvr_ctx* ctx, double* final_objective);
 
+/* Several frames at once: the replacement for the reference's frame loop,
+ * which runs sparse-inverse-recon once per hologram
+ * (src/QTGUI/rihvr.cpp:2414-2905, reconstructioncompute.cpp:117-142).  Frame i
+ * does rihvr_set_hologram(ctxs[i], holograms[i], is_device) and
+ * rihvr_reconstruct(ctxs[i], &final_objectives[i]).  Every context runs on its
+ * own host thread and CUDA stream, so the frames' kernels and host decisions
+ * overlap on the GPU; results are those of the sequential calls, bit for bit.
+ * The contexts must be distinct and may differ in size and parameters.
+ * final_objectives and statuses (n entries each) may be NULL; statuses[i]
+ * receives frame i's status.  Returns the first nonzero status in frame order. */
+int rihvr_reconstruct_batch(rihvr_ctx* const* ctxs, int n, const float* const* holograms, int is_device,
+                            double* final_objectives, int* statuses);
+
 /* Restart from x = 0 without changing the hologram. */
 int rihvr_reset(rihvr_ctx* ctx);
 

@@ -92,7 +92,8 @@ class FileParams(ctypes.Structure):
 # every symbol include/rihvr.h declares
 EXPORTED = (
     "rihvr_params_default", "rihvr_read_param_file", "rihvr_plane_list", "rihvr_create", "rihvr_destroy",
-    "rihvr_set_hologram", "rihvr_reconstruct", "rihvr_reset", "rihvr_iterate", "rihvr_iterate_timed",
+    "rihvr_set_hologram", "rihvr_reconstruct", "rihvr_reconstruct_batch", "rihvr_reset", "rihvr_iterate",
+    "rihvr_iterate_timed",
     "rihvr_iteration_count", "rihvr_objective", "rihvr_get_iterations", "rihvr_get_plane", "rihvr_get_volume",
     "rihvr_get_estimate", "rihvr_get_residual", "rihvr_forward", "rihvr_adjoint", "rihvr_prox_step",
     "rihvr_adjoint_noalloc", "rihvr_sparsity", "rihvr_initial_estimate",
@@ -135,6 +136,7 @@ def load_library(path: str = LIB_PATH):
     L.rihvr_destroy.restype = None
     L.rihvr_set_hologram.argtypes = [vp, vp, ip]
     L.rihvr_reconstruct.argtypes = [vp, P(ctypes.c_double)]
+    L.rihvr_reconstruct_batch.argtypes = [P(vp), ip, P(vp), ip, P(ctypes.c_double), P(ctypes.c_int)]
     L.rihvr_reset.argtypes = [vp]
     L.rihvr_iterate.argtypes = [vp, ip]
     L.rihvr_iterate_timed.argtypes = [vp, ip, fp]
@@ -206,6 +208,27 @@ def adjoint_noalloc(params: RihvrParams, width: int, height: int, residual_dev: 
     _check(load_library().rihvr_adjoint_noalloc(ctypes.byref(params), int(width), int(height),
                                                  ctypes.c_void_p(residual_dev), ctypes.c_void_p(volume_dev),
                                                  ctypes.c_void_p(stream)), "rihvr_adjoint_noalloc")
+
+
+def reconstruct_batch(solvers, holograms):
+    """Run several frames at once (rihvr_reconstruct_batch): frame i sets
+    solvers[i]'s hologram to holograms[i] and reconstructs from x = 0.  Returns
+    the final objectives; raises RihvrError with the first failing frame."""
+    n = len(solvers)
+    if n != len(holograms):
+        raise ValueError("one hologram per solver")
+    bufs = []
+    for s, b in zip(solvers, holograms):
+        b = np.ascontiguousarray(b, dtype=np.float32)
+        if b.shape != (s.height, s.width):
+            raise ValueError(f"hologram shape {b.shape} != {(s.height, s.width)}")
+        bufs.append(b)
+    ctxs = (ctypes.c_void_p * n)(*[s._h for s in solvers])
+    ptrs = (ctypes.c_void_p * n)(*[b.ctypes.data for b in bufs])
+    f = (ctypes.c_double * n)()
+    st = (ctypes.c_int * n)()
+    _check(load_library().rihvr_reconstruct_batch(ctxs, n, ptrs, 0, f, st), "rihvr_reconstruct_batch")
+    return [f[i] for i in range(n)]
 
 
 def _io_check(rc: int, where: str):

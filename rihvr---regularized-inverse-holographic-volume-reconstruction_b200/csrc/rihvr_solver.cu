@@ -17,6 +17,7 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/rihvr.h"
@@ -596,6 +597,42 @@ int rihvr_reconstruct(rihvr_ctx* c, double* final_objective) {
   RC(run_iterations(c, c->p.num_inverse_iterations));
   if (final_objective) RC(rihvr_objective(c, final_objective, nullptr));
   return RIHVR_OK;
+}
+
+int rihvr_reconstruct_batch(rihvr_ctx* const* ctxs, int n, const float* const* holograms, int is_device,
+                            double* final_objectives, int* statuses) {
+  if (!ctxs || !holograms || n <= 0) return fail(RIHVR_ERR_INVALID_ARGUMENT, "empty or NULL batch");
+  for (int i = 0; i < n; ++i) {
+    if (!ctxs[i] || !holograms[i]) return fail(RIHVR_ERR_INVALID_ARGUMENT, "NULL context or hologram in batch");
+    for (int j = 0; j < i; ++j)
+      if (ctxs[j] == ctxs[i]) return fail(RIHVR_ERR_INVALID_ARGUMENT, "a context appears twice in the batch");
+  }
+  std::vector<int> st(n, RIHVR_OK);
+  std::vector<std::string> msg(n);
+  auto frame = [&](int i) {
+    rihvr_ctx* c = ctxs[i];
+    int rc = cudaSetDevice(c->device) == cudaSuccess ? RIHVR_OK : RIHVR_ERR_CUDA;
+    if (rc == RIHVR_OK) rc = rihvr_set_hologram(c, holograms[i], is_device);
+    double f = 0.0;
+    if (rc == RIHVR_OK) rc = rihvr_reconstruct(c, &f);
+    if (final_objectives) final_objectives[i] = rc == RIHVR_OK ? f : 0.0;
+    st[i] = rc;
+    if (rc != RIHVR_OK) msg[i] = g_last_error;  // thread-local: carried back to the caller's thread
+  };
+  std::vector<std::thread> workers;
+  workers.reserve(n > 0 ? n - 1 : 0);
+  for (int i = 1; i < n; ++i) workers.emplace_back(frame, i);
+  frame(0);
+  for (auto& w : workers) w.join();
+  int first = RIHVR_OK;
+  for (int i = 0; i < n; ++i) {
+    if (statuses) statuses[i] = st[i];
+    if (first == RIHVR_OK && st[i] != RIHVR_OK) {
+      first = st[i];
+      g_last_error = "frame " + std::to_string(i) + ": " + msg[i];
+    }
+  }
+  return first;
 }
 
 int rihvr_iteration_count(const rihvr_ctx* c) { return c ? c->it : -1; }

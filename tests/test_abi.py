@@ -109,3 +109,19 @@ def test_status_strings(rihvr):
     assert L.rihvr_status_string(0) == b"ok"
     assert L.rihvr_status_string(7) == b"invalid argument"
     assert L.rihvr_status_string(22) == b"unsupported size"
+
+
+def test_batch_validates_before_touching_contexts(rihvr):
+    """rihvr_reconstruct_batch rejects empty batches and repeated contexts
+    without dereferencing them (the pointers below are never valid)."""
+    import ctypes
+
+    L = rihvr.load_library()
+    fake = (ctypes.c_void_p * 2)(ctypes.c_void_p(4096), ctypes.c_void_p(4096))
+    holo = (ctypes.c_void_p * 2)(ctypes.c_void_p(8192), ctypes.c_void_p(8192))
+    assert L.rihvr_reconstruct_batch(fake, 0, holo, 0, None, None) == rihvr.ERR_INVALID_ARGUMENT
+    assert L.rihvr_reconstruct_batch(None, 1, holo, 0, None, None) == rihvr.ERR_INVALID_ARGUMENT
+    assert L.rihvr_reconstruct_batch(fake, 2, holo, 0, None, None) == rihvr.ERR_INVALID_ARGUMENT
+    assert b"twice" in L.rihvr_last_error()
+    nul = (ctypes.c_void_p * 1)(None)
+    assert L.rihvr_reconstruct_batch(nul, 1, holo, 0, None, None) == rihvr.ERR_INVALID_ARGUMENT
