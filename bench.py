@@ -133,6 +133,62 @@ MEASURED_TRAFFIC_PER_VOXEL = {
 }
 
 
+GOLDEN_C2 = os.path.join(ROOT, "tests", "golden", "oracle_c2_1024x1024x1000.json")
+
+
+def time_to_objective(rihvr, cfg, b, s, storage, stream, hb, tol=1e-3):
+    """Seconds until the solver holds an iterate whose objective is within
+    `tol` (relative) of the FP64 oracle's objective after its 100 iterations
+    (committed oracle run of the same hologram).  An untimed pass with the
+    objective recorded at every iteration finds the first iteration k that is
+    within the band; the timed pass is what a user runs: hologram in from
+    pinned host memory, k iterations without per-iteration objective, the
+    objective at the end.  The iterates of the two passes are identical."""
+    import hashlib
+
+    import torch
+
+    if not os.path.exists(GOLDEN_C2):
+        return None
+    with open(GOLDEN_C2) as fh:
+        g = json.load(fh)
+    if g.get("workload") != cfg.name or hashlib.sha1(b.tobytes()).hexdigest() != g.get("b_sha1"):
+        return None
+    target = float(g["f_x"][-1])
+    p = rihvr.params_from_config(cfg, record_objective=1, storage=storage)
+    with rihvr.SparseCompressiveHolo(p, cfg.W, cfg.H) as t:
+        t.setHologram(b)
+        t.iterate(len(g["f_x"]))
+        fx = np.asarray(t.iterations()["f_x"], np.float64)
+    gx = np.asarray(g["f_x"], np.float64)
+    band = tol * abs(target)
+    hits = np.nonzero(np.abs(fx - target) <= band)[0]
+    ohits = np.nonzero(np.abs(gx - target) <= band)[0]
+    out = {"unit": "s", "target_objective": target, "tolerance": tol, "oracle_iterations": int(ohits[0]) + 1,
+           "oracle_seconds_100_iterations": g.get("oracle_seconds"), "oracle_threads": g.get("oracle_threads"),
+           "max_rel_gap_to_oracle_trajectory": float(np.max(np.abs(fx - gx) / np.abs(gx))),
+           "final_rel_gap": float((fx[-1] - target) / abs(target))}
+    if not len(hits):
+        out.update({"value": None, "reached": False})
+        return out
+    k = int(hits[0]) + 1
+    L = rihvr.load_library()
+    import ctypes
+
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    rihvr._check(L.rihvr_set_hologram(s._h, ctypes.c_void_p(hb.data_ptr()), 0), "set_hologram")
+    s.iterate(k)
+    f, _ = s.calcObjectiveFunction()
+    e1.record(stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    out.update({"value": ms / 1e3, "reached": True, "iterations": k, "objective": f,
+                "rel_gap": (f - target) / abs(target)})
+    return out
+
+
 def cpu_sample(cfg, b, steps: int, warmup: int):
     """Time the FP64 oracle on a bounded sample of the workload: the first 16
     planes of the volume, full plane size, one FISTA iteration per step."""
@@ -252,6 +308,10 @@ def run_ours(args):
            "h2d_bytes_per_step": int(b.nbytes) / args.steps, "d2h_bytes_per_step": (int(hout.numel() * 4) + 8) / args.steps,
            "ms": e2e_ms, "what": "set_hologram (H2D from pinned) + K iterations + estimate and objective (D2H)"}
 
+    tto = None
+    if ws == 1 and not args.nz and args.config == "c2":
+        tto = time_to_objective(rihvr, cfg, b, s, storage, stream, hb)
+
     # roofline of the dominant kernel class
     peak, peak_kind = peaks()
     sbytes = 8 if storage == 0 else 4
@@ -282,7 +342,7 @@ def run_ours(args):
                        "parallelism": f"{ws} independent frames" if ws > 1 else "single frame",
                        "l2": "inputs larger than L2 (volumes of %.1f GB each)" % (V * sbytes / 1e9),
                        "record_objective": False},
-            "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu,
+            "e2e": e2e, "time_to_objective": tto, "roofline": roofline, "cpu_baseline": cpu,
             "iteration_roofline": {"bytes_per_voxel_iter": 32 + 4 * sbytes,
                                    "achieved": iter_bytes * args.steps / (max_ms / 1e3) / 1e9, "peak": peak,
                                    "frac": iter_bytes * args.steps / (max_ms / 1e3) / 1e9 / peak},
