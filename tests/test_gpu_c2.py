@@ -7,8 +7,9 @@ oracle's, the same backtracking and restart decisions, and the oracle's
 100-iteration objective reached within 1e-3 at the same iteration count.
 BF16 / FP16 volume storage (FP32 arithmetic, FP64 phase): final objective within
 1e-2 of the oracle's, and volumes compared with the FP32 run's (relative L2).
-FP16 meets it; BF16 does not at this size and is marked as an expected failure.  Generating the hologram takes about a minute of CPU time on a
-fresh machine (cached under RIHVR_CACHE afterwards)."""
+FP16 meets it; BF16 does not at this size and is marked as an expected
+failure.  Generating the hologram takes about a minute of CPU time on a fresh
+machine (cached under RIHVR_CACHE afterwards)."""
 import ctypes
 import hashlib
 import json
