@@ -106,7 +106,7 @@ class ClockSampler:
 
 def workload(name: str):
     synth = importlib.import_module(PKG + ".synth")
-    return synth.config2() if name == "c2" else synth.config1()
+    return {"c1": synth.config1, "c2": synth.config2, "c5": synth.config5}[name]()
 
 
 # algorithmic bytes per voxel of each kernel class, s = bytes per stored voxel
@@ -364,7 +364,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="c2", choices=["c2", "c1"])
+    ap.add_argument("--config", default="c2", choices=["c2", "c1", "c5"])
     ap.add_argument("--storage", default="f32", choices=["f32", "bf16", "f16"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--nz", type=int, default=0, help="override the plane count (profiling cases)")

@@ -232,7 +232,9 @@ __device__ __forceinline__ void reg_fft(float2 (&a)[N]) {
 template <int N, int N2, bool INV>
 __device__ __forceinline__ void line_twiddle(float2 (&v)[N2], int n1) {
   if (n1 == 0) return;
-  constexpr int B = (N2 >= 8) ? 8 : N2;
+  // chain length: the largest of 8, 4, 2, 1 that divides N2 (every element is twiddled)
+  constexpr int B = (N2 % 8 == 0) ? 8 : (N2 % 4 == 0) ? 4 : (N2 % 2 == 0) ? 2 : 1;
+  static_assert(N2 % B == 0, "anchor blocks must tile the line");
   const float sgn = INV ? 2.0f : -2.0f;
   float s1, c1, s8, c8;
   sincospif(sgn * (float)n1 / (float)N, &s1, &c1);

@@ -15,6 +15,9 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <map>
+#include <mutex>
+#include <utility>
 
 #include "rihvr_device.cuh"
 #include "rihvr_kernels.cuh"
@@ -191,8 +194,8 @@ static cudaError_t rows_n(int inverse, int in_kind, const void* in, int out_kind
   return cudaGetLastError();
 }
 
-cudaError_t launch_rows(int inverse, int in_kind, const void* in, int out_kind, void* out, int W,
-                        long long nlines, float scale, cudaStream_t st) {
+static cudaError_t launch_rows_fast(int inverse, int in_kind, const void* in, int out_kind, void* out, int W,
+                                    long long nlines, float scale, cudaStream_t st) {
   switch (W) {
 #define RIHVR_CASE(NN) \
   case NN:             \
@@ -593,8 +596,8 @@ static cudaError_t adj_col_n(const float2* Rs, const double* cturn, const double
   return cudaGetLastError();
 }
 
-cudaError_t launch_adj_col(const float2* Rs, const double* cturn, const double* zlist, float2* U, int W, int H,
-                           int z0, int z1, cudaStream_t st) {
+static cudaError_t launch_adj_col_fast(const float2* Rs, const double* cturn, const double* zlist, float2* U, int W,
+                                      int H, int z0, int z1, cudaStream_t st) {
   if (W != H) return cudaErrorInvalidValue;
   switch (H) {
 #define RIHVR_CASE(NN) \
@@ -607,7 +610,7 @@ cudaError_t launch_adj_col(const float2* Rs, const double* cturn, const double* 
   }
 }
 
-int fwd_col_chunks(int W, int H, int Nz) {
+static int fwd_col_chunks_fast(int W, int H, int Nz) {
   int cc = 8;
   switch (H) {
 #define RIHVR_CASE(NN) \
@@ -647,8 +650,8 @@ static cudaError_t fwd_col_n(const float2* T, const double* cturn, const double*
   return cudaGetLastError();
 }
 
-cudaError_t launch_fwd_col(const float2* T, const double* cturn, const double* zlist, float2* Spart, int W, int H,
-                           int z0, int z1, int nchunks, cudaStream_t st) {
+static cudaError_t launch_fwd_col_fast(const float2* T, const double* cturn, const double* zlist, float2* Spart,
+                                      int W, int H, int z0, int z1, int nchunks, cudaStream_t st) {
   if (W != H) return cudaErrorInvalidValue;
   switch (H) {
 #define RIHVR_CASE(NN) \
@@ -678,8 +681,8 @@ static cudaError_t plane_col_n(int inverse, const float2* in, float2* out, int W
   return cudaGetLastError();
 }
 
-cudaError_t launch_plane_col(int inverse, const float2* in, float2* out, int W, int H, float scale,
-                             cudaStream_t st) {
+static cudaError_t launch_plane_col_fast(int inverse, const float2* in, float2* out, int W, int H, float scale,
+                                        cudaStream_t st) {
   if (W != H) return cudaErrorInvalidValue;
   switch (H) {
 #define RIHVR_CASE(NN) \
@@ -1950,6 +1953,390 @@ cudaError_t launch_prox6_finish(int storage, const ProxArgs& a, const float2* Y,
       break;
     default:
       k_prox6_finish<float2><<<blocks, FLAT_THREADS, 0, st>>>(a, Y);
+  }
+  return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Generic line FFT: plane sides without a register-resident four-step
+// configuration above (any length up to 8192 whose prime factors are 2, 3, 5
+// and 7, such as 640, 1536, 2048 or 2304) and rectangular planes.  The
+// reference takes such sizes through cuFFT (sparse_compressive_holo.cu:98);
+// W and H are multiples of 16 there (:126, 1948).
+//
+// A block transforms C lines of length n held in shared memory as [n][C]
+// (C a power of two, n C <= kGElems) by a self-sorting Stockham sequence of
+// radix-4, 2, 3, 5 and 7 stages between two shared-memory buffers: each
+// butterfly reads its R inputs, multiplies by the twiddles of the previous
+// stages' size, transforms in registers and writes its outputs in sorted
+// position.  Twiddles come from a per-length FP64-built table of
+// exp(-2 pi i k / n).  Rows load C contiguous lines, columns C adjacent
+// columns of a plane of any row pitch; the column passes keep the same fusion
+// as the fast ones (transfer function on the fly, z-sum in registers).
+// ---------------------------------------------------------------------------
+constexpr int kGThreads = 256;
+constexpr int kGElems = 4096;          // complex values per block (two 32 KB buffers)
+constexpr int kGMaxStages = 16;
+
+struct GPlan {
+  int n, ns;
+  int r[kGMaxStages];
+};
+
+static bool gplan_make(int n, GPlan* p) {
+  if (n < 2 || n > kGElems) return false;
+  p->n = n;
+  p->ns = 0;
+  int m = n;
+  const int order[5] = {4, 2, 3, 5, 7};
+  for (int k = 0; k < 5; ++k) {
+    while (m % order[k] == 0) {
+      if (p->ns == kGMaxStages) return false;
+      p->r[p->ns++] = order[k];
+      m /= order[k];
+    }
+  }
+  return m == 1;
+}
+
+bool generic_size_supported(int n) {
+  GPlan p;
+  return gplan_make(n, &p);
+}
+
+// lines per block: the largest power of two with n C <= kGElems, capped
+static int gplan_lines(int n, int cap) {
+  int c = 1;
+  while (2 * c * n <= kGElems && 2 * c <= cap) c *= 2;
+  return c;
+}
+
+__global__ void k_gtwiddles(int n, float2* __restrict__ tw) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k < n) {
+    double s, c;
+    sincospi(-2.0 * (double)k / (double)n, &s, &c);
+    tw[k] = make_float2((float)c, (float)s);
+  }
+}
+
+// exp(-2 pi i k / n), k < n: one table per (device, n), built once and kept
+// for the life of the process (at most 64 KB each)
+static const float2* gtwiddles(int n, cudaStream_t st, cudaError_t* err) {
+  static std::mutex mu;
+  static std::map<std::pair<int, int>, float2*> tables;
+  int dev = 0;
+  *err = cudaGetDevice(&dev);
+  if (*err != cudaSuccess) return nullptr;
+  std::lock_guard<std::mutex> lock(mu);
+  auto it = tables.find({dev, n});
+  if (it != tables.end()) return it->second;
+  float2* t = nullptr;
+  *err = cudaMalloc(&t, sizeof(float2) * (size_t)n);
+  if (*err != cudaSuccess) return nullptr;
+  k_gtwiddles<<<(n + 255) / 256, 256, 0, st>>>(n, t);
+  *err = cudaStreamSynchronize(st);
+  if (*err != cudaSuccess) {
+    cudaFree(t);
+    return nullptr;
+  }
+  tables[{dev, n}] = t;
+  return t;
+}
+
+template <int R, bool INV>
+__device__ __forceinline__ void gstage(const float2* src, float2* dst, int n, int logc, int ns,
+                                       const float2* __restrict__ tw) {
+  const int C = 1 << logc;
+  const int m = n / R;
+  const int total = m << logc;
+  const int tstep = n / (ns * R);
+  for (int b = threadIdx.x; b < total; b += kGThreads) {
+    const int c = b & (C - 1), j = b >> logc;
+    const int k = j % ns;
+    float2 v[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      float2 x = src[((j + r * m) << logc) + c];
+      if (r > 0 && k > 0) {
+        float2 w = __ldg(tw + k * r * tstep);
+        if (INV) w.y = -w.y;
+        x = cmul(x, w);
+      }
+      v[r] = x;
+    }
+    small_dft<R, INV>(v);
+    const int d = (((j - k) * R + k) << logc) + c;
+#pragma unroll
+    for (int r = 0; r < R; ++r) dst[d + ((r * ns) << logc)] = v[r];
+  }
+  __syncthreads();
+}
+
+// DFT of the C lines in buf[0] ([n][C]), using buf[1] as the other half of the
+// ping-pong; returns the buffer holding the result.  Every thread of the block
+// calls it, after a barrier that makes buf[0] complete.
+template <bool INV>
+__device__ float2* gfft(float2* b0, float2* b1, int logc, const GPlan& p, const float2* __restrict__ tw) {
+  int ns = 1;
+  float2* src = b0;
+  float2* dst = b1;
+  for (int s = 0; s < p.ns; ++s) {
+    switch (p.r[s]) {
+      case 4: gstage<4, INV>(src, dst, p.n, logc, ns, tw); break;
+      case 2: gstage<2, INV>(src, dst, p.n, logc, ns, tw); break;
+      case 3: gstage<3, INV>(src, dst, p.n, logc, ns, tw); break;
+      case 5: gstage<5, INV>(src, dst, p.n, logc, ns, tw); break;
+      default: gstage<7, INV>(src, dst, p.n, logc, ns, tw); break;
+    }
+    ns *= p.r[s];
+    float2* t = src;
+    src = dst;
+    dst = t;
+  }
+  return src;
+}
+
+template <bool INV>
+__global__ void __launch_bounds__(kGThreads) k_grows(GPlan p, const float2* __restrict__ tw, int in_kind,
+                                                     const void* __restrict__ in, int out_kind, void* __restrict__ out,
+                                                     long long nlines, float scale, int logc) {
+  extern __shared__ __align__(128) float2 gbuf[];
+  const int n = p.n, C = 1 << logc;
+  float2* const gb1 = gbuf + n * C;
+  const long long l0 = (long long)blockIdx.x << logc;
+  const int nl = (int)min((long long)C, nlines - l0);
+  for (int e = threadIdx.x; e < n * C; e += kGThreads) {
+    const int c = e / n, k = e - c * n;  // consecutive threads, consecutive elements of a line
+    gbuf[(k << logc) + c] = c < nl ? load_elem(in_kind, in, (size_t)(l0 + c) * n + k) : make_float2(0.f, 0.f);
+  }
+  __syncthreads();
+  const float2* res = gfft<INV>(gbuf, gb1, logc, p, tw);
+  for (int e = threadIdx.x; e < n * C; e += kGThreads) {
+    const int c = e / n, k = e - c * n;
+    if (c < nl) store_elem(out_kind, out, (size_t)(l0 + c) * n + k, cscale(res[(k << logc) + c], scale));
+  }
+}
+
+// adjoint column pass: U_z(:, x) = IDFT_y(conj(H'_z(:, x)) Rs(:, x)) for the
+// C columns x0.. of the block, planes [zb, ze)
+__global__ void __launch_bounds__(kGThreads) k_gadj_col(GPlan p, const float2* __restrict__ tw,
+                                                        const float2* __restrict__ Rs,
+                                                        const double* __restrict__ cturn,
+                                                        const double* __restrict__ zlist, float2* __restrict__ U,
+                                                        int W, int z0, int z1, int zpb, int logc) {
+  extern __shared__ __align__(128) float2 gbuf[];
+  const int H = p.n, C = 1 << logc;
+  float2* const gb1 = gbuf + H * C;
+  const int x0 = blockIdx.x << logc;
+  const int zb = z0 + blockIdx.y * zpb, ze = min(zb + zpb, z1);
+  const size_t HW = (size_t)H * W;
+  for (int z = zb; z < ze; ++z) {
+    const double zz = zlist[z];
+    for (int e = threadIdx.x; e < H * C; e += kGThreads) {
+      const int c = e & (C - 1), y = e >> logc, x = x0 + c;
+      float2 v = make_float2(0.f, 0.f);
+      if (x < W) {
+        const size_t i = (size_t)y * W + x;
+        v = cmul(Rs[i], transfer(zz, cturn[i], true));
+      }
+      gbuf[e] = v;
+    }
+    __syncthreads();
+    const float2* res = gfft<true>(gbuf, gb1, logc, p, tw);
+    float2* Uz = U + (size_t)z * HW;
+    for (int e = threadIdx.x; e < H * C; e += kGThreads) {
+      const int c = e & (C - 1), y = e >> logc, x = x0 + c;
+      if (x < W) Uz[(size_t)y * W + x] = res[e];
+    }
+    __syncthreads();
+  }
+}
+
+constexpr int kGAcc = kGElems / kGThreads;  // elements a thread accumulates
+
+// forward column pass with the z-sum: Spart[chunk](:, x) = sum_z H'_z(:, x) DFT_y(T_z(:, x))
+__global__ void __launch_bounds__(kGThreads) k_gfwd_col(GPlan p, const float2* __restrict__ tw,
+                                                        const float2* __restrict__ T,
+                                                        const double* __restrict__ cturn,
+                                                        const double* __restrict__ zlist, float2* __restrict__ Spart,
+                                                        int W, int z0, int z1, int zpb, int logc) {
+  extern __shared__ __align__(128) float2 gbuf[];
+  const int H = p.n, C = 1 << logc;
+  float2* const gb1 = gbuf + H * C;
+  const int x0 = blockIdx.x << logc;
+  const int zb = z0 + blockIdx.y * zpb, ze = min(zb + zpb, z1);
+  const size_t HW = (size_t)H * W;
+  float2 acc[kGAcc];
+#pragma unroll
+  for (int i = 0; i < kGAcc; ++i) acc[i] = make_float2(0.f, 0.f);
+  for (int z = zb; z < ze; ++z) {
+    const double zz = zlist[z];
+    const float2* Tz = T + (size_t)z * HW;
+    for (int e = threadIdx.x; e < H * C; e += kGThreads) {
+      const int c = e & (C - 1), y = e >> logc, x = x0 + c;
+      gbuf[e] = x < W ? Tz[(size_t)y * W + x] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    const float2* res = gfft<false>(gbuf, gb1, logc, p, tw);
+#pragma unroll
+    for (int i = 0; i < kGAcc; ++i) {
+      const int e = threadIdx.x + i * kGThreads;
+      if (e < H * C) {
+        const int c = e & (C - 1), y = e >> logc, x = x0 + c;
+        if (x < W) acc[i] = cadd(acc[i], cmul(res[e], transfer(zz, cturn[(size_t)y * W + x], false)));
+      }
+    }
+    __syncthreads();
+  }
+  float2* Sp = Spart + (size_t)blockIdx.y * HW;
+#pragma unroll
+  for (int i = 0; i < kGAcc; ++i) {
+    const int e = threadIdx.x + i * kGThreads;
+    if (e < H * C) {
+      const int c = e & (C - 1), y = e >> logc, x = x0 + c;
+      if (x < W) Sp[(size_t)y * W + x] = acc[i];
+    }
+  }
+}
+
+template <bool INV>
+__global__ void __launch_bounds__(kGThreads) k_gplane_col(GPlan p, const float2* __restrict__ tw,
+                                                          const float2* __restrict__ in, float2* __restrict__ out, int W,
+                                                          float scale, int logc) {
+  extern __shared__ __align__(128) float2 gbuf[];
+  const int H = p.n, C = 1 << logc;
+  float2* const gb1 = gbuf + H * C;
+  const int x0 = blockIdx.x << logc;
+  for (int e = threadIdx.x; e < H * C; e += kGThreads) {
+    const int c = e & (C - 1), y = e >> logc, x = x0 + c;
+    gbuf[e] = x < W ? in[(size_t)y * W + x] : make_float2(0.f, 0.f);
+  }
+  __syncthreads();
+  const float2* res = gfft<INV>(gbuf, gb1, logc, p, tw);
+  for (int e = threadIdx.x; e < H * C; e += kGThreads) {
+    const int c = e & (C - 1), y = e >> logc, x = x0 + c;
+    if (x < W) out[(size_t)y * W + x] = cscale(res[e], scale);
+  }
+}
+
+static int ilog2(int c) {
+  int l = 0;
+  while ((1 << l) < c) ++l;
+  return l;
+}
+
+// columns per block of the generic column passes: 8-byte elements, 16 columns
+// make 128-byte row segments
+constexpr int kGColsMax = 16;
+
+static bool fast_square(int W, int H) { return W == H && line_size_supported(W); }
+
+static int fwd_col_chunks_generic(int W, int H, int Nz) {
+  const int C = gplan_lines(H, kGColsMax);
+  const int strips = (W + C - 1) / C;
+  int chunks = (4 * num_sms() + strips - 1) / strips;
+  if (chunks > 16) chunks = 16;
+  if (chunks > Nz) chunks = Nz;
+  if (chunks < 1) chunks = 1;
+  return chunks;
+}
+
+int fwd_col_chunks(int W, int H, int Nz) {
+  return fast_square(W, H) ? fwd_col_chunks_fast(W, H, Nz) : fwd_col_chunks_generic(W, H, Nz);
+}
+
+cudaError_t launch_rows(int inverse, int in_kind, const void* in, int out_kind, void* out, int W, long long nlines,
+                        float scale, cudaStream_t st) {
+  if (line_size_supported(W)) return launch_rows_fast(inverse, in_kind, in, out_kind, out, W, nlines, scale, st);
+  GPlan p;
+  if (!gplan_make(W, &p)) return cudaErrorInvalidValue;
+  cudaError_t e;
+  const float2* tw = gtwiddles(W, st, &e);
+  if (!tw) return e;
+  const int C = gplan_lines(W, 64), logc = ilog2(C);
+  const size_t smem = 2 * sizeof(float2) * (size_t)W * C;
+  const long long blocks = (nlines + C - 1) / C;
+  if (inverse) {
+    e = allow_smem(k_grows<true>, smem);
+    if (e != cudaSuccess) return e;
+    k_grows<true><<<(unsigned)blocks, kGThreads, smem, st>>>(p, tw, in_kind, in, out_kind, out, nlines, scale, logc);
+  } else {
+    e = allow_smem(k_grows<false>, smem);
+    if (e != cudaSuccess) return e;
+    k_grows<false><<<(unsigned)blocks, kGThreads, smem, st>>>(p, tw, in_kind, in, out_kind, out, nlines, scale, logc);
+  }
+  return cudaGetLastError();
+}
+
+cudaError_t launch_adj_col(const float2* Rs, const double* cturn, const double* zlist, float2* U, int W, int H,
+                           int z0, int z1, cudaStream_t st) {
+  if (fast_square(W, H)) return launch_adj_col_fast(Rs, cturn, zlist, U, W, H, z0, z1, st);
+  const int nz = z1 - z0;
+  if (nz <= 0) return cudaSuccess;
+  GPlan p;
+  if (!gplan_make(H, &p)) return cudaErrorInvalidValue;
+  cudaError_t e;
+  const float2* tw = gtwiddles(H, st, &e);
+  if (!tw) return e;
+  const int C = gplan_lines(H, kGColsMax), logc = ilog2(C);
+  const int strips = (W + C - 1) / C;
+  int chunks = (8 * num_sms() + strips - 1) / strips;
+  if (chunks > nz) chunks = nz;
+  if (chunks < 1) chunks = 1;
+  const int zpb = (nz + chunks - 1) / chunks;
+  chunks = (nz + zpb - 1) / zpb;
+  const size_t smem = 2 * sizeof(float2) * (size_t)H * C;
+  e = allow_smem(k_gadj_col, smem);
+  if (e != cudaSuccess) return e;
+  k_gadj_col<<<dim3(strips, chunks), kGThreads, smem, st>>>(p, tw, Rs, cturn, zlist, U, W, z0, z1, zpb, logc);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_fwd_col(const float2* T, const double* cturn, const double* zlist, float2* Spart, int W, int H,
+                           int z0, int z1, int nchunks, cudaStream_t st) {
+  if (fast_square(W, H)) return launch_fwd_col_fast(T, cturn, zlist, Spart, W, H, z0, z1, nchunks, st);
+  const int nz = z1 - z0;
+  if (nz <= 0) return cudaSuccess;
+  GPlan p;
+  if (!gplan_make(H, &p)) return cudaErrorInvalidValue;
+  cudaError_t e;
+  const float2* tw = gtwiddles(H, st, &e);
+  if (!tw) return e;
+  const int C = gplan_lines(H, kGColsMax), logc = ilog2(C);
+  const int strips = (W + C - 1) / C;
+  const int zpb = (nz + nchunks - 1) / nchunks;
+  const int chunks = (nz + zpb - 1) / zpb;
+  if (chunks < nchunks) {  // unused chunk slots must read as zero
+    e = cudaMemsetAsync(Spart + (size_t)chunks * H * W, 0, sizeof(float2) * (size_t)(nchunks - chunks) * H * W, st);
+    if (e != cudaSuccess) return e;
+  }
+  const size_t smem = 2 * sizeof(float2) * (size_t)H * C;
+  e = allow_smem(k_gfwd_col, smem);
+  if (e != cudaSuccess) return e;
+  k_gfwd_col<<<dim3(strips, chunks), kGThreads, smem, st>>>(p, tw, T, cturn, zlist, Spart, W, z0, z1, zpb, logc);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_plane_col(int inverse, const float2* in, float2* out, int W, int H, float scale,
+                             cudaStream_t st) {
+  if (fast_square(W, H)) return launch_plane_col_fast(inverse, in, out, W, H, scale, st);
+  GPlan p;
+  if (!gplan_make(H, &p)) return cudaErrorInvalidValue;
+  cudaError_t e;
+  const float2* tw = gtwiddles(H, st, &e);
+  if (!tw) return e;
+  const int C = gplan_lines(H, kGColsMax), logc = ilog2(C);
+  const int strips = (W + C - 1) / C;
+  const size_t smem = 2 * sizeof(float2) * (size_t)H * C;
+  if (inverse) {
+    e = allow_smem(k_gplane_col<true>, smem);
+    if (e != cudaSuccess) return e;
+    k_gplane_col<true><<<strips, kGThreads, smem, st>>>(p, tw, in, out, W, scale, logc);
+  } else {
+    e = allow_smem(k_gplane_col<false>, smem);
+    if (e != cudaSuccess) return e;
+    k_gplane_col<false><<<strips, kGThreads, smem, st>>>(p, tw, in, out, W, scale, logc);
   }
   return cudaGetLastError();
 }

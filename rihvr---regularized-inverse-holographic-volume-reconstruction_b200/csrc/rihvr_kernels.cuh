@@ -39,6 +39,8 @@ struct ProxArgs {
 };
 
 bool line_size_supported(int n);
+// sides the generic line FFT handles (prime factors 2, 3, 5, 7; up to 8192)
+bool generic_size_supported(int n);
 // message returned by rihvr_last_error on this thread
 void set_last_error(const char* msg);
 size_t max_partial_blocks(int W, int H, int Nz);

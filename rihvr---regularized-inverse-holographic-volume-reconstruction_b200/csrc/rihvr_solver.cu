@@ -410,11 +410,16 @@ int copy_in(rihvr_ctx* c, void* dst, const void* src, size_t bytes, int is_devic
 int validate(const rihvr_params* p, int W, int H) {
   if (!p) return fail(RIHVR_ERR_INVALID_ARGUMENT, "params is NULL");
   if (W <= 0 || H <= 0) return fail(RIHVR_ERR_INVALID_ARGUMENT, "width and height must be positive");
-  if (W != H)
-    return fail(RIHVR_ERR_UNSUPPORTED_SIZE, "planes must be square (the reference zero-pads to square planes)");
-  if (!line_size_supported(W))
-    return fail(RIHVR_ERR_UNSUPPORTED_SIZE,
-                "unsupported plane side " + std::to_string(W) + " (supported: 32 48 64 128 256 384 512 768 1024)");
+  // Square planes of side 32, 48, 64, 128, 256, 384, 512, 768 or 1024 take the
+  // register-resident FFT passes; any other even width and height from 16 to
+  // 4096 whose prime factors are 2, 3, 5 and 7 takes the generic passes (the
+  // reference needs multiples of 16, :126, 1948).
+  for (int n : {W, H}) {
+    if (n < 16 || (n & 1) || !(line_size_supported(n) || generic_size_supported(n)))
+      return fail(RIHVR_ERR_UNSUPPORTED_SIZE,
+                  "unsupported plane size " + std::to_string(W) + " x " + std::to_string(H) +
+                      " (each side even, 16..4096, prime factors 2, 3, 5, 7 only)");
+  }
   if (p->num_planes < 1) return fail(RIHVR_ERR_INVALID_ARGUMENT, "num_planes must be >= 1");
   if (p->mode != 5 && p->mode != 6 && p->mode != 7)
     return fail(RIHVR_ERR_UNKNOWN_MODE, "mode must be 5, 6 or 7 (unsupported mode)");

@@ -118,6 +118,19 @@ def config2(**kw) -> HoloConfig:
     return c
 
 
+def config5(**kw) -> HoloConfig:
+    """Large volume: 2048x2048 padded by 128 px per side (2304x2304), Nz=512,
+    20000 tracer disks; run with FP16 volume storage."""
+    c = HoloConfig(name="fista_tv_2304x2304x512", width=2048, height=2048, zero_padding=128, num_planes=512,
+                   start_plane=1000.0, plane_stepsize=4.0, resolution=2.2, wavelength=0.532,
+                   regularization_param=0.05, regularization_TV_param=0.05,
+                   num_inverse_iterations=150, num_tv_iterations=10,
+                   n_disks=20000, disk_radius=(1.0, 3.0), noise_sigma=0.02)
+    for k, v in kw.items():
+        setattr(c, k, v)
+    return c
+
+
 def small_config(W=64, H=64, Nz=6, seed=0, **kw) -> HoloConfig:
     """Small case for parity tests (a few seconds in the oracle)."""
     c = HoloConfig(name=f"small_{W}x{H}x{Nz}", width=W, height=H, zero_padding=0, num_planes=Nz,

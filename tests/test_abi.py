@@ -94,8 +94,9 @@ def test_create_validates_arguments_before_touching_the_gpu(rihvr):
     h = ctypes.c_void_p()
     p = rihvr.default_params()
     p.num_planes = 4
-    assert L.rihvr_create(ctypes.byref(p), 100, 100, ctypes.byref(h)) == rihvr.ERR_UNSUPPORTED_SIZE
-    assert L.rihvr_create(ctypes.byref(p), 64, 32, ctypes.byref(h)) == rihvr.ERR_UNSUPPORTED_SIZE
+    # sides must be even, 16..4096, with prime factors 2, 3, 5 and 7 only
+    for w, hh in ((88, 88), (64, 22), (15, 16), (8, 8), (5000, 64), (64, 4802)):
+        assert L.rihvr_create(ctypes.byref(p), w, hh, ctypes.byref(h)) == rihvr.ERR_UNSUPPORTED_SIZE, (w, hh)
     p.mode = 4
     assert L.rihvr_create(ctypes.byref(p), 64, 64, ctypes.byref(h)) == rihvr.ERR_UNKNOWN_MODE
     p.mode = 7

@@ -51,7 +51,8 @@ def rand_volume(rng, nz, side, scale=0.05):
         np.complex64)
 
 
-@pytest.mark.parametrize("side,nz", [(32, 3), (64, 5), (128, 4), (384, 3), (1024, 2)])
+@pytest.mark.parametrize("side,nz", [(32, 3), (48, 4), (64, 5), (128, 4), (256, 2), (384, 3), (512, 2), (768, 2),
+                                     (1024, 2)])
 def test_forward_matches_oracle(rihvr, side, nz):
     p = make(rihvr, side, nz)
     rng = np.random.default_rng(side + nz)
@@ -62,7 +63,8 @@ def test_forward_matches_oracle(rihvr, side, nz):
     assert rel(d, ref) < TOL_F32
 
 
-@pytest.mark.parametrize("side,nz", [(32, 3), (64, 5), (384, 3), (1024, 2)])
+@pytest.mark.parametrize("side,nz", [(32, 3), (48, 4), (64, 5), (128, 2), (256, 2), (384, 3), (512, 2), (768, 2),
+                                     (1024, 2)])
 def test_adjoint_matches_oracle(rihvr, side, nz):
     p = make(rihvr, side, nz)
     rng = np.random.default_rng(7 * side + nz)
