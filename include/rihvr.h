@@ -129,7 +129,9 @@ int rihvr_plane_list(const rihvr_params* params, double* z_out);
 
 /* SparseCompressiveHolo::SparseCompressiveHolo(Hologram)
  * (src/core/sparse_compressive_holo.cu:58-135).  width x height is the padded
- * hologram size; planes must be square with a supported side. */
+ * hologram size.  Each side is even, 16..4096, with prime factors 2, 3, 5 and 7
+ * only (the reference needs multiples of 16); square planes of side 32, 48, 64,
+ * 128, 256, 384, 512, 768 or 1024 take the fastest FFT passes. */
 int rihvr_create(const rihvr_params* params, int width, int height, rihvr_ctx** out);
 
 /* SparseCompressiveHolo::destroy (:137-146). */
