@@ -1138,7 +1138,7 @@ struct TvsGrid {
 };
 
 // ---------------------------------------------------------------------------
-// Streaming form of the same prox (1 <= n_tv <= 6), the default.  The tiled
+// Streaming form of the same prox (1 <= n_tv <= 10), the default.  The tiled
 // kernel above recomputes a halo of n_tv + 1 rows and columns around every
 // 64 x 64 tile, so a third of its work is thrown away, and it needs a block
 // barrier per TV iteration.  Here a lane owns CPL adjacent columns and a warp a
@@ -1494,10 +1494,14 @@ static cudaError_t strip_dispatch(const ProxArgs& a, int* nb, cudaStream_t st) {
     case 4: return strip_launch<ST, 4>(a, nb, st);
     case 5: return strip_launch<ST, 5>(a, nb, st);
     case 6: return strip_launch<ST, 6>(a, nb, st);
+    case 7: return strip_launch<ST, 7>(a, nb, st);
+    case 8: return strip_launch<ST, 8>(a, nb, st);
+    case 9: return strip_launch<ST, 9>(a, nb, st);
+    case 10: return strip_launch<ST, 10>(a, nb, st);
     default: return cudaErrorInvalidValue;
   }
 }
-constexpr int kStripNtvMax = 6;
+constexpr int kStripNtvMax = 10;
 
 // RIHVR_TV_KERNEL=tiles forces the tiled kernel (comparison and fallback);
 // read once per process.
@@ -1975,7 +1979,8 @@ cudaError_t launch_prox6_finish(int storage, const ProxArgs& a, const float2* Y,
 // as the fast ones (transfer function on the fly, z-sum in registers).
 // ---------------------------------------------------------------------------
 constexpr int kGThreads = 256;
-constexpr int kGElems = 4096;          // complex values per block (two 32 KB buffers)
+constexpr int kGElems = 4096;          // complex values per row block (two 32 KB buffers)
+constexpr int kGColElems = 9216;       // per column block: 4 columns of 2304 (two 72 KB buffers)
 constexpr int kGMaxStages = 16;
 
 struct GPlan {
@@ -2004,10 +2009,10 @@ bool generic_size_supported(int n) {
   return gplan_make(n, &p);
 }
 
-// lines per block: the largest power of two with n C <= kGElems, capped
-static int gplan_lines(int n, int cap) {
+// lines per block: the largest power of two with n C <= budget, capped
+static int gplan_lines(int n, int cap, int budget = kGElems) {
   int c = 1;
-  while (2 * c * n <= kGElems && 2 * c <= cap) c *= 2;
+  while (2 * c * n <= budget && 2 * c <= cap) c *= 2;
   return c;
 }
 
@@ -2153,7 +2158,7 @@ __global__ void __launch_bounds__(kGThreads) k_gadj_col(GPlan p, const float2* _
   }
 }
 
-constexpr int kGAcc = kGElems / kGThreads;  // elements a thread accumulates
+constexpr int kGAcc = kGColElems / kGThreads;  // elements a thread accumulates
 
 // forward column pass with the z-sum: Spart[chunk](:, x) = sum_z H'_z(:, x) DFT_y(T_z(:, x))
 __global__ void __launch_bounds__(kGThreads) k_gfwd_col(GPlan p, const float2* __restrict__ tw,
@@ -2233,7 +2238,7 @@ constexpr int kGColsMax = 16;
 static bool fast_square(int W, int H) { return W == H && line_size_supported(W); }
 
 static int fwd_col_chunks_generic(int W, int H, int Nz) {
-  const int C = gplan_lines(H, kGColsMax);
+  const int C = gplan_lines(H, kGColsMax, kGColElems);
   const int strips = (W + C - 1) / C;
   int chunks = (4 * num_sms() + strips - 1) / strips;
   if (chunks > 16) chunks = 16;
@@ -2279,7 +2284,7 @@ cudaError_t launch_adj_col(const float2* Rs, const double* cturn, const double* 
   cudaError_t e;
   const float2* tw = gtwiddles(H, st, &e);
   if (!tw) return e;
-  const int C = gplan_lines(H, kGColsMax), logc = ilog2(C);
+  const int C = gplan_lines(H, kGColsMax, kGColElems), logc = ilog2(C);
   const int strips = (W + C - 1) / C;
   int chunks = (8 * num_sms() + strips - 1) / strips;
   if (chunks > nz) chunks = nz;
@@ -2303,7 +2308,7 @@ cudaError_t launch_fwd_col(const float2* T, const double* cturn, const double* z
   cudaError_t e;
   const float2* tw = gtwiddles(H, st, &e);
   if (!tw) return e;
-  const int C = gplan_lines(H, kGColsMax), logc = ilog2(C);
+  const int C = gplan_lines(H, kGColsMax, kGColElems), logc = ilog2(C);
   const int strips = (W + C - 1) / C;
   const int zpb = (nz + nchunks - 1) / nchunks;
   const int chunks = (nz + zpb - 1) / zpb;
@@ -2326,7 +2331,7 @@ cudaError_t launch_plane_col(int inverse, const float2* in, float2* out, int W, 
   cudaError_t e;
   const float2* tw = gtwiddles(H, st, &e);
   if (!tw) return e;
-  const int C = gplan_lines(H, kGColsMax), logc = ilog2(C);
+  const int C = gplan_lines(H, kGColsMax, kGColElems), logc = ilog2(C);
   const int strips = (W + C - 1) / C;
   const size_t smem = 2 * sizeof(float2) * (size_t)H * C;
   if (inverse) {

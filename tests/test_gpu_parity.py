@@ -108,9 +108,9 @@ def test_prox_step_matches_oracle(rihvr, mode, faithful):
 
 
 @pytest.mark.parametrize("side,nz,n_tv", [(32, 3, 5), (128, 3, 1), (128, 2, 2), (384, 2, 3), (256, 2, 6),
-                                         (128, 2, 7), (64, 3, 0)])
+                                         (128, 2, 7), (256, 2, 10), (64, 3, 0), (128, 2, 12)])
 def test_tv_prox_iteration_counts(rihvr, side, nz, n_tv):
-    """Streaming TV prox (1..6 Chambolle iterations) and the tiled one (other
+    """Streaming TV prox (1..10 Chambolle iterations) and the tiled one (other
     counts) against the oracle, on planes with several strips and runs."""
     p = make(rihvr, side, nz, mode=7, faithful=1, num_tv_iterations=n_tv)
     rng = np.random.default_rng(side * 10 + n_tv)
@@ -145,7 +145,8 @@ np.save(sys.argv[7], out)
 """
 
 
-@pytest.mark.parametrize("side,nz,ntv,storage", [(1024, 3, 5, 0), (384, 4, 3, 0), (768, 2, 6, 1), (256, 3, 4, 2)])
+@pytest.mark.parametrize("side,nz,ntv,storage", [(1024, 3, 5, 0), (384, 4, 3, 0), (768, 2, 6, 1), (256, 3, 4, 2),
+                                                 (512, 2, 10, 2), (640, 2, 8, 0)])
 def test_streaming_prox_bits_equal_tiled(rihvr, tmp_path, side, nz, ntv, storage):
     """The streaming TV prox reproduces the tiled kernel's P_new bit for bit
     (run lengths odd and even, every storage type)."""
