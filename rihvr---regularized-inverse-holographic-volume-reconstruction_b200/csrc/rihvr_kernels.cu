@@ -836,7 +836,9 @@ __device__ __forceinline__ void tv_dual(float2& gx, float2& gy, float2 y, float2
   const float2 py = f2fma(s2, f2sub(yu, y), gy);
   const float2 q = f2fma(py, py, f2mul(px, px));
   const float n2 = q.x + q.y;
-  const float sc = (n2 > 1.f) ? rsqrt_approx(n2) : 1.f;
+  // 1 / max(1, sqrt(n2)) as min(1, rsqrt(n2)): one instruction instead of a
+  // compare and a select (n2 = 0 gives rsqrt = inf, hence 1)
+  const float sc = fminf(1.f, rsqrt_approx(n2));
   const float2 sc2 = make_float2(sc, sc);
   gx = f2mul(px, sc2);
   gy = f2mul(py, sc2);
@@ -1159,9 +1161,11 @@ struct TvsGrid {
 // arithmetic is the tiled kernel's operation for operation, so P_new has the
 // same bits; the sums differ only in summation order.
 //
-// The step loop is unrolled by two.  With an odd number of steps that build
-// gave last rows of a run 1 ulp away from the tiled kernel, so runs of odd
-// length start one row earlier and every run has an even number of steps.
+// The step loop is unrolled by four (by two it needs 10% more instructions; by
+// eight the loop body outgrows the instruction cache).  With a step count that
+// is not a multiple of the unroll factor, unrolled builds gave the last row of a
+// run 1 ulp away from the tiled kernel, so runs start up to three rows earlier
+// and every run has a multiple of four steps.
 // ---------------------------------------------------------------------------
 template <int NTV, int CPL>
 struct TvwShape {
@@ -1233,7 +1237,7 @@ __device__ __forceinline__ void store_run(ST* p, const float2 (&v)[CPL]) {
 }
 
 template <typename ST, int NTV, bool NORMS, int CPL = 2, int NW = TvwShape<NTV, CPL>::NW,
-          int MINB = TvwShape<NTV, CPL>::MINB, int UNR = 2, int EVEN = 1>
+          int MINB = TvwShape<NTV, CPL>::MINB, int UNR = 4, int PADTO = 4>
 __global__ void __launch_bounds__(32 * NW, MINB) k_prox_tv2d_strip(ProxArgs a, TvsGrid gr) {
   using Sh = TvwShape<NTV, CPL>;
   constexpr int h = Sh::h, HX = Sh::HX, VW = Sh::VW, D = Sh::D, RM = D - 1, F4 = Sh::F4;
@@ -1272,13 +1276,13 @@ __global__ void __launch_bounds__(32 * NW, MINB) k_prox_tv2d_strip(ProxArgs a, T
     const bool lane_ok = (CPL * lane >= HX) && (CPL * lane < HX + VW) && (cu < W);
     const int r0 = seg * gr.seg_len;
     const int r1 = min(H, r0 + gr.seg_len);
-    // with EVEN, runs of odd length start one row earlier
-    const int pad = EVEN ? ((r1 - r0) & 1) : 0;
+    // runs start up to PADTO - 1 rows earlier so that the step count is a
+    // multiple of PADTO (the unroll factor)
+    const int pad = (PADTO - ((r1 - r0 + 2 * h) % PADTO)) % PADTO;
     const int nsteps = (r1 - r0) + 2 * h + pad;
-    int lrow = r0 - h - pad;
-    if (lrow < 0) lrow += H;
-    int orow = r0 - 2 * h - pad;
-    if (orow < 0) orow += H;
+    // the warm-up may reach back more than one plane height on short planes
+    int lrow = ((r0 - h - pad) % H + H) % H;
+    int orow = ((r0 - 2 * h - pad) % H + H) % H;
 
     // Ring slots are read as rows above r0 - h before any copy lands there;
     // those rows only feed rows above r0, which are not written.
@@ -1468,7 +1472,7 @@ static TvsGrid tvs_grid(int W, int H, int Nz, int VW, int warps_per_sm, int warm
 template <typename ST, int NTV, bool NORMS>
 static cudaError_t strip_launch_n(const ProxArgs& a, int* nblocks_out, cudaStream_t st) {
   using Sh = TvwShape<NTV, 2>;
-  const TvsGrid g = tvs_grid(a.W, a.H, a.Nz, Sh::VW, Sh::NW * Sh::MINB, 2 * Sh::h + 1);
+  const TvsGrid g = tvs_grid(a.W, a.H, a.Nz, Sh::VW, Sh::NW * Sh::MINB, 2 * Sh::h + 3);
   const long long runs = (long long)g.nstrips * g.nseg * a.Nz;
   const long long blocks = (runs + Sh::NW - 1) / Sh::NW;
   if (blocks > 0x7fffffffLL) return cudaErrorInvalidConfiguration;

@@ -52,7 +52,8 @@ def test_forward_and_adjoint(rihvr, W, H, nz):
     assert rel(g, O.adjoint(op, r.astype(np.float64))) < TOL_F32
 
 
-@pytest.mark.parametrize("W,H,nz,ntv", [(96, 64, 3, 5), (640, 128, 2, 3), (100, 210, 2, 8)])
+@pytest.mark.parametrize("W,H,nz,ntv", [(96, 64, 3, 5), (640, 128, 2, 3), (100, 210, 2, 8), (16, 16, 2, 10),
+                                        (32, 16, 2, 7), (16, 48, 2, 3)])
 def test_tv_prox_rectangular(rihvr, W, H, nz, ntv):
     p = make(rihvr, nz, num_tv_iterations=ntv)
     rng = np.random.default_rng(W + 3 * H)
