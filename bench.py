@@ -259,10 +259,11 @@ def run_ours(args):
     _, b0 = synth.make_hologram(cfg)
     b = synth.translated_frame(b0, frame)
     storage = {"f32": 0, "bf16": 1, "f16": 2}[args.storage]
-    p = rihvr.params_from_config(cfg, record_objective=0, storage=storage)
+    p = rihvr.params_from_config(cfg, record_objective=0, storage=storage, autotune=1 if args.autotune else 0)
     s = rihvr.SparseCompressiveHolo(p, cfg.W, cfg.H)
     V = cfg.voxels()
-    s.setHologram(b)
+    s.setHologram(b)  # tunes launch shapes first with --autotune
+    tuning = s.tuning()
     s.iterate(args.warmup)
 
     def barrier():
@@ -341,7 +342,7 @@ def run_ours(args):
                        "tv_iterations": cfg.num_tv_iterations, "storage": args.storage,
                        "parallelism": f"{ws} independent frames" if ws > 1 else "single frame",
                        "l2": "inputs larger than L2 (volumes of %.1f GB each)" % (V * sbytes / 1e9),
-                       "record_objective": False},
+                       "record_objective": False, "autotune": bool(args.autotune), "launch_shapes": tuning},
             "e2e": e2e, "time_to_objective": tto, "roofline": roofline, "cpu_baseline": cpu,
             "iteration_roofline": {"bytes_per_voxel_iter": 32 + 4 * sbytes,
                                    "achieved": iter_bytes * args.steps / (max_ms / 1e3) / 1e9, "peak": peak,
@@ -368,6 +369,8 @@ def main():
     ap.add_argument("--storage", default="f32", choices=["f32", "bf16", "f16"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--nz", type=int, default=0, help="override the plane count (profiling cases)")
+    ap.add_argument("--no-autotune", dest="autotune", action="store_false",
+                    help="keep the built-in launch shapes (by default they are tuned once before timing)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -79,6 +79,7 @@ typedef struct rihvr_params {
   int max_backtracks;            /* 2 in the reference (sparse_compressive_holo.cu:423) */
   double initial_step;           /* <= 0: 1/num_planes as the reference (:247) */
   int record_objective;          /* 1: objective terms at every iteration */
+  int autotune;                  /* 1: rihvr_set_hologram tunes launch shapes once (rihvr_autotune) */
 } rihvr_params;
 
 /* Per-iteration record (what inverseReconstruct prints, :561-565, plus terms). */
@@ -159,6 +160,24 @@ int rihvr_reconstruct(rihvr_ctx* ctx, double* final_objective);
  * receives frame i's status.  Returns the first nonzero status in frame order. */
 int rihvr_reconstruct_batch(rihvr_ctx* const* ctxs, int n, const float* const* holograms, int is_device,
                             double* final_objectives, int* statuses);
+
+/* Launch-shape autotuner (no reference counterpart).  Times the candidate
+ * shapes of the passes that have a free parameter on this context's own
+ * buffers - z-chunks of the adjoint column pass, z-chunks of the forward
+ * column pass, runs per plane of the streaming TV prox and streaming versus
+ * tiled TV prox - and keeps the fastest.  Results are cached per process for
+ * the plane size, plane count, TV iterations, mode, storage and objective
+ * recording, so later contexts of the same shape reuse them.  Safe between
+ * iterations (only scratch buffers are written).  Tuned shapes may change the
+ * order of the FP32 partial sums, hence the last bits of the sums; with
+ * autotune off the shapes are fixed.  best_ms (may be NULL) receives the sum
+ * of the chosen passes' times in milliseconds. */
+int rihvr_autotune(rihvr_ctx* ctx, double* best_ms);
+
+/* The launch shapes in use: z-chunks of the adjoint and forward column passes,
+ * runs per plane of the streaming TV prox and the TV kernel (1 tiled,
+ * 2 streaming); 0 means the built-in choice.  Any pointer may be NULL. */
+int rihvr_tuning(const rihvr_ctx* ctx, int* adj_chunks, int* fwd_chunks, int* tv_runs, int* tv_kernel);
 
 /* Restart from x = 0 without changing the hologram. */
 int rihvr_reset(rihvr_ctx* ctx);

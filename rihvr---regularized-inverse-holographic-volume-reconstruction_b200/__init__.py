@@ -56,7 +56,7 @@ class RihvrParams(ctypes.Structure):
         ("faithful", ctypes.c_int),
         ("max_backtracks", ctypes.c_int),
         ("initial_step", ctypes.c_double),
-        ("record_objective", ctypes.c_int),
+        ("record_objective", ctypes.c_int), ("autotune", ctypes.c_int),
     ]
 
 
@@ -92,7 +92,8 @@ class FileParams(ctypes.Structure):
 # every symbol include/rihvr.h declares
 EXPORTED = (
     "rihvr_params_default", "rihvr_read_param_file", "rihvr_plane_list", "rihvr_create", "rihvr_destroy",
-    "rihvr_set_hologram", "rihvr_reconstruct", "rihvr_reconstruct_batch", "rihvr_reset", "rihvr_iterate",
+    "rihvr_set_hologram", "rihvr_reconstruct", "rihvr_reconstruct_batch", "rihvr_autotune", "rihvr_tuning", "rihvr_reset",
+    "rihvr_iterate",
     "rihvr_iterate_timed",
     "rihvr_iteration_count", "rihvr_objective", "rihvr_get_iterations", "rihvr_get_plane", "rihvr_get_volume",
     "rihvr_get_estimate", "rihvr_get_residual", "rihvr_forward", "rihvr_adjoint", "rihvr_prox_step",
@@ -137,6 +138,8 @@ def load_library(path: str = LIB_PATH):
     L.rihvr_set_hologram.argtypes = [vp, vp, ip]
     L.rihvr_reconstruct.argtypes = [vp, P(ctypes.c_double)]
     L.rihvr_reconstruct_batch.argtypes = [P(vp), ip, P(vp), ip, P(ctypes.c_double), P(ctypes.c_int)]
+    L.rihvr_autotune.argtypes = [vp, P(ctypes.c_double)]
+    L.rihvr_tuning.argtypes = [vp, P(ctypes.c_int), P(ctypes.c_int), P(ctypes.c_int), P(ctypes.c_int)]
     L.rihvr_reset.argtypes = [vp]
     L.rihvr_iterate.argtypes = [vp, ip]
     L.rihvr_iterate_timed.argtypes = [vp, ip, fp]
@@ -332,6 +335,19 @@ class SparseCompressiveHolo:
         if b.shape != (self.height, self.width):
             raise ValueError(f"hologram shape {b.shape} != {(self.height, self.width)}")
         _check(self._L.rihvr_set_hologram(self._h, _ptr(b), 0), "rihvr_set_hologram")
+
+    def autotune(self) -> float:
+        """Tune launch shapes on this context (rihvr_autotune); returns the
+        chosen passes' total time in ms."""
+        ms = ctypes.c_double()
+        _check(self._L.rihvr_autotune(self._h, ctypes.byref(ms)), "rihvr_autotune")
+        return ms.value
+
+    def tuning(self) -> dict:
+        """Launch shapes in use (rihvr_tuning); 0 = built-in choice."""
+        v = [ctypes.c_int() for _ in range(4)]
+        _check(self._L.rihvr_tuning(self._h, *[ctypes.byref(x) for x in v]), "rihvr_tuning")
+        return dict(zip(("adj_chunks", "fwd_chunks", "tv_runs", "tv_kernel"), (x.value for x in v)))
 
     def inverseReconstruct(self, b: np.ndarray | None = None) -> float:
         if b is not None:

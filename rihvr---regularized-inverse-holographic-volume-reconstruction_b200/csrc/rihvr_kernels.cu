@@ -567,13 +567,13 @@ static bool plane_stack_map(CUtensorMap* m, void* base, int n, int nz, int cc, i
 
 template <int N>
 static cudaError_t adj_col_n(const float2* Rs, const double* cturn, const double* zlist, float2* U, int W,
-                             int z0, int z1, cudaStream_t st) {
+                             int z0, int z1, cudaStream_t st, int chunks_hint) {
   using Lay = ColLayout<N>;
   const int nz = z1 - z0;
   if (nz <= 0) return cudaSuccess;
   const int strips = col_strips<N>(W);
   const int target = 8 * num_sms();
-  int chunks = (target + strips - 1) / strips;
+  int chunks = chunks_hint > 0 ? chunks_hint : (target + strips - 1) / strips;
   if (chunks > nz) chunks = nz;
   if (chunks < 1) chunks = 1;
   const int zpb = (nz + chunks - 1) / chunks;
@@ -597,12 +597,12 @@ static cudaError_t adj_col_n(const float2* Rs, const double* cturn, const double
 }
 
 static cudaError_t launch_adj_col_fast(const float2* Rs, const double* cturn, const double* zlist, float2* U, int W,
-                                      int H, int z0, int z1, cudaStream_t st) {
+                                      int H, int z0, int z1, cudaStream_t st, int chunks_hint) {
   if (W != H) return cudaErrorInvalidValue;
   switch (H) {
 #define RIHVR_CASE(NN) \
   case NN:             \
-    return adj_col_n<NN>(Rs, cturn, zlist, U, W, z0, z1, st);
+    return adj_col_n<NN>(Rs, cturn, zlist, U, W, z0, z1, st, chunks_hint);
     RIHVR_FOR_EACH_SIZE(RIHVR_CASE)
 #undef RIHVR_CASE
     default:
@@ -1472,7 +1472,11 @@ static TvsGrid tvs_grid(int W, int H, int Nz, int VW, int warps_per_sm, int warm
 template <typename ST, int NTV, bool NORMS>
 static cudaError_t strip_launch_n(const ProxArgs& a, int* nblocks_out, cudaStream_t st) {
   using Sh = TvwShape<NTV, 2>;
-  const TvsGrid g = tvs_grid(a.W, a.H, a.Nz, Sh::VW, Sh::NW * Sh::MINB, 2 * Sh::h + 3);
+  TvsGrid g = tvs_grid(a.W, a.H, a.Nz, Sh::VW, Sh::NW * Sh::MINB, 2 * Sh::h + 3);
+  if (a.tv_nseg > 0) {  // tuned number of runs per plane
+    g.seg_len = (a.H + min(a.tv_nseg, a.H) - 1) / min(a.tv_nseg, a.H);
+    g.nseg = (a.H + g.seg_len - 1) / g.seg_len;
+  }
   const long long runs = (long long)g.nstrips * g.nseg * a.Nz;
   const long long blocks = (runs + Sh::NW - 1) / Sh::NW;
   if (blocks > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
@@ -1533,7 +1537,7 @@ size_t max_partial_blocks(int W, int H, int Nz) {
 
 cudaError_t launch_prox_tv2d(int storage, const ProxArgs& a, int* nblocks_out, cudaStream_t st) {
   if (a.n_tv < 0 || a.n_tv > 20) return cudaErrorInvalidValue;
-  if (a.n_tv >= 1 && a.n_tv <= kStripNtvMax && tv_stream_enabled()) {
+  if (a.n_tv >= 1 && a.n_tv <= kStripNtvMax && a.tv_kernel != 1 && tv_stream_enabled()) {
     switch (storage) {
       case STORE_BF16: return strip_dispatch<__nv_bfloat162>(a, nblocks_out, st);
       case STORE_F16: return strip_dispatch<__half2>(a, nblocks_out, st);
@@ -2279,8 +2283,8 @@ cudaError_t launch_rows(int inverse, int in_kind, const void* in, int out_kind, 
 }
 
 cudaError_t launch_adj_col(const float2* Rs, const double* cturn, const double* zlist, float2* U, int W, int H,
-                           int z0, int z1, cudaStream_t st) {
-  if (fast_square(W, H)) return launch_adj_col_fast(Rs, cturn, zlist, U, W, H, z0, z1, st);
+                           int z0, int z1, cudaStream_t st, int chunks_hint) {
+  if (fast_square(W, H)) return launch_adj_col_fast(Rs, cturn, zlist, U, W, H, z0, z1, st, chunks_hint);
   const int nz = z1 - z0;
   if (nz <= 0) return cudaSuccess;
   GPlan p;
@@ -2290,7 +2294,7 @@ cudaError_t launch_adj_col(const float2* Rs, const double* cturn, const double* 
   if (!tw) return e;
   const int C = gplan_lines(H, kGColsMax, kGColElems), logc = ilog2(C);
   const int strips = (W + C - 1) / C;
-  int chunks = (8 * num_sms() + strips - 1) / strips;
+  int chunks = chunks_hint > 0 ? chunks_hint : (8 * num_sms() + strips - 1) / strips;
   if (chunks > nz) chunks = nz;
   if (chunks < 1) chunks = 1;
   const int zpb = (nz + chunks - 1) / chunks;

@@ -36,6 +36,10 @@ struct ProxArgs {
   int faithful;       // reference quirks (separable shrink, restart weights)
   int want_norms;     // accumulate L1/TV of p and x
   double* partials;   // [blocks][kNumSums]
+  // tuning knobs (0 = built-in choice): runs per plane of the streaming 2-D TV
+  // prox, and the 2-D TV kernel (1 tiled, 2 streaming)
+  int tv_nseg = 0;
+  int tv_kernel = 0;
 };
 
 bool line_size_supported(int n);
@@ -46,7 +50,7 @@ void set_last_error(const char* msg);
 size_t max_partial_blocks(int W, int H, int Nz);
 
 cudaError_t launch_adj_col(const float2* Rs, const double* cturn, const double* zlist, float2* U, int W,
-                           int H, int z0, int z1, cudaStream_t st);
+                           int H, int z0, int z1, cudaStream_t st, int chunks_hint = 0);
 cudaError_t launch_rows(int inverse, int in_kind, const void* in, int out_kind, void* out, int W,
                         long long nlines, float scale, cudaStream_t st);
 cudaError_t launch_fwd_col(const float2* T, const double* cturn, const double* zlist, float2* Spart, int W,

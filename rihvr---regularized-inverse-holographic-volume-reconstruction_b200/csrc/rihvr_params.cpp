@@ -33,6 +33,7 @@ int rihvr_params_default(rihvr_params* p) {
   p->max_backtracks = 2;
   p->initial_step = 0.0;
   p->record_objective = 1;
+  p->autotune = 0;
   return RIHVR_OK;
 }
 

@@ -15,6 +15,9 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <new>
 #include <string>
 #include <thread>
@@ -67,6 +70,8 @@ const char* kClassNames[K_NUM] = {"adj_col", "adj_row", "prox", "fwd_row", "fwd_
 
 enum Slot { SLOT_PROX = 0, SLOT_FWD = 1, SLOT_MOM = 2, SLOT_NORM = 3, NUM_SLOTS = 4 };
 
+constexpr int kMaxFwdChunks = 16;  // partial spectra the forward column pass may use
+
 }  // namespace
 
 struct rihvr_ctx {
@@ -100,7 +105,10 @@ struct rihvr_ctx {
   double* sums_d = nullptr;
   double* red_scratch = nullptr;
   double* sums_h = nullptr;  // pinned
-  int nchunks = 1;
+  int nchunks = 1;        // z-chunks of the forward column pass (Spart holds kMaxFwdChunks)
+  // launch shapes chosen by the autotuner (0 = built-in choice)
+  int tune_adj_chunks = 0, tune_tv_nseg = 0, tune_tv_kernel = 0;
+  bool tuned = false;
   float2 *X1 = nullptr, *gx = nullptr, *gy = nullptr, *gz = nullptr, *Y = nullptr;  // mode 6
 
   double t = 0, alpha1 = 1, beta = 0, prev_f_resid = 0;
@@ -194,7 +202,7 @@ int reduce_into(rihvr_ctx* c, int nblocks, int slot) {
 int adjoint_volume(rihvr_ctx* c) {
   {
     ProfScope ps(c, K_ADJ_COL);
-    KL(launch_adj_col(c->Rs, c->cturn, c->zlist, c->U, c->W, c->H, 0, c->Nz, c->st));
+    KL(launch_adj_col(c->Rs, c->cturn, c->zlist, c->U, c->W, c->H, 0, c->Nz, c->st, c->tune_adj_chunks));
   }
   {
     ProfScope ps(c, K_ADJ_ROW);
@@ -241,6 +249,8 @@ ProxArgs prox_args(rihvr_ctx* c, double t) {
   a.faithful = c->p.faithful;
   a.want_norms = c->p.record_objective;
   a.partials = c->partials;
+  a.tv_nseg = c->tune_tv_nseg;
+  a.tv_kernel = c->tune_tv_kernel;
   return a;
 }
 
@@ -514,7 +524,7 @@ int rihvr_create(const rihvr_params* params, int width, int height, rihvr_ctx** 
   if (rc == RIHVR_OK) rc = dalloc_t(c, &c->G, c->V);
   if (rc == RIHVR_OK) rc = dalloc_t(c, &c->U, c->V);
   c->nchunks = fwd_col_chunks(width, height, c->Nz);
-  if (rc == RIHVR_OK) rc = dalloc_t(c, &c->Spart, c->HW * c->nchunks);
+  if (rc == RIHVR_OK) rc = dalloc_t(c, &c->Spart, c->HW * kMaxFwdChunks);
   if (rc == RIHVR_OK) rc = dalloc_t(c, &c->S, c->HW);
   if (rc == RIHVR_OK) rc = dalloc_t(c, &c->pc1, c->HW);
   if (rc == RIHVR_OK) rc = dalloc_t(c, &c->pc2, c->HW);
@@ -566,7 +576,159 @@ int rihvr_set_hologram(rihvr_ctx* c, const float* b, int is_device) {
   if (!c || !b) return fail(RIHVR_ERR_INVALID_ARGUMENT, "NULL argument");
   RC(copy_in(c, c->b, b, sizeof(float) * c->HW, is_device));
   c->have_holo = true;
-  return state_reset(c);
+  RC(state_reset(c));
+  if (c->p.autotune && !c->tuned) RC(rihvr_autotune(c, nullptr));
+  return RIHVR_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// Launch shapes tuned per (device, W, H, Nz, n_tv, mode, storage, norms).
+struct TuneKey {
+  int dev, W, H, Nz, ntv, mode, storage, norms;
+  bool operator<(const TuneKey& o) const {
+    return std::tie(dev, W, H, Nz, ntv, mode, storage, norms) <
+           std::tie(o.dev, o.W, o.H, o.Nz, o.ntv, o.mode, o.storage, o.norms);
+  }
+};
+struct TuneVal {
+  int adj_chunks, fwd_chunks, tv_nseg, tv_kernel;
+  double ms;
+};
+std::mutex g_tune_mu;
+std::map<TuneKey, TuneVal> g_tune;
+
+// fastest of three timed launches after one warm-up, in ms
+template <typename F>
+int time_min(rihvr_ctx* c, cudaEvent_t e0, cudaEvent_t e1, F launch, float* best) {
+  RC(launch());
+  *best = 1e30f;
+  for (int r = 0; r < 3; ++r) {
+    CK(cudaEventRecord(e0, c->st));
+    RC(launch());
+    CK(cudaEventRecord(e1, c->st));
+    CK(cudaEventSynchronize(e1));
+    float ms = 0;
+    CK(cudaEventElapsedTime(&ms, e0, e1));
+    *best = std::min(*best, ms);
+  }
+  return RIHVR_OK;
+}
+
+int autotune_run(rihvr_ctx* c, cudaEvent_t e0, cudaEvent_t e1, TuneVal* out) {
+  const int prev_profiling = c->profiling;
+  c->profiling = false;
+  float best;
+  // 1. z-chunks of the adjoint column pass
+  int best_adj = 0;
+  float t_adj = 1e30f;
+  for (int ch : {0, 2, 4, 8, 16, 32}) {
+    if (ch > c->Nz) continue;
+    RC(time_min(c, e0, e1, [&]() -> int {
+      KL(launch_adj_col(c->Rs, c->cturn, c->zlist, c->U, c->W, c->H, 0, c->Nz, c->st, ch));
+      return RIHVR_OK;
+    }, &best));
+    if (best < t_adj * 0.98f) {
+      t_adj = best;
+      best_adj = ch;
+    }
+  }
+  c->tune_adj_chunks = best_adj;
+  // a valid gradient volume for the prox candidates
+  KL(launch_rows(1, ELEM_C32, c->U, ELEM_C32, c->G, c->W, (long long)c->Nz * c->H, 1.0f, c->st));
+  // 2. 2-D TV prox: streaming with 1..8 runs per plane or the built-in count, or tiled
+  float t_tv = 0.f;
+  if (c->mode == 7 && c->p.num_tv_iterations >= 1 && c->p.regularization_TV_param > 0.f) {
+    const int cand[6][2] = {{0, 0}, {2, 1}, {2, 2}, {2, 4}, {2, 8}, {1, 0}};
+    t_tv = 1e30f;
+    int bk = 0, bn = 0;
+    for (const auto& cd : cand) {
+      c->tune_tv_kernel = cd[0];
+      c->tune_tv_nseg = cd[1];
+      ProxArgs a = prox_args(c, c->t);
+      RC(time_min(c, e0, e1, [&]() -> int {
+        int nb = 0;
+        KL(launch_prox_tv2d(c->storage, a, &nb, c->st));
+        return RIHVR_OK;
+      }, &best));
+      if (best < t_tv * 0.98f) {
+        t_tv = best;
+        bk = cd[0];
+        bn = cd[1];
+      }
+    }
+    c->tune_tv_kernel = bk;
+    c->tune_tv_nseg = bn;
+  }
+  // 3. z-chunks of the forward column pass (with the sum of the partial spectra)
+  int best_fwd = c->nchunks;
+  float t_fwd = 1e30f;
+  for (int ch : {c->nchunks, 1, 2, 4, 8, 16}) {
+    if (ch > c->Nz || ch > kMaxFwdChunks) continue;
+    RC(time_min(c, e0, e1, [&]() -> int {
+      KL(launch_fwd_col(c->U, c->cturn, c->zlist, c->Spart, c->W, c->H, 0, c->Nz, ch, c->st));
+      KL(launch_sum_chunks(c->Spart, ch, c->S, (long long)c->HW, c->st));
+      return RIHVR_OK;
+    }, &best));
+    if (best < t_fwd * 0.98f) {
+      t_fwd = best;
+      best_fwd = ch;
+    }
+  }
+  c->nchunks = best_fwd;
+  c->profiling = prev_profiling;
+  *out = TuneVal{c->tune_adj_chunks, c->nchunks, c->tune_tv_nseg, c->tune_tv_kernel,
+                 (double)t_adj + (double)t_tv + (double)t_fwd};
+  return RIHVR_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int rihvr_tuning(const rihvr_ctx* c, int* adj_chunks, int* fwd_chunks, int* tv_runs, int* tv_kernel) {
+  if (!c) return fail(RIHVR_ERR_INVALID_ARGUMENT, "NULL context");
+  if (adj_chunks) *adj_chunks = c->tune_adj_chunks;
+  if (fwd_chunks) *fwd_chunks = c->nchunks;
+  if (tv_runs) *tv_runs = c->tune_tv_nseg;
+  if (tv_kernel) *tv_kernel = c->tune_tv_kernel;
+  return RIHVR_OK;
+}
+
+int rihvr_autotune(rihvr_ctx* c, double* best_ms) {
+  if (!c) return fail(RIHVR_ERR_INVALID_ARGUMENT, "NULL context");
+  const TuneKey key{c->device, c->W, c->H, c->Nz, c->p.num_tv_iterations, c->mode, c->storage,
+                    c->p.record_objective ? 1 : 0};
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    auto it = g_tune.find(key);
+    if (it != g_tune.end()) {
+      c->tune_adj_chunks = it->second.adj_chunks;
+      c->nchunks = it->second.fwd_chunks;
+      c->tune_tv_nseg = it->second.tv_nseg;
+      c->tune_tv_kernel = it->second.tv_kernel;
+      c->tuned = true;
+      if (best_ms) *best_ms = it->second.ms;
+      return RIHVR_OK;
+    }
+  }
+  cudaEvent_t e0, e1;
+  CK(cudaEventCreate(&e0));
+  CK(cudaEventCreate(&e1));
+  TuneVal v{};
+  const int rc = autotune_run(c, e0, e1, &v);
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (rc != RIHVR_OK) return rc;
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    g_tune[key] = v;
+  }
+  c->tuned = true;
+  if (best_ms) *best_ms = v.ms;
+  return RIHVR_OK;
 }
 
 int rihvr_reset(rihvr_ctx* c) {
