@@ -122,14 +122,16 @@ def class_bytes(s: int) -> dict:
 
 # DRAM bytes per voxel that ncu measured for one launch of a kernel class
 # (dram__bytes_read.sum + dram__bytes_write.sum of a 1024 x 1024 x 16-plane
-# capture of `bench.py --nz 16`, divided by its voxels), keyed by (class,
-# stored bytes per voxel).  Scaled by the voxels of a launch, since traffic
-# grows with the planes processed.
+# capture of `bench.py --nz 16 --no-autotune`, 64 planes for the adjoint column
+# pass, divided by its voxels), keyed by (class, stored bytes per voxel).
+# Scaled by the voxels of a launch, since traffic grows with the planes
+# processed.
 MEASURED_TRAFFIC_PER_VOXEL = {
-    ("prox", 8): (454.7e6 + 116.2e6) / (1024 * 1024 * 16),
-    ("fwd_col", 8): (143.7e6 + 18.5e6) / (1024 * 1024 * 16),
-    ("fwd_row", 8): (134.3e6 + 86.4e6) / (1024 * 1024 * 16),
-    ("adj_row", 8): (134.3e6 + 86.7e6) / (1024 * 1024 * 16),
+    ("prox", 8): (462.4e6 + 115.3e6) / (1024 * 1024 * 16),
+    ("fwd_col", 8): (145.2e6 + 19.8e6) / (1024 * 1024 * 16),
+    ("fwd_row", 8): (134.3e6 + 85.1e6) / (1024 * 1024 * 16),
+    ("adj_row", 8): (134.3e6 + 85.6e6) / (1024 * 1024 * 16),
+    ("adj_col", 8): (79.2e6 + 483.9e6) / (1024 * 1024 * 64),
 }
 
 
@@ -359,7 +361,7 @@ def run_ours(args):
            "ms": e2e_ms, "what": "set_hologram (H2D from pinned) + K iterations + estimate and objective (D2H)"}
 
     tto = None
-    if ws == 1 and not args.nz and args.config == "c2":
+    if ws == 1 and not args.nz and args.config == "c2" and args.time_to_objective:
         tto = time_to_objective(rihvr, cfg, b, s, storage, stream, hb)
 
     # roofline of the dominant kernel class
@@ -419,6 +421,8 @@ def main():
     ap.add_argument("--storage", default="f32", choices=["f32", "bf16", "f16"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--nz", type=int, default=0, help="override the plane count (profiling cases)")
+    ap.add_argument("--no-time-to-objective", dest="time_to_objective", action="store_false",
+                    help="skip the time-to-oracle-objective measurement (profiling runs)")
     ap.add_argument("--no-autotune", dest="autotune", action="store_false",
                     help="keep the built-in launch shapes (by default they are tuned once before timing)")
     args = ap.parse_args()
