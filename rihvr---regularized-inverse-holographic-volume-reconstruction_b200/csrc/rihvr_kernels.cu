@@ -768,6 +768,20 @@ __device__ __forceinline__ float2 shrink(float2 v, float T, int faithful) {
 
 __device__ __forceinline__ float cabs2(float2 a) { return a.x * a.x + a.y * a.y; }
 
+// The prox arguments with the step and momentum scalars taken from their
+// device copy when one is given (captured launches, see ProxArgs::dscal).
+__device__ __forceinline__ ProxArgs resolve_scalars(const ProxArgs& a0) {
+  ProxArgs a = a0;
+  if (a0.dscal) {
+    a.beta = __ldg(a0.dscal + 0);
+    a.t = __ldg(a0.dscal + 1);
+    a.mu = __ldg(a0.dscal + 2);
+    a.s = __ldg(a0.dscal + 3);
+    a.thr = __ldg(a0.dscal + 4);
+  }
+  return a;
+}
+
 // Square roots of the objective's norm terms (L1 and TV sums) use the
 // hardware approximation (PTX sqrt.approx.f32, one instruction): they only
 // feed the reported objective, summed over millions of voxels in FP64.
@@ -876,7 +890,8 @@ struct Pair<__half2> {
 };
 
 template <typename ST>
-__global__ void __launch_bounds__(TV_THREADS, 2) k_prox_tv2d(ProxArgs a) {
+__global__ void __launch_bounds__(TV_THREADS, 2) k_prox_tv2d(ProxArgs a0) {
+  const ProxArgs a = resolve_scalars(a0);
   static_assert(TV_CPL == 2, "paired loads assume two columns per lane");
   extern __shared__ float2 smem[];
   float2* s_g = smem;                      // [EH][EW] gradient at load
@@ -1238,7 +1253,8 @@ __device__ __forceinline__ void store_run(ST* p, const float2 (&v)[CPL]) {
 
 template <typename ST, int NTV, bool NORMS, int CPL = 2, int NW = TvwShape<NTV, CPL>::NW,
           int MINB = TvwShape<NTV, CPL>::MINB, int UNR = 4, int PADTO = 4>
-__global__ void __launch_bounds__(32 * NW, MINB) k_prox_tv2d_strip(ProxArgs a, TvsGrid gr) {
+__global__ void __launch_bounds__(32 * NW, MINB) k_prox_tv2d_strip(ProxArgs a0, TvsGrid gr) {
+  const ProxArgs a = resolve_scalars(a0);
   using Sh = TvwShape<NTV, CPL>;
   constexpr int h = Sh::h, HX = Sh::HX, VW = Sh::VW, D = Sh::D, RM = D - 1, F4 = Sh::F4;
   constexpr int QS = F4 * 32;     // float4 between the arrays of a slot
@@ -1574,7 +1590,8 @@ cudaError_t launch_prox_tv2d(int storage, const ProxArgs& a, int* nblocks_out, c
 constexpr int FLAT_THREADS = 256;
 
 template <typename ST>
-__global__ void __launch_bounds__(FLAT_THREADS) k_prox_l1(ProxArgs a) {
+__global__ void __launch_bounds__(FLAT_THREADS) k_prox_l1(ProxArgs a0) {
+  const ProxArgs a = resolve_scalars(a0);
   const size_t HW = (size_t)a.W * a.H, n = HW * a.Nz;
   const ST* P = static_cast<const ST*>(a.P);
   const ST* Pp = static_cast<const ST*>(a.Pprev);
@@ -1702,8 +1719,9 @@ cudaError_t launch_finish_forward(const float2* c, const float* b, float* dnew, 
 // dX = d + beta (d - dY0); dY0 = d; r = dX - b.
 __global__ void __launch_bounds__(FLAT_THREADS) k_holo_momentum(const float* __restrict__ dnew, float* dY0,
                                                                 float* __restrict__ dX, const float* __restrict__ b,
-                                                                float* __restrict__ r, float beta, long long n,
-                                                                double* partials) {
+                                                                float* __restrict__ r, float beta0, long long n,
+                                                                double* partials, const float* __restrict__ dbeta) {
+  const float beta = dbeta ? __ldg(dbeta) : beta0;  // device copy for captured launches
   double acc[kNumSums];
 #pragma unroll
   for (int k = 0; k < kNumSums; ++k) acc[k] = 0.0;
@@ -1720,10 +1738,11 @@ __global__ void __launch_bounds__(FLAT_THREADS) k_holo_momentum(const float* __r
 }
 
 cudaError_t launch_holo_momentum(const float* dnew, float* dY0, float* dX, const float* b, float* r, float beta,
-                                 long long n, double* partials, int* nblocks_out, cudaStream_t st) {
+                                 long long n, double* partials, int* nblocks_out, cudaStream_t st,
+                                 const float* dbeta) {
   const int blocks = flat_blocks((size_t)n);
   *nblocks_out = blocks;
-  k_holo_momentum<<<blocks, FLAT_THREADS, 0, st>>>(dnew, dY0, dX, b, r, beta, n, partials);
+  k_holo_momentum<<<blocks, FLAT_THREADS, 0, st>>>(dnew, dY0, dX, b, r, beta, n, partials, dbeta);
   return cudaGetLastError();
 }
 

@@ -40,6 +40,10 @@ struct ProxArgs {
   // prox, and the 2-D TV kernel (1 tiled, 2 streaming)
   int tv_nseg = 0;
   int tv_kernel = 0;
+  // device copy of (beta, t, mu, s, thr); when set, the 2-D TV and L1 prox
+  // kernels read these instead of the values above, so that a captured
+  // launch picks up each attempt's step and momentum
+  const float* dscal = nullptr;
 };
 
 bool line_size_supported(int n);
@@ -67,7 +71,8 @@ size_t reduce_scratch_doubles();
 cudaError_t launch_finish_forward(const float2* c, const float* b, float* dnew, long long n, double* partials,
                                   int* nblocks_out, cudaStream_t st);
 cudaError_t launch_holo_momentum(const float* dnew, float* dY0, float* dX, const float* b, float* r,
-                                 float beta, long long n, double* partials, int* nblocks_out, cudaStream_t st);
+                                 float beta, long long n, double* partials, int* nblocks_out, cudaStream_t st,
+                                 const float* dbeta = nullptr);
 cudaError_t launch_momentum_norms(int storage, const void* P, const void* Pprev, float beta, int W, int H,
                                   int Nz, int mode, double* partials, int* nblocks_out, cudaStream_t st);
 cudaError_t launch_materialize_x(int storage, const void* P, const void* Pprev, float beta, float2* out,

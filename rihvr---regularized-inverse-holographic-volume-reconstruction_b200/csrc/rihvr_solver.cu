@@ -106,6 +106,17 @@ struct rihvr_ctx {
   double* red_scratch = nullptr;
   double* sums_h = nullptr;  // pinned
   int nchunks = 1;        // z-chunks of the forward column pass (Spart holds kMaxFwdChunks)
+  // Step and momentum scalars of the current attempt: pinned host copy and the
+  // device copy the prox and momentum kernels read ([0..4] beta, t, mu, s, thr;
+  // [8] hologram momentum beta), so that captured graphs replay every attempt.
+  float* scal_d = nullptr;
+  float* scal_h = nullptr;
+  cudaGraphExec_t g_att[2][3] = {};  // [backtrack attempt][index of P_k among the 3 volumes]
+  int g_att_n[2][3] = {};            // kernels in each graph
+  cudaGraphExec_t g_mom = nullptr;
+  int g_mom_n = 0;
+  bool graphs = true;                // cleared when a capture fails
+  bool warm = false;                 // one iteration ran eagerly (attributes, tables)
   // launch shapes chosen by the autotuner (0 = built-in choice)
   int tune_adj_chunks = 0, tune_tv_nseg = 0, tune_tv_kernel = 0;
   bool tuned = false;
@@ -230,7 +241,7 @@ int forward_volume(rihvr_ctx* c, int kind, const void* vol) {
   return reduce_into(c, nb, SLOT_FWD);
 }
 
-ProxArgs prox_args(rihvr_ctx* c, double t) {
+ProxArgs prox_args(rihvr_ctx* c, double t, bool device_scalars = false) {
   ProxArgs a;
   a.P = c->vol[c->iCur];
   a.Pprev = c->vol[c->iPrev];
@@ -251,17 +262,19 @@ ProxArgs prox_args(rihvr_ctx* c, double t) {
   a.partials = c->partials;
   a.tv_nseg = c->tune_tv_nseg;
   a.tv_kernel = c->tune_tv_kernel;
+  // proximalFusedLasso2d shrinks only if l1 > 0 (:3715)
+  if (c->mode == 7 && !(c->p.regularization_param > 0.f)) a.thr = 0.f;
+  if (device_scalars && c->mode != 6) a.dscal = c->scal_d;
   return a;
 }
 
 // P_{k+1} = prox(x_k - t G) for the active mode; sums into SLOT_PROX.
-int prox_volume(rihvr_ctx* c, double t) {
-  ProxArgs a = prox_args(c, t);
+int prox_volume(rihvr_ctx* c, double t, bool device_scalars = false) {
+  ProxArgs a = prox_args(c, t, device_scalars);
   int nb = 0;
   ProfScope ps(c, K_PROX);
   if (c->mode == 7) {
-    // proximalFusedLasso2d (:3652-3732); block_soft_threshold only if l1 > 0 (:3715)
-    if (!(c->p.regularization_param > 0.f)) a.thr = 0.f;
+    // proximalFusedLasso2d (:3652-3732)
     KL(launch_prox_tv2d(c->storage, a, &nb, c->st));
   } else if (c->mode == 5) {
     KL(launch_prox_l1(c->storage, a, &nb, c->st));
@@ -333,17 +346,92 @@ int norms_at_x(rihvr_ctx* c, double* l1x, double* tvx, double* nnz = nullptr) {
   return RIHVR_OK;
 }
 
-// One FISTA iteration (:299-611).
+// GPU work of one attempt: the attempt's scalars to the device, the gradient
+// (first attempt of an iteration), the prox, the forward operator and the sums
+// back to pinned host memory.  No host synchronisation inside: the same
+// sequence is launched eagerly or captured into a graph.
+int enqueue_attempt(rihvr_ctx* c, bool with_adjoint) {
+  CK(cudaMemcpyAsync(c->scal_d, c->scal_h, 5 * sizeof(float), cudaMemcpyHostToDevice, c->st));
+  if (with_adjoint) RC(adjoint_volume(c));
+  RC(prox_volume(c, c->t, true));
+  RC(forward_volume(c, elem_kind(c->storage), c->vol[c->iNew]));
+  CK(cudaMemcpyAsync(c->sums_h, c->sums_d, sizeof(double) * kNumSums * NUM_SLOTS, cudaMemcpyDeviceToHost, c->st));
+  return RIHVR_OK;
+}
+
+// Hologram momentum, residual at the new momentum point and its spectrum.
+int enqueue_momentum(rihvr_ctx* c) {
+  CK(cudaMemcpyAsync(c->scal_d + 8, c->scal_h + 8, sizeof(float), cudaMemcpyHostToDevice, c->st));
+  int nb = 0;
+  KL(launch_holo_momentum(c->dnew, c->dY0, c->dX, c->b, c->r, c->scal_h[8], (long long)c->HW, c->partials, &nb,
+                          c->st, c->scal_d + 8));
+  RC(reduce_into(c, nb, SLOT_MOM));
+  RC(residual_spectrum(c));
+  CK(cudaMemcpyAsync(c->sums_h, c->sums_d, sizeof(double) * kNumSums * NUM_SLOTS, cudaMemcpyDeviceToHost, c->st));
+  return RIHVR_OK;
+}
+
+void drop_graphs(rihvr_ctx* c) {
+  for (auto& row : c->g_att)
+    for (auto& g : row)
+      if (g) {
+        cudaGraphExecDestroy(g);
+        g = nullptr;
+      }
+  if (c->g_mom) cudaGraphExecDestroy(c->g_mom);
+  c->g_mom = nullptr;
+}
+
+bool use_graphs(const rihvr_ctx* c) { return c->graphs && c->warm && !c->profiling && c->mode != 6; }
+
+// Run `enqueue` as a CUDA graph (captured on first use) or eagerly.  A failed
+// capture turns graphs off for the context and runs the work eagerly.
+template <typename F>
+int run_captured(rihvr_ctx* c, cudaGraphExec_t* g, int* nkernels, F enqueue) {
+  if (!use_graphs(c)) return enqueue();
+  if (!*g) {
+    const long long l0 = c->launches;
+    cudaGraph_t graph = nullptr;
+    CK(cudaStreamBeginCapture(c->st, cudaStreamCaptureModeThreadLocal));
+    const int rc = enqueue();
+    cudaError_t e = cudaStreamEndCapture(c->st, &graph);
+    if (rc == RIHVR_OK && e == cudaSuccess) e = cudaGraphInstantiate(g, graph, 0);
+    if (graph) cudaGraphDestroy(graph);
+    const int n = (int)(c->launches - l0);
+    c->launches = l0;
+    if (rc != RIHVR_OK || e != cudaSuccess) {
+      *g = nullptr;
+      cudaGetLastError();
+      c->graphs = false;
+      return enqueue();
+    }
+    *nkernels = n;
+  }
+  CK(cudaGraphLaunch(*g, c->st));
+  c->launches += *nkernels;
+  return RIHVR_OK;
+}
+
+// One FISTA iteration (:299-611): one host synchronisation per attempt and one
+// after the momentum step.
 int one_iteration(rihvr_ctx* c) {
   double alpha0 = c->alpha1;
-  RC(adjoint_volume(c));
   int bt = 0;
   double f_resid = 0, lim = 0, ratio = 0;
   const double* sp = c->sums_h + SLOT_PROX * kNumSums;
   for (;;) {
-    RC(prox_volume(c, c->t));
-    RC(forward_volume(c, elem_kind(c->storage), c->vol[c->iNew]));
-    RC(fetch_sums(c));
+    {
+      const ProxArgs a = prox_args(c, c->t);
+      c->scal_h[0] = a.beta;
+      c->scal_h[1] = a.t;
+      c->scal_h[2] = a.mu;
+      c->scal_h[3] = a.s;
+      c->scal_h[4] = a.thr;
+    }
+    const int first = bt == 0 ? 0 : 1;
+    RC(run_captured(c, &c->g_att[first][c->iCur], &c->g_att_n[first][c->iCur],
+                    [&]() { return enqueue_attempt(c, bt == 0); }));
+    CK(cudaStreamSynchronize(c->st));
     if (bt == 0 && c->p.record_objective) settle_x_terms(c, sp);
     f_resid = 0.5 * c->sums_h[SLOT_FWD * kNumSums + SUM_RR];
     lim = sp[SUM_LIM1] + sp[SUM_LIM2] / (2.0 * c->t);
@@ -371,24 +459,22 @@ int one_iteration(rihvr_ctx* c) {
   rec.beta = beta;
   rec.restarted = restarted ? 1 : 0;
   // hologram momentum, residual at the new momentum point and its spectrum
-  int nb = 0;
-  KL(launch_holo_momentum(c->dnew, c->dY0, c->dX, c->b, c->r, (float)beta, (long long)c->HW, c->partials, &nb,
-                          c->st));
-  RC(reduce_into(c, nb, SLOT_MOM));
-  RC(residual_spectrum(c));
+  c->scal_h[8] = (float)beta;
+  RC(run_captured(c, &c->g_mom, &c->g_mom_n, [&]() { return enqueue_momentum(c); }));
+  CK(cudaStreamSynchronize(c->st));
   // rotate: P_{k-1} <- P_k, P_k <- P_{k+1}
   const int old_prev = c->iPrev;
   c->iPrev = c->iCur;
   c->iCur = c->iNew;
   c->iNew = old_prev;
   c->beta = beta;
-  RC(fetch_sums(c));
   c->prev_f_resid = 0.5 * c->sums_h[SLOT_MOM * kNumSums + SUM_RR];
   rec.f_resid_x = c->prev_f_resid;
   rec.f_x = rec.f_resid_x;
   c->log.push_back(rec);
   c->pending_x = (int)c->log.size() - 1;
   c->it++;
+  c->warm = true;
   return RIHVR_OK;
 }
 
@@ -550,6 +636,10 @@ int rihvr_create(const rihvr_params* params, int width, int height, rihvr_ctx** 
   if (rc != RIHVR_OK) return cleanup(rc);
   if (cudaMallocHost(&c->sums_h, sizeof(double) * kNumSums * NUM_SLOTS) != cudaSuccess)
     return cleanup(fail(RIHVR_ERR_OUT_OF_MEMORY, "cudaMallocHost failed"));
+  if (cudaMallocHost(&c->scal_h, 16 * sizeof(float)) != cudaSuccess)
+    return cleanup(fail(RIHVR_ERR_OUT_OF_MEMORY, "cudaMallocHost failed"));
+  std::memset(c->scal_h, 0, 16 * sizeof(float));
+  if (dalloc_t(c, &c->scal_d, 16) != RIHVR_OK) return cleanup(RIHVR_ERR_OUT_OF_MEMORY);
   std::vector<double> ct;
   phase_turns(height, width, (double)params->resolution, (double)params->wavelength, ct);
   std::vector<double> zl((size_t)c->Nz);
@@ -565,8 +655,10 @@ int rihvr_create(const rihvr_params* params, int width, int height, rihvr_ctx** 
 void rihvr_destroy(rihvr_ctx* c) {
   if (!c) return;
   if (c->st) cudaStreamSynchronize(c->st);
+  drop_graphs(c);
   for (void* p : c->allocs) cudaFree(p);
   if (c->sums_h) cudaFreeHost(c->sums_h);
+  if (c->scal_h) cudaFreeHost(c->scal_h);
   for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
   if (c->st) cudaStreamDestroy(c->st);
   delete c;
@@ -618,6 +710,7 @@ int time_min(rihvr_ctx* c, cudaEvent_t e0, cudaEvent_t e1, F launch, float* best
 }
 
 int autotune_run(rihvr_ctx* c, cudaEvent_t e0, cudaEvent_t e1, TuneVal* out) {
+  drop_graphs(c);  // captured launches carry the old shapes
   const int prev_profiling = c->profiling;
   c->profiling = false;
   float best;
@@ -705,6 +798,7 @@ int rihvr_autotune(rihvr_ctx* c, double* best_ms) {
     std::lock_guard<std::mutex> lock(g_tune_mu);
     auto it = g_tune.find(key);
     if (it != g_tune.end()) {
+      drop_graphs(c);
       c->tune_adj_chunks = it->second.adj_chunks;
       c->nchunks = it->second.fwd_chunks;
       c->tune_tv_nseg = it->second.tv_nseg;
