@@ -182,6 +182,15 @@ int rihvr_tuning(const rihvr_ctx* ctx, int* adj_chunks, int* fwd_chunks, int* tv
 /* Restart from x = 0 without changing the hologram. */
 int rihvr_reset(rihvr_ctx* ctx);
 
+/* Restart from a given volume instead of x = 0 (a warm start; the reference
+ * always starts from 0, sparse_compressive_holo.cu:273): x0 is num_planes x
+ * height x width complex interleaved (host or device), stored in the
+ * context's storage type.  The momentum restarts (P_{k-1} = P_k = x0, beta =
+ * 0), the estimated hologram, residual and step size are those of x0, and the
+ * iteration log is cleared.  Typical sources: the previous frame of a time
+ * series, or a network's estimate. */
+int rihvr_set_initial_volume(rihvr_ctx* ctx, const float* x0, int is_device);
+
 /* Continue the current solve by n iterations (the loop body :299-611). */
 int rihvr_iterate(rihvr_ctx* ctx, int n);
 

@@ -93,6 +93,7 @@ class FileParams(ctypes.Structure):
 EXPORTED = (
     "rihvr_params_default", "rihvr_read_param_file", "rihvr_plane_list", "rihvr_create", "rihvr_destroy",
     "rihvr_set_hologram", "rihvr_reconstruct", "rihvr_reconstruct_batch", "rihvr_autotune", "rihvr_tuning", "rihvr_reset",
+    "rihvr_set_initial_volume",
     "rihvr_iterate",
     "rihvr_iterate_timed",
     "rihvr_iteration_count", "rihvr_objective", "rihvr_get_iterations", "rihvr_get_plane", "rihvr_get_volume",
@@ -141,6 +142,7 @@ def load_library(path: str = LIB_PATH):
     L.rihvr_autotune.argtypes = [vp, P(ctypes.c_double)]
     L.rihvr_tuning.argtypes = [vp, P(ctypes.c_int), P(ctypes.c_int), P(ctypes.c_int), P(ctypes.c_int)]
     L.rihvr_reset.argtypes = [vp]
+    L.rihvr_set_initial_volume.argtypes = [vp, vp, ip]
     L.rihvr_iterate.argtypes = [vp, ip]
     L.rihvr_iterate_timed.argtypes = [vp, ip, fp]
     L.rihvr_iteration_count.argtypes = [vp]
@@ -335,6 +337,14 @@ class SparseCompressiveHolo:
         if b.shape != (self.height, self.width):
             raise ValueError(f"hologram shape {b.shape} != {(self.height, self.width)}")
         _check(self._L.rihvr_set_hologram(self._h, _ptr(b), 0), "rihvr_set_hologram")
+
+    def setInitialVolume(self, x0: np.ndarray):
+        """Warm start (rihvr_set_initial_volume): continue FISTA from x0
+        instead of 0; the hologram must be set."""
+        x0 = np.ascontiguousarray(x0, dtype=np.complex64)
+        if x0.shape != (self.depth, self.height, self.width):
+            raise ValueError("volume shape mismatch")
+        _check(self._L.rihvr_set_initial_volume(self._h, _ptr(x0), 0), "rihvr_set_initial_volume")
 
     def autotune(self) -> float:
         """Tune launch shapes on this context (rihvr_autotune); returns the

@@ -938,6 +938,26 @@ int rihvr_initial_estimate(rihvr_ctx* c, float* out, int is_device) {
   return state_reset(c);
 }
 
+int rihvr_set_initial_volume(rihvr_ctx* c, const float* x0, int is_device) {
+  if (!c || !x0) return fail(RIHVR_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (!c->have_holo) return fail(RIHVR_ERR_MISSING_DATA, "no hologram set");
+  RC(state_reset(c));
+  // P_{k-1} = P_k = x0 in the storage type, beta = 0
+  RC(copy_in(c, c->U, x0, sizeof(float2) * c->V, is_device));
+  KL(launch_store_volume(c->storage, c->U, c->vol[c->iCur], (long long)c->V, c->st));
+  CK(cudaMemcpyAsync(c->vol[c->iPrev], c->vol[c->iCur], c->esize * c->V, cudaMemcpyDeviceToDevice, c->st));
+  // the estimated hologram of the stored x0, then the momentum step with beta = 0:
+  // d(x) = d(P_k) = A x0, r = d - b and its spectrum
+  RC(forward_volume(c, elem_kind(c->storage), c->vol[c->iCur]));
+  int nb = 0;
+  KL(launch_holo_momentum(c->dnew, c->dY0, c->dX, c->b, c->r, 0.f, (long long)c->HW, c->partials, &nb, c->st));
+  RC(reduce_into(c, nb, SLOT_MOM));
+  RC(residual_spectrum(c));
+  RC(fetch_sums(c));
+  c->prev_f_resid = 0.5 * c->sums_h[SLOT_MOM * kNumSums + SUM_RR];
+  return RIHVR_OK;
+}
+
 int rihvr_get_iterations(const rihvr_ctx* c, rihvr_iter_record* out, int max_records, int* n_out) {
   if (!c || !n_out) return fail(RIHVR_ERR_INVALID_ARGUMENT, "NULL argument");
   const int n = (int)c->log.size();
