@@ -139,9 +139,21 @@ struct RowLayout {
   static constexpr size_t SMEM_BYTES = sizeof(float2) * SMEM;
 };
 
-template <int N, bool INV>
-__global__ void __launch_bounds__(kRowThreads) k_rows(int in_kind, const void* __restrict__ in, int out_kind,
-                                                     void* __restrict__ out, long long nlines, float scale) {
+// element of kind IN (compile time) as a complex value
+template <int IN>
+__device__ __forceinline__ float2 load_as(const void* p, size_t i) {
+  if constexpr (IN == ELEM_R32) return make_float2(static_cast<const float*>(p)[i], 0.f);
+  else if constexpr (IN == ELEM_STORE_BF16) return Store<__nv_bfloat162>::ld(static_cast<const __nv_bfloat162*>(p) + i);
+  else if constexpr (IN == ELEM_STORE_F16) return Store<__half2>::ld(static_cast<const __half2*>(p) + i);
+  else return static_cast<const float2*>(p)[i];
+}
+
+// The input element kind is a template parameter: with it known at compile
+// time the N2 loads of a thread issue back to back (a run-time kind switch
+// around each load serialises them).  Output is complex FP32.
+template <int N, bool INV, int IN>
+__global__ void __launch_bounds__(kRowThreads) k_rows(const void* __restrict__ in, float2* __restrict__ out,
+                                                     long long nlines, float scale) {
   using C = LineCfg<N>;
   using Lay = RowLayout<N>;
   constexpr int N1 = C::N1, N2 = C::N2, M = C::M, LD = C::LD;
@@ -154,7 +166,7 @@ __global__ void __launch_bounds__(kRowThreads) k_rows(int in_kind, const void* _
   const size_t base = (size_t)L * N;
   float2 v[N2];
 #pragma unroll
-  for (int n2 = 0; n2 < N2; ++n2) v[n2] = load_elem(in_kind, in, base + t + N1 * n2);
+  for (int n2 = 0; n2 < N2; ++n2) v[n2] = load_as<IN>(in, base + t + N1 * n2);
   reg_fft<N2, INV>(v);
   line_twiddle<N, N2, INV>(v, t);
   float2* sl = sm + li * Lay::LS;
@@ -170,28 +182,38 @@ __global__ void __launch_bounds__(kRowThreads) k_rows(int in_kind, const void* _
 #pragma unroll
     for (int j = 0; j < M; ++j)
 #pragma unroll
-      for (int k1 = 0; k1 < N1; ++k1)
-        store_elem(out_kind, out, base + t + N1 * j + N2 * k1, cscale(v[j * N1 + k1], scale));
+      for (int k1 = 0; k1 < N1; ++k1) out[base + t + N1 * j + N2 * k1] = cscale(v[j * N1 + k1], scale);
   }
+}
+
+template <int N, bool INV, int IN>
+static cudaError_t rows_launch(const void* in, float2* out, long long nlines, float scale, cudaStream_t st) {
+  using Lay = RowLayout<N>;
+  const long long blocks = (nlines + Lay::LPB - 1) / Lay::LPB;
+  if (blocks <= 0) return cudaSuccess;
+  cudaError_t e = allow_smem(k_rows<N, INV, IN>, Lay::SMEM_BYTES);
+  if (e != cudaSuccess) return e;
+  k_rows<N, INV, IN><<<(unsigned)blocks, kRowThreads, Lay::SMEM_BYTES, st>>>(in, out, nlines, scale);
+  return cudaGetLastError();
 }
 
 template <int N>
 static cudaError_t rows_n(int inverse, int in_kind, const void* in, int out_kind, void* out, long long nlines,
                           float scale, cudaStream_t st) {
-  using Lay = RowLayout<N>;
-  const long long blocks = (nlines + Lay::LPB - 1) / Lay::LPB;
-  if (blocks <= 0) return cudaSuccess;
-  cudaError_t e;
+  if (out_kind != ELEM_C32) return cudaErrorInvalidValue;
+  float2* o = static_cast<float2*>(out);
   if (inverse) {
-    e = allow_smem(k_rows<N, true>, Lay::SMEM_BYTES);
-    if (e != cudaSuccess) return e;
-    k_rows<N, true><<<(unsigned)blocks, kRowThreads, Lay::SMEM_BYTES, st>>>(in_kind, in, out_kind, out, nlines, scale);
-  } else {
-    e = allow_smem(k_rows<N, false>, Lay::SMEM_BYTES);
-    if (e != cudaSuccess) return e;
-    k_rows<N, false><<<(unsigned)blocks, kRowThreads, Lay::SMEM_BYTES, st>>>(in_kind, in, out_kind, out, nlines, scale);
+    if (in_kind != ELEM_C32 && in_kind != ELEM_STORE_F32) return cudaErrorInvalidValue;
+    return rows_launch<N, true, ELEM_C32>(in, o, nlines, scale, st);
   }
-  return cudaGetLastError();
+  switch (in_kind) {
+    case ELEM_C32:
+    case ELEM_STORE_F32: return rows_launch<N, false, ELEM_C32>(in, o, nlines, scale, st);
+    case ELEM_R32: return rows_launch<N, false, ELEM_R32>(in, o, nlines, scale, st);
+    case ELEM_STORE_BF16: return rows_launch<N, false, ELEM_STORE_BF16>(in, o, nlines, scale, st);
+    case ELEM_STORE_F16: return rows_launch<N, false, ELEM_STORE_F16>(in, o, nlines, scale, st);
+    default: return cudaErrorInvalidValue;
+  }
 }
 
 static cudaError_t launch_rows_fast(int inverse, int in_kind, const void* in, int out_kind, void* out, int W,
