@@ -78,37 +78,6 @@ static cudaError_t allow_smem(K kernel, size_t bytes) {
   return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
-// ---------------------------------------------------------------------------
-// element access by kind (uniform branches)
-// ---------------------------------------------------------------------------
-__device__ __forceinline__ float2 load_elem(int kind, const void* p, size_t i) {
-  switch (kind) {
-    case ELEM_R32:
-      return make_float2(static_cast<const float*>(p)[i], 0.f);
-    case ELEM_STORE_BF16:
-      return Store<__nv_bfloat162>::ld(static_cast<const __nv_bfloat162*>(p) + i);
-    case ELEM_STORE_F16:
-      return Store<__half2>::ld(static_cast<const __half2*>(p) + i);
-    default:
-      return static_cast<const float2*>(p)[i];
-  }
-}
-__device__ __forceinline__ void store_elem(int kind, void* p, size_t i, float2 v) {
-  switch (kind) {
-    case ELEM_R32:
-      static_cast<float*>(p)[i] = v.x;
-      break;
-    case ELEM_STORE_BF16:
-      Store<__nv_bfloat162>::st(static_cast<__nv_bfloat162*>(p) + i, v);
-      break;
-    case ELEM_STORE_F16:
-      Store<__half2>::st(static_cast<__half2*>(p) + i, v);
-      break;
-    default:
-      static_cast<float2*>(p)[i] = v;
-  }
-}
-
 template <int N1, int N2, bool INV>
 __device__ __forceinline__ void stage_b_dft(float2 (&w)[N2]) {
   constexpr int M = N2 / N1;
@@ -2058,6 +2027,12 @@ bool generic_size_supported(int n) {
   return gplan_make(n, &p);
 }
 
+static int ilog2(int c) {
+  int l = 0;
+  while ((1 << l) < c) ++l;
+  return l;
+}
+
 // lines per block: the largest power of two with n C <= budget, capped
 static int gplan_lines(int n, int cap, int budget = kGElems) {
   int c = 1;
@@ -2151,9 +2126,9 @@ __device__ float2* gfft(float2* b0, float2* b1, int logc, const GPlan& p, const 
   return src;
 }
 
-template <bool INV>
-__global__ void __launch_bounds__(kGThreads) k_grows(GPlan p, const float2* __restrict__ tw, int in_kind,
-                                                     const void* __restrict__ in, int out_kind, void* __restrict__ out,
+template <bool INV, int IN>
+__global__ void __launch_bounds__(kGThreads) k_grows(GPlan p, const float2* __restrict__ tw,
+                                                     const void* __restrict__ in, float2* __restrict__ out,
                                                      long long nlines, float scale, int logc) {
   extern __shared__ __align__(128) float2 gbuf[];
   const int n = p.n, C = 1 << logc;
@@ -2162,14 +2137,26 @@ __global__ void __launch_bounds__(kGThreads) k_grows(GPlan p, const float2* __re
   const int nl = (int)min((long long)C, nlines - l0);
   for (int e = threadIdx.x; e < n * C; e += kGThreads) {
     const int c = e / n, k = e - c * n;  // consecutive threads, consecutive elements of a line
-    gbuf[(k << logc) + c] = c < nl ? load_elem(in_kind, in, (size_t)(l0 + c) * n + k) : make_float2(0.f, 0.f);
+    gbuf[(k << logc) + c] = c < nl ? load_as<IN>(in, (size_t)(l0 + c) * n + k) : make_float2(0.f, 0.f);
   }
   __syncthreads();
   const float2* res = gfft<INV>(gbuf, gb1, logc, p, tw);
   for (int e = threadIdx.x; e < n * C; e += kGThreads) {
     const int c = e / n, k = e - c * n;
-    if (c < nl) store_elem(out_kind, out, (size_t)(l0 + c) * n + k, cscale(res[(k << logc) + c], scale));
+    if (c < nl) out[(size_t)(l0 + c) * n + k] = cscale(res[(k << logc) + c], scale);
   }
+}
+
+template <bool INV, int IN>
+static cudaError_t grows_launch(const GPlan& p, const float2* tw, const void* in, float2* out, long long nlines,
+                                float scale, int C, cudaStream_t st) {
+  const size_t smem = 2 * sizeof(float2) * (size_t)p.n * C;
+  const long long blocks = (nlines + C - 1) / C;
+  if (blocks <= 0) return cudaSuccess;
+  cudaError_t e = allow_smem(k_grows<INV, IN>, smem);
+  if (e != cudaSuccess) return e;
+  k_grows<INV, IN><<<(unsigned)blocks, kGThreads, smem, st>>>(p, tw, in, out, nlines, scale, ilog2(C));
+  return cudaGetLastError();
 }
 
 // adjoint column pass: U_z(:, x) = IDFT_y(conj(H'_z(:, x)) Rs(:, x)) for the
@@ -2274,12 +2261,6 @@ __global__ void __launch_bounds__(kGThreads) k_gplane_col(GPlan p, const float2*
   }
 }
 
-static int ilog2(int c) {
-  int l = 0;
-  while ((1 << l) < c) ++l;
-  return l;
-}
-
 // columns per block of the generic column passes: 8-byte elements, 16 columns
 // make 128-byte row segments
 constexpr int kGColsMax = 16;
@@ -2303,24 +2284,26 @@ int fwd_col_chunks(int W, int H, int Nz) {
 cudaError_t launch_rows(int inverse, int in_kind, const void* in, int out_kind, void* out, int W, long long nlines,
                         float scale, cudaStream_t st) {
   if (line_size_supported(W)) return launch_rows_fast(inverse, in_kind, in, out_kind, out, W, nlines, scale, st);
+  if (out_kind != ELEM_C32) return cudaErrorInvalidValue;
   GPlan p;
   if (!gplan_make(W, &p)) return cudaErrorInvalidValue;
   cudaError_t e;
   const float2* tw = gtwiddles(W, st, &e);
   if (!tw) return e;
-  const int C = gplan_lines(W, 64), logc = ilog2(C);
-  const size_t smem = 2 * sizeof(float2) * (size_t)W * C;
-  const long long blocks = (nlines + C - 1) / C;
+  const int C = gplan_lines(W, 64);
+  float2* o = static_cast<float2*>(out);
   if (inverse) {
-    e = allow_smem(k_grows<true>, smem);
-    if (e != cudaSuccess) return e;
-    k_grows<true><<<(unsigned)blocks, kGThreads, smem, st>>>(p, tw, in_kind, in, out_kind, out, nlines, scale, logc);
-  } else {
-    e = allow_smem(k_grows<false>, smem);
-    if (e != cudaSuccess) return e;
-    k_grows<false><<<(unsigned)blocks, kGThreads, smem, st>>>(p, tw, in_kind, in, out_kind, out, nlines, scale, logc);
+    if (in_kind != ELEM_C32 && in_kind != ELEM_STORE_F32) return cudaErrorInvalidValue;
+    return grows_launch<true, ELEM_C32>(p, tw, in, o, nlines, scale, C, st);
   }
-  return cudaGetLastError();
+  switch (in_kind) {
+    case ELEM_C32:
+    case ELEM_STORE_F32: return grows_launch<false, ELEM_C32>(p, tw, in, o, nlines, scale, C, st);
+    case ELEM_R32: return grows_launch<false, ELEM_R32>(p, tw, in, o, nlines, scale, C, st);
+    case ELEM_STORE_BF16: return grows_launch<false, ELEM_STORE_BF16>(p, tw, in, o, nlines, scale, C, st);
+    case ELEM_STORE_F16: return grows_launch<false, ELEM_STORE_F16>(p, tw, in, o, nlines, scale, C, st);
+    default: return cudaErrorInvalidValue;
+  }
 }
 
 cudaError_t launch_adj_col(const float2* Rs, const double* cturn, const double* zlist, float2* U, int W, int H,
