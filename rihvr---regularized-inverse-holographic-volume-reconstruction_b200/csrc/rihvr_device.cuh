@@ -145,17 +145,25 @@ __device__ __forceinline__ float2 cmul_tw(float2 a) {
 // ---------------------------------------------------------------------------
 template <int R, bool INV>
 __device__ __forceinline__ void small_dft(float2 (&a)[R]) {
+  // Radix 2 and 4 use packed FP32x2 adds (one instruction per complex add,
+  // same bits as two scalar adds).  The radix-4 outputs t1 -+ i d mix the
+  // halves of d, so they stay scalar; the swap and sign fold into the adds.
   if constexpr (R == 2) {
-    float2 t = a[0];
-    a[0] = cadd(t, a[1]);
-    a[1] = csub(t, a[1]);
+    const float2 t = a[0];
+    a[0] = f2add(t, a[1]);
+    a[1] = f2sub(t, a[1]);
   } else if constexpr (R == 4) {
-    float2 t0 = cadd(a[0], a[2]), t1 = csub(a[0], a[2]);
-    float2 t2 = cadd(a[1], a[3]), t3 = mul_mi<INV>(csub(a[1], a[3]));
-    a[0] = cadd(t0, t2);
-    a[2] = csub(t0, t2);
-    a[1] = cadd(t1, t3);
-    a[3] = csub(t1, t3);
+    const float2 t0 = f2add(a[0], a[2]), t1 = f2sub(a[0], a[2]);
+    const float2 t2 = f2add(a[1], a[3]), d = f2sub(a[1], a[3]);
+    a[0] = f2add(t0, t2);
+    a[2] = f2sub(t0, t2);
+    if (INV) {  // t3 = +i d = (-d.y, d.x)
+      a[1] = make_float2(t1.x - d.y, t1.y + d.x);
+      a[3] = make_float2(t1.x + d.y, t1.y - d.x);
+    } else {    // t3 = -i d = (d.y, -d.x)
+      a[1] = make_float2(t1.x + d.y, t1.y - d.x);
+      a[3] = make_float2(t1.x - d.y, t1.y + d.x);
+    }
   } else if constexpr (R == 3) {
     constexpr float h = 0.86602540378443864676f;  // sqrt(3)/2
     float2 t1 = cadd(a[1], a[2]), t2 = csub(a[1], a[2]);
@@ -253,6 +261,19 @@ __device__ __forceinline__ void line_twiddle(float2 (&v)[N2], int n1) {
       v[a * B + b] = cmul(v[a * B + b], cmul(anchor, pw[b]));
     }
     anchor = cmul(anchor, wB);
+  }
+}
+
+// The same twiddles w^(n1 k), k = 0..N2-1, each from its own sincospi, for
+// kernels that keep them in registers across many lines of the same n1.
+template <int N, int N2, bool INV>
+__device__ __forceinline__ void line_twiddles(float2 (&tw)[N2], int n1) {
+  const float sgn = INV ? 2.0f : -2.0f;
+#pragma unroll
+  for (int k = 0; k < N2; ++k) {
+    float s, c;
+    sincospif(sgn * (float)((n1 * k) % N) / (float)N, &s, &c);
+    tw[k] = make_float2(c, s);
   }
 }
 

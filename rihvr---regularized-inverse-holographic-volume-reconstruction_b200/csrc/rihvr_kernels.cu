@@ -312,6 +312,38 @@ __device__ __forceinline__ void col_exchange(float2 (&v)[LineCfg<N>::N2], float2
   stage_b_dft<N1, N2, INV>(v);
 }
 
+// The column passes walk many planes with the same thread-to-row assignment,
+// so a thread's inter-stage twiddles are the same for every plane.  For lines
+// of up to 32 elements a thread they are computed once and kept in registers
+// (one complex product an element per plane instead of two plus the anchor
+// products); the blocks are limited by shared memory to one per SM, which
+// leaves the registers free.  Longer lines regenerate them every plane.
+template <int N>
+constexpr bool kHoistTw = LineCfg<N>::N2 <= 32;
+
+template <int N, int N2, bool INV>
+__device__ __forceinline__ void apply_twiddles(float2 (&v)[N2], const float2 (&tw)[kHoistTw<N> ? N2 : 1], int t) {
+  if constexpr (kHoistTw<N>) {
+#pragma unroll
+    for (int k = 1; k < N2; ++k) v[k] = cmul(v[k], tw[k]);
+  } else {
+    line_twiddle<N, N2, INV>(v, launder_i(t));
+  }
+}
+
+// acc += v h: four fused multiply-adds where the twiddles are hoisted (lines
+// of up to 32 elements a thread); the longer lines keep the product-then-add
+// form, whose shorter live ranges keep them within the register file
+template <int N>
+__device__ __forceinline__ void cmac(float2& acc, float2 v, float2 h) {
+  if constexpr (kHoistTw<N>) {
+    acc.x = fmaf(v.x, h.x, fmaf(-v.y, h.y, acc.x));
+    acc.y = fmaf(v.x, h.y, fmaf(v.y, h.x, acc.y));
+  } else {
+    acc = cadd(acc, cmul(v, h));
+  }
+}
+
 // Adjoint column pass: U_z(:, x) = IDFT_y( conj(H'_z(:, x)) * Rs(:, x) ), z in [zb, ze).
 // Square planes: the row pitch equals the line length N, so every element
 // offset below is a compile-time multiple of N.  Rs already carries 1/(W H).
@@ -345,6 +377,8 @@ __global__ void __launch_bounds__(ColLayout<N>::THREADS) k_adj_col(const float2*
   }
   const float2* rs = Rs + (size_t)t * W + x;
   const double* ct = cturn + (size_t)t * W + x;
+  float2 tw[kHoistTw<N> ? N2 : 1];
+  if constexpr (kHoistTw<N>) line_twiddles<N, N2, true>(tw, t);
   double znext = zb < ze ? zlist[zb] : 0.0;
 #pragma unroll 1
   for (int z = zb; z < ze; ++z) {
@@ -371,7 +405,7 @@ __global__ void __launch_bounds__(ColLayout<N>::THREADS) k_adj_col(const float2*
       }
     }
     reg_fft<N2, true>(v);
-    line_twiddle<N, N2, true>(v, launder_i(t));
+    apply_twiddles<N, N2, true>(v, tw, t);
     // the exchange buffer also holds the previous plane's output tile: its
     // store must have read it (the exchange starts with a barrier)
     if (TMA && threadIdx.x == 0) bulk_wait_read_all();
@@ -436,6 +470,8 @@ __global__ void __launch_bounds__(ColLayout<N>::THREADS) k_fwd_col(const float2*
   float2 acc[N2];
 #pragma unroll
   for (int i = 0; i < N2; ++i) acc[i] = make_float2(0.f, 0.f);
+  float2 tw[kHoistTw<N> ? N2 : 1];
+  if constexpr (kHoistTw<N>) line_twiddles<N, N2, false>(tw, t);
   double znext = zb < ze ? zlist[zb] : 0.0;
 #pragma unroll 1
   for (int z = zb; z < ze; ++z) {
@@ -453,7 +489,7 @@ __global__ void __launch_bounds__(ColLayout<N>::THREADS) k_fwd_col(const float2*
       for (int n2 = 0; n2 < N2; ++n2) v[n2] = Tz[(size_t)n2 * N1 * W];
     }
     reg_fft<N2, false>(v);
-    line_twiddle<N, N2, false>(v, launder_i(t));
+    apply_twiddles<N, N2, false>(v, tw, t);
     // the exchange's first barrier also orders every thread's reads of s_t
     // before the refill below
     col_exchange<N, false>(v, sm, c, t);
@@ -465,7 +501,7 @@ __global__ void __launch_bounds__(ColLayout<N>::THREADS) k_fwd_col(const float2*
 #pragma unroll
         for (int k1 = 0; k1 < N1; ++k1) {
           const float2 h = transfer(zz, s_ct[(N1 * j + N2 * k1 + t) * CC + c], false);
-          acc[j * N1 + k1] = cadd(acc[j * N1 + k1], cmul(v[j * N1 + k1], h));
+          cmac<N>(acc[j * N1 + k1], v[j * N1 + k1], h);
         }
     } else {
       const double* ctz = launder(ct);
@@ -475,7 +511,7 @@ __global__ void __launch_bounds__(ColLayout<N>::THREADS) k_fwd_col(const float2*
         for (int q = 0; q < kPhaseGroup; ++q) {
           const int j = (g + q) / N1, k1 = (g + q) % N1;
           const float2 h = transfer(zz, __ldg(ctz + (size_t)(N1 * j + N2 * k1) * W), false);
-          acc[j * N1 + k1] = cadd(acc[j * N1 + k1], cmul(v[j * N1 + k1], h));
+          cmac<N>(acc[j * N1 + k1], v[j * N1 + k1], h);
         }
         sched_fence();
       }
