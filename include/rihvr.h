@@ -112,6 +112,9 @@ typedef struct rihvr_file_params {
   int roi_rect_x, roi_rect_y, roi_rect_w, roi_rect_h; /* 3011-3014 */
   int output_planes;               /* 7001 */
   int output_steps;                /* 7005 */
+  int segment_min_area;            /* 5009 */
+  double segment_min_intensity;    /* 5010 */
+  int segment_close_size;          /* 5011 */
 } rihvr_file_params;
 
 typedef struct rihvr_ctx rihvr_ctx;
@@ -259,6 +262,62 @@ int rihvr_preprocess(const float* holo, int width, int height, const float* back
                      const rihvr_file_params* files, int zero_padding, float* out, int* out_width, int* out_height);
 /* Message of the last failed image call on this thread. */
 const char* rihvr_io_error(void);
+
+/* Particle segmentation of a reconstructed volume: the reference's separate
+ * segmentation program (src/core/main_segmentation.cu:37-138,
+ * sparse_segmentation.cu, object_cloud.cu, blob3d.cu), run on the dense
+ * volume without the voxel-file round trip. */
+typedef struct rihvr_segment_params {
+  double min_intensity; /* 5010 segment_min_intensity: voxels with q > min_intensity * max q / 256 are on */
+  int close_size;       /* 5011 segment_close_size: radius of the closing ball (<= 0: none, at most 15) */
+  int min_area;         /* 5009 segment_min_area: objects with fewer voxels are dropped */
+  int faithful;         /* 1: the reference's in-plane neighbours (linear offsets, continuing on the
+                           next row past a row's end, :493-511); 0: the geometric 26-neighbourhood */
+} rihvr_segment_params;
+
+/* One object, as ObjectCloud::writeCentroids reports it (object_cloud.cu:408-470). */
+typedef struct rihvr_object {
+  float x, y, z;          /* centroid (pixels, pixels, planes), Blob3d::getCentroid */
+  float wx, wy, wz;       /* intensity-weighted centroid, Blob3d::getWeightedCentroid */
+  int num_voxels;
+  float max_value;        /* largest voxel intensity */
+  float mean_value;       /* mean voxel intensity */
+  int xmin, xmax, ymin, ymax, zmin, zmax; /* bounding box, Blob3d::getBounds */
+} rihvr_object;
+
+typedef struct rihvr_segment_info {
+  double max_intensity;     /* largest q (SparseVolume::calcMaxIntensity, sparse_volume.cu:482-516) */
+  double threshold;         /* min_intensity * max_intensity / 256 */
+  long long closed_voxels;  /* voxels on after the closing */
+  long long labelled_objects; /* components before the size filter */
+  int strel_size;           /* voxels in the closing ball */
+  long long kernel_launches;
+} rihvr_segment_info;
+
+/* HoloUi defaults (holo_ui.cpp:44-46): min_intensity 1, close_size 3,
+ * min_area 2; faithful 1. */
+int rihvr_segment_params_default(rihvr_segment_params* sp);
+/* Segment the context's current volume.  Each voxel's value is
+ * q = fl(fl(sqrt(I))^2) with I = fl(re^2 + im^2), what the reference computes
+ * from the voxel after writing I to its voxel file and loading (sqrt(I), 0)
+ * back (sparse_volume.cu:550, 645-650); the file's seven significant digits
+ * are not applied.  Objects come in the reference's order (first appearance
+ * by linear index, then the size filter's swaps).  At most max_objects are
+ * written; *num_objects receives the count, and a count above max_objects
+ * returns RIHVR_ERR_INVALID_ARGUMENT.  info may be NULL.  Temporary device
+ * memory: about 4 bytes a voxel plus the object lists. */
+int rihvr_segment(rihvr_ctx* ctx, const rihvr_segment_params* sp, rihvr_object* objects, int max_objects,
+                  int* num_objects, rihvr_segment_info* info);
+/* The same on a stack of voxel intensities I (num_planes x height x width
+ * floats, the values a voxel file holds; zero where the file has no voxel),
+ * on the device or the host. */
+int rihvr_segment_intensity(const float* intensity, int width, int height, int num_planes, int is_device,
+                            const rihvr_segment_params* sp, rihvr_object* objects, int max_objects,
+                            int* num_objects, rihvr_segment_info* info);
+/* ObjectCloud::writeCentroids (object_cloud.cu:408-470): centroids_XXXX.csv
+ * (weighted 0, verbose 0), centroids_weighted_XXXX.csv (weighted 1) and
+ * centroids_verbose_XXXX.csv (verbose 1). */
+int rihvr_write_centroids(const char* filename, const rihvr_object* objects, int n, int weighted, int verbose);
 
 /* Allocation-free adjoint.  No counterpart in the reference: for callers that
  * cannot allocate device memory - code running while a CUDA graph is captured,

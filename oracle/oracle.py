@@ -69,6 +69,9 @@ def lib():
         L.orc_solve.argtypes = [P(_Params), dp, ctypes.c_int, P(ctypes.c_int), P(ctypes.c_int),
                                 ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, dp, dp]
         L.orc_num_threads.restype = ctypes.c_int
+        L.orc_segment.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                                  ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, ctypes.c_int,
+                                  ctypes.POINTER(ctypes.c_double)]
         _lib = L
     return _lib
 
@@ -202,6 +205,30 @@ def solve(p: OracleParams, b: np.ndarray, n_iter: int, forced_bt=None, forced_rs
     if rc != 0:
         raise MemoryError("oracle could not allocate its volumes")
     return log, X, P, est, float(f0[0])
+
+
+SEG_OBJECT_DTYPE = np.dtype([
+    ("x", "f4"), ("y", "f4"), ("z", "f4"), ("wx", "f4"), ("wy", "f4"), ("wz", "f4"),
+    ("num_voxels", "i4"), ("max_value", "f4"), ("mean_value", "f4"),
+    ("xmin", "i4"), ("xmax", "i4"), ("ymin", "i4"), ("ymax", "i4"), ("zmin", "i4"), ("zmax", "i4"),
+])
+
+
+def segment(intensity: np.ndarray, min_intensity: float = 1.0, close_size: int = 3, min_area: int = 2,
+            faithful: int = 1):
+    """The reference's segmentation program on a (planes, height, width) stack of
+    voxel intensities: (objects in the reference's order, (max intensity, threshold))."""
+    I = np.ascontiguousarray(intensity, dtype=np.float32)
+    nz, h, w = I.shape
+    L = lib()
+    cap = max(16, I.size // 2 + 1)
+    out = np.zeros(cap, SEG_OBJECT_DTYPE)
+    info = (ctypes.c_double * 2)()
+    n = L.orc_segment(I.ctypes.data, w, h, nz, float(min_intensity), int(close_size), int(min_area),
+                      int(faithful), out.ctypes.data, cap, info)
+    if n < 0:
+        raise RuntimeError("orc_segment: object buffer too small")
+    return out[:n].copy(), (info[0], info[1])
 
 
 def num_threads() -> int:

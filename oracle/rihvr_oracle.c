@@ -809,3 +809,224 @@ int orc_num_threads(void)
     return 1;
 #endif
 }
+
+/* ------------------------------------------------------------------------ */
+/* Particle segmentation: the reference's separate segmentation program     */
+/* (src/core/main_segmentation.cu:37-138) on a dense stack of voxel          */
+/* intensities, the values its voxel file holds (zero = no voxel).  FP32    */
+/* where the reference computes in FP32, in the reference's loop order.      */
+/* ------------------------------------------------------------------------ */
+
+typedef struct {
+    float x, y, z, wx, wy, wz;
+    int num_voxels;
+    float max_value, mean_value;
+    int xmin, xmax, ymin, ymax, zmin, zmax;
+} orc_object;
+
+typedef struct {
+    long long sx, sy, sz;
+    float wsx, wsy, wsz, wsum, vmax;
+    double vsum;
+    int n, xmin, xmax, ymin, ymax, zmin, zmax;
+} orc_blob;
+
+/* SparseSegmentation::simpleMorph (sparse_segmentation.cu:265-372): for every
+ * on voxel, +1 at each in-bounds position of the ball around it; dilation
+ * keeps non-zero counts, erosion counts above (ball size - 0.1). */
+static void seg_morph(const unsigned char *in, unsigned char *out, int W, int H, int Nz, int cs, int erode)
+{
+    const size_t HW = (size_t)W * H, N = HW * Nz;
+    int *cnt = (int *)calloc(N, sizeof(int));
+    int nstrel = 0;
+    for (int sz = -cs; sz <= cs; ++sz)
+        for (int sx = -cs; sx <= cs; ++sx)
+            for (int sy = -cs; sy <= cs; ++sy)
+                if (sx * sx + sy * sy + sz * sz <= cs * cs) nstrel++;
+    for (int z = 0; z < Nz; ++z)
+        for (size_t p = 0; p < HW; ++p) {
+            if (!in[(size_t)z * HW + p]) continue;
+            const int x = (int)(p % W), y = (int)(p / W);
+            for (int sz = -cs; sz <= cs; ++sz) {
+                const int tz = z + sz;
+                if (tz < 0 || tz >= Nz) continue;
+                for (int sx = -cs; sx <= cs; ++sx)
+                    for (int sy = -cs; sy <= cs; ++sy) {
+                        const int tx = x + sx, ty = y + sy;
+                        if (sx * sx + sy * sy + sz * sz <= cs * cs && tx >= 0 && tx < W && ty >= 0 && ty < H)
+                            cnt[(size_t)tz * HW + (size_t)ty * W + tx] += 1;
+                    }
+            }
+        }
+    const double thr = nstrel - 0.1;
+    for (size_t i = 0; i < N; ++i) out[i] = erode ? ((double)cnt[i] > thr) : (cnt[i] != 0);
+    free(cnt);
+}
+
+/* In-plane neighbour of plane position p at offset (dx, dy): the reference's
+ * linear offset dy*W + dx, any position inside the plane (faithful,
+ * sparse_segmentation.cu:493-511), or the geometric neighbour. */
+static long long seg_neighbour(int W, int H, int faithful, size_t p, int dx, int dy)
+{
+    const int x = (int)(p % W), y = (int)(p / W);
+    if (faithful) {
+        const long long l = (long long)p + (long long)dy * W + dx;
+        return (l >= 0 && l < (long long)W * H) ? l : -1;
+    }
+    if (x + dx < 0 || x + dx >= W || y + dy < 0 || y + dy >= H) return -1;
+    return (long long)(y + dy) * W + (x + dx);
+}
+
+/* SparseSegmentation::labelConnectedComponents (:467-555): every on voxel
+ * starts with its linear index; sweeps in index order replace it with the
+ * smallest label among its 27-neighbourhood until nothing changes.  Planes
+ * outside the volume have no voxels. */
+static void seg_label(const unsigned char *on, unsigned long long *lab, int W, int H, int Nz, int faithful)
+{
+    const size_t HW = (size_t)W * H, N = HW * Nz;
+    for (size_t i = 0; i < N; ++i) lab[i] = on[i] ? (unsigned long long)i : ~0ull;
+    int changed = 1;
+    while (changed) {
+        changed = 0;
+        for (int z = 0; z < Nz; ++z)
+            for (size_t p = 0; p < HW; ++p) {
+                const size_t i = (size_t)z * HW + p;
+                if (!on[i]) continue;
+                unsigned long long v = lab[i];
+                for (int dx = -1; dx <= 1; ++dx)
+                    for (int dy = -1; dy <= 1; ++dy) {
+                        const long long q = seg_neighbour(W, H, faithful, p, dx, dy);
+                        if (q < 0) continue;
+                        for (int dz = -1; dz <= 1; ++dz) {
+                            const int zz = z + dz;
+                            if (zz < 0 || zz >= Nz) continue;
+                            const size_t j = (size_t)zz * HW + (size_t)q;
+                            if (on[j] && lab[j] < v) {
+                                v = lab[j];
+                                changed = 1;
+                            }
+                        }
+                    }
+                lab[i] = v;
+            }
+    }
+}
+
+/* Whole pipeline: binarize (:61-112; max from SparseVolume::calcMaxIntensity,
+ * sparse_volume.cu:482-516), close (:186-263), label, objects in order of
+ * first appearance (object_cloud.cu:127-265) with their intensities
+ * (:269-289) and Blob3d's centroid, weighted centroid, max, mean and bounds
+ * (blob3d.cu), blobSizeFilter (object_cloud.cu:313-328).  Returns the number
+ * of objects kept (or -1 if more than max_out); info2 = {max, threshold}. */
+int orc_segment(const float *inten, int W, int H, int Nz, double min_intensity, int close_size, int min_area,
+                int faithful, orc_object *out, int max_out, double *info2)
+{
+    const size_t HW = (size_t)W * H, N = HW * Nz;
+    float *q = (float *)malloc(sizeof(float) * N);
+    unsigned char *on0 = (unsigned char *)malloc(N), *on1 = (unsigned char *)malloc(N);
+    double maxq = 0.0;
+    for (size_t i = 0; i < N; ++i) {
+        /* the loaded voxel is (sqrt(I), 0); its intensity is re*re + im*im */
+        const float s = sqrtf(inten[i]);
+        q[i] = s * s;
+        const double d = q[i];
+        if (d > maxq) maxq = d;
+    }
+    const double thr = min_intensity * maxq / 256.0;
+    for (size_t i = 0; i < N; ++i) on0[i] = (double)q[i] > thr;
+    const unsigned char *closed = on0;
+    if (close_size > 0) {
+        unsigned char *dil = (unsigned char *)malloc(N);
+        seg_morph(on0, dil, W, H, Nz, close_size, 0);
+        seg_morph(dil, on1, W, H, Nz, close_size, 1);
+        free(dil);
+        closed = on1;
+    }
+    unsigned long long *lab = (unsigned long long *)malloc(sizeof(unsigned long long) * N);
+    seg_label(closed, lab, W, H, Nz, faithful);
+    /* object of each label: first appearance while scanning by index */
+    long long *obj_of = (long long *)malloc(sizeof(long long) * N);
+    for (size_t i = 0; i < N; ++i) obj_of[i] = -1;
+    size_t nobj = 0, cap = 1024;
+    orc_blob *b = (orc_blob *)malloc(sizeof(orc_blob) * cap);
+    for (size_t i = 0; i < N; ++i) {
+        if (!closed[i]) continue;
+        long long o = obj_of[lab[i]];
+        if (o < 0) {
+            if (nobj == cap) {
+                cap *= 2;
+                b = (orc_blob *)realloc(b, sizeof(orc_blob) * cap);
+            }
+            o = (long long)nobj++;
+            obj_of[lab[i]] = o;
+            memset(&b[o], 0, sizeof(orc_blob));
+        }
+        orc_blob *s = &b[o];
+        const int z = (int)(i / HW), y = (int)((i % HW) / W), x = (int)(i % W);
+        const float w = on0[i] ? q[i] : 0.0f; /* masked complex volume, :51-59 */
+        s->sx += x;
+        s->sy += y;
+        s->sz += z;
+        s->wsx += w * (float)x;
+        s->wsy += w * (float)y;
+        s->wsz += w * (float)z;
+        s->wsum += w;
+        s->vsum += (double)w;
+        if (s->n == 0 || w > s->vmax) s->vmax = w;
+        if (s->n == 0) {
+            s->xmin = s->xmax = x;
+            s->ymin = s->ymax = y;
+            s->zmin = s->zmax = z;
+        } else {
+            if (x < s->xmin) s->xmin = x;
+            if (x > s->xmax) s->xmax = x;
+            if (y < s->ymin) s->ymin = y;
+            if (y > s->ymax) s->ymax = y;
+            if (z < s->zmin) s->zmin = z;
+            if (z > s->zmax) s->zmax = z;
+        }
+        s->n += 1;
+    }
+    orc_object *o = (orc_object *)malloc(sizeof(orc_object) * (nobj ? nobj : 1));
+    for (size_t k = 0; k < nobj; ++k) {
+        const orc_blob *s = &b[k];
+        const float n = (float)s->n;
+        o[k].x = (float)s->sx / n;
+        o[k].y = (float)s->sy / n;
+        o[k].z = (float)s->sz / n;
+        o[k].wx = s->wsx / s->wsum;
+        o[k].wy = s->wsy / s->wsum;
+        o[k].wz = s->wsz / s->wsum;
+        o[k].num_voxels = s->n;
+        o[k].max_value = s->vmax;
+        o[k].mean_value = (float)s->vsum / n;
+        o[k].xmin = s->xmin;
+        o[k].xmax = s->xmax;
+        o[k].ymin = s->ymin;
+        o[k].ymax = s->ymax;
+        o[k].zmin = s->zmin;
+        o[k].zmax = s->zmax;
+    }
+    long long kept = (long long)nobj;
+    for (long long n = 0; n < kept; ++n)
+        if (o[n].num_voxels < min_area) {
+            o[n] = o[kept - 1];
+            --n;
+            --kept;
+        }
+    int rc = (int)kept;
+    if (kept > max_out) rc = -1;
+    else if (kept > 0) memcpy(out, o, sizeof(orc_object) * (size_t)kept);
+    if (info2) {
+        info2[0] = maxq;
+        info2[1] = thr;
+    }
+    free(o);
+    free(b);
+    free(obj_of);
+    free(lab);
+    free(q);
+    free(on0);
+    free(on1);
+    return rc;
+}

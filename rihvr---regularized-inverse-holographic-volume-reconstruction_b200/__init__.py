@@ -17,6 +17,7 @@ import numpy as np
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "librihvr_b200.so")
 CLI_PATH = os.path.join(_HERE, "sparse-inverse-recon")
+SEGMENT_CLI_PATH = os.path.join(_HERE, "sparse-segmentation")
 
 # status codes (include/rihvr.h)
 OK = 0
@@ -86,7 +87,40 @@ class FileParams(ctypes.Structure):
         ("roi_rect_h", ctypes.c_int),
         ("output_planes", ctypes.c_int),
         ("output_steps", ctypes.c_int),
+        ("segment_min_area", ctypes.c_int),
+        ("segment_min_intensity", ctypes.c_double),
+        ("segment_close_size", ctypes.c_int),
     ]
+
+
+class SegmentParams(ctypes.Structure):
+    """rihvr_segment_params: segment_min_intensity (5010), segment_close_size
+    (5011), segment_min_area (5009) and the neighbourhood switch."""
+    _fields_ = [
+        ("min_intensity", ctypes.c_double),
+        ("close_size", ctypes.c_int),
+        ("min_area", ctypes.c_int),
+        ("faithful", ctypes.c_int),
+    ]
+
+
+class SegmentInfo(ctypes.Structure):
+    _fields_ = [
+        ("max_intensity", ctypes.c_double),
+        ("threshold", ctypes.c_double),
+        ("closed_voxels", ctypes.c_longlong),
+        ("labelled_objects", ctypes.c_longlong),
+        ("strel_size", ctypes.c_int),
+        ("kernel_launches", ctypes.c_longlong),
+    ]
+
+
+# rihvr_object, one row per segmented object (ObjectCloud::writeCentroids fields)
+OBJECT_DTYPE = np.dtype([
+    ("x", "f4"), ("y", "f4"), ("z", "f4"), ("wx", "f4"), ("wy", "f4"), ("wz", "f4"),
+    ("num_voxels", "i4"), ("max_value", "f4"), ("mean_value", "f4"),
+    ("xmin", "i4"), ("xmax", "i4"), ("ymin", "i4"), ("ymax", "i4"), ("zmin", "i4"), ("zmax", "i4"),
+])
 
 
 # every symbol include/rihvr.h declares
@@ -100,6 +134,7 @@ EXPORTED = (
     "rihvr_get_estimate", "rihvr_get_residual", "rihvr_forward", "rihvr_adjoint", "rihvr_prox_step",
     "rihvr_adjoint_noalloc", "rihvr_sparsity", "rihvr_initial_estimate",
     "rihvr_read_image", "rihvr_write_tiff8", "rihvr_preprocess", "rihvr_io_error",
+    "rihvr_segment_params_default", "rihvr_segment", "rihvr_segment_intensity", "rihvr_write_centroids",
     "rihvr_set_profiling", "rihvr_kernel_times", "rihvr_get_stream", "rihvr_launch_count", "rihvr_device_bytes",
     "rihvr_status_string", "rihvr_last_error",
 )
@@ -161,6 +196,11 @@ def load_library(path: str = LIB_PATH):
     L.rihvr_write_tiff8.argtypes = [ctypes.c_char_p, vp, ip, ip]
     L.rihvr_preprocess.argtypes = [vp, ip, ip, vp, P(FileParams), ip, vp, P(ctypes.c_int), P(ctypes.c_int)]
     L.rihvr_io_error.restype = ctypes.c_char_p
+    L.rihvr_segment_params_default.argtypes = [P(SegmentParams)]
+    L.rihvr_segment.argtypes = [vp, P(SegmentParams), vp, ip, P(ctypes.c_int), P(SegmentInfo)]
+    L.rihvr_segment_intensity.argtypes = [vp, ip, ip, ip, ip, P(SegmentParams), vp, ip, P(ctypes.c_int),
+                                          P(SegmentInfo)]
+    L.rihvr_write_centroids.argtypes = [ctypes.c_char_p, vp, ip, ip, ip]
     L.rihvr_initial_estimate.argtypes = [vp, vp, ip]
     L.rihvr_set_profiling.argtypes = [vp, ip]
     L.rihvr_kernel_times.argtypes = [vp, P(ctypes.c_char_p), P(ctypes.c_double), P(ctypes.c_int), ip,
@@ -213,6 +253,65 @@ def adjoint_noalloc(params: RihvrParams, width: int, height: int, residual_dev: 
     _check(load_library().rihvr_adjoint_noalloc(ctypes.byref(params), int(width), int(height),
                                                  ctypes.c_void_p(residual_dev), ctypes.c_void_p(volume_dev),
                                                  ctypes.c_void_p(stream)), "rihvr_adjoint_noalloc")
+
+
+def segment_params(**kw) -> SegmentParams:
+    """Segmentation settings: the HoloUi defaults (holo_ui.cpp:44-46) with
+    any field overridden by keyword."""
+    sp = SegmentParams()
+    _check(load_library().rihvr_segment_params_default(ctypes.byref(sp)), "rihvr_segment_params_default")
+    for k, v in kw.items():
+        setattr(sp, k, v)
+    return sp
+
+
+def _segment_call(call, where: str, max_objects: int):
+    """Run a segmentation entry point, growing the object buffer once if needed."""
+    for _ in range(2):
+        out = np.zeros(max(1, max_objects), OBJECT_DTYPE)
+        n = ctypes.c_int()
+        info = SegmentInfo()
+        rc = call(out.ctypes.data, len(out), ctypes.byref(n), ctypes.byref(info))
+        if rc == ERR_INVALID_ARGUMENT and n.value > len(out):
+            max_objects = n.value
+            continue
+        _check(rc, where)
+        info_d = {k: getattr(info, k) for k, _ in SegmentInfo._fields_}
+        return out[:n.value].copy(), info_d
+    raise RihvrError(ERR_INVALID_ARGUMENT, where)
+
+
+def segment_intensity(intensity, sp: SegmentParams | None = None, max_objects: int = 1 << 16):
+    """Segment a stack of voxel intensities (num_planes x height x width: a
+    numpy array, or a CUDA torch tensor used in place).  Returns (objects as
+    an OBJECT_DTYPE array in the reference's order, info dict)."""
+    sp = sp or segment_params()
+    if hasattr(intensity, "is_cuda") and intensity.is_cuda:
+        t = intensity.contiguous()
+        if t.dtype.itemsize != 4 or t.dim() != 3:
+            raise ValueError("expected a float32 tensor of shape (planes, height, width)")
+        nz, h, w = t.shape
+        ptr, dev = t.data_ptr(), 1
+        keep = t
+    else:
+        keep = np.ascontiguousarray(intensity, dtype=np.float32)
+        if keep.ndim != 3:
+            raise ValueError("expected shape (planes, height, width)")
+        nz, h, w = keep.shape
+        ptr, dev = keep.ctypes.data, 0
+    L = load_library()
+    res = _segment_call(lambda o, m, n, i: L.rihvr_segment_intensity(ctypes.c_void_p(ptr), w, h, nz, dev,
+                                                                     ctypes.byref(sp), o, m, n, i),
+                        "rihvr_segment_intensity", max_objects)
+    del keep
+    return res
+
+
+def write_centroids(path: str, objects: np.ndarray, weighted: bool = False, verbose: bool = False):
+    """ObjectCloud::writeCentroids (object_cloud.cu:408-470)."""
+    objs = np.ascontiguousarray(objects, dtype=OBJECT_DTYPE)
+    _check(load_library().rihvr_write_centroids(path.encode(), objs.ctypes.data if len(objs) else None, len(objs),
+                                                int(bool(weighted)), int(bool(verbose))), "rihvr_write_centroids")
 
 
 def reconstruct_batch(solvers, holograms):
@@ -420,6 +519,13 @@ class SparseCompressiveHolo:
         out = np.empty((self.height, self.width), np.float32)
         _check(self._L.rihvr_get_residual(self._h, _ptr(out), 0), "rihvr_get_residual")
         return out
+
+    def segment(self, sp: SegmentParams | None = None, max_objects: int = 1 << 16):
+        """SparseSegmentation on the current volume (binarize, close, label,
+        extractObjects, blobSizeFilter): (objects, info), see segment_intensity."""
+        sp = sp or segment_params()
+        return _segment_call(lambda o, m, n, i: self._L.rihvr_segment(self._h, ctypes.byref(sp), o, m, n, i),
+                             "rihvr_segment", max_objects)
 
     # operators ---------------------------------------------------------------
     def forward(self, vol: np.ndarray) -> np.ndarray:

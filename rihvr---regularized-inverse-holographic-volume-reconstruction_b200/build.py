@@ -18,6 +18,7 @@ CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "librihvr_b200.so")
 CLI = os.path.join(HERE, "sparse-inverse-recon")
+SEG_CLI = os.path.join(HERE, "sparse-segmentation")
 INCLUDE = os.path.abspath(os.path.join(HERE, "..", "include"))
 
 NVCC = os.environ.get("NVCC", shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc")
@@ -28,8 +29,11 @@ CUDA_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr
 # nvcc and the host objects use the system g++.
 HOST_CXX = shutil.which("g++") or "g++"
 
-LIB_SOURCES = ["rihvr_kernels.cu", "rihvr_solver.cu", "rihvr_params.cpp", "rihvr_noalloc.cu", "rihvr_image.cpp"]
-CLI_SOURCES = ["sparse_inverse_recon.cpp"]
+LIB_SOURCES = ["rihvr_kernels.cu", "rihvr_solver.cu", "rihvr_params.cpp", "rihvr_noalloc.cu", "rihvr_image.cpp",
+               "rihvr_segment.cu"]
+CLI_SOURCES = ["sparse_inverse_recon.cpp", "sparse_segmentation.cpp"]
+# executable -> its sources (linked against the library)
+EXECUTABLES = {CLI: ["sparse_inverse_recon.cpp"], SEG_CLI: ["sparse_segmentation.cpp"]}
 HEADERS = ["rihvr_device.cuh", "rihvr_kernels.cuh", "rihvr_image.h"]
 
 
@@ -69,13 +73,14 @@ def build(force: bool = False, verbose: bool = False) -> str:
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)
-    cli_objs = [objs[s] for s in CLI_SOURCES if s in objs]
-    if len(cli_objs) == len(CLI_SOURCES) and (force or _mtime(CLI) < max([_mtime(LIB)] + [_mtime(o) for o in cli_objs])):
-        cmd = [HOST_CXX, "-O2", "-o", CLI] + cli_objs + [LIB, "-Wl,-rpath,$ORIGIN", "-L/usr/local/cuda/lib64",
-                                                         "-lcudart", "-lm"]
-        if verbose:
-            print(" ".join(cmd), flush=True)
-        subprocess.run(cmd, check=True)
+    for exe, srcs in EXECUTABLES.items():
+        exe_objs = [objs[s] for s in srcs if s in objs]
+        if len(exe_objs) == len(srcs) and (force or _mtime(exe) < max([_mtime(LIB)] + [_mtime(o) for o in exe_objs])):
+            cmd = [HOST_CXX, "-O2", "-o", exe] + exe_objs + [LIB, "-Wl,-rpath,$ORIGIN", "-L/usr/local/cuda/lib64",
+                                                             "-lcudart", "-lm"]
+            if verbose:
+                print(" ".join(cmd), flush=True)
+            subprocess.run(cmd, check=True)
     return LIB
 
 

@@ -3,6 +3,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "../../include/rihvr.h"
+
 namespace rihvr {
 
 // Slots of the per-block FP64 partial sums written by reduction kernels.
@@ -51,6 +53,11 @@ bool line_size_supported(int n);
 bool generic_size_supported(int n);
 // message returned by rihvr_last_error on this thread
 void set_last_error(const char* msg);
+
+// particle segmentation of a dense complex FP32 volume on stream st
+// (rihvr_segment.cu)
+int segment_complex(const float2* vol, int W, int H, int Nz, const rihvr_segment_params* sp, rihvr_object* objects,
+                    int max_objects, int* num_objects, rihvr_segment_info* info, cudaStream_t st);
 size_t max_partial_blocks(int W, int H, int Nz);
 
 cudaError_t launch_adj_col(const float2* Rs, const double* cturn, const double* zlist, float2* U, int W,

@@ -58,6 +58,9 @@ int rihvr_read_param_file(const char* path, rihvr_params* p, rihvr_file_params* 
   if (!f) f = &local;
   std::memset(f, 0, sizeof(*f));
   f->roi_x = f->roi_y = f->roi_size = -1;  // whole image (HoloUi defaults, holo_ui.cpp:17-20)
+  f->segment_min_area = 2;                  // segmentation defaults (holo_ui.cpp:44-46)
+  f->segment_min_intensity = 1.0;
+  f->segment_close_size = 3;
   bool set_full_filename = false;
   char buff[8192];
   char description[8192];
@@ -98,9 +101,12 @@ int rihvr_read_param_file(const char* path, rihvr_params* p, rihvr_file_params* 
       case 3012: f->roi_rect_y = (int)value; break;
       case 3013: f->roi_rect_w = (int)value; break;
       case 3014: f->roi_rect_h = (int)value; break;
-      // 4001-5011: classic reconstruction, simulation and segmentation settings
+      // 4001-5008: classic reconstruction and simulation settings
       case 4001: case 4002: case 5001: case 5002: case 5003: case 5004: case 5005:
-      case 5006: case 5007: case 5008: case 5009: case 5010: case 5011: break;
+      case 5006: case 5007: case 5008: break;
+      case 5009: f->segment_min_area = (int)value; break;
+      case 5010: f->segment_min_intensity = value; break;
+      case 5011: f->segment_close_size = (int)value; break;
       case 6001: p->num_inverse_iterations = (int)value; break;
       case 6002: p->regularization_param = value; break;
       case 6003: break;  // max_svd (unused by the sparse solver)

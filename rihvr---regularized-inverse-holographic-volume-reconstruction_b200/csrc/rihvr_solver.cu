@@ -975,6 +975,19 @@ int rihvr_get_volume(rihvr_ctx* c, float* out, int is_device) {
   return copy_out(c, out, c->U, sizeof(float2) * c->V, is_device);
 }
 
+int rihvr_segment(rihvr_ctx* c, const rihvr_segment_params* sp, rihvr_object* objects, int max_objects,
+                  int* num_objects, rihvr_segment_info* info) {
+  if (!c) return fail(RIHVR_ERR_INVALID_ARGUMENT, "NULL context");
+  // the volume rihvr_get_volume returns, materialised in the intermediate buffer
+  KL(launch_materialize_x(c->storage, c->vol[c->iCur], c->vol[c->iPrev], (float)c->beta, c->U, (long long)c->V,
+                          c->st));
+  rihvr_segment_info local{};
+  const int rc = segment_complex(c->U, c->W, c->H, c->Nz, sp, objects, max_objects, num_objects, &local, c->st);
+  c->launches += local.kernel_launches;
+  if (info) *info = local;
+  return rc;
+}
+
 int rihvr_get_plane(rihvr_ctx* c, int z, float* out, int is_device) {
   if (!c || !out) return fail(RIHVR_ERR_INVALID_ARGUMENT, "NULL argument");
   if (z < 0 || z >= c->Nz) return fail(RIHVR_ERR_INVALID_ARGUMENT, "plane out of bounds");  // :950-954

@@ -1,5 +1,9 @@
 // sparse-inverse-recon: command-line driver with the reference's interface
-// (src/core/main_sparse_inverse.cu:43-198): -F <file.param> [-S 0|1].
+// (src/core/main_sparse_inverse.cu:43-198): -F <file.param> [-S 0|1] [-G 0|1].
+// -G 1 also runs the reference's separate segmentation program
+// (src/core/main_segmentation.cu:37-138) on the final volume in device memory
+// and writes centroids_XXXX.csv, centroids_weighted_XXXX.csv and
+// centroids_verbose_XXXX.csv with the .param file's segment_* settings.
 //
 // Reads the .param file, loads and preprocesses the hologram frame, runs the
 // reconstruction through the C ABI and writes the reference's output files:
@@ -170,14 +174,45 @@ bool save_sparse(Planes& pl, const std::string& output_path, const std::string& 
   return true;
 }
 
+// SparseSegmentation + ObjectCloud::blobSizeFilter + writeCentroids
+// (main_segmentation.cu:100-128)
+bool segment_and_save(rihvr_ctx* ctx, const rihvr_file_params& files, const std::string& out) {
+  rihvr_segment_params sp;
+  rihvr_segment_params_default(&sp);
+  sp.min_intensity = files.segment_min_intensity;
+  sp.close_size = files.segment_close_size;
+  sp.min_area = files.segment_min_area;
+  std::vector<rihvr_object> objs(1 << 16);
+  int n = 0;
+  rihvr_segment_info info;
+  int rc = rihvr_segment(ctx, &sp, objs.data(), (int)objs.size(), &n, &info);
+  if (rc == RIHVR_ERR_INVALID_ARGUMENT && n > (int)objs.size()) {
+    objs.resize(n);
+    rc = rihvr_segment(ctx, &sp, objs.data(), (int)objs.size(), &n, &info);
+  }
+  if (rc != RIHVR_OK) return fail_msg(std::string("rihvr_segment: ") + rihvr_last_error());
+  std::printf("max intensity = %f, thr = %f\n", info.max_intensity, info.threshold);
+  std::printf("Number of particles: %lld\n", info.labelled_objects);
+  std::printf("blobSizeFilter removed %lld objects\n", info.labelled_objects - n);
+  char name[4096];
+  const char* kinds[3] = {"centroids", "centroids_weighted", "centroids_verbose"};
+  for (int k = 0; k < 3; ++k) {
+    std::snprintf(name, sizeof(name), "%s/%s_%04d.csv", out.c_str(), kinds[k], files.start_image);
+    if (rihvr_write_centroids(name, objs.data(), n, k == 1, k == 2) != RIHVR_OK)
+      return fail_msg(rihvr_last_error());
+  }
+  return true;
+}
+
 int run(int argc, char** argv) {
   std::string param_file;
-  bool subfolder = false;
+  bool subfolder = false, segment = false;
   int c;
-  while ((c = getopt(argc, argv, "F:S:")) != -1) {
+  while ((c = getopt(argc, argv, "F:S:G:")) != -1) {
     switch (c) {
       case 'F': param_file = optarg; break;
       case 'S': subfolder = std::atoi(optarg) != 0; break;
+      case 'G': segment = std::atoi(optarg) != 0; break;
       default: std::printf("Unknown input argument\n"); return -1;
     }
   }
@@ -269,6 +304,7 @@ int run(int argc, char** argv) {
   }
   if (!save_projections(pl, out, "cmb")) return done(-1);
   if (!save_sparse(pl, out, "inverse_voxels")) return done(-1);
+  if (segment && !segment_and_save(ctx, files, out)) return done(-1);
   std::printf("Done.\n");
   return done(0);
 }

@@ -75,3 +75,86 @@ def test_cli_errors(rihvr, tmp_path):
     bad.write_text("image_file 2001 /nonexistent_%04d.tif\n")
     r = subprocess.run([rihvr.CLI_PATH, "-F", str(bad)], capture_output=True, text=True, timeout=60)
     assert r.returncode != 0
+
+
+def _write_param(path, frame_pattern, out, cfg, n_iter, extra=""):
+    path.write_text(
+        f"image_file 2001 {frame_pattern}\n"
+        f"output_path 2004 {out}/\n"
+        "start_image 1002 7\n"
+        f"start_plane 3001 {cfg.start_plane}\n"
+        f"plane_stepsize 3002 {cfg.plane_stepsize}\n"
+        f"num_planes 3003 {cfg.num_planes}\n"
+        f"wavelength 3004 {cfg.wavelength}\n"
+        f"resolution 3005 {cfg.resolution}\n"
+        "zero_padding 3010 0\n"
+        f"num_inverse_iterations 6001 {n_iter}\n"
+        f"sparsity 6002 {cfg.regularization_param}\n"
+        f"tv 6004 {cfg.regularization_TV_param}\n"
+        f"tv_iterations 6005 {cfg.num_tv_iterations}\n"
+        "output_planes 7001 false\n" + extra)
+
+
+def test_cli_segmentation(rihvr, synthmod, tmp_path):
+    """sparse-inverse-recon -G 1 segments the final volume in device memory;
+    sparse-segmentation reads the voxel file as the reference's segmentation
+    program does.  The first matches the library's segmentation of the same
+    volume, the second the oracle's segmentation of the file's values, both
+    to the byte in the three centroid files."""
+    import oracle as O
+
+    cfg = synthmod.small_config(W=64, H=64, Nz=8, seed=3, zero_padding=0)
+    img, _ = synthmod.make_hologram(cfg, cache_dir=str(tmp_path / "cache"))
+    frame = tmp_path / "holo_0007.tif"
+    assert cv2.imwrite(str(frame), img)
+    seg = "segment_min_area 5009 2\nsegment_min_intensity 5010 4\nsegment_close_size 5011 1\n"
+    out = tmp_path / "out"
+    out.mkdir()
+    param = tmp_path / "run.param"
+    _write_param(param, f"{tmp_path}/holo_%04d.tif", out, cfg, 10, seg)
+    r = subprocess.run([rihvr.CLI_PATH, "-F", str(param), "-G", "1"], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    names = ("centroids_0007.csv", "centroids_weighted_0007.csv", "centroids_verbose_0007.csv")
+    for n in names:
+        assert (out / n).exists(), n
+
+    # the library on the same frame
+    p, fp = rihvr.read_param_file(str(param))
+    raw, _ = rihvr.read_image(str(frame))
+    bb = rihvr.preprocess(raw, p.zero_padding)
+    sp = rihvr.segment_params(min_intensity=fp.segment_min_intensity, close_size=fp.segment_close_size,
+                              min_area=fp.segment_min_area)
+    with rihvr.SparseCompressiveHolo(p, 64, 64) as s:
+        s.setHologram(bb)
+        s.iterate(10)
+        objs, _ = s.segment(sp)
+    assert len(objs) > 0
+    lib_dir = tmp_path / "lib"
+    lib_dir.mkdir()
+    for n, (wt, vb) in zip(names, ((0, 0), (1, 0), (0, 1))):
+        rihvr.write_centroids(str(lib_dir / n), objs, weighted=wt, verbose=vb)
+        assert (lib_dir / n).read_text() == (out / n).read_text(), n
+
+    # the reference's file round trip: voxel file -> segmentation program
+    seg_out = tmp_path / "seg"
+    seg_out.mkdir()
+    (seg_out / "inverse_voxels_0007.csv").write_text((out / "inverse_voxels.csv").read_text())
+    param2 = tmp_path / "seg.param"
+    _write_param(param2, f"{tmp_path}/holo_%04d.tif", seg_out, cfg, 10, seg)
+    r = subprocess.run([rihvr.SEGMENT_CLI_PATH, "-F", str(param2)], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    import ctypes
+
+    libc = ctypes.CDLL(None)
+    libc.strtof.restype = ctypes.c_float
+    libc.strtof.argtypes = [ctypes.c_char_p, ctypes.c_void_p]
+    rows = np.loadtxt(seg_out / "inverse_voxels_0007.csv", delimiter=",", skiprows=1, ndmin=2, dtype=str)
+    I = np.zeros((cfg.num_planes, 64, 64), np.float32)
+    for x, y, z, v in rows:
+        I[int(z), int(y), int(x)] = libc.strtof(v.strip().encode(), None)  # fscanf's direct decimal to float
+    ref, _ = O.segment(I, fp.segment_min_intensity, fp.segment_close_size, fp.segment_min_area, 1)
+    orc_dir = tmp_path / "orc"
+    orc_dir.mkdir()
+    for n, (wt, vb) in zip(names, ((0, 0), (1, 0), (0, 1))):
+        rihvr.write_centroids(str(orc_dir / n), ref.astype(rihvr.OBJECT_DTYPE), weighted=wt, verbose=vb)
+        assert (orc_dir / n).read_text() == (seg_out / n).read_text(), n
