@@ -9,7 +9,9 @@ iterations per second over all ranks, timed on the device with CUDA events;
 ``e2e`` is the same metric through the C ABI from a host hologram to host
 results.
 
-    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config c2|c1]
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config c2|c1|c5]
+    python bench.py --config series    # uneven time series, batched vs frame by frame
+    python bench.py --config segment   # particle segmentation of the reconstructed volume
 """
 from __future__ import annotations
 
@@ -282,6 +284,78 @@ def run_frames(args):
     return 0
 
 
+def run_segment(args):
+    """Particle segmentation of the reconstructed 1024x1024x1000 volume (the
+    reference's segmentation program with its default settings: threshold at
+    max/256, closing with a ball of radius 3, 26-connected labels, centroids of
+    objects of 2 voxels or more) on the volume in device memory.  A step is one
+    rihvr_segment call, timed on the host around a device synchronisation (the
+    call itself synchronises three times to size its buffers).  Prints one
+    JSON line."""
+    import torch
+
+    torch.cuda.set_device(0)
+    rihvr = importlib.import_module(PKG)
+    synth = importlib.import_module(PKG + ".synth")
+    cfg = workload("c2")
+    if args.nz:
+        cfg.num_planes = args.nz
+        cfg.name = f"{cfg.name}_nz{args.nz}"
+    _, b = synth.make_hologram(cfg)
+    p = rihvr.params_from_config(cfg, record_objective=0)
+    s = rihvr.SparseCompressiveHolo(p, cfg.W, cfg.H)
+    s.setHologram(b)
+    s.iterate(cfg.num_inverse_iterations)
+    sp = rihvr.segment_params()
+    for _ in range(args.warmup):
+        objs, info = s.segment(sp)
+    launches0 = s.launch_count()
+    times = []
+    with ClockSampler(0) as clk:
+        time.sleep(0.3)
+        for _ in range(args.steps):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            objs, info = s.segment(sp)
+            torch.cuda.synchronize()
+            times.append(time.perf_counter() - t0)
+    launches = (s.launch_count() - launches0) // args.steps
+    V = cfg.voxels()
+    t = float(np.median(times))
+    peak, peak_kind = peaks()
+    # HBM bytes a voxel: P and P_prev read by the max pass and again by the
+    # threshold pass (16 B each at FP32); the bit volumes are 1/8 B a voxel
+    bpv = 32
+    cpu = None
+    if not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+
+        nzs = min(16, cfg.num_planes)
+        planes = np.stack([s.getPlane(z) for z in range(nzs)])
+        I = (planes.real * planes.real + planes.imag * planes.imag).astype(np.float32)
+        t0 = time.perf_counter()
+        O.segment(I, sp.min_intensity, sp.close_size, sp.min_area, sp.faithful)
+        dt = time.perf_counter() - t0
+        cpu = {"value": I.size / dt, "unit": "voxels/s", "cores": 1, "kind": "port",
+               "sample": f"oracle segmentation of the first {nzs} of {cfg.num_planes} planes ({dt:.2f} s)"}
+    line = {"metric": "segmented voxels per second (1024x1024x1000 reconstructed volume)", "value": V / t,
+            "unit": "voxels/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3,
+            "higher_is_better": True, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "segment_" + cfg.name, "min_intensity": sp.min_intensity,
+                       "close_size": sp.close_size, "min_area": sp.min_area, "faithful": sp.faithful,
+                       "fista_iterations_before": cfg.num_inverse_iterations},
+            "objects": int(len(objs)), "labelled_objects": int(info["labelled_objects"]),
+            "closed_voxels": int(info["closed_voxels"]), "threshold": info["threshold"],
+            "roofline": {"bound": "hbm", "bytes_per_voxel": bpv, "achieved": bpv * V / t / 1e9, "peak": peak,
+                         "unit": "GB/s", "frac": bpv * V / t / 1e9 / peak, "peak_source": peak_kind},
+            "cpu_baseline": cpu, "clocks": clk.summary(), "gpu_launches": launches,
+            "step_ms_all": [x * 1e3 for x in times]}
+    print(json.dumps(line), flush=True)
+    s.destroy()
+    return 0
+
+
 def run_ours(args):
     ws, rank, local = dist_env()
     import torch
@@ -419,7 +493,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="c2", choices=["c2", "c1", "c5", "series"])
+    ap.add_argument("--config", default="c2", choices=["c2", "c1", "c5", "series", "segment"])
     ap.add_argument("--frames", type=int, default=8, help="frames of the uneven series (--config series)")
     ap.add_argument("--storage", default="f32", choices=["f32", "bf16", "f16"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -435,6 +509,8 @@ def main():
         return run_reference(args)
     if args.config == "series":
         return run_frames(args)
+    if args.config == "segment":
+        return run_segment(args)
     return run_ours(args)
 
 

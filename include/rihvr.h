@@ -304,13 +304,17 @@ int rihvr_segment_params_default(rihvr_segment_params* sp);
  * are not applied.  Objects come in the reference's order (first appearance
  * by linear index, then the size filter's swaps).  At most max_objects are
  * written; *num_objects receives the count, and a count above max_objects
- * returns RIHVR_ERR_INVALID_ARGUMENT.  info may be NULL.  Temporary device
- * memory: about 4 bytes a voxel plus the object lists. */
+ * returns RIHVR_ERR_INVALID_ARGUMENT.  info may be NULL.  Device memory:
+ * three bit-packed volumes and two 32-bit counts a 32-voxel word (about half a
+ * byte a voxel) plus lists over the voxels that are on after the closing and
+ * over the objects; the context keeps them for the next call and
+ * rihvr_destroy frees them. */
 int rihvr_segment(rihvr_ctx* ctx, const rihvr_segment_params* sp, rihvr_object* objects, int max_objects,
                   int* num_objects, rihvr_segment_info* info);
 /* The same on a stack of voxel intensities I (num_planes x height x width
  * floats, the values a voxel file holds; zero where the file has no voxel),
- * on the device or the host. */
+ * on the device or the host.  Runs on the legacy default stream; its device
+ * buffers are allocated and freed within the call. */
 int rihvr_segment_intensity(const float* intensity, int width, int height, int num_planes, int is_device,
                             const rihvr_segment_params* sp, rihvr_object* objects, int max_objects,
                             int* num_objects, rihvr_segment_info* info);

@@ -317,4 +317,12 @@ __device__ __forceinline__ double warp_sum(double v) {
   return v;
 }
 
+// the FISTA point x = P + beta (P - Pprev) of voxel i, as every kernel that
+// reads the volume forms it
+template <typename ST>
+__device__ __forceinline__ float2 xval(const ST* P, const ST* Pp, float beta, size_t i) {
+  const float2 p = Store<ST>::ld(P + i), pp = Store<ST>::ld(Pp + i);
+  return make_float2(fmaf(beta, p.x - pp.x, p.x), fmaf(beta, p.y - pp.y, p.y));
+}
+
 }  // namespace rihvr

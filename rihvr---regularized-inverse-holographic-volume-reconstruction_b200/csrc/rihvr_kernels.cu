@@ -1776,11 +1776,6 @@ cudaError_t launch_holo_momentum(const float* dnew, float* dY0, float* dX, const
 // L1 and TV norms of the momentum point x = P + beta (P - Pprev):
 // calcL1NormComplex (sparse_volume.cu:194-235), calcTVNorm2d (:365-446),
 // calcTVNorm (:240-363, periodic in z).
-template <typename ST>
-__device__ __forceinline__ float2 xval(const ST* P, const ST* Pp, float beta, size_t i) {
-  const float2 p = Store<ST>::ld(P + i), pp = Store<ST>::ld(Pp + i);
-  return make_float2(fmaf(beta, p.x - pp.x, p.x), fmaf(beta, p.y - pp.y, p.y));
-}
 
 template <typename ST>
 __global__ void __launch_bounds__(FLAT_THREADS) k_momentum_norms(const ST* __restrict__ P, const ST* __restrict__ Pp,

@@ -54,10 +54,14 @@ bool generic_size_supported(int n);
 // message returned by rihvr_last_error on this thread
 void set_last_error(const char* msg);
 
-// particle segmentation of a dense complex FP32 volume on stream st
-// (rihvr_segment.cu)
-int segment_complex(const float2* vol, int W, int H, int Nz, const rihvr_segment_params* sp, rihvr_object* objects,
-                    int max_objects, int* num_objects, rihvr_segment_info* info, cudaStream_t st);
+// particle segmentation of the volume x = P + beta (P - Pprev) on stream st,
+// with device buffers kept in a workspace between calls (rihvr_segment.cu)
+struct SegWorkspace;
+SegWorkspace* seg_workspace_create();
+void seg_workspace_destroy(SegWorkspace* ws);
+int segment_volume(int storage, const void* P, const void* Pprev, float beta, int W, int H, int Nz,
+                   const rihvr_segment_params* sp, rihvr_object* objects, int max_objects, int* num_objects,
+                   rihvr_segment_info* info, SegWorkspace* ws, cudaStream_t st);
 size_t max_partial_blocks(int W, int H, int Nz);
 
 cudaError_t launch_adj_col(const float2* Rs, const double* cturn, const double* zlist, float2* U, int W,

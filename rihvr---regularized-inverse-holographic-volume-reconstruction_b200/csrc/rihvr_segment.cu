@@ -20,7 +20,9 @@
 //    intensity the CSV would hold, which is what every step of the reference
 //    computes from a loaded voxel; only the CSV's printing of I to seven
 //    significant digits is skipped (rihvr_segment_intensity takes I as given,
-//    so a CSV's values reproduce the reference's input exactly);
+//    so a CSV's values reproduce the reference's input exactly).  The
+//    solver's volume is read in place, x = P + beta (P - Pprev) formed per
+//    voxel as the solver forms it;
 //  * the binary volumes are bit-packed, 32 voxels of a row per word, rows
 //    padded to whole words; binarization packs with a warp ballot;
 //  * dilation and erosion by the ball are word-parallel: for every (dz, dy)
@@ -32,22 +34,30 @@
 //  * labelling is a lock-free union-find in which every link points to a
 //    smaller linear index, so each root is its component's smallest index,
 //    the reference's label;
-//  * object ids follow the order of the roots (an exclusive scan of per-word
-//    root counts), which is the reference's order of first appearance; each
-//    object's voxels are sorted by index and reduced by one thread in that
-//    order, so the FP32 weighted sums round exactly as the reference's
-//    sequential loops do.  The final divisions and the size filter run on the
-//    host, in the reference's order.
+//  * labels live in rank space (one entry per voxel that is on after the
+//    closing, numbered in index order), so memory follows the particles, not
+//    the volume;
+//  * object ids follow the order of the roots (an exclusive scan of root
+//    flags), which is the reference's order of first appearance; a stable
+//    radix sort (CUB) on the object id puts each object's voxels together in
+//    index order, and one thread per object reduces them in that order, so
+//    the FP32 weighted sums round exactly as the reference's sequential loops
+//    do.  The final divisions and the size filter run on the host, in the
+//    reference's order.
 #include <cuda_runtime.h>
+
+#include <cub/device/device_radix_sort.cuh>
 
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/rihvr.h"
+#include "rihvr_device.cuh"
 #include "rihvr_kernels.cuh"
 
 namespace rihvr {
@@ -71,37 +81,88 @@ __device__ __forceinline__ float q_from_intensity(float I) {
   const float s = sqrtf(I);
   return __fmul_rn(s, s);
 }
-__device__ __forceinline__ float q_at(const float2* v, size_t i) {
-  const float2 a = v[i];
+__device__ __forceinline__ float q_from_value(float2 a) {
   return q_from_intensity(__fadd_rn(__fmul_rn(a.x, a.x), __fmul_rn(a.y, a.y)));
 }
-__device__ __forceinline__ float q_at(const float* v, size_t i) { return q_from_intensity(v[i]); }
 
-// largest q (non-negative floats order like their bit patterns)
+// Voxel sources.  IntensitySrc: the intensities of a voxel file.  VolumeSrc:
+// the solver's volume x = P + beta (P - Pprev), formed on the fly as the
+// solver forms it, in the storage type of P.
+struct IntensitySrc {
+  const float* I;
+  __device__ __forceinline__ float q(size_t i) const { return q_from_intensity(__ldg(I + i)); }
+};
+// q values already formed (stored by the max pass)
+struct QSrc {
+  const float* q_;
+  __device__ __forceinline__ float q(size_t i) const { return __ldg(q_ + i); }
+};
+template <typename ST>
+struct VolumeSrc {
+  const ST* P;
+  const ST* Pp;
+  float beta;
+  __device__ __forceinline__ float q(size_t i) const { return q_from_value(xval(P, Pp, beta, i)); }
+};
+
+// largest q (non-negative floats order like their bit patterns); four
+// independent loads a thread in flight
+// (qout, when given, receives every q for the threshold pass)
 template <typename SRC>
-__global__ void k_max_q(const SRC* __restrict__ src, unsigned long long n, unsigned* __restrict__ out_bits) {
+__global__ void k_max_q(SRC src, unsigned long long n, unsigned* __restrict__ out_bits, float* __restrict__ qout) {
   unsigned m = 0;
-  for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
-       i += (unsigned long long)gridDim.x * blockDim.x)
-    m = max(m, __float_as_uint(q_at(src, i)));
+  const unsigned long long stride = (unsigned long long)gridDim.x * blockDim.x;
+  unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x;
+  for (; i + 3 * stride < n; i += 4 * stride) {
+    const float a = src.q(i), b = src.q(i + stride), c = src.q(i + 2 * stride), e = src.q(i + 3 * stride);
+    if (qout) {
+      qout[i] = a;
+      qout[i + stride] = b;
+      qout[i + 2 * stride] = c;
+      qout[i + 3 * stride] = e;
+    }
+    m = max(m, max(max(__float_as_uint(a), __float_as_uint(b)), max(__float_as_uint(c), __float_as_uint(e))));
+  }
+  for (; i < n; i += stride) {
+    const float a = src.q(i);
+    if (qout) qout[i] = a;
+    m = max(m, __float_as_uint(a));
+  }
   m = __reduce_max_sync(0xffffffffu, m);
   if ((threadIdx.x & 31) == 0) atomicMax(out_bits, m);
 }
 
-// one warp per word: lane b holds voxel 32 w + b of the row; q > thr compared
-// in FP64 as binarize_kernel does (sparse_segmentation.cu:39-49)
+// A warp makes eight words at a time (eight loads a lane in flight): lane b
+// holds voxel 32 w + b of its row; q > thr compared in FP64 as binarize_kernel
+// does (sparse_segmentation.cu:39-49).  Rows with a voxel on are flagged for
+// the morphology.
 template <typename SRC>
-__global__ void k_binarize(const SRC* __restrict__ src, Dims d, double thr, unsigned* __restrict__ bits) {
+__global__ void k_binarize(SRC src, Dims d, double thr, unsigned* __restrict__ bits,
+                           unsigned char* __restrict__ row_on) {
+  constexpr int U = 8;
   const int lane = threadIdx.x & 31;
-  const long long warp = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-  const long long nwarps = ((long long)gridDim.x * blockDim.x) >> 5;
-  for (long long w = warp; w < d.nwords; w += nwarps) {
-    const long long row = w / d.WW;
-    const int x = (int)(w - row * d.WW) * 32 + lane;
-    bool on = false;
-    if (x < d.W) on = (double)q_at(src, (size_t)row * d.W + x) > thr;
-    const unsigned b = __ballot_sync(0xffffffffu, on);
-    if (lane == 0) bits[w] = b;
+  const unsigned nw = (unsigned)d.nwords, WW = (unsigned)d.WW;  // indices fit in 32 bits
+  const unsigned warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const unsigned nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (unsigned w0 = warp * U; w0 < nw; w0 += nwarps * U) {
+    float q[U];
+    unsigned row[U];
+#pragma unroll
+    for (int k = 0; k < U; ++k) {
+      const unsigned w = w0 + k;
+      row[k] = w / WW;
+      const int x = (int)(w - row[k] * WW) * 32 + lane;
+      q[k] = (w < nw && x < d.W) ? src.q((size_t)row[k] * d.W + x) : -1.f;
+    }
+#pragma unroll
+    for (int k = 0; k < U; ++k) {
+      const unsigned b = __ballot_sync(0xffffffffu, q[k] >= 0.f && (double)q[k] > thr);
+      const unsigned w = w0 + k;
+      if (lane == 0 && w < nw) {
+        bits[w] = b;
+        if (b) row_on[row[k]] = 1;
+      }
+    }
   }
 }
 
@@ -110,41 +171,66 @@ __device__ __forceinline__ unsigned shifted(unsigned wm1, unsigned w0, unsigned 
   return s >= 0 ? __funnelshift_r(w0, wp1, s) : __funnelshift_l(wm1, w0, -s);
 }
 
-// One output word a thread.  DILATE: OR over the ball of the in-bounds input
-// bits; otherwise (erosion) AND over the ball with out-of-bounds positions
-// as 0.  Bits past the row's end stay 0.
+// One warp per 32 consecutive words of a row; lane l makes word 32 c + l.
+// DILATE: OR over the ball of the in-bounds input bits; otherwise (erosion)
+// AND over the ball with out-of-bounds positions as 0.  Bits past the row's
+// end stay 0.  The ball's rows are taken 32 at a time: each lane looks up
+// one row's flag (row_in: the row has a voxel on), a ballot gives the warp the
+// rows to visit; the dilation visits only those, the erosion ends at 0 when
+// any is missing.  Rows of the output with a voxel on are flagged in row_out.
 template <bool DILATE>
-__global__ void k_morph(const unsigned* __restrict__ in, unsigned* __restrict__ out, Dims d, int nrows) {
-  for (long long w = (long long)blockIdx.x * blockDim.x + threadIdx.x; w < d.nwords;
-       w += (long long)gridDim.x * blockDim.x) {
-    const long long row = w / d.WW;
-    const int wx = (int)(w - row * d.WW);
-    const int y = (int)(row % d.H), z = (int)(row / d.H);
+__global__ void k_morph(const unsigned* __restrict__ in, unsigned* __restrict__ out, Dims d, int nrows,
+                        const unsigned char* __restrict__ row_in, unsigned char* __restrict__ row_out) {
+  const int lane = threadIdx.x & 31;
+  const unsigned WW = (unsigned)d.WW, Hu = (unsigned)d.H;  // 32-bit indices
+  const unsigned chunks = (WW + 31) / 32;
+  const unsigned ntask = (unsigned)d.H * (unsigned)d.Nz * chunks;
+  const unsigned warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const unsigned nwarps = (gridDim.x * blockDim.x) >> 5;
+  for (unsigned task = warp; task < ntask; task += nwarps) {
+    const unsigned row = task / chunks;
+    const int wx = (int)(task - row * chunks) * 32 + lane;
+    const unsigned zu = row / Hu;
+    const int y = (int)(row - zu * Hu), z = (int)zu;
     unsigned acc = DILATE ? 0u : ~0u;
-    for (int r = 0; r < nrows; ++r) {
-      const int e = c_rows[r];
-      const int dz = (e >> 16) - 64, dy = ((e >> 8) & 0xff) - 64, rx = e & 0xff;
-      const int zz = z + dz, yy = y + dy;
-      if (zz < 0 || zz >= d.Nz || yy < 0 || yy >= d.H) {
-        if (DILATE) continue;
-        acc = 0u;
+    bool zero = false;
+    for (int r0 = 0; r0 < nrows && !zero; r0 += 32) {
+      const int r = r0 + lane;
+      bool live = false;
+      if (r < nrows) {
+        const int e = c_rows[r];
+        const int zz = z + (e >> 16) - 64, yy = y + ((e >> 8) & 0xff) - 64;
+        live = zz >= 0 && zz < d.Nz && yy >= 0 && yy < d.H && __ldg(row_in + (unsigned)zz * Hu + yy);
+      }
+      unsigned mask = __ballot_sync(0xffffffffu, live);
+      const int nin = min(32, nrows - r0);
+      if (!DILATE && mask != (nin == 32 ? 0xffffffffu : (1u << nin) - 1u)) {
+        zero = true;
         break;
       }
-      const unsigned* rp = in + ((long long)zz * d.H + yy) * d.WW;
-      const unsigned w0 = __ldg(rp + wx);
-      const unsigned wm1 = wx > 0 ? __ldg(rp + wx - 1) : 0u;
-      const unsigned wp1 = wx + 1 < d.WW ? __ldg(rp + wx + 1) : 0u;
-      unsigned a = w0;
-      for (int s = 1; s <= rx; ++s) {
-        const unsigned l = shifted(wm1, w0, wp1, -s), h = shifted(wm1, w0, wp1, s);
-        a = DILATE ? (a | l | h) : (a & l & h);
+      for (; mask; mask &= mask - 1) {
+        const int e = c_rows[r0 + __ffs(mask) - 1];
+        const int zz = z + (e >> 16) - 64, yy = y + ((e >> 8) & 0xff) - 64, rx = e & 0xff;
+        if (wx >= d.WW) continue;
+        const unsigned* rp = in + ((unsigned)zz * Hu + yy) * WW;
+        const unsigned w0 = __ldg(rp + wx);
+        const unsigned wm1 = wx > 0 ? __ldg(rp + wx - 1) : 0u;
+        const unsigned wp1 = wx + 1 < d.WW ? __ldg(rp + wx + 1) : 0u;
+        unsigned a = w0;
+        for (int s = 1; s <= rx; ++s) {
+          const unsigned l = shifted(wm1, w0, wp1, -s), h = shifted(wm1, w0, wp1, s);
+          a = DILATE ? (a | l | h) : (a & l & h);
+        }
+        acc = DILATE ? (acc | a) : (acc & a);
       }
-      acc = DILATE ? (acc | a) : (acc & a);
-      if (!DILATE && acc == 0u) break;
     }
-    const int valid = d.W - wx * 32;
-    if (valid < 32) acc &= (1u << valid) - 1u;
-    out[w] = acc;
+    if (zero) acc = 0u;
+    if (wx < d.WW) {
+      const int valid = d.W - wx * 32;
+      if (valid < 32) acc &= (1u << valid) - 1u;
+      out[row * WW + wx] = acc;
+    }
+    if (__any_sync(0xffffffffu, wx < d.WW && acc != 0u) && lane == 0) row_out[row] = 1;
   }
 }
 
@@ -182,9 +268,14 @@ __device__ void unite(unsigned* L, unsigned a, unsigned b, int* err) {
   atomicExch(err, 1);
 }
 
-__device__ __forceinline__ bool bit_at(const unsigned* bits, const Dims& d, int x, int y, int z) {
-  const long long w = ((long long)z * d.H + y) * d.WW + (x >> 5);
-  return (__ldg(bits + w) >> (x & 31)) & 1u;
+// rank of an on voxel among all on voxels in index order: the on-voxel count
+// of the words before it plus the bits below it in its word
+__device__ __forceinline__ unsigned rank_at(const unsigned* bits, const unsigned* onoff, const Dims& d, int x,
+                                            int y, int z, bool* on) {
+  const unsigned w = ((unsigned)z * (unsigned)d.H + (unsigned)y) * (unsigned)d.WW + (unsigned)(x >> 5);
+  const unsigned m = __ldg(bits + w);
+  *on = (m >> (x & 31)) & 1u;
+  return __ldg(onoff + w) + __popc(m & ((1u << (x & 31)) - 1u));
 }
 
 // in-plane neighbour (x + dx, y + dy).  Reference neighbourhood (faithful):
@@ -205,93 +296,89 @@ __device__ __forceinline__ bool neighbour_xy(const Dims& d, int faithful, int x,
   return *nx >= 0 && *nx < d.W && *ny >= 0 && *ny < d.H;
 }
 
-template <int PHASE>  // 0: labels[i] = i; 1: unite with the 13 earlier neighbours; 2: labels[i] = root
-__global__ void k_ccl(const unsigned* __restrict__ bits, unsigned* L, Dims d, int faithful, int* err) {
-  for (long long w = (long long)blockIdx.x * blockDim.x + threadIdx.x; w < d.nwords;
-       w += (long long)gridDim.x * blockDim.x) {
+// Labels live in rank space (one entry per on voxel, in index order), so a
+// smaller rank is a smaller linear index and each root is its component's
+// smallest index.
+__global__ void k_label_init(unsigned* __restrict__ L, unsigned m) {
+  for (unsigned r = blockIdx.x * blockDim.x + threadIdx.x; r < m; r += gridDim.x * blockDim.x) L[r] = r;
+}
+
+// linear index of every on voxel, by rank
+__global__ void k_rank_index(const unsigned* __restrict__ bits, const unsigned* __restrict__ onoff, Dims d,
+                             unsigned* __restrict__ idx) {
+  const unsigned nw = (unsigned)d.nwords, WW = (unsigned)d.WW;
+  for (unsigned w = blockIdx.x * blockDim.x + threadIdx.x; w < nw; w += gridDim.x * blockDim.x) {
     unsigned m = bits[w];
     if (!m) continue;
-    const long long row = w / d.WW;
-    const int x0 = (int)(w - row * d.WW) * 32;
-    const int y = (int)(row % d.H), z = (int)(row / d.H);
-    const unsigned base = (unsigned)(row * d.W);
-    while (m) {
-      const int b = __ffs(m) - 1;
-      m &= m - 1;
-      const int x = x0 + b;
-      const unsigned i = base + (unsigned)x;
-      if (PHASE == 0) {
-        L[i] = i;
-      } else if (PHASE == 2) {
-        L[i] = find_root(L, i, err);
-      } else {
+    const unsigned row = w / WW;
+    const unsigned base = row * (unsigned)d.W + (w - row * WW) * 32u;
+    for (unsigned r = onoff[w]; m; m &= m - 1, ++r) idx[r] = base + (unsigned)(__ffs(m) - 1);
+  }
+}
+
+// union of every on voxel (one thread each) with its 13 earlier neighbours
+// (the plane below, or a negative in-plane offset).  When the voxel before it
+// in the row (offset -1) is on, the neighbours the two share are already
+// joined to that voxel by its own thread, and only the 4 on the far side
+// (dx = +1: one in the plane, three below) remain.
+__global__ void k_label_merge(const unsigned* __restrict__ bits, const unsigned* __restrict__ onoff,
+                              const unsigned* __restrict__ idx, unsigned* L, unsigned m, Dims d, int faithful,
+                              int* err) {
+  const unsigned HW = (unsigned)d.W * (unsigned)d.H;
+  for (unsigned r = blockIdx.x * blockDim.x + threadIdx.x; r < m; r += gridDim.x * blockDim.x) {
+    const unsigned i = idx[r];
+    const int z = (int)(i / HW);
+    const unsigned pl = i - (unsigned)z * HW;
+    const int y = (int)(pl / (unsigned)d.W), x = (int)(pl - (unsigned)y * d.W);
+    int nx, ny;
+    bool left = false;
+    if (neighbour_xy(d, faithful, x, y, -1, 0, &nx, &ny)) {
+      const unsigned rl = rank_at(bits, onoff, d, nx, ny, z, &left);
+      if (left) unite(L, r, rl, err);
+    }
 #pragma unroll 1
-        for (int dz = -1; dz <= 0; ++dz) {
-          const int zz = z + dz;
-          if (zz < 0) continue;
-#pragma unroll 1
-          for (int dy = -1; dy <= 1; ++dy)
-#pragma unroll 1
-            for (int dx = -1; dx <= 1; ++dx) {
-              // earlier neighbours only: the plane below, or a negative in-plane offset
-              if (dz == 0 && dy * d.W + dx >= 0) continue;
-              int nx, ny;
-              if (!neighbour_xy(d, faithful, x, y, dx, dy, &nx, &ny)) continue;
-              if (!bit_at(bits, d, nx, ny, zz)) continue;
-              unite(L, i, (unsigned)(((long long)zz * d.H + ny) * d.W + nx), err);
-            }
+    for (int dz = -1; dz <= 0; ++dz) {
+      const int zz = z + dz;
+      if (zz < 0) continue;
+#pragma unroll
+      for (int dy = -1; dy <= 1; ++dy)
+#pragma unroll
+        for (int dx = -1; dx <= 1; ++dx) {
+          if (dz == 0 && (dy * d.W + dx >= 0 || (dy == 0 && dx == -1))) continue;  // later, or the left one
+          if (left && dx != 1) continue;
+          if (!neighbour_xy(d, faithful, x, y, dx, dy, &nx, &ny)) continue;
+          bool on;
+          const unsigned rj = rank_at(bits, onoff, d, nx, ny, zz, &on);
+          if (on) unite(L, r, rj, err);
         }
-      }
     }
   }
 }
 
-// roots (labels[i] == i) as a bit volume, and their count a word
-__global__ void k_roots(const unsigned* __restrict__ bits, const unsigned* __restrict__ L, Dims d,
-                        unsigned* __restrict__ rbits, unsigned* __restrict__ rcount) {
-  for (long long w = (long long)blockIdx.x * blockDim.x + threadIdx.x; w < d.nwords;
-       w += (long long)gridDim.x * blockDim.x) {
-    unsigned m = bits[w], r = 0;
-    const long long row = w / d.WW;
-    const unsigned base = (unsigned)(row * d.W) + (unsigned)(w - row * d.WW) * 32u;
-    while (m) {
-      const int b = __ffs(m) - 1;
-      m &= m - 1;
-      if (L[base + b] == base + b) r |= 1u << b;
-    }
-    rbits[w] = r;
-    rcount[w] = __popc(r);
+// labels to roots; root flags for the object numbering
+__global__ void k_label_flatten(unsigned* L, unsigned m, unsigned* __restrict__ is_root, int* err) {
+  for (unsigned r = blockIdx.x * blockDim.x + threadIdx.x; r < m; r += gridDim.x * blockDim.x) {
+    const unsigned root = find_root(L, r, err);
+    L[r] = root;
+    is_root[r] = root == r;
   }
 }
 
-// object id of root r: roots before it in index order
-__device__ __forceinline__ unsigned object_of(unsigned r, const Dims& d, const unsigned* rbits,
-                                              const unsigned* roff) {
-  const unsigned row = r / (unsigned)d.W;
-  const unsigned x = r - row * (unsigned)d.W;
-  const long long w = (long long)row * d.WW + (x >> 5);
-  return roff[w] + __popc(rbits[w] & ((1u << (x & 31)) - 1u));
+// object of every on voxel (the number of roots before its root), its rank
+// as the sort value, and the voxel counts per object
+__global__ void k_object_keys(const unsigned* __restrict__ L, const unsigned* __restrict__ root_rank, unsigned m,
+                              unsigned* __restrict__ key, unsigned* __restrict__ val, unsigned* __restrict__ cnt) {
+  for (unsigned r = blockIdx.x * blockDim.x + threadIdx.x; r < m; r += gridDim.x * blockDim.x) {
+    const unsigned o = root_rank[L[r]];
+    key[r] = o;
+    val[r] = r;
+    atomicAdd(cnt + o, 1u);
+  }
 }
 
-template <int PHASE>  // 0: count voxels per object; 1: scatter voxel indices
-__global__ void k_objects(const unsigned* __restrict__ bits, const unsigned* __restrict__ L, Dims d,
-                          const unsigned* __restrict__ rbits, const unsigned* __restrict__ roff,
-                          unsigned* __restrict__ cnt, const unsigned* __restrict__ off,
-                          unsigned* __restrict__ vox) {
-  for (long long w = (long long)blockIdx.x * blockDim.x + threadIdx.x; w < d.nwords;
-       w += (long long)gridDim.x * blockDim.x) {
-    unsigned m = bits[w];
-    const long long row = w / d.WW;
-    const unsigned base = (unsigned)(row * d.W) + (unsigned)(w - row * d.WW) * 32u;
-    while (m) {
-      const int b = __ffs(m) - 1;
-      m &= m - 1;
-      const unsigned i = base + b;
-      const unsigned o = object_of(L[i], d, rbits, roff);
-      const unsigned k = atomicAdd(cnt + o, 1u);
-      if (PHASE == 1) vox[off[o] + k] = i;
-    }
-  }
+__global__ void k_popc(const unsigned* __restrict__ bits, unsigned* __restrict__ cnt, long long n) {
+  for (long long w = (long long)blockIdx.x * blockDim.x + threadIdx.x; w < n; w += (long long)gridDim.x * blockDim.x)
+    cnt[w] = __popc(bits[w]);
 }
 
 struct ObjSums {
@@ -302,58 +389,48 @@ struct ObjSums {
   int n, xmin, xmax, ymin, ymax, zmin, zmax;
 };
 
-// in-place heapsort of one object's voxel indices (distinct keys)
-__device__ void heap_sort(unsigned* a, unsigned n) {
-  auto sift = [&](unsigned i, unsigned end) {
-    for (;;) {
-      unsigned c = 2 * i + 1;
-      if (c >= end) return;
-      if (c + 1 < end && a[c + 1] > a[c]) ++c;
-      if (a[i] >= a[c]) return;
-      const unsigned t = a[i];
-      a[i] = a[c];
-      a[c] = t;
-      i = c;
-    }
-  };
-  if (n < 2) return;
-  for (unsigned i = n / 2; i-- > 0;) sift(i, n);
-  for (unsigned end = n - 1; end > 0; --end) {
-    const unsigned t = a[0];
-    a[0] = a[end];
-    a[end] = t;
-    sift(0, end);
+// Voxels sorted by (object, index): their coordinates and weights, in that
+// order.  The weight of a voxel is its q where the thresholded volume had it
+// (the masked complex volume, sparse_segmentation.cu:51-59, 95-96), else 0
+// (object_cloud.cu:269-289).
+template <typename SRC>
+__global__ void k_gather(SRC src, const unsigned* __restrict__ bits0, Dims d,
+                         const unsigned* __restrict__ idx, const unsigned* __restrict__ sorted_rank, unsigned m,
+                         int4* __restrict__ rec) {
+  const unsigned HW = (unsigned)d.W * (unsigned)d.H;
+  for (unsigned j = blockIdx.x * blockDim.x + threadIdx.x; j < m; j += gridDim.x * blockDim.x) {
+    const unsigned i = idx[sorted_rank[j]];
+    const int z = (int)(i / HW);
+    const unsigned pl = i - (unsigned)z * HW;
+    const int y = (int)(pl / (unsigned)d.W), x = (int)(pl - (unsigned)y * d.W);
+    const long long w = ((long long)z * d.H + y) * d.WW + (x >> 5);
+    const bool on = (bits0[w] >> (x & 31)) & 1u;
+    rec[j] = make_int4(x, y, z, __float_as_int(on ? src.q(i) : 0.f));
   }
 }
 
-// One object a thread: sort its voxels, then the reference's sequential sums.
-// The weight of a voxel is its q where the thresholded volume had it (the
-// masked complex volume, sparse_segmentation.cu:51-59, 95-96), else 0
-// (object_cloud.cu:269-289).
-template <typename SRC>
-__global__ void k_finish(const SRC* __restrict__ src, const unsigned* __restrict__ bits0, Dims d,
-                         const unsigned* __restrict__ off, unsigned nobj, unsigned* __restrict__ vox,
+// One object a thread, over its voxels in index order: the reference's
+// sequential sums (Blob3d::getCentroid, getWeightedCentroid, getMaxValue,
+// getMeanValue, findBounds).
+__global__ void k_finish(const int4* __restrict__ rec, const unsigned* __restrict__ off, unsigned nobj,
                          ObjSums* __restrict__ out) {
   const unsigned o = blockIdx.x * blockDim.x + threadIdx.x;
   if (o >= nobj) return;
-  unsigned* v = vox + off[o];
-  const unsigned n = off[o + 1] - off[o];
-  heap_sort(v, n);
+  const unsigned j0 = off[o], j1 = off[o + 1];
   ObjSums s;
   s.sx = s.sy = s.sz = 0;
   s.wsx = s.wsy = s.wsz = s.wsum = 0.f;
   s.vsum = 0.0;
-  s.n = (int)n;
-  float vmax = 0.f;
-  const unsigned HW = (unsigned)d.W * (unsigned)d.H;
-  for (unsigned k = 0; k < n; ++k) {
-    const unsigned i = v[k];
-    const int z = (int)(i / HW);
-    const unsigned p = i - (unsigned)z * HW;
-    const int y = (int)(p / (unsigned)d.W), x = (int)(p - (unsigned)y * d.W);
-    const long long w = ((long long)z * d.H + y) * d.WW + (x >> 5);
-    const bool on = (bits0[w] >> (x & 31)) & 1u;
-    const float q = on ? q_at(src, i) : 0.f;
+  s.n = (int)(j1 - j0);
+  const int4 f = rec[j0];
+  s.xmin = s.xmax = f.x;
+  s.ymin = s.ymax = f.y;
+  s.zmin = s.zmax = f.z;
+  float vmax = __int_as_float(f.w);
+  for (unsigned j = j0; j < j1; ++j) {
+    const int4 e = rec[j];
+    const int x = e.x, y = e.y, z = e.z;
+    const float q = __int_as_float(e.w);
     s.sx += x;
     s.sy += y;
     s.sz += z;
@@ -362,19 +439,13 @@ __global__ void k_finish(const SRC* __restrict__ src, const unsigned* __restrict
     s.wsz = __fadd_rn(s.wsz, __fmul_rn(q, (float)z));
     s.wsum = __fadd_rn(s.wsum, q);
     s.vsum = __dadd_rn(s.vsum, (double)q);
-    vmax = (k == 0 || q > vmax) ? q : vmax;
-    if (k == 0) {
-      s.xmin = s.xmax = x;
-      s.ymin = s.ymax = y;
-      s.zmin = s.zmax = z;
-    } else {
-      s.xmin = min(s.xmin, x);
-      s.xmax = max(s.xmax, x);
-      s.ymin = min(s.ymin, y);
-      s.ymax = max(s.ymax, y);
-      s.zmin = min(s.zmin, z);
-      s.zmax = max(s.zmax, z);
-    }
+    vmax = q > vmax ? q : vmax;
+    s.xmin = min(s.xmin, x);
+    s.xmax = max(s.xmax, x);
+    s.ymin = min(s.ymin, y);
+    s.ymax = max(s.ymax, y);
+    s.zmin = min(s.zmin, z);
+    s.zmax = max(s.zmax, z);
   }
   s.vmax = vmax;
   out[o] = s;
@@ -450,21 +521,45 @@ int seg_fail(int code, const std::string& msg) {
                       std::string(#call) + ": " + cudaGetErrorString(e_));                         \
   } while (0)
 
-// device buffers of one call, released on every return path
-struct Buffers {
-  std::vector<void*> ptrs;
-  ~Buffers() {
-    for (void* p : ptrs) cudaFree(p);
+}  // namespace
+
+namespace rihvr {
+// Device buffers of the segmentation, kept between calls and grown on demand:
+// a context owns one, so repeated segmentations allocate nothing after the
+// first; a standalone call uses a temporary one.
+struct SegWorkspace {
+  static constexpr int kSlots = 32;
+  void* p[kSlots] = {};
+  size_t cap[kSlots] = {};
+  int device = -1;
+  ~SegWorkspace() {
+    for (void* q : p)
+      if (q) cudaFree(q);
   }
   template <typename T>
-  cudaError_t alloc(T** p, size_t count) {
-    void* q = nullptr;
-    const cudaError_t e = cudaMalloc(&q, std::max<size_t>(count, 1) * sizeof(T));
-    if (e == cudaSuccess) ptrs.push_back(q);
-    *p = static_cast<T*>(q);
-    return e;
+  cudaError_t get(int slot, T** out, size_t count) {
+    const size_t bytes = std::max<size_t>(count, 1) * sizeof(T);
+    if (cap[slot] < bytes) {
+      if (p[slot]) cudaFree(p[slot]);
+      p[slot] = nullptr;
+      cap[slot] = 0;
+      const cudaError_t e = cudaMalloc(&p[slot], bytes);
+      if (e != cudaSuccess) return e;
+      cap[slot] = bytes;
+    }
+    *out = static_cast<T*>(p[slot]);
+    return cudaSuccess;
   }
 };
+SegWorkspace* seg_workspace_create() { return new SegWorkspace(); }
+void seg_workspace_destroy(SegWorkspace* ws) { delete ws; }
+}  // namespace rihvr
+
+namespace {
+
+enum Slot { S_MAX, S_ERR, S_Q, S_BITS0, S_BITS1, S_BITS2, S_ROW0, S_ROW1, S_ROW2, S_ONCNT, S_ONOFF, S_IDX, S_LAB, S_ROOT, S_RRANK, S_CNT,
+            S_OFF, S_KEY, S_VAL, S_KEY_S, S_VAL_S, S_REC, S_SUMS, S_SORT_TMP,
+            S_SCAN0 };  // S_SCAN0.. : block sums of the scan levels
 
 int grid_for(long long items, int threads) {
   static int sms = 0;
@@ -479,18 +574,19 @@ int grid_for(long long items, int threads) {
 }
 
 // exclusive scan of n counts, out[n] = total (out has n + 1 entries)
-int scan_exclusive(const unsigned* in, unsigned* out, long long n, Buffers& buf, cudaStream_t st,
+int scan_exclusive(const unsigned* in, unsigned* out, long long n, SegWorkspace& ws, int level, cudaStream_t st,
                    long long* launches) {
+  if (S_SCAN0 + 2 * level + 1 >= SegWorkspace::kSlots) return seg_fail(RIHVR_ERR_UNSUPPORTED_SIZE, "scan too deep");
   const long long nb = (n + kScanItems - 1) / kScanItems;
   unsigned* sums = nullptr;
-  SCK(buf.alloc(&sums, (size_t)nb + 1));
+  SCK(ws.get(S_SCAN0 + 2 * level, &sums, (size_t)nb + 1));
   k_scan_block<<<(unsigned)std::max<long long>(nb, 1), kScanThreads, 0, st>>>(in, out, n, sums);
   SCK(cudaGetLastError());
   ++*launches;
   if (nb > 1) {
     unsigned* offs = nullptr;
-    SCK(buf.alloc(&offs, (size_t)nb + 1));
-    int rc = scan_exclusive(sums, offs, nb, buf, st, launches);
+    SCK(ws.get(S_SCAN0 + 2 * level + 1, &offs, (size_t)nb + 1));
+    const int rc = scan_exclusive(sums, offs, nb, ws, level + 1, st, launches);
     if (rc != RIHVR_OK) return rc;
     k_scan_add<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(out, n, offs);
     SCK(cudaGetLastError());
@@ -519,14 +615,14 @@ int ball_rows(int cs, std::vector<int>& rows, int* nstrel) {
 }
 
 template <typename SRC>
-int segment_impl(const SRC* src, int W, int H, int Nz, const rihvr_segment_params* sp, rihvr_object* objects,
-                 int max_objects, int* num_objects, rihvr_segment_info* info, cudaStream_t st) {
+int segment_impl(SRC src, int W, int H, int Nz, const rihvr_segment_params* sp, rihvr_object* objects,
+                 int max_objects, int* num_objects, rihvr_segment_info* info, SegWorkspace& ws, cudaStream_t st) {
   if (!sp || !num_objects || (max_objects > 0 && !objects) || max_objects < 0)
     return seg_fail(RIHVR_ERR_INVALID_ARGUMENT, "NULL or negative argument");
   if (W <= 0 || H <= 0 || Nz <= 0) return seg_fail(RIHVR_ERR_INVALID_ARGUMENT, "volume dimensions must be positive");
   const unsigned long long nvox = (unsigned long long)W * H * Nz;
   if (nvox >= 0xffffffffull)
-    return seg_fail(RIHVR_ERR_UNSUPPORTED_SIZE, "volumes of 2^32 - 1 voxels or more are not supported (32-bit labels)");
+    return seg_fail(RIHVR_ERR_UNSUPPORTED_SIZE, "volumes of 2^32 - 1 voxels or more are not supported (32-bit indices)");
   if (sp->close_size > kMaxClose)
     return seg_fail(RIHVR_ERR_INVALID_ARGUMENT, "close_size above " + std::to_string(kMaxClose));
   Dims d;
@@ -537,23 +633,33 @@ int segment_impl(const SRC* src, int W, int H, int Nz, const rihvr_segment_param
   d.nwords = (long long)d.WW * H * Nz;
   d.nvox = nvox;
   long long launches = 0;
-  Buffers buf;
-  unsigned *maxbits, *bits0, *bits1, *bits2, *labels, *rbits, *rcount, *roff;
+  unsigned *maxbits, *bits0, *bits1, *bits2, *oncnt, *onoff;
   int* err;
-  SCK(buf.alloc(&maxbits, 1));
-  SCK(buf.alloc(&err, 1));
-  SCK(buf.alloc(&bits0, (size_t)d.nwords));
-  SCK(buf.alloc(&bits1, (size_t)d.nwords));
-  SCK(buf.alloc(&bits2, (size_t)d.nwords));
-  SCK(buf.alloc(&labels, (size_t)nvox));
-  SCK(buf.alloc(&rbits, (size_t)d.nwords));
-  SCK(buf.alloc(&rcount, (size_t)d.nwords));
-  SCK(buf.alloc(&roff, (size_t)d.nwords + 1));
+  SCK(ws.get(S_MAX, &maxbits, 1));
+  SCK(ws.get(S_ERR, &err, 1));
+  SCK(ws.get(S_BITS0, &bits0, (size_t)d.nwords));
+  SCK(ws.get(S_BITS1, &bits1, (size_t)d.nwords));
+  SCK(ws.get(S_BITS2, &bits2, (size_t)d.nwords));
+  SCK(ws.get(S_ONCNT, &oncnt, (size_t)d.nwords));
+  SCK(ws.get(S_ONOFF, &onoff, (size_t)d.nwords + 1));
+  unsigned char *row0, *row1, *row2;
+  const size_t nrows_vol = (size_t)H * Nz;
+  SCK(ws.get(S_ROW0, &row0, nrows_vol));
+  SCK(ws.get(S_ROW1, &row1, nrows_vol));
+  SCK(ws.get(S_ROW2, &row2, nrows_vol));
+  SCK(cudaMemsetAsync(row0, 0, nrows_vol, st));
+  SCK(cudaMemsetAsync(row1, 0, nrows_vol, st));
+  SCK(cudaMemsetAsync(row2, 0, nrows_vol, st));
   SCK(cudaMemsetAsync(maxbits, 0, sizeof(unsigned), st));
   SCK(cudaMemsetAsync(err, 0, sizeof(int), st));
 
-  // binarize (sparse_segmentation.cu:61-112): thr = min_intensity * max / 256
-  k_max_q<<<grid_for((long long)nvox, 256), 256, 0, st>>>(src, nvox, maxbits);
+  // binarize (sparse_segmentation.cu:61-112): thr = min_intensity * max / 256.
+  // A volume source's q values are kept from the max pass (4 bytes a voxel
+  // instead of reading P and Pprev again); intensities are read directly.
+  constexpr bool kStoreQ = !std::is_same<SRC, IntensitySrc>::value;
+  float* qbuf = nullptr;
+  if (kStoreQ) SCK(ws.get(S_Q, &qbuf, (size_t)nvox));
+  k_max_q<<<grid_for((long long)nvox, 256), 256, 0, st>>>(src, nvox, maxbits, qbuf);
   SCK(cudaGetLastError());
   ++launches;
   unsigned mb = 0;
@@ -562,72 +668,101 @@ int segment_impl(const SRC* src, int W, int H, int Nz, const rihvr_segment_param
   float maxq;
   std::memcpy(&maxq, &mb, sizeof(float));
   const double thr = sp->min_intensity * (double)maxq / 256.0;
-  k_binarize<<<grid_for(d.nwords * 32, 256), 256, 0, st>>>(src, d, thr, bits0);
+  if (kStoreQ)
+    k_binarize<<<grid_for(d.nwords * 4, 256), 256, 0, st>>>(QSrc{qbuf}, d, thr, bits0, row0);
+  else
+    k_binarize<<<grid_for(d.nwords * 4, 256), 256, 0, st>>>(src, d, thr, bits0, row0);
   SCK(cudaGetLastError());
   ++launches;
 
   // closing (:186-372): dilate then erode with the ball of radius close_size
   const unsigned* closed = bits0;
   int nstrel = 0;
+  const int gw = grid_for(d.nwords, 256);
   if (sp->close_size > 0) {
     std::vector<int> rows;
     const int nrows = ball_rows(sp->close_size, rows, &nstrel);
     SCK(cudaMemcpyToSymbolAsync(c_rows, rows.data(), sizeof(int) * nrows, 0, cudaMemcpyHostToDevice, st));
-    k_morph<true><<<grid_for(d.nwords, 256), 256, 0, st>>>(bits0, bits1, d, nrows);
+    const long long mtasks = (long long)H * Nz * ((d.WW + 31) / 32);
+    k_morph<true><<<grid_for(mtasks * 32, 256), 256, 0, st>>>(bits0, bits1, d, nrows, row0, row1);
     SCK(cudaGetLastError());
-    k_morph<false><<<grid_for(d.nwords, 256), 256, 0, st>>>(bits1, bits2, d, nrows);
+    k_morph<false><<<grid_for(mtasks * 32, 256), 256, 0, st>>>(bits1, bits2, d, nrows, row1, row2);
     SCK(cudaGetLastError());
     launches += 2;
     closed = bits2;
   }
 
-  // 26-connected labels, smallest linear index of each component (:467-555)
-  const int gw = grid_for(d.nwords, 256);
-  k_ccl<0><<<gw, 256, 0, st>>>(closed, labels, d, sp->faithful, err);
+  // on voxels in index order (their ranks), then 26-connected labels in rank
+  // space: each root is its component's smallest index (:467-555)
+  k_popc<<<gw, 256, 0, st>>>(closed, oncnt, d.nwords);
   SCK(cudaGetLastError());
-  k_ccl<1><<<gw, 256, 0, st>>>(closed, labels, d, sp->faithful, err);
-  SCK(cudaGetLastError());
-  k_ccl<2><<<gw, 256, 0, st>>>(closed, labels, d, sp->faithful, err);
-  SCK(cudaGetLastError());
-  k_roots<<<gw, 256, 0, st>>>(closed, labels, d, rbits, rcount);
-  SCK(cudaGetLastError());
-  launches += 4;
-  int rc = scan_exclusive(rcount, roff, d.nwords, buf, st, &launches);
+  ++launches;
+  int rc = scan_exclusive(oncnt, onoff, d.nwords, ws, 0, st, &launches);
   if (rc != RIHVR_OK) return rc;
-  unsigned nobj = 0;
-  int herr = 0;
-  SCK(cudaMemcpyAsync(&nobj, roff + d.nwords, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
-  SCK(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+  unsigned non = 0;
+  SCK(cudaMemcpyAsync(&non, onoff + d.nwords, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
   SCK(cudaStreamSynchronize(st));
-  if (herr) return seg_fail(RIHVR_ERR_INFINITE_LOOP, "connected-component labelling exceeded its iteration bound");
-
-  // objects in root order, each reduced over its voxels in index order
-  std::vector<ObjSums> sums(nobj);
-  unsigned nclosed = 0;
-  if (nobj > 0) {
-    unsigned *cnt, *off, *vox;
+  unsigned nobj = 0;
+  std::vector<ObjSums> sums;
+  if (non > 0) {
+    unsigned *idx, *lab, *is_root, *root_rank, *cnt, *off, *key, *val, *key_s, *val_s;
+    int4* rec;
     ObjSums* osum;
-    SCK(buf.alloc(&cnt, nobj));
-    SCK(buf.alloc(&off, (size_t)nobj + 1));
+    SCK(ws.get(S_IDX, &idx, non));
+    SCK(ws.get(S_LAB, &lab, non));
+    SCK(ws.get(S_ROOT, &is_root, non));
+    SCK(ws.get(S_RRANK, &root_rank, (size_t)non + 1));
+    const int gm = grid_for(non, 256);
+    k_rank_index<<<gw, 256, 0, st>>>(closed, onoff, d, idx);
+    SCK(cudaGetLastError());
+    k_label_init<<<gm, 256, 0, st>>>(lab, non);
+    SCK(cudaGetLastError());
+    k_label_merge<<<gm, 256, 0, st>>>(closed, onoff, idx, lab, non, d, sp->faithful, err);
+    SCK(cudaGetLastError());
+    k_label_flatten<<<gm, 256, 0, st>>>(lab, non, is_root, err);
+    SCK(cudaGetLastError());
+    launches += 4;
+    rc = scan_exclusive(is_root, root_rank, non, ws, 0, st, &launches);
+    if (rc != RIHVR_OK) return rc;
+    int herr = 0;
+    SCK(cudaMemcpyAsync(&nobj, root_rank + non, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
+    SCK(cudaMemcpyAsync(&herr, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    SCK(cudaStreamSynchronize(st));
+    if (herr) return seg_fail(RIHVR_ERR_INFINITE_LOOP, "connected-component labelling exceeded its iteration bound");
+
+    // voxels ordered by (object, index): a stable radix sort on the object id
+    // of voxels listed in index order; then each object is reduced in order
+    SCK(ws.get(S_CNT, &cnt, nobj));
+    SCK(ws.get(S_OFF, &off, (size_t)nobj + 1));
+    SCK(ws.get(S_KEY, &key, non));
+    SCK(ws.get(S_VAL, &val, non));
+    SCK(ws.get(S_KEY_S, &key_s, non));
+    SCK(ws.get(S_VAL_S, &val_s, non));
+    SCK(ws.get(S_REC, &rec, non));
+    SCK(ws.get(S_SUMS, &osum, nobj));
     SCK(cudaMemsetAsync(cnt, 0, sizeof(unsigned) * nobj, st));
-    k_objects<0><<<gw, 256, 0, st>>>(closed, labels, d, rbits, roff, cnt, nullptr, nullptr);
+    k_object_keys<<<gm, 256, 0, st>>>(lab, root_rank, non, key, val, cnt);
     SCK(cudaGetLastError());
     ++launches;
-    rc = scan_exclusive(cnt, off, nobj, buf, st, &launches);
+    rc = scan_exclusive(cnt, off, nobj, ws, 0, st, &launches);
     if (rc != RIHVR_OK) return rc;
-    SCK(cudaMemcpyAsync(&nclosed, off + nobj, sizeof(unsigned), cudaMemcpyDeviceToHost, st));
-    SCK(cudaStreamSynchronize(st));
-    SCK(buf.alloc(&vox, nclosed));
-    SCK(buf.alloc(&osum, nobj));
-    SCK(cudaMemsetAsync(cnt, 0, sizeof(unsigned) * nobj, st));
-    k_objects<1><<<gw, 256, 0, st>>>(closed, labels, d, rbits, roff, cnt, off, vox);
+    int end_bit = 1;
+    while (end_bit < 32 && (nobj >> end_bit) != 0) ++end_bit;
+    size_t tmp_bytes = 0;
+    SCK(cub::DeviceRadixSort::SortPairs(nullptr, tmp_bytes, key, key_s, val, val_s, (int)non, 0, end_bit, st));
+    unsigned char* tmp = nullptr;
+    SCK(ws.get(S_SORT_TMP, &tmp, tmp_bytes));
+    SCK(cub::DeviceRadixSort::SortPairs(tmp, tmp_bytes, key, key_s, val, val_s, (int)non, 0, end_bit, st));
+    k_gather<<<gm, 256, 0, st>>>(src, bits0, d, idx, val_s, non, rec);
     SCK(cudaGetLastError());
-    k_finish<<<(nobj + 127) / 128, 128, 0, st>>>(src, bits0, d, off, nobj, vox, osum);
+    k_finish<<<(nobj + 127) / 128, 128, 0, st>>>(rec, off, nobj, osum);
     SCK(cudaGetLastError());
     launches += 2;
+    sums.resize(nobj);
     SCK(cudaMemcpyAsync(sums.data(), osum, sizeof(ObjSums) * nobj, cudaMemcpyDeviceToHost, st));
     SCK(cudaStreamSynchronize(st));
   }
+  const unsigned nclosed = non;
 
   // Blob3d::getCentroid / getWeightedCentroid / getMaxValue / getMeanValue /
   // getBounds (blob3d.cu), then ObjectCloud::blobSizeFilter (object_cloud.cu:313-328)
@@ -678,9 +813,20 @@ int segment_impl(const SRC* src, int W, int H, int Nz, const rihvr_segment_param
 }  // namespace
 
 namespace rihvr {
-int segment_complex(const float2* vol, int W, int H, int Nz, const rihvr_segment_params* sp, rihvr_object* objects,
-                    int max_objects, int* num_objects, rihvr_segment_info* info, cudaStream_t st) {
-  return segment_impl(vol, W, H, Nz, sp, objects, max_objects, num_objects, info, st);
+int segment_volume(int storage, const void* P, const void* Pprev, float beta, int W, int H, int Nz,
+                   const rihvr_segment_params* sp, rihvr_object* objects, int max_objects, int* num_objects,
+                   rihvr_segment_info* info, SegWorkspace* ws, cudaStream_t st) {
+  switch (storage) {
+    case STORE_BF16:
+      return segment_impl(VolumeSrc<__nv_bfloat162>{(const __nv_bfloat162*)P, (const __nv_bfloat162*)Pprev, beta},
+                          W, H, Nz, sp, objects, max_objects, num_objects, info, *ws, st);
+    case STORE_F16:
+      return segment_impl(VolumeSrc<__half2>{(const __half2*)P, (const __half2*)Pprev, beta}, W, H, Nz, sp,
+                          objects, max_objects, num_objects, info, *ws, st);
+    default:
+      return segment_impl(VolumeSrc<float2>{(const float2*)P, (const float2*)Pprev, beta}, W, H, Nz, sp, objects,
+                          max_objects, num_objects, info, *ws, st);
+  }
 }
 }  // namespace rihvr
 
@@ -715,9 +861,12 @@ int rihvr_segment_intensity(const float* intensity, int width, int height, int n
     if (e != cudaSuccess) rc = seg_fail(RIHVR_ERR_CUDA, std::string("staging the intensities: ") + cudaGetErrorString(e));
     src = staged;
   }
-  if (rc == RIHVR_OK)
-    rc = segment_impl(src, width, height, num_planes, sp, objects, max_objects, num_objects, info, st);
-  cudaStreamSynchronize(st);
+  if (rc == RIHVR_OK) {
+    SegWorkspace ws;
+    rc = segment_impl(IntensitySrc{src}, width, height, num_planes, sp, objects, max_objects, num_objects, info,
+                      ws, st);
+    cudaStreamSynchronize(st);
+  }
   if (staged) cudaFree(staged);
   return rc;
 }

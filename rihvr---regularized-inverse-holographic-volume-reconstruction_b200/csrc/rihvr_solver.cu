@@ -117,6 +117,7 @@ struct rihvr_ctx {
   int g_mom_n = 0;
   bool graphs = true;                // cleared when a capture fails
   bool warm = false;                 // one iteration ran eagerly (attributes, tables)
+  SegWorkspace* seg_ws = nullptr;    // segmentation buffers, grown on first use
   // launch shapes chosen by the autotuner (0 = built-in choice)
   int tune_adj_chunks = 0, tune_tv_nseg = 0, tune_tv_kernel = 0;
   bool tuned = false;
@@ -656,6 +657,7 @@ void rihvr_destroy(rihvr_ctx* c) {
   if (!c) return;
   if (c->st) cudaStreamSynchronize(c->st);
   drop_graphs(c);
+  if (c->seg_ws) seg_workspace_destroy(c->seg_ws);
   for (void* p : c->allocs) cudaFree(p);
   if (c->sums_h) cudaFreeHost(c->sums_h);
   if (c->scal_h) cudaFreeHost(c->scal_h);
@@ -978,11 +980,11 @@ int rihvr_get_volume(rihvr_ctx* c, float* out, int is_device) {
 int rihvr_segment(rihvr_ctx* c, const rihvr_segment_params* sp, rihvr_object* objects, int max_objects,
                   int* num_objects, rihvr_segment_info* info) {
   if (!c) return fail(RIHVR_ERR_INVALID_ARGUMENT, "NULL context");
-  // the volume rihvr_get_volume returns, materialised in the intermediate buffer
-  KL(launch_materialize_x(c->storage, c->vol[c->iCur], c->vol[c->iPrev], (float)c->beta, c->U, (long long)c->V,
-                          c->st));
+  // the volume rihvr_get_volume returns, read in place
+  if (!c->seg_ws) c->seg_ws = seg_workspace_create();
   rihvr_segment_info local{};
-  const int rc = segment_complex(c->U, c->W, c->H, c->Nz, sp, objects, max_objects, num_objects, &local, c->st);
+  const int rc = segment_volume(c->storage, c->vol[c->iCur], c->vol[c->iPrev], (float)c->beta, c->W, c->H, c->Nz,
+                                sp, objects, max_objects, num_objects, &local, c->seg_ws, c->st);
   c->launches += local.kernel_launches;
   if (info) *info = local;
   return rc;

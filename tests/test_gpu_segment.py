@@ -66,14 +66,16 @@ def test_device_input_equals_host_input(rihvr):
     same_bits(as_rows(a), as_rows(c))
 
 
-def test_segment_of_a_solved_volume(rihvr, synthmod):
-    """Reconstruct a small hologram, then segment the solver's volume: the
-    oracle gets the voxel intensities |v|^2 (FP32, no contraction) of the
-    volume the solver returns."""
+@pytest.mark.parametrize("storage", [0, 1, 2])
+def test_segment_of_a_solved_volume(rihvr, synthmod, storage):
+    """Reconstruct a small hologram (FP32, BF16 or FP16 volume storage), then
+    segment the solver's volume in place: the oracle gets the voxel
+    intensities |v|^2 (FP32, no contraction) of the volume the solver
+    returns."""
     cfg = synthmod.config1()
     cfg.num_planes = 16
     _, b = synthmod.make_hologram(cfg)
-    p = rihvr.params_from_config(cfg)
+    p = rihvr.params_from_config(cfg, storage=storage)
     with rihvr.SparseCompressiveHolo(p, cfg.W, cfg.H) as s:
         s.setHologram(b)
         s.iterate(15)
