@@ -14,6 +14,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <mutex>
@@ -74,6 +75,95 @@ constexpr int kMaxFwdChunks = 16;  // partial spectra the forward column pass ma
 
 }  // namespace
 
+namespace {
+
+// FISTA control state kept on the device, so that whole iterations (attempt,
+// backtracks, momentum) replay as one graph without a host round trip.
+struct IterCtl {
+  double t, alpha1, beta, prev_f_resid;  // the host fields of the same names
+  double f_resid, lim, ratio;            // of the last attempt
+  int bt, it, it_base, pad;
+};
+// One iteration's record as the device writes it, plus the x-norm sums of its
+// first prox sweep, which settle the previous record (objective recording).
+struct DevRec {
+  rihvr_iter_record rec;
+  double prev_l1x, prev_tvx;
+};
+constexpr int kDevLogCap = 256;  // iterations between two host reads of the log
+
+// The attempt's prox scalars from t and beta, as prox_args computes them.
+__global__ void k_ctl_prep(IterCtl* s, float* scal, double tv, double l1, int zero_thr, int first) {
+  if (first) s->bt = 0;
+  const double t = s->t;
+  scal[0] = (float)s->beta;
+  scal[1] = (float)t;
+  scal[2] = (float)__dmul_rn(t, tv);
+  scal[3] = tv > 0 ? (float)__ddiv_rn(1.0, __dmul_rn(__dmul_rn(12.0, t), tv)) : 0.f;
+  scal[4] = zero_thr ? 0.f : (float)__dmul_rn(t, l1);
+}
+
+// Backtracking test of one_iteration: ratio = f_resid / (prev + lim); halve t
+// and go again while the ratio is outside [0, 1] and backtracks remain.
+__global__ void k_ctl_decide(IterCtl* s, const double* sums, int max_bt, cudaGraphConditionalHandle h, DevRec* log,
+                             int first) {
+  const double* sp = sums + SLOT_PROX * kNumSums;
+  if (first) {
+    DevRec& r = log[s->it - s->it_base];
+    r.prev_l1x = sp[SUM_L1X];
+    r.prev_tvx = sp[SUM_TVX];
+  }
+  const double t = s->t;
+  const double f_resid = 0.5 * sums[SLOT_FWD * kNumSums + SUM_RR];
+  const double lim = __dadd_rn(sp[SUM_LIM1], __ddiv_rn(sp[SUM_LIM2], __dmul_rn(2.0, t)));
+  const double ratio = __ddiv_rn(f_resid, __dadd_rn(s->prev_f_resid, lim));
+  s->f_resid = f_resid;
+  s->lim = lim;
+  s->ratio = ratio;
+  unsigned again = 0;
+  if (((ratio > 1.0) || (ratio < 0.0)) && s->bt < max_bt) {
+    s->t = t * 0.5;
+    s->bt += 1;
+    again = 1;
+  }
+  cudaGraphSetConditional(h, again);
+}
+
+// Record of the accepted attempt, fistaRestart (:471-475) and the alpha/beta
+// update (:476-481); beta goes to the hologram momentum.
+__global__ void k_ctl_finish(IterCtl* s, const double* sums, float* scal, DevRec* log, double l1, double tvw) {
+  const double* sp = sums + SLOT_PROX * kNumSums;
+  rihvr_iter_record& rec = log[s->it - s->it_base].rec;
+  rec.f_resid_prox = s->f_resid;
+  rec.lim = s->lim;
+  rec.ratio = s->ratio;
+  rec.t = s->t;
+  rec.backtracks = s->bt;
+  rec.restart_sum = sp[SUM_RS];
+  rec.f_prox = __dadd_rn(__dadd_rn(s->f_resid, __dmul_rn(l1, sp[SUM_L1P])), __dmul_rn(tvw, sp[SUM_TVP]));
+  rec.l1_x = rec.tv_x = 0.0;
+  const bool restarted = sp[SUM_RS] > 0.0;
+  const double alpha0 = restarted ? 1.0 : s->alpha1;
+  const double alpha1 = __ddiv_rn(__dadd_rn(1.0, sqrt(__dadd_rn(1.0, __dmul_rn(__dmul_rn(4.0, alpha0), alpha0)))), 2.0);
+  const double beta = __ddiv_rn(alpha0 - 1.0, alpha1);
+  rec.beta = beta;
+  rec.restarted = restarted ? 1 : 0;
+  s->alpha1 = alpha1;
+  s->beta = beta;
+  scal[8] = (float)beta;
+}
+
+// Residual at the new momentum point closes the record.
+__global__ void k_ctl_post(IterCtl* s, const double* sums, DevRec* log) {
+  rihvr_iter_record& rec = log[s->it - s->it_base].rec;
+  s->prev_f_resid = 0.5 * sums[SLOT_MOM * kNumSums + SUM_RR];
+  rec.f_resid_x = s->prev_f_resid;
+  rec.f_x = rec.f_resid_x;
+  s->it += 1;
+}
+
+}  // namespace
+
 struct rihvr_ctx {
   rihvr_params p{};
   int W = 0, H = 0, Nz = 0;
@@ -116,6 +206,15 @@ struct rihvr_ctx {
   cudaGraphExec_t g_mom = nullptr;
   int g_mom_n = 0;
   bool graphs = true;                // cleared when a capture fails
+  // whole iterations with the backtracking decided on the device: one graph
+  // per index of P_k, kernels in [first attempt + finish/momentum, backtrack]
+  cudaGraphExec_t g_iter[3] = {};
+  int g_iter_n[3][2] = {};
+  bool dev_loop = true;              // cleared when building such a graph fails
+  IterCtl* ctl_d = nullptr;
+  IterCtl* ctl_h = nullptr;          // pinned
+  DevRec* dlog_d = nullptr;
+  DevRec* dlog_h = nullptr;          // pinned
   bool warm = false;                 // one iteration ran eagerly (attributes, tables)
   SegWorkspace* seg_ws = nullptr;    // segmentation buffers, grown on first use
   // launch shapes chosen by the autotuner (0 = built-in choice)
@@ -381,6 +480,11 @@ void drop_graphs(rihvr_ctx* c) {
       }
   if (c->g_mom) cudaGraphExecDestroy(c->g_mom);
   c->g_mom = nullptr;
+  for (auto& g : c->g_iter)
+    if (g) {
+      cudaGraphExecDestroy(g);
+      g = nullptr;
+    }
 }
 
 bool use_graphs(const rihvr_ctx* c) { return c->graphs && c->warm && !c->profiling && c->mode != 6; }
@@ -411,6 +515,188 @@ int run_captured(rihvr_ctx* c, cudaGraphExec_t* g, int* nkernels, F enqueue) {
   CK(cudaGraphLaunch(*g, c->st));
   c->launches += *nkernels;
   return RIHVR_OK;
+}
+
+// Device-decided iterations.  An attempt: scalars from the device state, the
+// gradient (first attempt only), the prox, the forward operator and the
+// backtracking test, which sets the graph condition for another attempt.
+int enqueue_attempt_dev(rihvr_ctx* c, bool first, cudaGraphConditionalHandle h) {
+  const double tv = (double)c->p.regularization_TV_param, l1 = (double)c->p.regularization_param;
+  const int zero_thr = (c->mode == 7 && !(c->p.regularization_param > 0.f)) ? 1 : 0;
+  KL((k_ctl_prep<<<1, 1, 0, c->st>>>(c->ctl_d, c->scal_d, tv, l1, zero_thr, first ? 1 : 0), cudaGetLastError()));
+  if (first) RC(adjoint_volume(c));
+  RC(prox_volume(c, c->t, true));
+  RC(forward_volume(c, elem_kind(c->storage), c->vol[c->iNew]));
+  KL((k_ctl_decide<<<1, 1, 0, c->st>>>(c->ctl_d, c->sums_d, c->p.max_backtracks, h, c->dlog_d, first ? 1 : 0),
+      cudaGetLastError()));
+  return RIHVR_OK;
+}
+
+// Record, restart and momentum factor, then the hologram momentum, the residual
+// at the new momentum point and its spectrum.
+int enqueue_momentum_dev(rihvr_ctx* c) {
+  KL((k_ctl_finish<<<1, 1, 0, c->st>>>(c->ctl_d, c->sums_d, c->scal_d, c->dlog_d,
+                                       (double)c->p.regularization_param, tv_weight(c)),
+      cudaGetLastError()));
+  int nb = 0;
+  KL(launch_holo_momentum(c->dnew, c->dY0, c->dX, c->b, c->r, 0.f, (long long)c->HW, c->partials, &nb, c->st,
+                          c->scal_d + 8));
+  RC(reduce_into(c, nb, SLOT_MOM));
+  RC(residual_spectrum(c));
+  KL((k_ctl_post<<<1, 1, 0, c->st>>>(c->ctl_d, c->sums_d, c->dlog_d), cudaGetLastError()));
+  return RIHVR_OK;
+}
+
+// One iteration as a graph: first attempt, a WHILE node whose body is a
+// backtracking attempt (run while the test asks for one), then the momentum
+// step.  Built by capturing into the graph around the conditional node.
+int build_iter_graph(rihvr_ctx* c, cudaGraphExec_t* out, int* n_main, int* n_body) {
+  const cudaStreamCaptureMode mode = cudaStreamCaptureModeThreadLocal;
+  cudaGraph_t g = nullptr;
+  CK(cudaGraphCreate(&g, 0));
+  struct GraphGuard {
+    cudaGraph_t& g;
+    ~GraphGuard() {
+      if (g) cudaGraphDestroy(g);
+    }
+  } guard{g};
+  cudaGraphConditionalHandle h;
+  CK(cudaGraphConditionalHandleCreate(&h, g, 0, 0));
+  const long long l0 = c->launches;
+  CK(cudaStreamBeginCaptureToGraph(c->st, g, nullptr, nullptr, 0, mode));
+  int rc = enqueue_attempt_dev(c, true, h);
+  cudaStreamCaptureStatus status;
+  const cudaGraphNode_t* deps = nullptr;
+  size_t ndeps = 0;
+  cudaError_t e = cudaStreamGetCaptureInfo(c->st, &status, nullptr, nullptr, &deps, &ndeps);
+  std::vector<cudaGraphNode_t> tail(deps, deps + (e == cudaSuccess ? ndeps : 0));
+  cudaGraph_t cap = nullptr;
+  const cudaError_t e2 = cudaStreamEndCapture(c->st, &cap);
+  if (rc != RIHVR_OK) return rc;
+  CK(e);
+  CK(e2);
+  const long long l1 = c->launches;
+  cudaGraphNodeParams cp = {};
+  cp.type = cudaGraphNodeTypeConditional;
+  cp.conditional.handle = h;
+  cp.conditional.type = cudaGraphCondTypeWhile;
+  cp.conditional.size = 1;
+  cudaGraphNode_t cond;
+  CK(cudaGraphAddNode(&cond, g, tail.data(), tail.size(), &cp));
+  cudaGraph_t body = cp.conditional.phGraph_out[0];
+  CK(cudaStreamBeginCaptureToGraph(c->st, body, nullptr, nullptr, 0, mode));
+  rc = enqueue_attempt_dev(c, false, h);
+  e = cudaStreamEndCapture(c->st, &cap);
+  if (rc != RIHVR_OK) return rc;
+  CK(e);
+  const long long l2 = c->launches;
+  CK(cudaStreamBeginCaptureToGraph(c->st, g, &cond, nullptr, 1, mode));
+  rc = enqueue_momentum_dev(c);
+  e = cudaStreamEndCapture(c->st, &cap);
+  if (rc != RIHVR_OK) return rc;
+  CK(e);
+  CK(cudaGraphInstantiate(out, g, 0));
+  *n_main = (int)((l1 - l0) + (c->launches - l2));
+  *n_body = (int)(l2 - l1);
+  c->launches = l0;
+  return RIHVR_OK;
+}
+
+// Append the device log of n iterations to the host log, settling the
+// momentum-point terms of each record from the next iteration's first sweep
+// (what settle_x_terms does on the host path).
+void pull_dev_log(rihvr_ctx* c, int n) {
+  for (int k = 0; k < n; ++k) {
+    const DevRec& d = c->dlog_h[k];
+    if (c->p.record_objective) {
+      double sx[kNumSums] = {0};
+      sx[SUM_L1X] = d.prev_l1x;
+      sx[SUM_TVX] = d.prev_tvx;
+      settle_x_terms(c, sx);
+    }
+    c->log.push_back(d.rec);
+    c->pending_x = (int)c->log.size() - 1;
+  }
+}
+
+// n iterations without host synchronisation between them: the graphs are
+// launched back to back and the log is read every kDevLogCap iterations.
+int run_iterations_dev(rihvr_ctx* c, int n) {
+  for (int done = 0; done < n;) {
+    const int m = std::min(n - done, kDevLogCap);
+    IterCtl& h = *c->ctl_h;
+    h.t = c->t;
+    h.alpha1 = c->alpha1;
+    h.beta = c->beta;
+    h.prev_f_resid = c->prev_f_resid;
+    h.f_resid = h.lim = h.ratio = 0.0;
+    h.bt = 0;
+    h.it = c->it;
+    h.it_base = c->it;
+    h.pad = 0;
+    CK(cudaMemcpyAsync(c->ctl_d, c->ctl_h, sizeof(IterCtl), cudaMemcpyHostToDevice, c->st));
+    for (int k = 0; k < m; ++k) {
+      const int slot = c->iCur;
+      CK(cudaGraphLaunch(c->g_iter[slot], c->st));
+      c->launches += c->g_iter_n[slot][0];
+      const int old_prev = c->iPrev;
+      c->iPrev = c->iCur;
+      c->iCur = c->iNew;
+      c->iNew = old_prev;
+    }
+    CK(cudaMemcpyAsync(c->ctl_h, c->ctl_d, sizeof(IterCtl), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaMemcpyAsync(c->dlog_h, c->dlog_d, sizeof(DevRec) * m, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    c->t = h.t;
+    c->alpha1 = h.alpha1;
+    c->beta = h.beta;
+    c->prev_f_resid = h.prev_f_resid;
+    c->it = h.it;
+    for (int k = 0; k < m; ++k) c->launches += (long long)c->dlog_h[k].rec.backtracks * c->g_iter_n[0][1];
+    pull_dev_log(c, m);
+    done += m;
+  }
+  return RIHVR_OK;
+}
+
+// RIHVR_ITER_LOOP=host selects the host-synchronised loop (one_iteration)
+// instead, for comparison; both give the same iterates bit for bit.
+bool dev_loop_enabled() {
+  static const bool on = [] {
+    const char* v = std::getenv("RIHVR_ITER_LOOP");
+    return !(v && std::strcmp(v, "host") == 0);
+  }();
+  return on;
+}
+
+bool use_dev_loop(const rihvr_ctx* c) { return c->dev_loop && dev_loop_enabled() && use_graphs(c) && c->mode != 6; }
+
+// The three iteration graphs, one per position of P_k in the rotation
+// (iPrev, iCur, iNew) = (iCur + 2, iCur, iCur + 1) mod 3, built before any is
+// launched; on failure none is kept.
+int ensure_iter_graphs(rihvr_ctx* c) {
+  const int p0 = c->iPrev, c0 = c->iCur, n0 = c->iNew;
+  int rc = RIHVR_OK;
+  for (int slot = 0; slot < 3 && rc == RIHVR_OK; ++slot) {
+    if (c->g_iter[slot]) continue;
+    c->iCur = slot;
+    c->iPrev = (slot + 2) % 3;
+    c->iNew = (slot + 1) % 3;
+    rc = build_iter_graph(c, &c->g_iter[slot], &c->g_iter_n[slot][0], &c->g_iter_n[slot][1]);
+    if (rc != RIHVR_OK) c->g_iter[slot] = nullptr;
+  }
+  c->iPrev = p0;
+  c->iCur = c0;
+  c->iNew = n0;
+  if (rc != RIHVR_OK) {
+    for (auto& g : c->g_iter)
+      if (g) {
+        cudaGraphExecDestroy(g);
+        g = nullptr;
+      }
+    cudaGetLastError();
+  }
+  return rc;
 }
 
 // One FISTA iteration (:299-611): one host synchronisation per attempt and one
@@ -481,7 +767,20 @@ int one_iteration(rihvr_ctx* c) {
 
 int run_iterations(rihvr_ctx* c, int n) {
   if (!c->have_holo) return fail(RIHVR_ERR_MISSING_DATA, "no hologram set");
-  for (int i = 0; i < n; ++i) RC(one_iteration(c));
+  int i = 0;
+  if (n > 0 && !c->warm) {  // the first iteration of a context runs eagerly
+    RC(one_iteration(c));
+    ++i;
+  }
+  if (i < n && use_dev_loop(c)) {
+    if (ensure_iter_graphs(c) == RIHVR_OK) {
+      RC(run_iterations_dev(c, n - i));
+      i = n;
+    } else {
+      c->dev_loop = false;  // the attempt and momentum graphs of one_iteration instead
+    }
+  }
+  for (; i < n; ++i) RC(one_iteration(c));
   if (c->p.record_objective && c->pending_x >= 0) {
     double l1x, tvx;
     RC(norms_at_x(c, &l1x, &tvx));
@@ -641,6 +940,11 @@ int rihvr_create(const rihvr_params* params, int width, int height, rihvr_ctx** 
     return cleanup(fail(RIHVR_ERR_OUT_OF_MEMORY, "cudaMallocHost failed"));
   std::memset(c->scal_h, 0, 16 * sizeof(float));
   if (dalloc_t(c, &c->scal_d, 16) != RIHVR_OK) return cleanup(RIHVR_ERR_OUT_OF_MEMORY);
+  if (cudaMallocHost(&c->ctl_h, sizeof(IterCtl)) != cudaSuccess ||
+      cudaMallocHost(&c->dlog_h, sizeof(DevRec) * kDevLogCap) != cudaSuccess)
+    return cleanup(fail(RIHVR_ERR_OUT_OF_MEMORY, "cudaMallocHost failed"));
+  if (dalloc_t(c, &c->ctl_d, 1) != RIHVR_OK || dalloc_t(c, &c->dlog_d, kDevLogCap) != RIHVR_OK)
+    return cleanup(RIHVR_ERR_OUT_OF_MEMORY);
   std::vector<double> ct;
   phase_turns(height, width, (double)params->resolution, (double)params->wavelength, ct);
   std::vector<double> zl((size_t)c->Nz);
@@ -661,6 +965,8 @@ void rihvr_destroy(rihvr_ctx* c) {
   for (void* p : c->allocs) cudaFree(p);
   if (c->sums_h) cudaFreeHost(c->sums_h);
   if (c->scal_h) cudaFreeHost(c->scal_h);
+  if (c->ctl_h) cudaFreeHost(c->ctl_h);
+  if (c->dlog_h) cudaFreeHost(c->dlog_h);
   for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
   if (c->st) cudaStreamDestroy(c->st);
   delete c;
