@@ -340,6 +340,37 @@ int rihvr_write_centroids(const char* filename, const rihvr_object* objects, int
 int rihvr_adjoint_noalloc(const rihvr_params* params, int width, int height, const float* residual,
                           float* volume_out, void* stream);
 
+/* Learned warm start.  No counterpart in the reference: its reconstruction
+ * always starts from x = 0 (sparse_compressive_holo.cu:273), which stays the
+ * fallback and the judge.  A 3-D U-Net (3 levels, 16/32/64 channels, BF16
+ * tensor-core convolutions with FP32 accumulation, FP32 master weights) maps
+ * the back-propagated volume xbp = t A^H b (t the initial step) to an initial
+ * iterate x0 = g * alpha * xbp, g a per-voxel gain in (0, 1).  Volumes are
+ * depth x height x width complex interleaved device arrays; each side a
+ * multiple of 4.  Calls run on the legacy default stream and return when done. */
+typedef struct rihvr_unet rihvr_unet;
+int rihvr_unet_create(int depth, int height, int width, unsigned long long seed, rihvr_unet** out);
+void rihvr_unet_destroy(rihvr_unet* net);
+long long rihvr_unet_param_count(const rihvr_unet* net);
+/* all parameters as FP32 (convolution weights [cout][27][cin] and biases per
+ * layer, then the head's 16 weights, its bias and alpha) */
+int rihvr_unet_get_params(rihvr_unet* net, float* out);
+int rihvr_unet_set_params(rihvr_unet* net, const float* in);
+int rihvr_unet_predict(rihvr_unet* net, const float* xbp, float* x0);
+/* loss sum |x0 - x*|^2 / sum |x*|^2 against a solution x* and its gradient
+ * (host array of rihvr_unet_param_count floats; may be NULL) */
+int rihvr_unet_gradients(rihvr_unet* net, const float* xbp, const float* xstar, float* grad_out, double* loss);
+/* one Adam step (beta 0.9 / 0.999) on that loss */
+int rihvr_unet_train_step(rihvr_unet* net, const float* xbp, const float* xstar, float lr, double* loss);
+long long rihvr_unet_launch_count(const rihvr_unet* net);
+/* xbp = t A^H b of the context's hologram (t its initial step); leaves the
+ * solve reset to x = 0. */
+int rihvr_backpropagate(rihvr_ctx* ctx, float* xbp_out, int is_device);
+/* Start the solve from the network's x0 for the context's hologram (as
+ * rihvr_set_initial_volume does); the network's volume must be the context's
+ * num_planes x height x width. */
+int rihvr_warm_start(rihvr_ctx* ctx, rihvr_unet* net);
+
 /* Device time per kernel class of the iterations run with profiling on
  * (names "adj_col", "adj_row", "prox", "fwd_row", "fwd_col", "plane").
  * Enabling records a pair of CUDA events around each launch. */

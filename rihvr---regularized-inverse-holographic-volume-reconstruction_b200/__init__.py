@@ -135,6 +135,9 @@ EXPORTED = (
     "rihvr_adjoint_noalloc", "rihvr_sparsity", "rihvr_initial_estimate",
     "rihvr_read_image", "rihvr_write_tiff8", "rihvr_preprocess", "rihvr_io_error",
     "rihvr_segment_params_default", "rihvr_segment", "rihvr_segment_intensity", "rihvr_write_centroids",
+    "rihvr_unet_create", "rihvr_unet_destroy", "rihvr_unet_param_count", "rihvr_unet_get_params",
+    "rihvr_unet_set_params", "rihvr_unet_predict", "rihvr_unet_gradients", "rihvr_unet_train_step",
+    "rihvr_unet_launch_count", "rihvr_backpropagate", "rihvr_warm_start",
     "rihvr_set_profiling", "rihvr_kernel_times", "rihvr_get_stream", "rihvr_launch_count", "rihvr_device_bytes",
     "rihvr_status_string", "rihvr_last_error",
 )
@@ -201,6 +204,20 @@ def load_library(path: str = LIB_PATH):
     L.rihvr_segment_intensity.argtypes = [vp, ip, ip, ip, ip, P(SegmentParams), vp, ip, P(ctypes.c_int),
                                           P(SegmentInfo)]
     L.rihvr_write_centroids.argtypes = [ctypes.c_char_p, vp, ip, ip, ip]
+    L.rihvr_unet_create.argtypes = [ip, ip, ip, ctypes.c_ulonglong, P(vp)]
+    L.rihvr_unet_destroy.argtypes = [vp]
+    L.rihvr_unet_destroy.restype = None
+    L.rihvr_unet_param_count.argtypes = [vp]
+    L.rihvr_unet_param_count.restype = ctypes.c_longlong
+    L.rihvr_unet_get_params.argtypes = [vp, vp]
+    L.rihvr_unet_set_params.argtypes = [vp, vp]
+    L.rihvr_unet_predict.argtypes = [vp, vp, vp]
+    L.rihvr_unet_gradients.argtypes = [vp, vp, vp, vp, P(ctypes.c_double)]
+    L.rihvr_unet_train_step.argtypes = [vp, vp, vp, ctypes.c_float, P(ctypes.c_double)]
+    L.rihvr_unet_launch_count.argtypes = [vp]
+    L.rihvr_unet_launch_count.restype = ctypes.c_longlong
+    L.rihvr_backpropagate.argtypes = [vp, vp, ip]
+    L.rihvr_warm_start.argtypes = [vp, vp]
     L.rihvr_initial_estimate.argtypes = [vp, vp, ip]
     L.rihvr_set_profiling.argtypes = [vp, ip]
     L.rihvr_kernel_times.argtypes = [vp, P(ctypes.c_char_p), P(ctypes.c_double), P(ctypes.c_int), ip,
@@ -312,6 +329,86 @@ def write_centroids(path: str, objects: np.ndarray, weighted: bool = False, verb
     objs = np.ascontiguousarray(objects, dtype=OBJECT_DTYPE)
     _check(load_library().rihvr_write_centroids(path.encode(), objs.ctypes.data if len(objs) else None, len(objs),
                                                 int(bool(weighted)), int(bool(verbose))), "rihvr_write_centroids")
+
+
+def _dev_complex(a):
+    """A CUDA complex64 tensor holding `a` (numpy array or tensor), contiguous."""
+    import torch
+
+    if isinstance(a, torch.Tensor):
+        t = a.to(device="cuda", dtype=torch.complex64)
+    else:
+        t = torch.from_numpy(np.ascontiguousarray(a, dtype=np.complex64)).cuda()
+    return t.contiguous()
+
+
+class UNet:
+    """The learned warm start (rihvr_unet_*): a 3-D U-Net mapping the
+    back-propagated volume xbp = t A^H b (depth x height x width complex) to an
+    initial iterate x0 = g * alpha * xbp.  Volumes may be numpy arrays or CUDA
+    tensors; results are CUDA complex64 tensors."""
+
+    def __init__(self, depth: int, height: int, width: int, seed: int = 0):
+        self._L = load_library()
+        self._h = ctypes.c_void_p()
+        _check(self._L.rihvr_unet_create(int(depth), int(height), int(width), int(seed), ctypes.byref(self._h)),
+               "rihvr_unet_create")
+        self.shape = (depth, height, width)
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.destroy()
+
+    def destroy(self):
+        if self._h:
+            self._L.rihvr_unet_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def param_count(self) -> int:
+        return int(self._L.rihvr_unet_param_count(self._h))
+
+    def params(self) -> np.ndarray:
+        out = np.empty(self.param_count(), np.float32)
+        _check(self._L.rihvr_unet_get_params(self._h, _ptr(out)), "rihvr_unet_get_params")
+        return out
+
+    def set_params(self, p):
+        p = np.ascontiguousarray(p, dtype=np.float32)
+        if p.size != self.param_count():
+            raise ValueError(f"{p.size} parameters, the network has {self.param_count()}")
+        _check(self._L.rihvr_unet_set_params(self._h, _ptr(p)), "rihvr_unet_set_params")
+
+    def predict(self, xbp):
+        import torch
+
+        a = _dev_complex(xbp)
+        out = torch.empty_like(a)
+        _check(self._L.rihvr_unet_predict(self._h, ctypes.c_void_p(a.data_ptr()), ctypes.c_void_p(out.data_ptr())),
+               "rihvr_unet_predict")
+        return out
+
+    def gradients(self, xbp, xstar):
+        a, b = _dev_complex(xbp), _dev_complex(xstar)
+        g = np.empty(self.param_count(), np.float32)
+        loss = ctypes.c_double()
+        _check(self._L.rihvr_unet_gradients(self._h, ctypes.c_void_p(a.data_ptr()), ctypes.c_void_p(b.data_ptr()),
+                                            _ptr(g), ctypes.byref(loss)), "rihvr_unet_gradients")
+        return loss.value, g
+
+    def train_step(self, xbp, xstar, lr: float = 1e-3) -> float:
+        a, b = _dev_complex(xbp), _dev_complex(xstar)
+        loss = ctypes.c_double()
+        _check(self._L.rihvr_unet_train_step(self._h, ctypes.c_void_p(a.data_ptr()), ctypes.c_void_p(b.data_ptr()),
+                                             float(lr), ctypes.byref(loss)), "rihvr_unet_train_step")
+        return loss.value
+
+    def save(self, path: str):
+        np.save(path, self.params())
+
+    def load(self, path: str):
+        self.set_params(np.load(path))
 
 
 def reconstruct_batch(solvers, holograms):
@@ -519,6 +616,16 @@ class SparseCompressiveHolo:
         out = np.empty((self.height, self.width), np.float32)
         _check(self._L.rihvr_get_residual(self._h, _ptr(out), 0), "rihvr_get_residual")
         return out
+
+    def backpropagate(self) -> np.ndarray:
+        """xbp = t A^H b of the hologram (t the initial step); resets the solve."""
+        out = np.empty((self.depth, self.height, self.width), np.complex64)
+        _check(self._L.rihvr_backpropagate(self._h, _ptr(out), 0), "rihvr_backpropagate")
+        return out
+
+    def warmStart(self, net: "UNet"):
+        """Start the solve from the network's x0 (rihvr_warm_start)."""
+        _check(self._L.rihvr_warm_start(self._h, net._h), "rihvr_warm_start")
 
     def segment(self, sp: SegmentParams | None = None, max_objects: int = 1 << 16):
         """SparseSegmentation on the current volume (binarize, close, label,

@@ -59,6 +59,10 @@ void set_last_error(const char* msg);
 struct SegWorkspace;
 SegWorkspace* seg_workspace_create();
 void seg_workspace_destroy(SegWorkspace* ws);
+// learned warm start (rihvr_unet.cu)
+int unet_predict_on(rihvr_unet* u, const float2* xbp, float scale, float2* x0, cudaStream_t st);
+void unet_dims(const rihvr_unet* u, int* D, int* H, int* W);
+
 int segment_volume(int storage, const void* P, const void* Pprev, float beta, int W, int H, int Nz,
                    const rihvr_segment_params* sp, rihvr_object* objects, int max_objects, int* num_objects,
                    rihvr_segment_info* info, SegWorkspace* ws, cudaStream_t st);

@@ -1246,12 +1246,13 @@ int rihvr_initial_estimate(rihvr_ctx* c, float* out, int is_device) {
   return state_reset(c);
 }
 
-int rihvr_set_initial_volume(rihvr_ctx* c, const float* x0, int is_device) {
-  if (!c || !x0) return fail(RIHVR_ERR_INVALID_ARGUMENT, "NULL argument");
-  if (!c->have_holo) return fail(RIHVR_ERR_MISSING_DATA, "no hologram set");
-  RC(state_reset(c));
-  // P_{k-1} = P_k = x0 in the storage type, beta = 0
-  RC(copy_in(c, c->U, x0, sizeof(float2) * c->V, is_device));
+}  // extern "C"
+
+namespace {
+
+// Start from the volume in U (complex FP32): P_{k-1} = P_k = x0 in the
+// storage type, beta = 0, the estimated hologram and residual of x0.
+int start_from_U(rihvr_ctx* c) {
   KL(launch_store_volume(c->storage, c->U, c->vol[c->iCur], (long long)c->V, c->st));
   CK(cudaMemcpyAsync(c->vol[c->iPrev], c->vol[c->iCur], c->esize * c->V, cudaMemcpyDeviceToDevice, c->st));
   // the estimated hologram of the stored x0, then the momentum step with beta = 0:
@@ -1264,6 +1265,58 @@ int rihvr_set_initial_volume(rihvr_ctx* c, const float* x0, int is_device) {
   RC(fetch_sums(c));
   c->prev_f_resid = 0.5 * c->sums_h[SLOT_MOM * kNumSums + SUM_RR];
   return RIHVR_OK;
+}
+
+int flat_blocks_for(size_t n) { return (int)std::min<size_t>((n + 255) / 256, 148 * 16); }
+
+__global__ void k_scale_c(float2* __restrict__ v, long long n, float s) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    v[i] = make_float2(v[i].x * s, v[i].y * s);
+}
+
+// G = A^H b (the residual of x = 0 with the sign flipped)
+int backproject_into_G(rihvr_ctx* c) {
+  CK(cudaMemcpyAsync(c->r, c->b, sizeof(float) * c->HW, cudaMemcpyDeviceToDevice, c->st));
+  RC(residual_spectrum(c));
+  return adjoint_volume(c);
+}
+
+}  // namespace
+
+extern "C" {
+
+int rihvr_set_initial_volume(rihvr_ctx* c, const float* x0, int is_device) {
+  if (!c || !x0) return fail(RIHVR_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (!c->have_holo) return fail(RIHVR_ERR_MISSING_DATA, "no hologram set");
+  RC(state_reset(c));
+  RC(copy_in(c, c->U, x0, sizeof(float2) * c->V, is_device));
+  return start_from_U(c);
+}
+
+int rihvr_backpropagate(rihvr_ctx* c, float* out, int is_device) {
+  if (!c || !out) return fail(RIHVR_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (!c->have_holo) return fail(RIHVR_ERR_MISSING_DATA, "no hologram set");
+  RC(state_reset(c));
+  RC(backproject_into_G(c));
+  KL((k_scale_c<<<flat_blocks_for(c->V), 256, 0, c->st>>>(c->G, (long long)c->V, (float)c->t), cudaGetLastError()));
+  RC(copy_out(c, out, c->G, sizeof(float2) * c->V, is_device));
+  return state_reset(c);
+}
+
+int rihvr_warm_start(rihvr_ctx* c, rihvr_unet* net) {
+  if (!c || !net) return fail(RIHVR_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (!c->have_holo) return fail(RIHVR_ERR_MISSING_DATA, "no hologram set");
+  int D, H, W;
+  unet_dims(net, &D, &H, &W);
+  if (D != c->Nz || H != c->H || W != c->W)
+    return fail(RIHVR_ERR_INVALID_ARGUMENT, "network volume " + std::to_string(D) + "x" + std::to_string(H) + "x" +
+                                                std::to_string(W) + " differs from the context's");
+  RC(state_reset(c));
+  RC(backproject_into_G(c));
+  // x0 = g alpha t A^H b into U
+  const int rc = unet_predict_on(net, c->G, (float)c->t, c->U, c->st);
+  if (rc != RIHVR_OK) return rc;
+  return start_from_U(c);
 }
 
 int rihvr_get_iterations(const rihvr_ctx* c, rihvr_iter_record* out, int max_records, int* n_out) {
