@@ -12,6 +12,7 @@ results.
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--config c2|c1|c5]
     python bench.py --config series    # uneven time series, batched vs frame by frame
     python bench.py --config segment   # particle segmentation of the reconstructed volume
+    python bench.py --config warmstart --frames 16   # learned warm start against FISTA from zero
 """
 from __future__ import annotations
 
@@ -356,6 +357,48 @@ def run_segment(args):
     return 0
 
 
+def run_warmstart(args):
+    """Learned warm start at 128x128x32 (the physics of the 512x512x200
+    warm-start configuration): on held-out synthetic holograms, the iterations
+    and the device time plain FISTA from zero and FISTA from the trained
+    network's x0 need to reach plain FISTA's 100-iteration objective within
+    1e-3, and the network's own inference time.  Prints one JSON line."""
+    import torch
+
+    torch.cuda.set_device(0)
+    rihvr = importlib.import_module(PKG)
+    ws = importlib.import_module(PKG + ".warmstart")
+    seeds = np.arange(300_000, 300_000 + args.frames)
+    with rihvr.UNet(ws.PLANES, ws.SIZE, ws.SIZE) as net:
+        net.load(ws.WEIGHTS)
+        rows = ws.evaluate(net, seeds)
+        # inference alone, on one held-out hologram
+        data = ws.make_set(seeds[:1])
+        xbp = data[0][1]
+        for _ in range(3):
+            net.predict(xbp)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            net.predict(xbp)
+        torch.cuda.synchronize()
+        infer_ms = (time.perf_counter() - t0) / args.steps * 1e3
+    s = ws.summary(rows)
+    vox = ws.PLANES * ws.SIZE * ws.SIZE
+    flops = 0
+    for cin, cout, lvl in [(16, 16, 0), (16, 16, 0), (16, 32, 1), (32, 32, 1), (32, 64, 2), (64, 64, 2),
+                           (96, 32, 1), (32, 32, 1), (48, 16, 0), (16, 16, 0)]:
+        flops += 2 * 27 * cin * cout * vox // (8 ** lvl)
+    line = {"metric": "iterations and device ms to plain FISTA's 100-iteration objective (1e-3), warm start vs zero",
+            "value": s["mean_iters_warm"], "unit": "iterations", "higher_is_better": False, "n_gpus": 1,
+            "data": "synthetic", "config": {"workload": f"warmstart_{ws.SIZE}x{ws.SIZE}x{ws.PLANES}",
+                                             "holograms": len(rows), "weights": os.path.basename(ws.WEIGHTS)},
+            "summary": s, "inference_ms": infer_ms, "inference_tflops": flops / (infer_ms * 1e-3) / 1e12,
+            "conv_flops": flops, "rows": rows}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_ours(args):
     ws, rank, local = dist_env()
     import torch
@@ -493,7 +536,7 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="c2", choices=["c2", "c1", "c5", "series", "segment"])
+    ap.add_argument("--config", default="c2", choices=["c2", "c1", "c5", "series", "segment", "warmstart"])
     ap.add_argument("--frames", type=int, default=8, help="frames of the uneven series (--config series)")
     ap.add_argument("--storage", default="f32", choices=["f32", "bf16", "f16"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -511,6 +554,8 @@ def main():
         return run_frames(args)
     if args.config == "segment":
         return run_segment(args)
+    if args.config == "warmstart":
+        return run_warmstart(args)
     return run_ours(args)
 
 

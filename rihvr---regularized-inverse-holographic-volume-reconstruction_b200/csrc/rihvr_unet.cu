@@ -72,92 +72,127 @@ __device__ __forceinline__ void tap_offsets(int k, int* dz, int* dy, int* dx) {
 // Y[v][co] = act(bias[co] + sum_k sum_ci X[v + off_k][ci] Wt[co][k][ci]) for
 // the output channels co0 .. co0 + Cn - 1 of Cout (Cn a multiple of 8, at most
 // 64); Cin a multiple of 16.  Taps are mirrored when `mirror` (the data
-// gradient).  128 threads, 64 voxels a block.
+// gradient).
+//
+// A block makes a brick of 2 (z) x 4 (y) x 16 (x) output voxels; each of its
+// 4 warps two rows of 16 voxels (two m-tiles).  Per 16-channel slice of the
+// input it stages the brick's halo (4 x 6 x 18 voxels, zero outside the
+// volume, BF16) and the slice's weights for all 27 taps in shared memory,
+// then runs the 27 taps from there: the A fragment of a tap is the halo
+// shifted by the tap's offset, so nothing is restaged between taps.  Rows are
+// padded to 24 BF16 (48 bytes) so fragment loads hit distinct banks.
 constexpr int kConvThreads = 128;
+constexpr int kBZ = 2, kBY = 4, kBX = 16;
+constexpr int kHZ = kBZ + 2, kHY = kBY + 2, kHX = kBX + 2;
+constexpr int kHalo = kHZ * kHY * kHX;  // 432 voxels
+constexpr int kRow = 24;                // BF16 per shared row (16 used)
+constexpr size_t kConvSmem = sizeof(__nv_bfloat16) * kRow * (kHalo + 27 * 64);
+
 __global__ void __launch_bounds__(kConvThreads) k_conv3(const float* __restrict__ X, int Cin,
                                                         const __nv_bfloat16* __restrict__ Wt, int Cout, int co0,
                                                         int Cn, const float* __restrict__ bias,
                                                         float* __restrict__ Y, Vol v, int relu, int mirror) {
-  __shared__ __align__(16) __nv_bfloat16 As[64][16];
-  __shared__ __align__(16) __nv_bfloat16 Bs[64][16];
+  extern __shared__ __align__(16) __nv_bfloat16 csm[];
+  __nv_bfloat16* Hs = csm;                  // [kHalo][kRow]
+  __nv_bfloat16* Ws = csm + kHalo * kRow;   // [27 * Cn][kRow]
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int g = lane >> 2, t = lane & 3;
-  const long long n = v.n();
-  const long long vox0 = (long long)blockIdx.x * 64;
-  // the voxel this thread stages (two threads a voxel, 8 channels each)
-  const int sm = tid >> 1, sh = tid & 1;
-  const long long sv = vox0 + sm;
-  int sz = 0, sy = 0, sx = 0;
-  if (sv < n) {
-    sx = (int)(sv % v.W);
-    sy = (int)((sv / v.W) % v.H);
-    sz = (int)(sv / ((long long)v.W * v.H));
-  }
+  const int nbx = (v.W + kBX - 1) / kBX, nby = (v.H + kBY - 1) / kBY;
+  const int bx = blockIdx.x % nbx, by = (blockIdx.x / nbx) % nby, bz = blockIdx.x / (nbx * nby);
+  const int x0 = bx * kBX, y0 = by * kBY, z0 = bz * kBZ;
   const int ntile = Cn / 8;
-  float acc[8][4];
+  float acc[2][8][4];
 #pragma unroll
-  for (int j = 0; j < 8; ++j) acc[j][0] = acc[j][1] = acc[j][2] = acc[j][3] = 0.f;
+  for (int r = 0; r < 2; ++r)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) acc[r][j][0] = acc[r][j][1] = acc[r][j][2] = acc[r][j][3] = 0.f;
   const int nslice = Cin / 16;
-  for (int k = 0; k < 27; ++k) {
-    int dz, dy, dx;
-    tap_offsets(mirror ? 26 - k : k, &dz, &dy, &dx);
-    const int zz = sz + dz, yy = sy + dy, xx = sx + dx;
-    const bool inb = sv < n && zz >= 0 && zz < v.D && yy >= 0 && yy < v.H && xx >= 0 && xx < v.W;
-    const float* src = X + (((long long)zz * v.H + yy) * v.W + xx) * Cin + sh * 8;
-    for (int s = 0; s < nslice; ++s) {
-      // activation tile: 64 voxels x 16 channels, BF16
+  for (int s = 0; s < nslice; ++s) {
+    // halo of the brick, 16 channels: two threads a voxel row of 8 channels
+    for (int e = tid; e < kHalo * 2; e += kConvThreads) {
+      const int h = e >> 1, half = e & 1;
+      const int hx = h % kHX, hy = (h / kHX) % kHY, hz = h / (kHX * kHY);
+      const int xx = x0 + hx - 1, yy = y0 + hy - 1, zz = z0 + hz - 1;
       float4 lo = make_float4(0.f, 0.f, 0.f, 0.f), hi = lo;
-      if (inb) {
-        lo = *reinterpret_cast<const float4*>(src + s * 16);
-        hi = *reinterpret_cast<const float4*>(src + s * 16 + 4);
+      if (xx >= 0 && xx < v.W && yy >= 0 && yy < v.H && zz >= 0 && zz < v.D) {
+        const float* src = X + (((long long)zz * v.H + yy) * v.W + xx) * Cin + s * 16 + half * 8;
+        lo = *reinterpret_cast<const float4*>(src);
+        hi = *reinterpret_cast<const float4*>(src + 4);
       }
       uint4 pk;
       pk.x = pack_bf16(lo.x, lo.y);
       pk.y = pack_bf16(lo.z, lo.w);
       pk.z = pack_bf16(hi.x, hi.y);
       pk.w = pack_bf16(hi.z, hi.w);
-      *reinterpret_cast<uint4*>(&As[sm][sh * 8]) = pk;
-      // weight tile: Cout x 16 (row co holds the 16 input channels of tap k)
-      if (tid < Cn * 2) {
-        const int co = tid >> 1, half = tid & 1;
-        *reinterpret_cast<uint4*>(&Bs[co][half * 8]) =
-            *reinterpret_cast<const uint4*>(Wt + ((long long)(co0 + co) * 27 + k) * Cin + s * 16 + half * 8);
-      }
-      __syncthreads();
-      const int m0 = warp * 16;
-      const unsigned a0 = *reinterpret_cast<const unsigned*>(&As[m0 + g][2 * t]);
-      const unsigned a1 = *reinterpret_cast<const unsigned*>(&As[m0 + g + 8][2 * t]);
-      const unsigned a2 = *reinterpret_cast<const unsigned*>(&As[m0 + g][2 * t + 8]);
-      const unsigned a3 = *reinterpret_cast<const unsigned*>(&As[m0 + g + 8][2 * t + 8]);
+      *reinterpret_cast<uint4*>(Hs + h * kRow + half * 8) = pk;
+    }
+    // weights of the slice for every tap: row k * Cn + co
+    for (int e = tid; e < 27 * Cn * 2; e += kConvThreads) {
+      const int row = e >> 1, half = e & 1;
+      const int k = row / Cn, co = row - k * Cn;
+      *reinterpret_cast<uint4*>(Ws + row * kRow + half * 8) =
+          *reinterpret_cast<const uint4*>(Wt + ((long long)(co0 + co) * 27 + k) * Cin + s * 16 + half * 8);
+    }
+    __syncthreads();
+#pragma unroll 1
+    for (int k = 0; k < 27; ++k) {
+      int dz, dy, dx;
+      tap_offsets(mirror ? 26 - k : k, &dz, &dy, &dx);
 #pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        if (j < ntile) {
-          const unsigned b0 = *reinterpret_cast<const unsigned*>(&Bs[j * 8 + g][2 * t]);
-          const unsigned b1 = *reinterpret_cast<const unsigned*>(&Bs[j * 8 + g][2 * t + 8]);
-          mma_bf16(acc[j], a0, a1, a2, a3, b0, b1);
+      for (int r = 0; r < 2; ++r) {
+        // m-tile r of this warp: the x-row (z, y) of the brick, voxels x = 0..15
+        const int row = warp * 2 + r;
+        const int mz = row / kBY, my = row % kBY;
+        const int hb = ((mz + dz + 1) * kHY + (my + dy + 1)) * kHX + dx + 1;
+        const __nv_bfloat16* a_lo = Hs + (hb + g) * kRow;
+        const __nv_bfloat16* a_hi = Hs + (hb + g + 8) * kRow;
+        const unsigned a0 = *reinterpret_cast<const unsigned*>(a_lo + 2 * t);
+        const unsigned a1 = *reinterpret_cast<const unsigned*>(a_hi + 2 * t);
+        const unsigned a2 = *reinterpret_cast<const unsigned*>(a_lo + 2 * t + 8);
+        const unsigned a3 = *reinterpret_cast<const unsigned*>(a_hi + 2 * t + 8);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          if (j < ntile) {
+            const __nv_bfloat16* b = Ws + (k * Cn + j * 8 + g) * kRow;
+            const unsigned b0 = *reinterpret_cast<const unsigned*>(b + 2 * t);
+            const unsigned b1 = *reinterpret_cast<const unsigned*>(b + 2 * t + 8);
+            mma_bf16(acc[r][j], a0, a1, a2, a3, b0, b1);
+          }
         }
       }
-      __syncthreads();
     }
+    __syncthreads();
   }
-  // epilogue: rows g and g + 8 of the warp's 16 voxels, columns 2t, 2t + 1 of each tile
+  // epilogue: rows g and g + 8 of each m-tile, columns 2t, 2t + 1 of each n-tile
 #pragma unroll
-  for (int j = 0; j < 8; ++j) {
-    if (j >= ntile) continue;
-    const int co = co0 + j * 8 + 2 * t;
-    const float b0 = bias ? bias[co] : 0.f, b1 = bias ? bias[co + 1] : 0.f;
+  for (int r = 0; r < 2; ++r) {
+    const int row = warp * 2 + r;
+    const int zz = z0 + row / kBY, yy = y0 + row % kBY;
+    if (zz >= v.D || yy >= v.H) continue;
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
-      const long long vo = vox0 + warp * 16 + g + h * 8;
-      if (vo >= n) continue;
-      float y0 = acc[j][2 * h] + b0, y1 = acc[j][2 * h + 1] + b1;
-      if (relu) {
-        y0 = fmaxf(y0, 0.f);
-        y1 = fmaxf(y1, 0.f);
+    for (int j = 0; j < 8; ++j) {
+      if (j >= ntile) continue;
+      const int co = co0 + j * 8 + 2 * t;
+      const float b0 = bias ? bias[co] : 0.f, b1 = bias ? bias[co + 1] : 0.f;
+#pragma unroll
+      for (int h = 0; h < 2; ++h) {
+        const int xx = x0 + g + h * 8;
+        if (xx >= v.W) continue;
+        float y0v = acc[r][j][2 * h] + b0, y1v = acc[r][j][2 * h + 1] + b1;
+        if (relu) {
+          y0v = fmaxf(y0v, 0.f);
+          y1v = fmaxf(y1v, 0.f);
+        }
+        *reinterpret_cast<float2*>(Y + (((long long)zz * v.H + yy) * v.W + xx) * Cout + co) =
+            make_float2(y0v, y1v);
       }
-      *reinterpret_cast<float2*>(Y + vo * Cout + co) = make_float2(y0, y1);
     }
   }
+}
+
+// grid of k_conv3 for a volume: one block a 2 x 4 x 16 brick
+inline unsigned conv_blocks(const Vol& v) {
+  return (unsigned)(((v.W + kBX - 1) / kBX) * ((v.H + kBY - 1) / kBY) * ((v.D + kBZ - 1) / kBZ));
 }
 
 // dW[co][k][ci] += sum_v dY[v][co] X[v + off_k][ci] over a chunk of voxels:
@@ -534,8 +569,8 @@ int ualloc(rihvr_unet* u, T** p, size_t count) {
 int conv_fwd(rihvr_unet* u, int li, const float* X, float* Y) {
   const Conv& L = u->layers[li];
   const Vol v = u->lv[L.level];
-  k_conv3<<<(unsigned)((v.n() + 63) / 64), kConvThreads, 0, u->st>>>(X, L.cin, u->wb + u->wb_off[li], L.cout, 0,
-                                                                      L.cout, u->w + L.b_off, Y, v, 1, 0);
+  k_conv3<<<conv_blocks(v), kConvThreads, kConvSmem, u->st>>>(X, L.cin, u->wb + u->wb_off[li], L.cout, 0, L.cout,
+                                                               u->w + L.b_off, Y, v, 1, 0);
   ++u->launches;
   UCK(cudaGetLastError());
   return RIHVR_OK;
@@ -554,8 +589,8 @@ int conv_back(rihvr_unet* u, int li, const float* X, float* dY, float* dX) {
   u->launches += 3;
   // the data gradient: output channels of the transposed weights in windows of 64
   for (int co0 = 0; dX && co0 < L.cin; co0 += 64) {
-    k_conv3<<<(unsigned)((n + 63) / 64), kConvThreads, 0, u->st>>>(dY, L.cout, u->wt + u->wb_off[li], L.cin, co0,
-                                                                    std::min(64, L.cin - co0), nullptr, dX, v, 0, 1);
+    k_conv3<<<conv_blocks(v), kConvThreads, kConvSmem, u->st>>>(dY, L.cout, u->wt + u->wb_off[li], L.cin, co0,
+                                                                 std::min(64, L.cin - co0), nullptr, dX, v, 0, 1);
     ++u->launches;
   }
   UCK(cudaGetLastError());
@@ -729,6 +764,8 @@ int rihvr_unet_create(int depth, int height, int width, unsigned long long seed,
       cudaMemset(u->m, 0, sizeof(float) * u->nparam) != cudaSuccess ||
       cudaMemset(u->s, 0, sizeof(float) * u->nparam) != cudaSuccess)
     return bail(unet_fail(RIHVR_ERR_CUDA, "initial copies failed"));
+  if (cudaFuncSetAttribute(k_conv3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kConvSmem) != cudaSuccess)
+    return bail(unet_fail(RIHVR_ERR_CUDA, "shared-memory opt-in failed"));
   u->st = nullptr;
   if ((rc = refresh_bf16(u)) != RIHVR_OK) return bail(rc);
   if (cudaStreamSynchronize(nullptr) != cudaSuccess) return bail(unet_fail(RIHVR_ERR_CUDA, "initialisation failed"));
