@@ -11,8 +11,8 @@ learns x0 = g * alpha * xbp against x*.  Evaluation runs plain FISTA from zero
 the iterations each needs to come within 1e-3 (relative) of plain FISTA's
 final objective.
 
-    python -m <package>.warmstart train --out weights.npy [--samples 256 --epochs 20]
-    python -m <package>.warmstart evaluate --weights weights.npy [--samples 16]
+    python warmstart.py train --out weights.npy [--samples 1024 --epochs 50]
+    python warmstart.py evaluate --weights weights.npy [--samples 16]
 """
 from __future__ import annotations
 
@@ -161,8 +161,8 @@ def main(argv=None):
     sub = ap.add_subparsers(dest="cmd", required=True)
     tr = sub.add_parser("train")
     tr.add_argument("--out", default=WEIGHTS)
-    tr.add_argument("--samples", type=int, default=256)
-    tr.add_argument("--epochs", type=int, default=20)
+    tr.add_argument("--samples", type=int, default=1024)
+    tr.add_argument("--epochs", type=int, default=50)
     tr.add_argument("--lr", type=float, default=1e-3)
     tr.add_argument("--eval", type=int, default=8)
     ev = sub.add_parser("evaluate")
