@@ -74,44 +74,55 @@ __device__ __forceinline__ void tap_offsets(int k, int* dz, int* dy, int* dx) {
 // 64); Cin a multiple of 16.  Taps are mirrored when `mirror` (the data
 // gradient).
 //
-// A block makes a brick of 2 (z) x 4 (y) x 16 (x) output voxels; each of its
-// 4 warps two rows of 16 voxels (two m-tiles).  Per 16-channel slice of the
-// input it stages the brick's halo (4 x 6 x 18 voxels, zero outside the
-// volume, BF16) and the slice's weights for all 27 taps in shared memory,
-// then runs the 27 taps from there: the A fragment of a tap is the halo
-// shifted by the tap's offset, so nothing is restaged between taps.  Rows are
-// padded to 24 BF16 (48 bytes) so fragment loads hit distinct banks.
+// A block makes a brick of 2 (z) x 2 MT (y) x 16 (x) output voxels; each of
+// its 4 warps MT rows of 16 voxels (MT m-tiles) and NT tiles of 8 output
+// channels.  Per 16-channel slice of the input it stages the brick's halo
+// (4 x (2 MT + 2) x 18 voxels, zero outside the volume, BF16) and the slice's
+// weights for all 27 taps in shared memory, then runs the 27 taps from there:
+// the A fragment of a tap is the halo shifted by the tap's offset, so nothing
+// is restaged between taps.  Rows are padded to 24 BF16 (48 bytes) so fragment
+// loads hit distinct banks.  Narrow layers (16 or 32 channels) take MT = 4:
+// taller bricks, fewer halo voxels per output and smaller weight tiles, so
+// more blocks fit per SM.
 constexpr int kConvThreads = 128;
-constexpr int kBZ = 2, kBY = 4, kBX = 16;
-constexpr int kHZ = kBZ + 2, kHY = kBY + 2, kHX = kBX + 2;
-constexpr int kHalo = kHZ * kHY * kHX;  // 432 voxels
-constexpr int kRow = 24;                // BF16 per shared row (16 used)
-constexpr size_t kConvSmem = sizeof(__nv_bfloat16) * kRow * (kHalo + 27 * 64);
+constexpr int kBZ = 2, kBX = 16, kHX = kBX + 2;
+constexpr int kRow = 24;  // BF16 per shared row (16 used)
 
+template <int MT>
+struct Brick {
+  static constexpr int BY = 2 * MT, HZ = kBZ + 2, HY = BY + 2, HALO = HZ * HY * kHX;
+};
+template <int MT>
+constexpr size_t conv_smem(int Cn) {
+  return sizeof(__nv_bfloat16) * kRow * (Brick<MT>::HALO + 27 * (size_t)Cn);
+}
+
+template <int NT, int MT>
 __global__ void __launch_bounds__(kConvThreads) k_conv3(const float* __restrict__ X, int Cin,
                                                         const __nv_bfloat16* __restrict__ Wt, int Cout, int co0,
-                                                        int Cn, const float* __restrict__ bias,
-                                                        float* __restrict__ Y, Vol v, int relu, int mirror) {
+                                                        const float* __restrict__ bias, float* __restrict__ Y,
+                                                        Vol v, int relu, int mirror) {
+  using Bk = Brick<MT>;
+  constexpr int Cn = NT * 8;
   extern __shared__ __align__(16) __nv_bfloat16 csm[];
-  __nv_bfloat16* Hs = csm;                  // [kHalo][kRow]
-  __nv_bfloat16* Ws = csm + kHalo * kRow;   // [27 * Cn][kRow]
+  __nv_bfloat16* Hs = csm;                    // [HALO][kRow]
+  __nv_bfloat16* Ws = csm + Bk::HALO * kRow;  // [27 * Cn][kRow]
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int g = lane >> 2, t = lane & 3;
-  const int nbx = (v.W + kBX - 1) / kBX, nby = (v.H + kBY - 1) / kBY;
+  const int nbx = (v.W + kBX - 1) / kBX, nby = (v.H + Bk::BY - 1) / Bk::BY;
   const int bx = blockIdx.x % nbx, by = (blockIdx.x / nbx) % nby, bz = blockIdx.x / (nbx * nby);
-  const int x0 = bx * kBX, y0 = by * kBY, z0 = bz * kBZ;
-  const int ntile = Cn / 8;
-  float acc[2][8][4];
+  const int x0 = bx * kBX, y0 = by * Bk::BY, z0 = bz * kBZ;
+  float acc[MT][NT][4];
 #pragma unroll
-  for (int r = 0; r < 2; ++r)
+  for (int r = 0; r < MT; ++r)
 #pragma unroll
-    for (int j = 0; j < 8; ++j) acc[r][j][0] = acc[r][j][1] = acc[r][j][2] = acc[r][j][3] = 0.f;
+    for (int j = 0; j < NT; ++j) acc[r][j][0] = acc[r][j][1] = acc[r][j][2] = acc[r][j][3] = 0.f;
   const int nslice = Cin / 16;
   for (int s = 0; s < nslice; ++s) {
     // halo of the brick, 16 channels: two threads a voxel row of 8 channels
-    for (int e = tid; e < kHalo * 2; e += kConvThreads) {
+    for (int e = tid; e < Bk::HALO * 2; e += kConvThreads) {
       const int h = e >> 1, half = e & 1;
-      const int hx = h % kHX, hy = (h / kHX) % kHY, hz = h / (kHX * kHY);
+      const int hx = h % kHX, hy = (h / kHX) % Bk::HY, hz = h / (kHX * Bk::HY);
       const int xx = x0 + hx - 1, yy = y0 + hy - 1, zz = z0 + hz - 1;
       float4 lo = make_float4(0.f, 0.f, 0.f, 0.f), hi = lo;
       if (xx >= 0 && xx < v.W && yy >= 0 && yy < v.H && zz >= 0 && zz < v.D) {
@@ -138,12 +149,19 @@ __global__ void __launch_bounds__(kConvThreads) k_conv3(const float* __restrict_
     for (int k = 0; k < 27; ++k) {
       int dz, dy, dx;
       tap_offsets(mirror ? 26 - k : k, &dz, &dy, &dx);
+      unsigned b[NT][2];
 #pragma unroll
-      for (int r = 0; r < 2; ++r) {
+      for (int j = 0; j < NT; ++j) {
+        const __nv_bfloat16* bp = Ws + (k * Cn + j * 8 + g) * kRow;
+        b[j][0] = *reinterpret_cast<const unsigned*>(bp + 2 * t);
+        b[j][1] = *reinterpret_cast<const unsigned*>(bp + 2 * t + 8);
+      }
+#pragma unroll
+      for (int r = 0; r < MT; ++r) {
         // m-tile r of this warp: the x-row (z, y) of the brick, voxels x = 0..15
-        const int row = warp * 2 + r;
-        const int mz = row / kBY, my = row % kBY;
-        const int hb = ((mz + dz + 1) * kHY + (my + dy + 1)) * kHX + dx + 1;
+        const int row = warp * MT + r;
+        const int mz = row / Bk::BY, my = row % Bk::BY;
+        const int hb = ((mz + dz + 1) * Bk::HY + (my + dy + 1)) * kHX + dx + 1;
         const __nv_bfloat16* a_lo = Hs + (hb + g) * kRow;
         const __nv_bfloat16* a_hi = Hs + (hb + g + 8) * kRow;
         const unsigned a0 = *reinterpret_cast<const unsigned*>(a_lo + 2 * t);
@@ -151,27 +169,19 @@ __global__ void __launch_bounds__(kConvThreads) k_conv3(const float* __restrict_
         const unsigned a2 = *reinterpret_cast<const unsigned*>(a_lo + 2 * t + 8);
         const unsigned a3 = *reinterpret_cast<const unsigned*>(a_hi + 2 * t + 8);
 #pragma unroll
-        for (int j = 0; j < 8; ++j) {
-          if (j < ntile) {
-            const __nv_bfloat16* b = Ws + (k * Cn + j * 8 + g) * kRow;
-            const unsigned b0 = *reinterpret_cast<const unsigned*>(b + 2 * t);
-            const unsigned b1 = *reinterpret_cast<const unsigned*>(b + 2 * t + 8);
-            mma_bf16(acc[r][j], a0, a1, a2, a3, b0, b1);
-          }
-        }
+        for (int j = 0; j < NT; ++j) mma_bf16(acc[r][j], a0, a1, a2, a3, b[j][0], b[j][1]);
       }
     }
     __syncthreads();
   }
   // epilogue: rows g and g + 8 of each m-tile, columns 2t, 2t + 1 of each n-tile
 #pragma unroll
-  for (int r = 0; r < 2; ++r) {
-    const int row = warp * 2 + r;
-    const int zz = z0 + row / kBY, yy = y0 + row % kBY;
+  for (int r = 0; r < MT; ++r) {
+    const int row = warp * MT + r;
+    const int zz = z0 + row / Bk::BY, yy = y0 + row % Bk::BY;
     if (zz >= v.D || yy >= v.H) continue;
 #pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      if (j >= ntile) continue;
+    for (int j = 0; j < NT; ++j) {
       const int co = co0 + j * 8 + 2 * t;
       const float b0 = bias ? bias[co] : 0.f, b1 = bias ? bias[co + 1] : 0.f;
 #pragma unroll
@@ -190,9 +200,33 @@ __global__ void __launch_bounds__(kConvThreads) k_conv3(const float* __restrict_
   }
 }
 
-// grid of k_conv3 for a volume: one block a 2 x 4 x 16 brick
-inline unsigned conv_blocks(const Vol& v) {
-  return (unsigned)(((v.W + kBX - 1) / kBX) * ((v.H + kBY - 1) / kBY) * ((v.D + kBZ - 1) / kBZ));
+template <int NT, int MT>
+cudaError_t conv3_launch(const float* X, int Cin, const __nv_bfloat16* Wt, int Cout, int co0, const float* bias,
+                         float* Y, Vol v, int relu, int mirror, cudaStream_t st) {
+  const size_t smem = conv_smem<MT>(NT * 8);
+  static bool opted = false;  // shared-memory opt-in, once per instantiation
+  if (!opted) {
+    const cudaError_t e = cudaFuncSetAttribute(k_conv3<NT, MT>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                               (int)smem);
+    if (e != cudaSuccess) return e;
+    opted = true;
+  }
+  const unsigned blocks = (unsigned)(((v.W + kBX - 1) / kBX) * ((v.H + Brick<MT>::BY - 1) / Brick<MT>::BY) *
+                                     ((v.D + kBZ - 1) / kBZ));
+  k_conv3<NT, MT><<<blocks, kConvThreads, smem, st>>>(X, Cin, Wt, Cout, co0, bias, Y, v, relu, mirror);
+  return cudaGetLastError();
+}
+
+// output channels co0 .. co0 + Cn - 1 (Cn 16, 32, 48 or 64)
+cudaError_t conv3(const float* X, int Cin, const __nv_bfloat16* Wt, int Cout, int co0, int Cn, const float* bias,
+                  float* Y, Vol v, int relu, int mirror, cudaStream_t st) {
+  switch (Cn) {
+    case 16: return conv3_launch<2, 4>(X, Cin, Wt, Cout, co0, bias, Y, v, relu, mirror, st);
+    case 32: return conv3_launch<4, 4>(X, Cin, Wt, Cout, co0, bias, Y, v, relu, mirror, st);
+    case 48: return conv3_launch<6, 2>(X, Cin, Wt, Cout, co0, bias, Y, v, relu, mirror, st);
+    case 64: return conv3_launch<8, 2>(X, Cin, Wt, Cout, co0, bias, Y, v, relu, mirror, st);
+    default: return cudaErrorInvalidValue;
+  }
 }
 
 // dW[co][k][ci] += sum_v dY[v][co] X[v + off_k][ci] over a chunk of voxels:
@@ -569,10 +603,8 @@ int ualloc(rihvr_unet* u, T** p, size_t count) {
 int conv_fwd(rihvr_unet* u, int li, const float* X, float* Y) {
   const Conv& L = u->layers[li];
   const Vol v = u->lv[L.level];
-  k_conv3<<<conv_blocks(v), kConvThreads, kConvSmem, u->st>>>(X, L.cin, u->wb + u->wb_off[li], L.cout, 0, L.cout,
-                                                               u->w + L.b_off, Y, v, 1, 0);
+  UCK(conv3(X, L.cin, u->wb + u->wb_off[li], L.cout, 0, L.cout, u->w + L.b_off, Y, v, 1, 0, u->st));
   ++u->launches;
-  UCK(cudaGetLastError());
   return RIHVR_OK;
 }
 
@@ -589,8 +621,8 @@ int conv_back(rihvr_unet* u, int li, const float* X, float* dY, float* dX) {
   u->launches += 3;
   // the data gradient: output channels of the transposed weights in windows of 64
   for (int co0 = 0; dX && co0 < L.cin; co0 += 64) {
-    k_conv3<<<conv_blocks(v), kConvThreads, kConvSmem, u->st>>>(dY, L.cout, u->wt + u->wb_off[li], L.cin, co0,
-                                                                 std::min(64, L.cin - co0), nullptr, dX, v, 0, 1);
+    UCK(conv3(dY, L.cout, u->wt + u->wb_off[li], L.cin, co0, std::min(64, L.cin - co0), nullptr, dX, v, 0, 1,
+              u->st));
     ++u->launches;
   }
   UCK(cudaGetLastError());
@@ -764,8 +796,6 @@ int rihvr_unet_create(int depth, int height, int width, unsigned long long seed,
       cudaMemset(u->m, 0, sizeof(float) * u->nparam) != cudaSuccess ||
       cudaMemset(u->s, 0, sizeof(float) * u->nparam) != cudaSuccess)
     return bail(unet_fail(RIHVR_ERR_CUDA, "initial copies failed"));
-  if (cudaFuncSetAttribute(k_conv3, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kConvSmem) != cudaSuccess)
-    return bail(unet_fail(RIHVR_ERR_CUDA, "shared-memory opt-in failed"));
   u->st = nullptr;
   if ((rc = refresh_bf16(u)) != RIHVR_OK) return bail(rc);
   if (cudaStreamSynchronize(nullptr) != cudaSuccess) return bail(unet_fail(RIHVR_ERR_CUDA, "initialisation failed"));
