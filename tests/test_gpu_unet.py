@@ -1,8 +1,7 @@
 """The warm-start U-Net on the GPU (BF16 tensor-core convolutions, FP32
 accumulation) against the FP64 numpy reference ``unet_ref.py``: the
-prediction, the loss and the gradient of every layer.  Tolerances allow for
-BF16 operands: relative L2 2e-2 on the prediction and loss, 5e-2 on each
-layer's gradient.  Then training reduces the loss, and the warm-start entry
+prediction, the loss and the gradient of every layer, at the tolerances the
+first test states.  Then training reduces the loss, and the warm-start entry
 point of the solver equals the manual path (back-propagate, predict, set the
 initial volume)."""
 import numpy as np
