@@ -157,12 +157,28 @@ int rihvr_reconstruct(rihvr_ctx* ctx, double* final_objective);
  * does rihvr_set_hologram(ctxs[i], holograms[i], is_device) and
  * rihvr_reconstruct(ctxs[i], &final_objectives[i]).  Every context runs on its
  * own host thread and CUDA stream, so the frames' kernels and host decisions
- * overlap on the GPU; results are those of the sequential calls, bit for bit.
- * The contexts must be distinct and may differ in size and parameters.
+ * overlap on the GPU (batch mode 0, the default).  In batch mode 1
+ * (rihvr_set_batch_mode), frames that share a device and iteration count run
+ * the iterations after the first as ONE graph launch per iteration for all
+ * frames: each frame's iteration (its attempts, backtracking test and
+ * momentum step, decided on the device) is a branch of the same graph.
+ * Either way the results are those of the sequential calls, bit for bit.  The
+ * contexts must be distinct and may differ in size and parameters.
  * final_objectives and statuses (n entries each) may be NULL; statuses[i]
  * receives frame i's status.  Returns the first nonzero status in frame order. */
 int rihvr_reconstruct_batch(rihvr_ctx* const* ctxs, int n, const float* const* holograms, int is_device,
                             double* final_objectives, int* statuses);
+
+/* Process-wide batch mode: 0 = one host thread and stream per frame
+ * (default), 1 = one graph launch per iteration for all frames.  Mode 1 pays
+ * a graph build per call and keeps the frames in step at every iteration; it
+ * measured slower than mode 0 on every frame set tried.  Returns
+ * RIHVR_ERR_INVALID_ARGUMENT for other values. */
+int rihvr_set_batch_mode(int mode);
+
+/* 1 when the last rihvr_reconstruct_batch call on this host thread ran its
+ * frames as one graph launch per iteration, else 0. */
+int rihvr_batch_last_combined(void);
 
 /* Launch-shape autotuner (no reference counterpart).  Times the candidate
  * shapes of the passes that have a free parameter on this context's own

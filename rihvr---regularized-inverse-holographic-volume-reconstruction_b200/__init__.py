@@ -126,7 +126,8 @@ OBJECT_DTYPE = np.dtype([
 # every symbol include/rihvr.h declares
 EXPORTED = (
     "rihvr_params_default", "rihvr_read_param_file", "rihvr_plane_list", "rihvr_create", "rihvr_destroy",
-    "rihvr_set_hologram", "rihvr_reconstruct", "rihvr_reconstruct_batch", "rihvr_autotune", "rihvr_tuning", "rihvr_reset",
+    "rihvr_set_hologram", "rihvr_reconstruct", "rihvr_reconstruct_batch", "rihvr_set_batch_mode",
+    "rihvr_batch_last_combined", "rihvr_autotune", "rihvr_tuning", "rihvr_reset",
     "rihvr_set_initial_volume",
     "rihvr_iterate",
     "rihvr_iterate_timed",
@@ -177,6 +178,8 @@ def load_library(path: str = LIB_PATH):
     L.rihvr_set_hologram.argtypes = [vp, vp, ip]
     L.rihvr_reconstruct.argtypes = [vp, P(ctypes.c_double)]
     L.rihvr_reconstruct_batch.argtypes = [P(vp), ip, P(vp), ip, P(ctypes.c_double), P(ctypes.c_int)]
+    L.rihvr_set_batch_mode.argtypes = [ip]
+    L.rihvr_batch_last_combined.argtypes = []
     L.rihvr_autotune.argtypes = [vp, P(ctypes.c_double)]
     L.rihvr_tuning.argtypes = [vp, P(ctypes.c_int), P(ctypes.c_int), P(ctypes.c_int), P(ctypes.c_int)]
     L.rihvr_reset.argtypes = [vp]
@@ -430,6 +433,18 @@ def reconstruct_batch(solvers, holograms):
     st = (ctypes.c_int * n)()
     _check(load_library().rihvr_reconstruct_batch(ctxs, n, ptrs, 0, f, st), "rihvr_reconstruct_batch")
     return [f[i] for i in range(n)]
+
+
+def set_batch_mode(mode: int):
+    """rihvr_set_batch_mode: 0 = one host thread and stream per frame
+    (default), 1 = one graph launch per iteration for all frames."""
+    _check(load_library().rihvr_set_batch_mode(int(mode)), "rihvr_set_batch_mode")
+
+
+def batch_last_combined() -> bool:
+    """Whether the last reconstruct_batch on this thread ran its frames as one
+    graph launch per iteration (rihvr_batch_last_combined)."""
+    return bool(load_library().rihvr_batch_last_combined())
 
 
 def _io_check(rc: int, where: str):

@@ -21,6 +21,7 @@
 #include <tuple>
 #include <new>
 #include <string>
+#include <atomic>
 #include <thread>
 #include <vector>
 
@@ -547,22 +548,21 @@ int enqueue_momentum_dev(rihvr_ctx* c) {
   return RIHVR_OK;
 }
 
-// One iteration as a graph: first attempt, a WHILE node whose body is a
-// backtracking attempt (run while the test asks for one), then the momentum
-// step.  Built by capturing into the graph around the conditional node.
-int build_iter_graph(rihvr_ctx* c, cudaGraphExec_t* out, int* n_main, int* n_body) {
+// One iteration captured into graph g as a branch of its own (root nodes, no
+// dependencies): first attempt, a WHILE node whose body is a backtracking
+// attempt (run while the test asks for one), then the momentum step.  The
+// condition handle belongs to g, so several contexts' iterations can share
+// one graph.  n_main / n_body: kernels outside / inside the WHILE body.
+int capture_iteration(rihvr_ctx* c, cudaGraph_t g, int* n_main, int* n_body) {
   const cudaStreamCaptureMode mode = cudaStreamCaptureModeThreadLocal;
-  cudaGraph_t g = nullptr;
-  CK(cudaGraphCreate(&g, 0));
-  struct GraphGuard {
-    cudaGraph_t& g;
-    ~GraphGuard() {
-      if (g) cudaGraphDestroy(g);
-    }
-  } guard{g};
   cudaGraphConditionalHandle h;
   CK(cudaGraphConditionalHandleCreate(&h, g, 0, 0));
   const long long l0 = c->launches;
+  struct LaunchGuard {
+    rihvr_ctx* c;
+    long long l0;
+    ~LaunchGuard() { c->launches = l0; }
+  } lguard{c, l0};
   CK(cudaStreamBeginCaptureToGraph(c->st, g, nullptr, nullptr, 0, mode));
   int rc = enqueue_attempt_dev(c, true, h);
   cudaStreamCaptureStatus status;
@@ -595,10 +595,24 @@ int build_iter_graph(rihvr_ctx* c, cudaGraphExec_t* out, int* n_main, int* n_bod
   e = cudaStreamEndCapture(c->st, &cap);
   if (rc != RIHVR_OK) return rc;
   CK(e);
-  CK(cudaGraphInstantiate(out, g, 0));
   *n_main = (int)((l1 - l0) + (c->launches - l2));
   *n_body = (int)(l2 - l1);
-  c->launches = l0;
+  return RIHVR_OK;
+}
+
+struct GraphGuard {
+  cudaGraph_t g = nullptr;
+  ~GraphGuard() {
+    if (g) cudaGraphDestroy(g);
+  }
+};
+
+// One iteration of one context as an executable graph.
+int build_iter_graph(rihvr_ctx* c, cudaGraphExec_t* out, int* n_main, int* n_body) {
+  GraphGuard guard;
+  CK(cudaGraphCreate(&guard.g, 0));
+  RC(capture_iteration(c, guard.g, n_main, n_body));
+  CK(cudaGraphInstantiate(out, guard.g, 0));
   return RIHVR_OK;
 }
 
@@ -621,41 +635,147 @@ void pull_dev_log(rihvr_ctx* c, int n) {
 
 // n iterations without host synchronisation between them: the graphs are
 // launched back to back and the log is read every kDevLogCap iterations.
+// The host's loop state into the pinned control block, before a run of
+// device-decided iterations.
+void stage_ctl(rihvr_ctx* c) {
+  IterCtl& h = *c->ctl_h;
+  h.t = c->t;
+  h.alpha1 = c->alpha1;
+  h.beta = c->beta;
+  h.prev_f_resid = c->prev_f_resid;
+  h.f_resid = h.lim = h.ratio = 0.0;
+  h.bt = 0;
+  h.it = c->it;
+  h.it_base = c->it;
+  h.pad = 0;
+}
+
+// After m device-decided iterations (control block and log read back): the
+// loop state, the launch count of the backtracking attempts (n_body kernels
+// each) and the iteration log.
+void take_ctl(rihvr_ctx* c, int m, int n_body) {
+  const IterCtl& h = *c->ctl_h;
+  c->t = h.t;
+  c->alpha1 = h.alpha1;
+  c->beta = h.beta;
+  c->prev_f_resid = h.prev_f_resid;
+  c->it = h.it;
+  for (int k = 0; k < m; ++k) c->launches += (long long)c->dlog_h[k].rec.backtracks * n_body;
+  pull_dev_log(c, m);
+}
+
+void rotate(rihvr_ctx* c) {
+  const int old_prev = c->iPrev;
+  c->iPrev = c->iCur;
+  c->iCur = c->iNew;
+  c->iNew = old_prev;
+}
+
 int run_iterations_dev(rihvr_ctx* c, int n) {
   for (int done = 0; done < n;) {
     const int m = std::min(n - done, kDevLogCap);
-    IterCtl& h = *c->ctl_h;
-    h.t = c->t;
-    h.alpha1 = c->alpha1;
-    h.beta = c->beta;
-    h.prev_f_resid = c->prev_f_resid;
-    h.f_resid = h.lim = h.ratio = 0.0;
-    h.bt = 0;
-    h.it = c->it;
-    h.it_base = c->it;
-    h.pad = 0;
+    stage_ctl(c);
     CK(cudaMemcpyAsync(c->ctl_d, c->ctl_h, sizeof(IterCtl), cudaMemcpyHostToDevice, c->st));
     for (int k = 0; k < m; ++k) {
       const int slot = c->iCur;
       CK(cudaGraphLaunch(c->g_iter[slot], c->st));
       c->launches += c->g_iter_n[slot][0];
-      const int old_prev = c->iPrev;
-      c->iPrev = c->iCur;
-      c->iCur = c->iNew;
-      c->iNew = old_prev;
+      rotate(c);
     }
     CK(cudaMemcpyAsync(c->ctl_h, c->ctl_d, sizeof(IterCtl), cudaMemcpyDeviceToHost, c->st));
     CK(cudaMemcpyAsync(c->dlog_h, c->dlog_d, sizeof(DevRec) * m, cudaMemcpyDeviceToHost, c->st));
     CK(cudaStreamSynchronize(c->st));
-    c->t = h.t;
-    c->alpha1 = h.alpha1;
-    c->beta = h.beta;
-    c->prev_f_resid = h.prev_f_resid;
-    c->it = h.it;
-    for (int k = 0; k < m; ++k) c->launches += (long long)c->dlog_h[k].rec.backtracks * c->g_iter_n[0][1];
-    pull_dev_log(c, m);
+    take_ctl(c, m, c->g_iter_n[0][1]);
     done += m;
   }
+  return RIHVR_OK;
+}
+
+// Several contexts' iterations as one graph launch per iteration: each
+// context's iteration is a branch of the same graph with its own WHILE node
+// and condition, so the frames' kernels run concurrently and the host launches
+// once per iteration for all of them.  Every branch is the sequence
+// build_iter_graph captures for its context alone, so each frame's iterates
+// are those of run_iterations_dev, bit for bit.
+struct BatchGraphs {
+  cudaGraphExec_t g[3] = {};
+  std::vector<int> n_main[3];
+  std::vector<int> n_body;
+  BatchGraphs() = default;
+  BatchGraphs(const BatchGraphs&) = delete;
+  BatchGraphs& operator=(const BatchGraphs&) = delete;
+  ~BatchGraphs() {
+    for (auto& x : g)
+      if (x) cudaGraphExecDestroy(x);
+  }
+};
+
+// One graph per position of P_k in the rotation, as ensure_iter_graphs.
+int build_batch_graphs(rihvr_ctx* const* cs, int n, BatchGraphs& B) {
+  B.n_body.assign(n, 0);
+  for (int slot = 0; slot < 3; ++slot) {
+    B.n_main[slot].assign(n, 0);
+    GraphGuard guard;
+    CK(cudaGraphCreate(&guard.g, 0));
+    for (int i = 0; i < n; ++i) {
+      rihvr_ctx* c = cs[i];
+      const int p0 = c->iPrev, c0 = c->iCur, n0 = c->iNew;
+      c->iCur = slot;
+      c->iPrev = (slot + 2) % 3;
+      c->iNew = (slot + 1) % 3;
+      const int rc = capture_iteration(c, guard.g, &B.n_main[slot][i], &B.n_body[i]);
+      c->iPrev = p0;
+      c->iCur = c0;
+      c->iNew = n0;
+      if (rc != RIHVR_OK) return rc;
+    }
+    CK(cudaGraphInstantiate(&B.g[slot], guard.g, 0));
+  }
+  return RIHVR_OK;
+}
+
+struct EventGuard {
+  cudaEvent_t e = nullptr;
+  ~EventGuard() {
+    if (e) cudaEventDestroy(e);
+  }
+};
+
+// n iterations of every context through the batch graphs, launched on the
+// first context's stream; the other streams are ordered before and after it.
+// The contexts share a device and a rotation position.
+int run_iterations_batch(rihvr_ctx* const* cs, int nc, int n, const BatchGraphs& B) {
+  cudaStream_t st = cs[0]->st;
+  EventGuard ev;
+  CK(cudaEventCreateWithFlags(&ev.e, cudaEventDisableTiming));
+  for (int i = 1; i < nc; ++i) {
+    CK(cudaEventRecord(ev.e, cs[i]->st));
+    CK(cudaStreamWaitEvent(st, ev.e, 0));
+  }
+  for (int done = 0; done < n;) {
+    const int m = std::min(n - done, kDevLogCap);
+    for (int i = 0; i < nc; ++i) {
+      stage_ctl(cs[i]);
+      CK(cudaMemcpyAsync(cs[i]->ctl_d, cs[i]->ctl_h, sizeof(IterCtl), cudaMemcpyHostToDevice, st));
+    }
+    for (int k = 0; k < m; ++k) {
+      const int slot = cs[0]->iCur;
+      CK(cudaGraphLaunch(B.g[slot], st));
+      for (int i = 0; i < nc; ++i) {
+        cs[i]->launches += B.n_main[slot][i];
+        rotate(cs[i]);
+      }
+    }
+    for (int i = 0; i < nc; ++i) {
+      CK(cudaMemcpyAsync(cs[i]->ctl_h, cs[i]->ctl_d, sizeof(IterCtl), cudaMemcpyDeviceToHost, st));
+      CK(cudaMemcpyAsync(cs[i]->dlog_h, cs[i]->dlog_d, sizeof(DevRec) * m, cudaMemcpyDeviceToHost, st));
+    }
+    CK(cudaStreamSynchronize(st));
+    for (int i = 0; i < nc; ++i) take_ctl(cs[i], m, B.n_body[i]);
+    done += m;
+  }
+  CK(cudaEventRecord(ev.e, st));
+  for (int i = 1; i < nc; ++i) CK(cudaStreamWaitEvent(cs[i]->st, ev.e, 0));
   return RIHVR_OK;
 }
 
@@ -668,6 +788,15 @@ bool dev_loop_enabled() {
   }();
   return on;
 }
+
+// How rihvr_reconstruct_batch runs the iterations after the first
+// (rihvr_set_batch_mode): 0 = each frame's own device loop on its own host
+// thread and stream, 1 = one graph launch per iteration for all frames.
+std::atomic<int> g_batch_mode{0};
+
+// whether the last rihvr_reconstruct_batch call on this host thread ran its
+// frames as one graph launch per iteration
+thread_local int g_batch_combined = 0;
 
 bool use_dev_loop(const rihvr_ctx* c) { return c->dev_loop && dev_loop_enabled() && use_graphs(c) && c->mode != 6; }
 
@@ -765,22 +894,8 @@ int one_iteration(rihvr_ctx* c) {
   return RIHVR_OK;
 }
 
-int run_iterations(rihvr_ctx* c, int n) {
-  if (!c->have_holo) return fail(RIHVR_ERR_MISSING_DATA, "no hologram set");
-  int i = 0;
-  if (n > 0 && !c->warm) {  // the first iteration of a context runs eagerly
-    RC(one_iteration(c));
-    ++i;
-  }
-  if (i < n && use_dev_loop(c)) {
-    if (ensure_iter_graphs(c) == RIHVR_OK) {
-      RC(run_iterations_dev(c, n - i));
-      i = n;
-    } else {
-      c->dev_loop = false;  // the attempt and momentum graphs of one_iteration instead
-    }
-  }
-  for (; i < n; ++i) RC(one_iteration(c));
+// The momentum-point terms of the last record, when the objective is recorded.
+int settle_pending(rihvr_ctx* c) {
   if (c->p.record_objective && c->pending_x >= 0) {
     double l1x, tvx;
     RC(norms_at_x(c, &l1x, &tvx));
@@ -790,6 +905,38 @@ int run_iterations(rihvr_ctx* c, int n) {
     settle_x_terms(c, s);
   }
   return RIHVR_OK;
+}
+
+// Iterations i .. n-1 of a run, after the eager first one (when it ran).
+int run_iterations_from(rihvr_ctx* c, int i, int n) {
+  if (i < n && use_dev_loop(c)) {
+    if (ensure_iter_graphs(c) == RIHVR_OK) {
+      RC(run_iterations_dev(c, n - i));
+      i = n;
+    } else {
+      c->dev_loop = false;  // the attempt and momentum graphs of one_iteration instead
+    }
+  }
+  for (; i < n; ++i) RC(one_iteration(c));
+  return settle_pending(c);
+}
+
+// The first iteration of a context runs eagerly (it sets kernel attributes
+// and builds tables that graph capture must not see); returns how many ran.
+int eager_start(rihvr_ctx* c, int n, int* ran) {
+  *ran = 0;
+  if (n > 0 && !c->warm) {
+    RC(one_iteration(c));
+    *ran = 1;
+  }
+  return RIHVR_OK;
+}
+
+int run_iterations(rihvr_ctx* c, int n) {
+  if (!c->have_holo) return fail(RIHVR_ERR_MISSING_DATA, "no hologram set");
+  int i = 0;
+  RC(eager_start(c, n, &i));
+  return run_iterations_from(c, i, n);
 }
 
 int copy_out(rihvr_ctx* c, void* dst, const void* src, size_t bytes, int is_device) {
@@ -1170,31 +1317,73 @@ int rihvr_reconstruct(rihvr_ctx* c, double* final_objective) {
 
 int rihvr_reconstruct_batch(rihvr_ctx* const* ctxs, int n, const float* const* holograms, int is_device,
                             double* final_objectives, int* statuses) {
+  g_batch_combined = 0;
   if (!ctxs || !holograms || n <= 0) return fail(RIHVR_ERR_INVALID_ARGUMENT, "empty or NULL batch");
   for (int i = 0; i < n; ++i) {
     if (!ctxs[i] || !holograms[i]) return fail(RIHVR_ERR_INVALID_ARGUMENT, "NULL context or hologram in batch");
     for (int j = 0; j < i; ++j)
       if (ctxs[j] == ctxs[i]) return fail(RIHVR_ERR_INVALID_ARGUMENT, "a context appears twice in the batch");
   }
-  std::vector<int> st(n, RIHVR_OK);
+  std::vector<int> st(n, RIHVR_OK), ran(n, 0);
   std::vector<std::string> msg(n);
-  auto frame = [&](int i) {
-    rihvr_ctx* c = ctxs[i];
-    int rc = cudaSetDevice(c->device) == cudaSuccess ? RIHVR_OK : RIHVR_ERR_CUDA;
-    if (rc == RIHVR_OK) rc = rihvr_set_hologram(c, holograms[i], is_device);
-    double f = 0.0;
-    if (rc == RIHVR_OK) rc = rihvr_reconstruct(c, &f);
-    if (final_objectives) final_objectives[i] = rc == RIHVR_OK ? f : 0.0;
-    st[i] = rc;
-    if (rc != RIHVR_OK) msg[i] = g_last_error;  // thread-local: carried back to the caller's thread
+  // run fn on every frame still without error, one host thread per frame
+  auto each_frame = [&](auto fn) {
+    auto one = [&](int i) -> void {
+      if (st[i] != RIHVR_OK) return;
+      rihvr_ctx* c = ctxs[i];
+      int rc = cudaSetDevice(c->device) == cudaSuccess ? RIHVR_OK : RIHVR_ERR_CUDA;
+      if (rc == RIHVR_OK) rc = fn(i, c);
+      st[i] = rc;
+      if (rc != RIHVR_OK) msg[i] = g_last_error;  // thread-local: carried back to the caller's thread
+    };
+    std::vector<std::thread> workers;
+    workers.reserve(n - 1);
+    for (int i = 1; i < n; ++i) workers.emplace_back(one, i);
+    one(0);
+    for (auto& w : workers) w.join();
   };
-  std::vector<std::thread> workers;
-  workers.reserve(n > 0 ? n - 1 : 0);
-  for (int i = 1; i < n; ++i) workers.emplace_back(frame, i);
-  frame(0);
-  for (auto& w : workers) w.join();
+  // hologram in, state reset and the eager first iteration, frames overlapping
+  each_frame([&](int i, rihvr_ctx* c) -> int {
+    RC(rihvr_set_hologram(c, holograms[i], is_device));
+    RC(state_reset(c));
+    return eager_start(c, c->p.num_inverse_iterations, &ran[i]);
+  });
+  // the remaining iterations: in batch mode 1, one graph launch per iteration
+  // for all frames when they share a device, run the device-decided loop and
+  // are at the same point; else each frame's own loop on its own thread
+  bool combined = n > 1 && g_batch_mode.load() == 1;
+  const int rest = ctxs[0]->p.num_inverse_iterations - ran[0];
+  for (int i = 0; i < n && combined; ++i) {
+    const rihvr_ctx* c = ctxs[i];
+    combined = st[i] == RIHVR_OK && use_dev_loop(c) && c->device == ctxs[0]->device &&
+               c->p.num_inverse_iterations - ran[i] == rest && c->iCur == ctxs[0]->iCur;
+  }
+  combined = combined && rest > 0;
+  if (combined) {
+    BatchGraphs B;
+    if (cudaSetDevice(ctxs[0]->device) == cudaSuccess && build_batch_graphs(ctxs, n, B) == RIHVR_OK) {
+      const int rc = run_iterations_batch(ctxs, n, rest, B);
+      for (int i = 0; i < n; ++i) {
+        st[i] = rc;
+        if (rc != RIHVR_OK) msg[i] = g_last_error;
+      }
+      g_batch_combined = 1;
+    } else {
+      cudaGetLastError();
+      combined = false;
+    }
+  }
+  each_frame([&](int i, rihvr_ctx* c) -> int {
+    if (combined) RC(settle_pending(c));
+    else RC(run_iterations_from(c, ran[i], c->p.num_inverse_iterations));
+    double f = 0.0;
+    RC(rihvr_objective(c, &f, nullptr));
+    if (final_objectives) final_objectives[i] = f;
+    return RIHVR_OK;
+  });
   int first = RIHVR_OK;
   for (int i = 0; i < n; ++i) {
+    if (final_objectives && st[i] != RIHVR_OK) final_objectives[i] = 0.0;
     if (statuses) statuses[i] = st[i];
     if (first == RIHVR_OK && st[i] != RIHVR_OK) {
       first = st[i];
@@ -1203,6 +1392,14 @@ int rihvr_reconstruct_batch(rihvr_ctx* const* ctxs, int n, const float* const* h
   }
   return first;
 }
+
+int rihvr_set_batch_mode(int mode) {
+  if (mode != 0 && mode != 1) return fail(RIHVR_ERR_INVALID_ARGUMENT, "batch mode must be 0 or 1");
+  g_batch_mode.store(mode);
+  return RIHVR_OK;
+}
+
+int rihvr_batch_last_combined(void) { return g_batch_combined; }
 
 int rihvr_iteration_count(const rihvr_ctx* c) { return c ? c->it : -1; }
 

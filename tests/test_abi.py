@@ -126,3 +126,15 @@ def test_batch_validates_before_touching_contexts(rihvr):
     assert b"twice" in L.rihvr_last_error()
     nul = (ctypes.c_void_p * 1)(None)
     assert L.rihvr_reconstruct_batch(nul, 1, holo, 0, None, None) == rihvr.ERR_INVALID_ARGUMENT
+
+
+def test_batch_mode_setting(rihvr):
+    """rihvr_set_batch_mode takes 0 or 1 only; a rejected batch ran no frame
+    as one graph per iteration."""
+    L = rihvr.load_library()
+    assert L.rihvr_set_batch_mode(2) == rihvr.ERR_INVALID_ARGUMENT
+    assert L.rihvr_set_batch_mode(-1) == rihvr.ERR_INVALID_ARGUMENT
+    assert L.rihvr_set_batch_mode(1) == rihvr.OK
+    assert L.rihvr_reconstruct_batch(None, 1, None, 0, None, None) == rihvr.ERR_INVALID_ARGUMENT
+    assert L.rihvr_batch_last_combined() == 0
+    assert L.rihvr_set_batch_mode(0) == rihvr.OK

@@ -49,3 +49,59 @@ def test_batch_reports_the_failing_frame(rihvr, synthmod, cache_dir):
     finally:
         s1.destroy()
         s2.destroy()
+
+
+def test_batch_as_one_graph_per_iteration(rihvr, synthmod, cache_dir):
+    """Batch mode 1: frames of different sizes, TV settings and storage but the
+    same iteration count run as one graph launch per iteration (each frame a
+    branch with its own device-side backtracking loop); every frame's volume,
+    objective and iteration log equal its sequential run bit for bit, on cold
+    contexts (eager first iteration) and again on warm ones."""
+    cfgs = [synthmod.small_config(W=64, H=64, Nz=5, seed=21, num_inverse_iterations=9),
+            synthmod.small_config(W=128, H=128, Nz=4, seed=22, num_inverse_iterations=9, num_tv_iterations=3),
+            synthmod.small_config(W=32, H=32, Nz=7, seed=23, num_inverse_iterations=9),
+            synthmod.small_config(W=64, H=64, Nz=3, seed=24, num_inverse_iterations=9, regularization_TV_param=0.0)]
+    storage = [0, 0, 2, 1]
+    holos = [synthmod.make_hologram(c, cache_dir=cache_dir)[1] for c in cfgs]
+    seq = []
+    for c, b, sto in zip(cfgs, holos, storage):
+        with rihvr.SparseCompressiveHolo(rihvr.params_from_config(c, storage=sto), c.W, c.H) as s:
+            f = s.inverseReconstruct(b)
+            seq.append((f, s.getVolume(), s.iterations()))
+    solvers = [rihvr.SparseCompressiveHolo(rihvr.params_from_config(c, storage=sto), c.W, c.H)
+               for c, sto in zip(cfgs, storage)]
+    rihvr.set_batch_mode(1)
+    try:
+        for _ in range(2):
+            fs = rihvr.reconstruct_batch(solvers, holos)
+            assert rihvr.batch_last_combined()
+            for (f, X, log), fb, s in zip(seq, fs, solvers):
+                assert fb == f
+                assert np.array_equal(s.getVolume(), X)
+                got = s.iterations()
+                for name in ("f_x", "f_prox", "t", "beta", "backtracks", "restarted"):
+                    assert np.array_equal(got[name], log[name]), name
+    finally:
+        rihvr.set_batch_mode(0)
+        for s in solvers:
+            s.destroy()
+    with pytest.raises(rihvr.RihvrError):
+        rihvr.set_batch_mode(2)
+
+
+def test_uneven_iteration_counts_run_frame_by_frame(rihvr, synthmod, cache_dir):
+    """Batch mode 1 with frames at different iteration counts falls back to one
+    loop per frame."""
+    cfgs = [synthmod.small_config(W=64, H=64, Nz=3, seed=25, num_inverse_iterations=4),
+            synthmod.small_config(W=64, H=64, Nz=3, seed=26, num_inverse_iterations=6)]
+    holos = [synthmod.make_hologram(c, cache_dir=cache_dir)[1] for c in cfgs]
+    solvers = [rihvr.SparseCompressiveHolo(rihvr.params_from_config(c), c.W, c.H) for c in cfgs]
+    rihvr.set_batch_mode(1)
+    try:
+        rihvr.reconstruct_batch(solvers, holos)
+        assert not rihvr.batch_last_combined()
+        assert [s.iterations().shape[0] for s in solvers] == [4, 6]
+    finally:
+        rihvr.set_batch_mode(0)
+        for s in solvers:
+            s.destroy()
