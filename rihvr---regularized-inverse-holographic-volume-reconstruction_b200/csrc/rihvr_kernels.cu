@@ -1224,13 +1224,25 @@ struct TvwShape {
   static constexpr int D = (h + 2 <= 8) ? 8 : 16;     // rows in use: h + 1, plus one landing
   static constexpr int F4 = CPL / 2;                  // float4 per array per lane row (FP32)
   static constexpr int SLOT = 3 * F4 * 32;            // float4 per ring slot, whole warp
-  static constexpr int NW = 4;                        // warps per block
+  // Two warps per block.  Without the objective's norm terms and with the
+  // 8-row ring (n_tv <= 5), the kernel fits 128 registers with at most a few
+  // bytes of spill, and 8 blocks (16 warps) share an SM; the norm terms need
+  // about 165 registers, which caps them at 6 blocks (12 warps).  Blocks of 4
+  // warps at 3 per SM took 10.42 ms per launch at 1024 x 1024 x 1000 (n_tv = 5),
+  // 2-warp blocks at 16 per SM 9.5 ms.
+  static constexpr int NW = 2;
   static constexpr size_t SMEM = sizeof(float4) * (size_t)SLOT * D * NW;
-  // blocks per SM; a fourth block (128 registers) spills and runs far slower
-  static constexpr int MINB = (3 * (SMEM + 1024) <= 228 * 1024) ? 3 : 2;
   static_assert(CPL == 2 || CPL == 4, "columns per lane");
   static_assert(VW > 0, "halo wider than the strip");
 };
+
+// Blocks per SM the register allocation targets (__launch_bounds__).  At 7
+// two-warp blocks ptxas caps the kernel at 128 registers (8 blocks then fit);
+// asking for 8 gives the same cap with ten times the spill.
+template <int NTV, bool NORMS>
+constexpr int tvw_minb() {
+  return TvwShape<NTV, 2>::D == 8 ? (NORMS ? 6 : 7) : 4;
+}
 
 // copy CPL complex values in storage type (16-byte aligned source for
 // CPL * sizeof(ST) >= 16, else 8-byte aligned) to shared memory
@@ -1284,7 +1296,7 @@ __device__ __forceinline__ void store_run(ST* p, const float2 (&v)[CPL]) {
 }
 
 template <typename ST, int NTV, bool NORMS, int CPL = 2, int NW = TvwShape<NTV, CPL>::NW,
-          int MINB = TvwShape<NTV, CPL>::MINB, int UNR = 4, int PADTO = 4>
+          int MINB = tvw_minb<NTV, NORMS>(), int UNR = 4, int PADTO = 4>
 __global__ void __launch_bounds__(32 * NW, MINB) k_prox_tv2d_strip(ProxArgs a0, TvsGrid gr) {
   const ProxArgs a = resolve_scalars(a0);
   using Sh = TvwShape<NTV, CPL>;
@@ -1520,17 +1532,28 @@ static TvsGrid tvs_grid(int W, int H, int Nz, int VW, int warps_per_sm, int warm
 template <typename ST, int NTV, bool NORMS>
 static cudaError_t strip_launch_n(const ProxArgs& a, int* nblocks_out, cudaStream_t st) {
   using Sh = TvwShape<NTV, 2>;
-  TvsGrid g = tvs_grid(a.W, a.H, a.Nz, Sh::VW, Sh::NW * Sh::MINB, 2 * Sh::h + 3);
+  cudaError_t e = allow_smem(k_prox_tv2d_strip<ST, NTV, NORMS>, Sh::SMEM);
+  if (e != cudaSuccess) return e;
+  // resident blocks per SM, for the choice of runs per plane
+  static const int resident = [] {
+    int b = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_prox_tv2d_strip<ST, NTV, NORMS>, 32 * Sh::NW, Sh::SMEM) !=
+            cudaSuccess ||
+        b <= 0) {
+      cudaGetLastError();
+      b = tvw_minb<NTV, NORMS>();
+    }
+    return b;
+  }();
+  TvsGrid g = tvs_grid(a.W, a.H, a.Nz, Sh::VW, Sh::NW * resident, 2 * Sh::h + 3);
   if (a.tv_nseg > 0) {  // tuned number of runs per plane
     g.seg_len = (a.H + min(a.tv_nseg, a.H) - 1) / min(a.tv_nseg, a.H);
     g.nseg = (a.H + g.seg_len - 1) / g.seg_len;
   }
   const long long runs = (long long)g.nstrips * g.nseg * a.Nz;
   const long long blocks = (runs + Sh::NW - 1) / Sh::NW;
-  if (blocks > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
+  if (blocks > 0x7fffffffLL || blocks > a.partial_cap) return cudaErrorInvalidConfiguration;
   *nblocks_out = (int)blocks;
-  cudaError_t e = allow_smem(k_prox_tv2d_strip<ST, NTV, NORMS>, Sh::SMEM);
-  if (e != cudaSuccess) return e;
   k_prox_tv2d_strip<ST, NTV, NORMS><<<(unsigned)blocks, 32 * Sh::NW, Sh::SMEM, st>>>(a, g);
   return cudaGetLastError();
 }
@@ -1576,11 +1599,15 @@ static void tv_grid(const ProxArgs& a, dim3* g) {
 }
 
 size_t max_partial_blocks(int W, int H, int Nz) {
-  // the TV prox with the largest halo it accepts (n_tv <= 20) bounds all grids
+  // the tiled TV prox with the largest halo it accepts (n_tv <= 20)
   const int h = 21, VW = TV_EW - 2 * h, VH = TV_EH - 2 * h;
-  size_t tv = (size_t)((W + VW - 1) / VW) * ((H + VH - 1) / VH) * Nz;
-  size_t flat = 4096;
-  return tv > flat ? tv : flat;
+  const size_t tv = (size_t)((W + VW - 1) / VW) * ((H + VH - 1) / VH) * Nz;
+  // the streaming TV prox with its narrowest strips (n_tv = 10) and the most
+  // runs per plane (64), one block per run
+  using Sh = TvwShape<kStripNtvMax, 2>;
+  const size_t strip = (size_t)((W + Sh::VW - 1) / Sh::VW) * (size_t)std::min(64, H) * Nz;
+  const size_t flat = 4096;
+  return std::max(std::max(tv, strip), flat);
 }
 
 cudaError_t launch_prox_tv2d(int storage, const ProxArgs& a, int* nblocks_out, cudaStream_t st) {

@@ -38,6 +38,7 @@ struct ProxArgs {
   int faithful;       // reference quirks (separable shrink, restart weights)
   int want_norms;     // accumulate L1/TV of p and x
   double* partials;   // [blocks][kNumSums]
+  long long partial_cap = 0;  // blocks partials holds; a launch needing more is refused
   // tuning knobs (0 = built-in choice): runs per plane of the streaming 2-D TV
   // prox, and the 2-D TV kernel (1 tiled, 2 streaming)
   int tv_nseg = 0;

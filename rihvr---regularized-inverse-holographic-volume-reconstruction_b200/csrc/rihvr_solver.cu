@@ -361,6 +361,7 @@ ProxArgs prox_args(rihvr_ctx* c, double t, bool device_scalars = false) {
   a.faithful = c->p.faithful;
   a.want_norms = c->p.record_objective;
   a.partials = c->partials;
+  a.partial_cap = (long long)c->partial_cap;
   a.tv_nseg = c->tune_tv_nseg;
   a.tv_kernel = c->tune_tv_kernel;
   // proximalFusedLasso2d shrinks only if l1 > 0 (:3715)
