@@ -128,9 +128,10 @@ def class_bytes(s: int) -> dict:
 # capture of `bench.py --nz 16 --no-autotune`, 64 planes for the adjoint column
 # pass, divided by its voxels), keyed by (class, stored bytes per voxel).
 # Scaled by the voxels of a launch, since traffic grows with the planes
-# processed.
+# processed.  The prox figure is dram__bytes.sum.per_second x duration of the
+# 2-warp-block kernel (2.754 TB/s x 201.98 us).
 MEASURED_TRAFFIC_PER_VOXEL = {
-    ("prox", 8): (462.4e6 + 115.3e6) / (1024 * 1024 * 16),
+    ("prox", 8): 2.753885e12 * 201.984e-6 / (1024 * 1024 * 16),
     ("fwd_col", 8): (145.2e6 + 19.8e6) / (1024 * 1024 * 16),
     ("fwd_row", 8): (134.3e6 + 85.1e6) / (1024 * 1024 * 16),
     ("adj_row", 8): (134.3e6 + 85.6e6) / (1024 * 1024 * 16),
