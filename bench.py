@@ -195,15 +195,16 @@ def time_to_objective(rihvr, cfg, b, s, storage, stream, hb, tol=1e-3):
     return out
 
 
-def cpu_sample(cfg, b, steps: int, warmup: int):
-    """Time the FP64 oracle on a bounded sample of the workload: the first 16
-    planes of the volume, full plane size, one FISTA iteration per step."""
+def cpu_sample(cfg, b, steps: int, warmup: int, planes: int = 16):
+    """Time the FP64 oracle on a bounded sample of the workload: the first
+    `planes` planes of the volume, full plane size, one FISTA iteration per
+    step."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
 
     rihvr = importlib.import_module(PKG)
     p = rihvr.params_from_config(cfg)
-    nz = min(16, cfg.num_planes)
+    nz = min(planes, cfg.num_planes)
     z = rihvr.plane_list(p)[:nz]
     op = O.OracleParams(W=cfg.W, H=cfg.H, z=z, dx=cfg.dx(), lam=cfg.lam(), l1=cfg.l1(), tv=cfg.tv(),
                         n_tv=cfg.num_tv_iterations, mode=7, faithful=1)
@@ -505,7 +506,8 @@ def run_ours(args):
     if rank == 0:
         cpu = None
         if ws == 1 and not args.no_cpu_baseline:
-            cpu = cpu_sample(cfg, b, steps=2, warmup=1)
+            # 96 planes: about 10 s of oracle work on a 16-core host
+            cpu = cpu_sample(cfg, b, steps=2, warmup=1, planes=96)
         line = {
             "metric": METRIC, "value": value, "unit": "voxel-iters/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True, "scaling": "weak",
