@@ -506,8 +506,8 @@ def run_ours(args):
     if rank == 0:
         cpu = None
         if ws == 1 and not args.no_cpu_baseline:
-            # 96 planes: about 10 s of oracle work on a 16-core host
-            cpu = cpu_sample(cfg, b, steps=2, warmup=1, planes=96)
+            # 192 planes: about 10 s of oracle work on a 16-core host
+            cpu = cpu_sample(cfg, b, steps=2, warmup=1, planes=192)
         line = {
             "metric": METRIC, "value": value, "unit": "voxel-iters/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True, "scaling": "weak",
