@@ -80,13 +80,18 @@ __device__ __forceinline__ void tap_offsets(int k, int* dz, int* dy, int* dx) {
 // (4 x (2 MT + 2) x 18 voxels, zero outside the volume, BF16) and the slice's
 // weights for all 27 taps in shared memory, then runs the 27 taps from there:
 // the A fragment of a tap is the halo shifted by the tap's offset, so nothing
-// is restaged between taps.  Rows are padded to 24 BF16 (48 bytes) so fragment
-// loads hit distinct banks.  Narrow layers (16 or 32 channels) take MT = 4:
-// taller bricks, fewer halo voxels per output and smaller weight tiles, so
-// more blocks fit per SM.
+// is restaged between taps.  A shared row holds 16 BF16 (two 16-byte chunks)
+// with no padding; chunk c of row r sits at position c ^ ((r >> 2) & 1), so the
+// 8 consecutive rows of a fragment load cover the 32 banks once whatever the
+// first row (rows r and r + 4 land 16 bytes apart).  Narrow layers (16 or 32
+// channels) take MT = 4: taller bricks, fewer halo voxels per output and
+// smaller weight tiles, so more blocks fit per SM.
 constexpr int kConvThreads = 128;
 constexpr int kBZ = 2, kBX = 16, kHX = kBX + 2;
-constexpr int kRow = 24;  // BF16 per shared row (16 used)
+constexpr int kRow = 16;  // BF16 per shared row
+
+// element offset of 16-byte chunk c (0 or 1) of shared row r
+__device__ __forceinline__ int swz(int r, int c) { return r * kRow + ((c ^ (r >> 2)) & 1) * 8; }
 
 template <int MT>
 struct Brick {
@@ -135,13 +140,13 @@ __global__ void __launch_bounds__(kConvThreads) k_conv3(const float* __restrict_
       pk.y = pack_bf16(lo.z, lo.w);
       pk.z = pack_bf16(hi.x, hi.y);
       pk.w = pack_bf16(hi.z, hi.w);
-      *reinterpret_cast<uint4*>(Hs + h * kRow + half * 8) = pk;
+      *reinterpret_cast<uint4*>(Hs + swz(h, half)) = pk;
     }
     // weights of the slice for every tap: row k * Cn + co
     for (int e = tid; e < 27 * Cn * 2; e += kConvThreads) {
       const int row = e >> 1, half = e & 1;
       const int k = row / Cn, co = row - k * Cn;
-      *reinterpret_cast<uint4*>(Ws + row * kRow + half * 8) =
+      *reinterpret_cast<uint4*>(Ws + swz(row, half)) =
           *reinterpret_cast<const uint4*>(Wt + ((long long)(co0 + co) * 27 + k) * Cin + s * 16 + half * 8);
     }
     __syncthreads();
@@ -152,9 +157,9 @@ __global__ void __launch_bounds__(kConvThreads) k_conv3(const float* __restrict_
       unsigned b[NT][2];
 #pragma unroll
       for (int j = 0; j < NT; ++j) {
-        const __nv_bfloat16* bp = Ws + (k * Cn + j * 8 + g) * kRow;
-        b[j][0] = *reinterpret_cast<const unsigned*>(bp + 2 * t);
-        b[j][1] = *reinterpret_cast<const unsigned*>(bp + 2 * t + 8);
+        const int br = k * Cn + j * 8 + g;
+        b[j][0] = *reinterpret_cast<const unsigned*>(Ws + swz(br, 0) + 2 * t);
+        b[j][1] = *reinterpret_cast<const unsigned*>(Ws + swz(br, 1) + 2 * t);
       }
 #pragma unroll
       for (int r = 0; r < MT; ++r) {
@@ -162,12 +167,11 @@ __global__ void __launch_bounds__(kConvThreads) k_conv3(const float* __restrict_
         const int row = warp * MT + r;
         const int mz = row / Bk::BY, my = row % Bk::BY;
         const int hb = ((mz + dz + 1) * Bk::HY + (my + dy + 1)) * kHX + dx + 1;
-        const __nv_bfloat16* a_lo = Hs + (hb + g) * kRow;
-        const __nv_bfloat16* a_hi = Hs + (hb + g + 8) * kRow;
-        const unsigned a0 = *reinterpret_cast<const unsigned*>(a_lo + 2 * t);
-        const unsigned a1 = *reinterpret_cast<const unsigned*>(a_hi + 2 * t);
-        const unsigned a2 = *reinterpret_cast<const unsigned*>(a_lo + 2 * t + 8);
-        const unsigned a3 = *reinterpret_cast<const unsigned*>(a_hi + 2 * t + 8);
+        const int rl = hb + g, rh = hb + g + 8;
+        const unsigned a0 = *reinterpret_cast<const unsigned*>(Hs + swz(rl, 0) + 2 * t);
+        const unsigned a1 = *reinterpret_cast<const unsigned*>(Hs + swz(rh, 0) + 2 * t);
+        const unsigned a2 = *reinterpret_cast<const unsigned*>(Hs + swz(rl, 1) + 2 * t);
+        const unsigned a3 = *reinterpret_cast<const unsigned*>(Hs + swz(rh, 1) + 2 * t);
 #pragma unroll
         for (int j = 0; j < NT; ++j) mma_bf16(acc[r][j], a0, a1, a2, a3, b[j][0], b[j][1]);
       }
