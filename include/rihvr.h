@@ -358,7 +358,7 @@ int rihvr_adjoint_noalloc(const rihvr_params* params, int width, int height, con
 
 /* Learned warm start.  No counterpart in the reference: its reconstruction
  * always starts from x = 0 (sparse_compressive_holo.cu:273), which stays the
- * fallback and the judge.  A 3-D U-Net (3 levels, 16/32/64 channels, BF16
+ * fallback and the reference.  A 3-D U-Net (3 levels, 16/32/64 channels, BF16
  * tensor-core convolutions with FP32 accumulation, FP32 master weights) maps
  * the back-propagated volume xbp = t A^H b (t the initial step) to an initial
  * iterate x0 = g * alpha * xbp, g a per-voxel gain in (0, 1).  Volumes are

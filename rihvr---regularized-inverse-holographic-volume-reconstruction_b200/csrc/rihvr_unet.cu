@@ -1,7 +1,7 @@
 // Learned warm start: a 3-D U-Net that maps the back-propagated volume
 // t A^H b to an initial FISTA iterate.  No counterpart in the reference (its
 // reconstruction always starts from x = 0, sparse_compressive_holo.cu:273);
-// plain FISTA from zero stays the fallback and the judge of the result.
+// plain FISTA from zero stays the fallback and the reference for the result.
 //
 // Network (3 levels, 16/32/64 channels), activations FP32 channels-last
 // [z][y][x][c], weights FP32 masters with BF16 copies:

@@ -7,7 +7,7 @@ propagation, |1 + field|^2, camera noise, the reference's preprocessing).  For
 each one the library computes the back-propagated volume xbp = t A^H b and
 the plain-FISTA solution x* after the configured iterations; the network
 learns x0 = g * alpha * xbp against x*.  Evaluation runs plain FISTA from zero
-(the judge) and FISTA from the network's x0 on held-out holograms and counts
+(the reference run) and FISTA from the network's x0 on held-out holograms and counts
 the iterations each needs to come within 1e-3 (relative) of plain FISTA's
 final objective.
 

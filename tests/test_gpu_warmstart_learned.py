@@ -1,7 +1,7 @@
 """What the trained warm-start network gains: on held-out synthetic holograms
 (seeds outside the training set), FISTA started from the network's x0 reaches
 plain FISTA's 100-iteration objective (within 1e-3) in fewer iterations than
-plain FISTA from zero, which stays the judge.  Uses the committed weights
+plain FISTA from zero, which stays the reference.  Uses the committed weights
 (trained by ``warmstart.py train``)."""
 import os
 
