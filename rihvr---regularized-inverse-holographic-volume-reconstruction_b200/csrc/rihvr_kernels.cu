@@ -1227,9 +1227,9 @@ struct TvwShape {
   // Two warps per block.  Without the objective's norm terms and with the
   // 8-row ring (n_tv <= 5), the kernel fits 128 registers with at most a few
   // bytes of spill, and 8 blocks (16 warps) share an SM; the norm terms need
-  // about 165 registers, which caps them at 6 blocks (12 warps).  Blocks of 4
-  // warps at 3 per SM took 10.42 ms per launch at 1024 x 1024 x 1000 (n_tv = 5),
-  // 2-warp blocks at 16 per SM 9.5 ms.
+  // about 160 registers, which caps them at 6 blocks (12 warps).  At
+  // 1024 x 1024 x 1000 (n_tv = 5, no norm terms) a launch took 10.42 ms with
+  // 4-warp blocks at 12 warps per SM, 9.5 ms with 2-warp blocks at 16.
   static constexpr int NW = 2;
   static constexpr size_t SMEM = sizeof(float4) * (size_t)SLOT * D * NW;
   static_assert(CPL == 2 || CPL == 4, "columns per lane");
@@ -1237,8 +1237,9 @@ struct TvwShape {
 };
 
 // Blocks per SM the register allocation targets (__launch_bounds__).  At 7
-// two-warp blocks ptxas caps the kernel at 128 registers (8 blocks then fit);
-// asking for 8 gives the same cap with ten times the spill.
+// two-warp blocks ptxas caps the kernel at 128 registers (8 blocks then fit,
+// as registers are split per scheduler); asking for 8 gives the same cap with
+// ten times the spill.
 template <int NTV, bool NORMS>
 constexpr int tvw_minb() {
   return TvwShape<NTV, 2>::D == 8 ? (NORMS ? 6 : 7) : 4;
