@@ -37,6 +37,8 @@ def test_roofline_inputs():
     for s in (8, 4):
         cb = bench.class_bytes(s)
         assert cb["prox"] == 8 + 3 * s and cb["fwd_row"] == s + 8 and cb["fwd_col"] == 8
+        # as built: the minimal 32 + 4 s plus G written and read back (16 B)
+        assert sum(cb.values()) == 48 + 4 * s
     # the prox's measured DRAM traffic (the roofline's `traffic`) is within 10 %
     # above its algorithmic bytes; the FFT passes' 16-plane captures leave part
     # of their writes in L2, so only the prox is held to this
