@@ -1,12 +1,12 @@
 // Allocation-free variant of the adjoint operator (rihvr_adjoint_noalloc).
 //
-// Some callers cannot allocate device memory: code that runs while a CUDA
-// graph is being captured (allocation calls are not capturable), plugin hosts
-// that own every byte of device memory through their own pool, and real-time
-// pipelines that must not take the latency of cudaMalloc in the loop.  This
-// entry point needs no context and no allocation: the caller passes the input
-// residual and the output volume (device memory), and the scratch the adjoint
-// needs lives in one file-scope __device__ array of fixed size.
+// Some callers cannot allocate device memory: plugin hosts that hand out every
+// byte of device memory from their own pool and forbid other allocations, and
+// real-time pipelines that must not take the latency (and the implicit device
+// synchronisation) of cudaMalloc inside their loop.  This entry point needs no
+// context and no allocation: the caller passes the input residual and the
+// output volume (device memory), and the scratch the adjoint needs lives in one
+// file-scope __device__ array of fixed size.
 //
 // Limits: square planes of a supported side up to 1024 and at most 4096
 // planes.  The array takes 24 MiB + 32 KiB on every GPU that loads the library
@@ -17,7 +17,6 @@
 #include <cuda_runtime.h>
 
 #include <cmath>
-#include <mutex>
 #include <string>
 
 #include "../../include/rihvr.h"
@@ -38,9 +37,6 @@ constexpr size_t kTurnsOff = kInterOff + kMaxPlaneElems * sizeof(float2);
 constexpr size_t kZOff = kTurnsOff + kMaxPlaneElems * sizeof(double);
 constexpr size_t kScratchBytes = kZOff + (size_t)kMaxPlanes * sizeof(double);
 
-constexpr int kMaxDevices = 64;
-std::mutex g_setup_mutex;
-void* g_scratch_addr[kMaxDevices] = {};
 }  // namespace
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kScratchBytes];
@@ -70,23 +66,19 @@ int noalloc_fail(int code, const std::string& msg) {
   return code;
 }
 
-// Device address of the scratch array for the current device.  Looked up once
-// per device, with that device current: in host code the array's name is only
-// a host-side stand-in, never a device address.
+// Device address of the scratch array in the current device's context.  In
+// host code the array's name is only a host-side stand-in, never a device
+// address, so every call asks the runtime with the target device current.  The
+// lookup is a cheap host query; it is repeated on each call instead of cached
+// because the address belongs to a context: after cudaDeviceReset, or when a
+// host makes its own driver-API context current, the array lives elsewhere.
+// The first call in a context may also load the library's module there.
 int scratch_address(unsigned char** out) {
-  int dev = -1;
-  cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess) return noalloc_fail(RIHVR_ERR_NO_DEVICE, std::string("cudaGetDevice: ") + cudaGetErrorString(e));
-  if (dev < 0 || dev >= kMaxDevices) return noalloc_fail(RIHVR_ERR_NO_DEVICE, "device ordinal out of range");
-  std::lock_guard<std::mutex> lock(g_setup_mutex);
-  if (!g_scratch_addr[dev]) {
-    void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess || !p)
-      return noalloc_fail(RIHVR_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
-    g_scratch_addr[dev] = p;
-  }
-  *out = static_cast<unsigned char*>(g_scratch_addr[dev]);
+  void* p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+  if (e != cudaSuccess || !p)
+    return noalloc_fail(RIHVR_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+  *out = static_cast<unsigned char*>(p);
   return RIHVR_OK;
 }
 
