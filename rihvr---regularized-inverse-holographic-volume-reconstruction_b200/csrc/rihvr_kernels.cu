@@ -12,6 +12,7 @@
 // operator, the sum over z, so the Nz transformed planes never go back to memory.
 #include <cuda.h>  // CUtensorMap and its enums; the encoder is resolved at run time
 
+#include <atomic>
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
@@ -60,15 +61,21 @@ bool line_size_supported(int n) {
   }
 }
 
-static int g_num_sms = 0;
+// SM count of the current device, cached per device ordinal.  Worker threads of
+// a frame batch and callers on other host threads read it concurrently, so the
+// cache entries are atomics (a racing first fill writes the same value twice).
+constexpr int kSmCacheDevices = 64;
+static std::atomic<int> g_num_sms[kSmCacheDevices];
 static int num_sms() {
-  if (g_num_sms == 0) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
-    if (g_num_sms <= 0) g_num_sms = 148;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) dev = 0;
+  std::atomic<int>* slot = (dev >= 0 && dev < kSmCacheDevices) ? &g_num_sms[dev] : nullptr;
+  int n = slot ? slot->load(std::memory_order_relaxed) : 0;
+  if (n <= 0) {
+    if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) n = 148;
+    if (slot) slot->store(n, std::memory_order_relaxed);
   }
-  return g_num_sms;
+  return n;
 }
 
 template <typename K>
@@ -1772,6 +1779,51 @@ cudaError_t launch_finish_forward(const float2* c, const float* b, float* dnew, 
   const int blocks = flat_blocks((size_t)n);
   *nblocks_out = blocks;
   k_finish_forward<<<blocks, FLAT_THREADS, 0, st>>>(c, b, dnew, n, partials);
+  return cudaGetLastError();
+}
+
+// Counter-based uniform fill in [-1, 1) for both parts of a complex volume
+// (splitmix64 of the seed and the element index), so that a host model can
+// regenerate exactly the same start vector.
+__device__ __forceinline__ unsigned long long splitmix64(unsigned long long z) {
+  z += 0x9E3779B97F4A7C15ull;
+  z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+  z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+  return z ^ (z >> 31);
+}
+__device__ __forceinline__ float unit_from_bits(unsigned long long r) {
+  // top 24 bits -> [0, 1), then [-1, 1): exact in float
+  return (float)(r >> 40) * (1.0f / 16777216.0f) * 2.0f - 1.0f;
+}
+__global__ void __launch_bounds__(FLAT_THREADS) k_fill_uniform_c(float2* __restrict__ x, long long n,
+                                                                 unsigned long long seed) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const unsigned long long k = seed * 0x100000001B3ull + 2ull * (unsigned long long)i;
+    x[i] = make_float2(unit_from_bits(splitmix64(k)), unit_from_bits(splitmix64(k + 1)));
+  }
+}
+
+cudaError_t launch_fill_uniform_c(float2* x, long long n, unsigned long long seed, cudaStream_t st) {
+  k_fill_uniform_c<<<flat_blocks((size_t)n), FLAT_THREADS, 0, st>>>(x, n, seed);
+  return cudaGetLastError();
+}
+
+// sum x^2 over n floats in FP64 (the SUM_RR entry of the block partials)
+__global__ void __launch_bounds__(FLAT_THREADS) k_sumsq(const float* __restrict__ x, long long n, double* partials) {
+  double acc[kNumSums];
+#pragma unroll
+  for (int k = 0; k < kNumSums; ++k) acc[k] = 0.0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const double v = x[i];
+    acc[SUM_RR] += v * v;
+  }
+  block_write_sums<FLAT_THREADS>(acc, partials, blockIdx.x);
+}
+
+cudaError_t launch_sumsq(const float* x, long long n, double* partials, int* nblocks_out, cudaStream_t st) {
+  const int blocks = flat_blocks((size_t)n);
+  *nblocks_out = blocks;
+  k_sumsq<<<blocks, FLAT_THREADS, 0, st>>>(x, n, partials);
   return cudaGetLastError();
 }
 
