@@ -141,9 +141,20 @@ int rihvr_create(const rihvr_params* params, int width, int height, rihvr_ctx** 
 /* SparseCompressiveHolo::destroy (:137-146). */
 void rihvr_destroy(rihvr_ctx* ctx);
 
+/* Testing hook, no counterpart in the reference: once n more device or pinned
+ * host allocations of rihvr_create have succeeded, the next one fails as if
+ * memory were exhausted (RIHVR_ERR_OUT_OF_MEMORY), so that a test can walk
+ * every cleanup path of rihvr_create without exhausting a GPU.  n < 0 (the
+ * default) turns the injection off.  Process-wide; returns the previous
+ * setting. */
+int rihvr_debug_fail_allocations_after(int n);
+
 /* The measured hologram b (the preprocessed, padded Hologram passed to the
  * constructor and to inverseReconstruct): real, height x width floats.  Also
- * resets the iterate to x = 0. */
+ * resets the iterate to x = 0.  A hologram holding NaN or infinite samples is
+ * refused with RIHVR_ERR_INVALID_DATA and the context is left unchanged (the
+ * reference only prints a warning per bad sample, check_isnan_mdata,
+ * sparse_compressive_holo.cu:9-35, and goes on to a solve full of NaNs). */
 int rihvr_set_hologram(rihvr_ctx* ctx, const float* b, int is_device);
 
 /* SparseCompressiveHolo::inverseReconstruct(Hologram, mode) (:173-633): runs
@@ -247,6 +258,21 @@ int rihvr_sparsity(rihvr_ctx* ctx, double* fraction);
  * reference as estimate_initial.tif.  Leaves the solve reset to x = 0. */
 int rihvr_initial_estimate(rihvr_ctx* ctx, float* estimate_out, int is_device);
 
+/* Lipschitz constant of the data term's gradient, L = largest eigenvalue of
+ * A^H A, by an FP64 power iteration on the device: x_0 has seeded uniform
+ * entries in [-1, 1) (splitmix64 of seed * 0x100000001B3 + 2 i and + 2 i + 1
+ * for the real and imaginary parts of element i), each step forms A x_k and
+ * A^H A x_k with the solver's own operators, the norms are reduced in FP64,
+ * and *L_out receives the last Rayleigh quotient ||A x_k||^2 / ||x_k||^2
+ * (history, if not NULL, all `iterations` of them; they rise towards L).
+ * For this operator L = num_planes (reached by volumes constant over x, y and
+ * z), which is why the reference fixes the step at 1 / num_planes.  The
+ * reference's estimateLipschitz (sparse_compressive_holo.cu:2205-2464, called
+ * at :226-246) is a one-step estimate from two random volumes whose result
+ * the solve then discards (:247); as there, the value is reported and not
+ * used.  Needs a hologram; leaves the solve reset to x = 0. */
+int rihvr_lipschitz(rihvr_ctx* ctx, int iterations, unsigned long long seed, double* L_out, double* history);
+
 /* Operator entry points. */
 /* backPropagate (:1935-2077): d = Re(IFFT(sum_z H'_z FFT(x_z))), x complex
  * interleaved Nz x height x width, d height x width floats. */
@@ -340,9 +366,9 @@ int rihvr_segment_intensity(const float* intensity, int width, int height, int n
 int rihvr_write_centroids(const char* filename, const rihvr_object* objects, int n, int weighted, int verbose);
 
 /* Allocation-free adjoint.  No counterpart in the reference: for callers that
- * cannot allocate device memory - code running while a CUDA graph is captured,
- * plugin hosts that hand out all device memory from their own pool, real-time
- * loops that cannot take an allocation's latency.  Computes what rihvr_adjoint
+ * cannot allocate device memory - plugin hosts that hand out all device memory
+ * from their own pool and forbid other allocations, real-time loops that
+ * cannot take an allocation's latency and implicit synchronisation.  Computes what rihvr_adjoint
  * computes (g_z = IFFT(conj(H'_z) FFT(r)) for every plane) without a context:
  * `residual` (height x width floats) and `volume_out` (Nz x height x width
  * complex interleaved) are device memory owned by the caller; `stream` is a
@@ -350,9 +376,11 @@ int rihvr_write_centroids(const char* filename, const rihvr_object* objects, int
  * Scratch lives in one fixed 24 MiB + 32 KiB device array that every GPU
  * loading the library holds until exit: planes must be square with a supported
  * side of at most 1024 and num_planes at most 4096, otherwise
- * RIHVR_ERR_UNSUPPORTED_SIZE is returned.  The first call on a device looks the
- * array up (and may load the module), so make it before any stream capture.
- * Calls share the array and race if they overlap on the GPU; serialise them. */
+ * RIHVR_ERR_UNSUPPORTED_SIZE is returned.  Every call looks the array's device
+ * address up in the current context; the first call on a device (or in a new
+ * context) may also load the library's module there, so make that first call
+ * before any stream capture.  Calls share the array and race if they overlap
+ * on the GPU; serialise them. */
 int rihvr_adjoint_noalloc(const rihvr_params* params, int width, int height, const float* residual,
                           float* volume_out, void* stream);
 

@@ -25,6 +25,7 @@ ERR_INVALID_ARGUMENT = 7
 ERR_UNKNOWN_MODE = 6
 ERR_MISSING_DATA = 3
 ERR_INVALID_FILE = 9
+ERR_INVALID_DATA = 10
 ERR_BAD_FILENAME = 2
 ERR_OUT_OF_MEMORY = 5
 ERR_CUDA = 20
@@ -126,14 +127,14 @@ OBJECT_DTYPE = np.dtype([
 # every symbol include/rihvr.h declares
 EXPORTED = (
     "rihvr_params_default", "rihvr_read_param_file", "rihvr_plane_list", "rihvr_create", "rihvr_destroy",
-    "rihvr_set_hologram", "rihvr_reconstruct", "rihvr_reconstruct_batch", "rihvr_set_batch_mode",
+    "rihvr_debug_fail_allocations_after", "rihvr_set_hologram", "rihvr_reconstruct", "rihvr_reconstruct_batch", "rihvr_set_batch_mode",
     "rihvr_batch_last_combined", "rihvr_autotune", "rihvr_tuning", "rihvr_reset",
     "rihvr_set_initial_volume",
     "rihvr_iterate",
     "rihvr_iterate_timed",
     "rihvr_iteration_count", "rihvr_objective", "rihvr_get_iterations", "rihvr_get_plane", "rihvr_get_volume",
     "rihvr_get_estimate", "rihvr_get_residual", "rihvr_forward", "rihvr_adjoint", "rihvr_prox_step",
-    "rihvr_adjoint_noalloc", "rihvr_sparsity", "rihvr_initial_estimate",
+    "rihvr_adjoint_noalloc", "rihvr_sparsity", "rihvr_initial_estimate", "rihvr_lipschitz",
     "rihvr_read_image", "rihvr_write_tiff8", "rihvr_preprocess", "rihvr_io_error",
     "rihvr_segment_params_default", "rihvr_segment", "rihvr_segment_intensity", "rihvr_write_centroids",
     "rihvr_unet_create", "rihvr_unet_destroy", "rihvr_unet_param_count", "rihvr_unet_get_params",
@@ -174,6 +175,7 @@ def load_library(path: str = LIB_PATH):
     L.rihvr_plane_list.argtypes = [P(RihvrParams), P(ctypes.c_double)]
     L.rihvr_create.argtypes = [P(RihvrParams), ip, ip, P(vp)]
     L.rihvr_destroy.argtypes = [vp]
+    L.rihvr_debug_fail_allocations_after.argtypes = [ip]
     L.rihvr_destroy.restype = None
     L.rihvr_set_hologram.argtypes = [vp, vp, ip]
     L.rihvr_reconstruct.argtypes = [vp, P(ctypes.c_double)]
@@ -198,6 +200,7 @@ def load_library(path: str = LIB_PATH):
     L.rihvr_prox_step.argtypes = [vp, vp, vp, dp, vp, P(ctypes.c_double), ip]
     L.rihvr_adjoint_noalloc.argtypes = [P(RihvrParams), ip, ip, vp, vp, vp]
     L.rihvr_sparsity.argtypes = [vp, P(ctypes.c_double)]
+    L.rihvr_lipschitz.argtypes = [vp, ip, ctypes.c_ulonglong, P(ctypes.c_double), vp]
     L.rihvr_read_image.argtypes = [ctypes.c_char_p, vp, P(ctypes.c_int), P(ctypes.c_int), P(ctypes.c_int)]
     L.rihvr_write_tiff8.argtypes = [ctypes.c_char_p, vp, ip, ip]
     L.rihvr_preprocess.argtypes = [vp, ip, ip, vp, P(FileParams), ip, vp, P(ctypes.c_int), P(ctypes.c_int)]
@@ -606,6 +609,15 @@ class SparseCompressiveHolo:
         v = ctypes.c_double()
         _check(self._L.rihvr_sparsity(self._h, ctypes.byref(v)), "rihvr_sparsity")
         return v.value
+
+    def estimateLipschitz(self, iterations: int = 20, seed: int = 0):
+        """FP64 power iteration for the largest eigenvalue of A^H A:
+        (L, Rayleigh quotients of every step).  Resets the solve to x = 0."""
+        L = ctypes.c_double()
+        hist = np.zeros(int(iterations), np.float64)
+        _check(self._L.rihvr_lipschitz(self._h, int(iterations), int(seed), ctypes.byref(L),
+                                       hist.ctypes.data_as(ctypes.c_void_p)), "rihvr_lipschitz")
+        return L.value, hist
 
     def initialEstimate(self) -> np.ndarray:
         out = np.empty((self.height, self.width), np.float32)

@@ -192,6 +192,7 @@ struct rihvr_ctx {
   double* cturn = nullptr;
   double* zlist = nullptr;
   double* partials = nullptr;
+  unsigned* nonfinite_d = nullptr;  // count of non-finite hologram samples (rihvr_set_hologram)
   size_t partial_cap = 0;
   double* sums_d = nullptr;
   double* red_scratch = nullptr;
@@ -244,7 +245,24 @@ struct rihvr_ctx {
 
 namespace {
 
+// Allocation-failure injection for the cleanup tests (rihvr_debug_fail_allocations_after):
+// when >= 0, the number of device or pinned host allocations that still
+// succeed; the one after them fails as if the device were out of memory.
+std::atomic<int> g_alloc_budget{-1};
+
+bool injected_alloc_failure() {
+  int b = g_alloc_budget.load();
+  while (b >= 0) {
+    if (g_alloc_budget.compare_exchange_weak(b, b - 1)) return b == 0;
+  }
+  return false;
+}
+
 int dalloc(rihvr_ctx* c, void** p, size_t n) {
+  if (injected_alloc_failure()) {
+    *p = nullptr;
+    return fail(RIHVR_ERR_OUT_OF_MEMORY, "cudaMalloc of " + std::to_string(n) + " bytes failed (injected)");
+  }
   cudaError_t e = cudaMalloc(p, n);
   if (e != cudaSuccess) {
     *p = nullptr;
@@ -260,6 +278,28 @@ int dalloc(rihvr_ctx* c, void** p, size_t n) {
 template <typename T>
 int dalloc_t(rihvr_ctx* c, T** p, size_t count) {
   return dalloc(c, reinterpret_cast<void**>(p), sizeof(T) * count);
+}
+
+// pinned host memory; rihvr_destroy frees what is not NULL
+template <typename T>
+int halloc(T** p, size_t bytes) {
+  *p = nullptr;
+  if (injected_alloc_failure() || cudaMallocHost(reinterpret_cast<void**>(p), bytes) != cudaSuccess) {
+    cudaGetLastError();
+    *p = nullptr;
+    return fail(RIHVR_ERR_OUT_OF_MEMORY, "cudaMallocHost of " + std::to_string(bytes) + " bytes failed");
+  }
+  return RIHVR_OK;
+}
+
+// Non-finite samples of a device hologram: one atomic per warp that holds any.
+__global__ void k_count_nonfinite(const float* __restrict__ b, size_t n, unsigned* __restrict__ count) {
+  unsigned bad = 0;
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    bad += isfinite(b[i]) ? 0u : 1u;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) bad += __shfl_xor_sync(0xffffffffu, bad, o);
+  if ((threadIdx.x & 31) == 0 && bad) atomicAdd(count, bad);
 }
 
 int elem_kind(int storage) {
@@ -1025,6 +1065,8 @@ const char* rihvr_status_string(int s) {
   }
 }
 
+int rihvr_debug_fail_allocations_after(int n) { return g_alloc_budget.exchange(n < 0 ? -1 : n); }
+
 int rihvr_create(const rihvr_params* params, int width, int height, rihvr_ctx** out) {
   if (!out) return fail(RIHVR_ERR_INVALID_ARGUMENT, "out is NULL");
   *out = nullptr;
@@ -1081,16 +1123,14 @@ int rihvr_create(const rihvr_params* params, int width, int height, rihvr_ctx** 
   if (rc == RIHVR_OK) rc = dalloc_t(c, &c->partials, c->partial_cap * kNumSums);
   if (rc == RIHVR_OK) rc = dalloc_t(c, &c->sums_d, (size_t)kNumSums * NUM_SLOTS);
   if (rc == RIHVR_OK) rc = dalloc_t(c, &c->red_scratch, reduce_scratch_doubles());
+  if (rc == RIHVR_OK) rc = dalloc_t(c, &c->nonfinite_d, 1);
   if (rc != RIHVR_OK) return cleanup(rc);
-  if (cudaMallocHost(&c->sums_h, sizeof(double) * kNumSums * NUM_SLOTS) != cudaSuccess)
-    return cleanup(fail(RIHVR_ERR_OUT_OF_MEMORY, "cudaMallocHost failed"));
-  if (cudaMallocHost(&c->scal_h, 16 * sizeof(float)) != cudaSuccess)
-    return cleanup(fail(RIHVR_ERR_OUT_OF_MEMORY, "cudaMallocHost failed"));
+  if (halloc(&c->sums_h, sizeof(double) * kNumSums * NUM_SLOTS) != RIHVR_OK) return cleanup(RIHVR_ERR_OUT_OF_MEMORY);
+  if (halloc(&c->scal_h, 16 * sizeof(float)) != RIHVR_OK) return cleanup(RIHVR_ERR_OUT_OF_MEMORY);
   std::memset(c->scal_h, 0, 16 * sizeof(float));
   if (dalloc_t(c, &c->scal_d, 16) != RIHVR_OK) return cleanup(RIHVR_ERR_OUT_OF_MEMORY);
-  if (cudaMallocHost(&c->ctl_h, sizeof(IterCtl)) != cudaSuccess ||
-      cudaMallocHost(&c->dlog_h, sizeof(DevRec) * kDevLogCap) != cudaSuccess)
-    return cleanup(fail(RIHVR_ERR_OUT_OF_MEMORY, "cudaMallocHost failed"));
+  if (halloc(&c->ctl_h, sizeof(IterCtl)) != RIHVR_OK || halloc(&c->dlog_h, sizeof(DevRec) * kDevLogCap) != RIHVR_OK)
+    return cleanup(RIHVR_ERR_OUT_OF_MEMORY);
   if (dalloc_t(c, &c->ctl_d, 1) != RIHVR_OK || dalloc_t(c, &c->dlog_d, kDevLogCap) != RIHVR_OK)
     return cleanup(RIHVR_ERR_OUT_OF_MEMORY);
   std::vector<double> ct;
@@ -1122,6 +1162,24 @@ void rihvr_destroy(rihvr_ctx* c) {
 
 int rihvr_set_hologram(rihvr_ctx* c, const float* b, int is_device) {
   if (!c || !b) return fail(RIHVR_ERR_INVALID_ARGUMENT, "NULL argument");
+  // A NaN or infinite sample would poison every later iterate.  The reference
+  // only prints a warning per bad sample and carries on (check_isnan_mdata,
+  // sparse_compressive_holo.cu:9-35); here the hologram is refused with the
+  // reference's HOLO_ERROR_INVALID_DATA code and the context keeps its state.
+  size_t bad = 0;
+  if (!is_device) {
+    for (size_t i = 0; i < c->HW; ++i) bad += std::isfinite(b[i]) ? 0 : 1;
+  } else {
+    CK(cudaMemsetAsync(c->nonfinite_d, 0, sizeof(unsigned), c->st));
+    const int blocks = (int)std::min<size_t>((c->HW + 255) / 256, 1184);
+    KL((k_count_nonfinite<<<blocks, 256, 0, c->st>>>(b, c->HW, c->nonfinite_d), cudaGetLastError()));
+    unsigned n = 0;
+    CK(cudaMemcpyAsync(&n, c->nonfinite_d, sizeof(unsigned), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    bad = n;
+  }
+  if (bad)
+    return fail(RIHVR_ERR_INVALID_DATA, "hologram has " + std::to_string(bad) + " non-finite samples");
   RC(copy_in(c, c->b, b, sizeof(float) * c->HW, is_device));
   c->have_holo = true;
   RC(state_reset(c));
@@ -1565,6 +1623,47 @@ int rihvr_get_estimate(rihvr_ctx* c, float* out, int is_device) {
 int rihvr_get_residual(rihvr_ctx* c, float* out, int is_device) {
   if (!c || !out) return fail(RIHVR_ERR_INVALID_ARGUMENT, "NULL argument");
   return copy_out(c, out, c->r, sizeof(float) * c->HW, is_device);
+}
+
+int rihvr_lipschitz(rihvr_ctx* c, int iterations, unsigned long long seed, double* L_out, double* history) {
+  if (!c || !L_out) return fail(RIHVR_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (iterations < 1 || iterations > 100000) return fail(RIHVR_ERR_INVALID_ARGUMENT, "iterations must be 1..100000");
+  if (!c->have_holo) return fail(RIHVR_ERR_MISSING_DATA, "no hologram set");
+  // FP64 sum of squares of n floats on the device, read back
+  auto sumsq = [&](const float* x, long long n, double* out) -> int {
+    int nb = 0;
+    KL(launch_sumsq(x, n, c->partials, &nb, c->st));
+    RC(reduce_into(c, nb, SLOT_NORM));
+    RC(fetch_sums(c));
+    *out = c->sums_h[SLOT_NORM * kNumSums + SUM_RR];
+    return RIHVR_OK;
+  };
+  // x_0: seeded uniform entries in [-1, 1) for both parts, held in G
+  KL(launch_fill_uniform_c(c->G, (long long)c->V, seed, c->st));
+  double nx2 = 0;
+  RC(sumsq(reinterpret_cast<const float*>(c->G), 2LL * (long long)c->V, &nx2));
+  double L = 0;
+  for (int k = 0; k < iterations; ++k) {
+    // A x_k (dnew), its squared norm, and the Rayleigh quotient ||A x||^2 / ||x||^2
+    RC(forward_volume(c, ELEM_C32, c->G));
+    double ax2 = 0;
+    RC(sumsq(c->dnew, (long long)c->HW, &ax2));
+    L = ax2 / nx2;
+    if (history) history[k] = L;
+    // x_{k+1} = A^H A x_k / ||A^H A x_k||
+    CK(cudaMemcpyAsync(c->r, c->dnew, sizeof(float) * c->HW, cudaMemcpyDeviceToDevice, c->st));
+    RC(residual_spectrum(c));
+    RC(adjoint_volume(c));
+    double ny2 = 0;
+    RC(sumsq(reinterpret_cast<const float*>(c->G), 2LL * (long long)c->V, &ny2));
+    if (!(ny2 > 0)) break;
+    const float scale = (float)(1.0 / std::sqrt(ny2));
+    KL((k_scale_c<<<1184, 256, 0, c->st>>>(c->G, (long long)c->V, scale), cudaGetLastError()));
+    nx2 = ny2 * (double)scale * (double)scale;
+  }
+  *L_out = L;
+  // the operator passes overwrote the hologram-side buffers: restart from x = 0
+  return state_reset(c);
 }
 
 int rihvr_forward(rihvr_ctx* c, const float* volume, float* holo_out, int is_device) {
