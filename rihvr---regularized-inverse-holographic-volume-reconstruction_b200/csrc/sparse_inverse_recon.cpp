@@ -66,112 +66,123 @@ struct Planes {
   }
 };
 
+// cv::magnitude of a complex voxel, in float as OpenCV computes it
+inline float magnitude(std::complex<float> v) { return std::sqrt(v.real() * v.real() + v.imag() * v.imag()); }
+
+// cv::Mat::convertTo(CV_8U, 255) of a value already scaled to [0, 1]:
+// saturate_cast<uchar>, rounding half to even
+inline uint8_t u8_of_unit(float v) { return to_u8(v * 255.0f); }
+
+// The affine map (plane - lo) / (hi - lo) that the reference writes as a
+// cv::Mat expression, which OpenCV evaluates as convertTo(alpha, beta) with
+// alpha = 1 / (hi - lo) and beta = -lo * alpha, in float.
+struct UnitMap {
+  float alpha, beta;
+  UnitMap(double lo, double hi) {
+    const double a = 1.0 / (hi - lo);
+    alpha = (float)a;
+    beta = (float)(-lo * a);
+  }
+  float operator()(float v) const { return v * alpha + beta; }
+};
+
+// Global magnitude range over the planes (the first loop of savePlanes,
+// sparse_compressive_holo.cu:1045-1063, and of saveProjections,
+// sparse_volume.cu:708-726): one pass over the volume.
 bool magnitude_range(Planes& pl, double& lo, double& hi) {
   lo = hi = 0;
   for (int z = 0; z < pl.Nz; ++z) {
     const auto* p = pl.get(z);
     if (!p) return fail_msg(rihvr_last_error());
-    double a = 1e300, b = -1e300;
-    for (size_t i = 0; i < (size_t)pl.W * pl.H; ++i) {
-      const double m = std::abs(p[i]);
+    float a = magnitude(p[0]), b = a;
+    for (size_t i = 1; i < (size_t)pl.W * pl.H; ++i) {
+      const float m = magnitude(p[i]);
       a = std::min(a, m);
       b = std::max(b, m);
     }
     if (z == 0) { lo = a; hi = b; }
-    lo = std::min(lo, a);
-    hi = std::max(hi, b);
+    lo = std::min(lo, (double)a);
+    hi = std::max(hi, (double)b);
   }
   return true;
 }
 
-// SparseCompressiveHolo::savePlanes (sparse_compressive_holo.cu:1039-1194)
-bool save_planes(Planes& pl, const std::string& prefix) {
-  double gmin, gmax;
-  if (!magnitude_range(pl, gmin, gmax)) return false;
-  const size_t n = (size_t)pl.W * pl.H;
-  std::vector<uint8_t> px(n);
-  std::string err;
-  const double rmax = std::sqrt(gmax) / 10.0, rmin = -rmax;
-  char name[4096];
-  for (int z = 0; z < pl.Nz; ++z) {
-    const auto* p = pl.get(z);
-    if (!p) return fail_msg(rihvr_last_error());
-    for (size_t i = 0; i < n; ++i) px[i] = to_u8((std::abs(p[i]) - gmin) / (gmax - gmin) * 255.0);
-    std::snprintf(name, sizeof(name), "%s_%04d.tif", prefix.c_str(), z);
-    if (!rihvr_io::write_tiff8(name, px.data(), pl.W, pl.H, err)) return fail_msg(err);
-    for (size_t i = 0; i < n; ++i) {
-      double ph = std::atan2((double)p[i].imag(), (double)p[i].real());  // cv::phase: [0, 2 pi)
-      if (ph < 0) ph += 2.0 * M_PI;
-      px[i] = to_u8(ph / (2.0 * M_PI) * 255.0);
-    }
-    std::snprintf(name, sizeof(name), "%s_phase_%04d.tif", prefix.c_str(), z);
-    if (!rihvr_io::write_tiff8(name, px.data(), pl.W, pl.H, err)) return fail_msg(err);
-    for (size_t i = 0; i < n; ++i) px[i] = to_u8((p[i].real() - rmin) / (rmax - rmin) * 255.0);
-    std::snprintf(name, sizeof(name), "%s_real_%04d.tif", prefix.c_str(), z);
-    if (!rihvr_io::write_tiff8(name, px.data(), pl.W, pl.H, err)) return fail_msg(err);
-    for (size_t i = 0; i < n; ++i) px[i] = to_u8((p[i].imag() - rmin) / (rmax - rmin) * 255.0);
-    std::snprintf(name, sizeof(name), "%s_imag_%04d.tif", prefix.c_str(), z);
-    if (!rihvr_io::write_tiff8(name, px.data(), pl.W, pl.H, err)) return fail_msg(err);
-  }
-  return true;
-}
-
-// SparseVolume::saveProjections, MAX_CMB (sparse_volume.cu:684-813).  The
-// reference starts the XY projection from zeros and folds in planes z > 0 only.
-bool save_projections(Planes& pl, const std::string& output_path, const std::string& prefix) {
+// The reference's three volume writers in one further pass over the planes:
+// * SparseCompressiveHolo::savePlanes (sparse_compressive_holo.cu:1039-1194):
+//   prefix_XXXX.tif magnitude over the global range, prefix_phase_XXXX.tif
+//   phase in [0, 2 pi) over 2 pi, prefix_real/imag_XXXX.tif over
+//   +-sqrt(global max) / 10 (when planes_prefix is not empty);
+// * SparseVolume::saveProjections, MAX_CMB (sparse_volume.cu:684-813):
+//   cmb_xy/xz/yz.tif maxima of the scaled magnitude; the XY projection starts
+//   from zeros and folds in planes z > 0 only, as the reference does;
+// * SparseVolume::saveData (sparse_volume.cu:518-560): inverse_voxels.csv,
+//   the non-zero voxels with their intensity, plane by plane in raster order.
+bool save_volume_outputs(Planes& pl, const std::string& planes_prefix, const std::string& output_path,
+                         const std::string& cmb_prefix, const std::string& sparse_prefix) {
   double gmin, gmax;
   if (!magnitude_range(pl, gmin, gmax)) return false;
   const int W = pl.W, H = pl.H, Z = pl.Nz;
-  std::vector<float> xy((size_t)W * H, 0.f), xz((size_t)Z * W, 0.f), yz((size_t)H * Z, 0.f);
+  const size_t n = (size_t)W * H;
+  const UnitMap mag_map(gmin, gmax);
+  const double rmax = std::sqrt(gmax) / 10.0;
+  const UnitMap ri_map(-rmax, rmax);
+  std::vector<uint8_t> px(n);
+  std::vector<float> xy(n, 0.f), xz((size_t)Z * W, 0.f), yz((size_t)H * Z, 0.f), colmax(W);
+  std::string err;
+  char name[4096];
+  const std::string csv = output_path + "/" + sparse_prefix + ".csv";
+  FILE* f = std::fopen(csv.c_str(), "w");
+  if (!f) return fail_msg("Unable to open file: " + csv);
+  std::fprintf(f, "x, y, z, value\n");
+  auto bail = [&](const std::string& m) {
+    std::fclose(f);
+    return fail_msg(m);
+  };
   for (int z = 0; z < Z; ++z) {
     const auto* p = pl.get(z);
-    if (!p) return fail_msg(rihvr_last_error());
-    std::vector<float> colmax(W, -1e30f);
+    if (!p) return bail(rihvr_last_error());
+    if (!planes_prefix.empty()) {
+      for (size_t i = 0; i < n; ++i) px[i] = u8_of_unit(mag_map(magnitude(p[i])));
+      std::snprintf(name, sizeof(name), "%s_%04d.tif", planes_prefix.c_str(), z);
+      if (!rihvr_io::write_tiff8(name, px.data(), W, H, err)) return bail(err);
+      for (size_t i = 0; i < n; ++i) {
+        float ph = std::atan2(p[i].imag(), p[i].real());  // cv::phase: [0, 2 pi)
+        if (ph < 0) ph += (float)(2.0 * M_PI);
+        px[i] = u8_of_unit(ph * (float)(1.0 / (2.0 * M_PI)));
+      }
+      std::snprintf(name, sizeof(name), "%s_phase_%04d.tif", planes_prefix.c_str(), z);
+      if (!rihvr_io::write_tiff8(name, px.data(), W, H, err)) return bail(err);
+      for (size_t i = 0; i < n; ++i) px[i] = u8_of_unit(ri_map(p[i].real()));
+      std::snprintf(name, sizeof(name), "%s_real_%04d.tif", planes_prefix.c_str(), z);
+      if (!rihvr_io::write_tiff8(name, px.data(), W, H, err)) return bail(err);
+      for (size_t i = 0; i < n; ++i) px[i] = u8_of_unit(ri_map(p[i].imag()));
+      std::snprintf(name, sizeof(name), "%s_imag_%04d.tif", planes_prefix.c_str(), z);
+      if (!rihvr_io::write_tiff8(name, px.data(), W, H, err)) return bail(err);
+    }
+    std::fill(colmax.begin(), colmax.end(), -1e30f);
     for (int y = 0; y < H; ++y) {
       float rowmax = -1e30f;
       for (int x = 0; x < W; ++x) {
-        const float v = (float)((std::abs(p[(size_t)y * W + x]) - gmin) / (gmax - gmin));
-        rowmax = std::max(rowmax, v);
-        colmax[x] = std::max(colmax[x], v);
-        if (z > 0) xy[(size_t)y * W + x] = std::max(xy[(size_t)y * W + x], v);
+        const std::complex<float> v = p[(size_t)y * W + x];
+        const float s = mag_map(magnitude(v));
+        rowmax = std::max(rowmax, s);
+        colmax[x] = std::max(colmax[x], s);
+        if (z > 0) xy[(size_t)y * W + x] = std::max(xy[(size_t)y * W + x], s);
+        if (v.real() != 0.f || v.imag() != 0.f)
+          std::fprintf(f, "%d, %d, %d, %e\n", x, y, z, v.real() * v.real() + v.imag() * v.imag());
       }
       yz[(size_t)y * Z + z] = rowmax;
     }
     for (int x = 0; x < W; ++x) xz[(size_t)z * W + x] = colmax[x];
   }
+  std::fclose(f);
   auto put = [&](const std::vector<float>& v, int w, int h, const std::string& tag) {
-    std::vector<uint8_t> px(v.size());
-    for (size_t i = 0; i < v.size(); ++i) px[i] = to_u8(v[i] * 255.0);
-    std::string err;
-    const std::string name = output_path + prefix + "_" + tag + ".tif";  // no separator, as the reference
-    return rihvr_io::write_tiff8(name, px.data(), w, h, err) || fail_msg(err);
+    std::vector<uint8_t> q(v.size());
+    for (size_t i = 0; i < v.size(); ++i) q[i] = u8_of_unit(v[i]);
+    const std::string file = output_path + cmb_prefix + "_" + tag + ".tif";  // no separator, as the reference
+    return rihvr_io::write_tiff8(file, q.data(), w, h, err) || fail_msg(err);
   };
   return put(xy, W, H, "xy") && put(xz, W, Z, "xz") && put(yz, Z, H, "yz");
-}
-
-// SparseVolume::saveData (sparse_volume.cu:518-560): non-zero voxels with
-// their intensity, plane by plane (raster order within a plane).
-bool save_sparse(Planes& pl, const std::string& output_path, const std::string& prefix) {
-  const std::string name = output_path + "/" + prefix + ".csv";
-  FILE* f = std::fopen(name.c_str(), "w");
-  if (!f) return fail_msg("Unable to open file: " + name);
-  std::fprintf(f, "x, y, z, value\n");
-  for (int z = 0; z < pl.Nz; ++z) {
-    const auto* p = pl.get(z);
-    if (!p) {
-      std::fclose(f);
-      return fail_msg(rihvr_last_error());
-    }
-    for (int y = 0; y < pl.H; ++y)
-      for (int x = 0; x < pl.W; ++x) {
-        const std::complex<float> v = p[(size_t)y * pl.W + x];
-        if (v.real() == 0.f && v.imag() == 0.f) continue;
-        const float intensity = v.real() * v.real() + v.imag() * v.imag();
-        std::fprintf(f, "%d, %d, %d, %e\n", x, y, z, intensity);
-      }
-  }
-  std::fclose(f);
-  return true;
 }
 
 // SparseSegmentation + ObjectCloud::blobSizeFilter + writeCentroids
@@ -266,23 +277,35 @@ int run(int argc, char** argv) {
   FILE* metrics = std::fopen((out + "/all_metrics.csv").c_str(), "a");
   if (!metrics) return fail_msg("Unable to open file: " + out + "/all_metrics.csv"), done(-1);
   std::fprintf(metrics, "it, f, sparsity, stepsize, total_backtracks\n");
-  int total_bt = 0;
-  for (int it = 0; it < p.num_inverse_iterations; ++it) {
-    if (rihvr_iterate(ctx, 1) != RIHVR_OK) {
+  // Without per-step outputs the iterations run in one call, which keeps them
+  // on the device (one host synchronisation per 256 iterations) and reads the
+  // log once at the end.  With output_steps the reference writes the sparsity
+  // of every iterate (:586-589), which needs the volume after each iteration.
+  const int n_iter = p.num_inverse_iterations;
+  std::vector<rihvr_iter_record> recs((size_t)std::max(n_iter, 1));
+  std::vector<double> sparsity((size_t)std::max(n_iter, 1), 0.0);
+  for (int it = 0; it < n_iter;) {
+    const int step = files.output_steps ? 1 : n_iter;
+    if (rihvr_iterate(ctx, step) != RIHVR_OK) {
       std::fclose(metrics);
       return fail_msg(rihvr_last_error()), done(-1);
     }
-    std::vector<rihvr_iter_record> recs(it + 1);
-    int n = 0;
-    rihvr_get_iterations(ctx, recs.data(), it + 1, &n);
-    const rihvr_iter_record& r = recs[it];
+    it += step;
+    if (files.output_steps) rihvr_sparsity(ctx, &sparsity[(size_t)it - 1]);
+  }
+  int n_rec = 0;
+  if (rihvr_get_iterations(ctx, recs.data(), n_iter, &n_rec) != RIHVR_OK) {
+    std::fclose(metrics);
+    return fail_msg(rihvr_last_error()), done(-1);
+  }
+  int total_bt = 0;
+  for (int it = 0; it < n_rec; ++it) {
+    const rihvr_iter_record& r = recs[(size_t)it];
     total_bt += r.backtracks;
-    double sparsity = 0;
-    if (files.output_steps) rihvr_sparsity(ctx, &sparsity);
-    std::printf("FASTA iteration %d of %d: new f = %e, backtracks %d, stepsize %g%s\n", it + 1,
-                p.num_inverse_iterations, r.f_x, total_bt, r.t, r.restarted ? ", restarted" : "");
+    std::printf("FASTA iteration %d of %d: new f = %e, backtracks %d, stepsize %g%s\n", it + 1, n_iter, r.f_x,
+                total_bt, r.t, r.restarted ? ", restarted" : "");
     if (files.output_steps)
-      std::fprintf(metrics, "%d, %f, %f, %f, %d\n", it, r.f_x, sparsity, r.t, total_bt);
+      std::fprintf(metrics, "%d, %f, %f, %f, %d\n", it, r.f_x, sparsity[(size_t)it], r.t, total_bt);
   }
   std::fclose(metrics);
   const auto mm = std::minmax_element(b.begin(), b.end());
@@ -292,18 +315,17 @@ int run(int argc, char** argv) {
   write_scaled(out + "/residual_final.tif", res, W, H, *mm.first, *mm.second);
 
   Planes pl{ctx, W, H, p.num_planes, {}};
+  std::string planes_prefix;
   if (files.output_planes) {
-    std::string prefix = out + "/inverse";
+    planes_prefix = out + "/inverse";
     if (subfolder) {
       char sub[4096];
       std::snprintf(sub, sizeof(sub), "%s/%04d/", out.c_str(), files.start_image);
       mkdir(sub, 0755);
-      prefix = std::string(sub) + "inverse";
+      planes_prefix = std::string(sub) + "inverse";
     }
-    if (!save_planes(pl, prefix)) return done(-1);
   }
-  if (!save_projections(pl, out, "cmb")) return done(-1);
-  if (!save_sparse(pl, out, "inverse_voxels")) return done(-1);
+  if (!save_volume_outputs(pl, planes_prefix, out, "cmb", "inverse_voxels")) return done(-1);
   if (segment && !segment_and_save(ctx, files, out)) return done(-1);
   std::printf("Done.\n");
   return done(0);

@@ -158,3 +158,51 @@ def test_cli_segmentation(rihvr, synthmod, tmp_path):
     for n, (wt, vb) in zip(names, ((0, 0), (1, 0), (0, 1))):
         rihvr.write_centroids(str(orc_dir / n), ref.astype(rihvr.OBJECT_DTYPE), weighted=wt, verbose=vb)
         assert (orc_dir / n).read_text() == (seg_out / n).read_text(), n
+
+
+def _circular_u8_diff(a, b):
+    d = np.abs(a.astype(np.int16) - b.astype(np.int16))
+    return np.minimum(d, 256 - d)
+
+
+def test_cli_images_match_the_reference_scaling(rihvr, synthmod, tmp_path):
+    """The 8-bit plane images (inverse_XXXX, _phase_, _real_, _imag_) and the
+    max projections (cmb_xy/xz/yz) the driver writes, against the restatement
+    of savePlanes and saveProjections (oracle/outputs.py) on the same volume.
+    OpenCV's own magnitude and phase (a fast arctangent) feed the restatement;
+    the driver uses sqrt and atan2 in float, so a pixel may sit one level away
+    where a value falls within rounding of a level boundary."""
+    import outputs as OUT
+
+    cfg = synthmod.small_config(W=64, H=64, Nz=6, seed=11, zero_padding=0)
+    img, _ = synthmod.make_hologram(cfg, cache_dir=str(tmp_path / "cache"))
+    frame = tmp_path / "holo_0007.tif"
+    assert cv2.imwrite(str(frame), img)
+    out = tmp_path / "out"
+    out.mkdir()
+    param = tmp_path / "run.param"
+    _write_param(param, f"{tmp_path}/holo_%04d.tif", out, cfg, 12)
+    param.write_text(param.read_text().replace("output_planes 7001 false", "output_planes 7001 true"))
+    r = subprocess.run([rihvr.CLI_PATH, "-F", str(param)], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stdout + r.stderr
+    p, _ = rihvr.read_param_file(str(param))
+    raw, _ = rihvr.read_image(str(frame))
+    with rihvr.SparseCompressiveHolo(p, 64, 64) as s:
+        s.setHologram(rihvr.preprocess(raw, p.zero_padding))
+        s.iterate(12)
+        X = s.getVolume()
+    assert np.count_nonzero(X) > 0
+    planes = OUT.save_planes(X)
+    for kind, tag in (("mag", ""), ("phase", "_phase"), ("real", "_real"), ("imag", "_imag")):
+        got = np.stack([cv2.imread(str(out / f"inverse{tag}_{z:04d}.tif"), cv2.IMREAD_UNCHANGED)
+                        for z in range(cfg.num_planes)])
+        d = _circular_u8_diff(got, planes[kind]) if kind == "phase" else np.abs(
+            got.astype(np.int16) - planes[kind].astype(np.int16))
+        assert d.max() <= 1, (kind, int(d.max()))
+        assert np.mean(d != 0) < 2e-3, (kind, float(np.mean(d != 0)))
+    proj = OUT.save_projections(X)
+    for tag in ("xy", "xz", "yz"):
+        got = cv2.imread(str(out / f"cmb_{tag}.tif"), cv2.IMREAD_UNCHANGED)
+        assert got.shape == proj[tag].shape
+        d = np.abs(got.astype(np.int16) - proj[tag].astype(np.int16))
+        assert d.max() <= 1 and np.mean(d != 0) < 2e-3, (tag, int(d.max()))
