@@ -164,7 +164,8 @@ def time_to_objective(rihvr, cfg, b, s, storage, stream, hb, tol=1e-3):
     p = rihvr.params_from_config(cfg, record_objective=1, storage=storage)
     with rihvr.SparseCompressiveHolo(p, cfg.W, cfg.H) as t:
         t.setHologram(b)
-        t.iterate(len(g["f_x"]))
+        t.iterate(1)  # first iteration runs eagerly (tables, graph capture)
+        rec_ms = t.iterate_timed(len(g["f_x"]) - 1)  # the library default: objective at every iteration
         fx = np.asarray(t.iterations()["f_x"], np.float64)
     gx = np.asarray(g["f_x"], np.float64)
     band = tol * abs(target)
@@ -172,6 +173,7 @@ def time_to_objective(rihvr, cfg, b, s, storage, stream, hb, tol=1e-3):
     ohits = np.nonzero(np.abs(gx - target) <= band)[0]
     out = {"unit": "s", "target_objective": target, "tolerance": tol, "oracle_iterations": int(ohits[0]) + 1,
            "oracle_seconds_100_iterations": g.get("oracle_seconds"), "oracle_threads": g.get("oracle_threads"),
+           "ms_per_iteration_recording_objective": rec_ms / (len(g["f_x"]) - 1),
            "max_rel_gap_to_oracle_trajectory": float(np.max(np.abs(fx - gx) / np.abs(gx))),
            "final_rel_gap": float((fx[-1] - target) / abs(target))}
     if not len(hits):
@@ -195,17 +197,20 @@ def time_to_objective(rihvr, cfg, b, s, storage, stream, hb, tol=1e-3):
     return out
 
 
-def cpu_sample(cfg, b, steps: int, warmup: int, planes: int = 16):
+CPU_SAMPLE_PLANES = 192  # about 5 s of FP64 oracle work per FISTA iteration on a 16-core host
+
+
+def cpu_sample(cfg, b, steps: int, warmup: int, planes: int = CPU_SAMPLE_PLANES):
     """Time the FP64 oracle on a bounded sample of the workload: the first
     `planes` planes of the volume, full plane size, one FISTA iteration per
-    step."""
+    step.  Parameters come from the workload description alone (float plane
+    list, lambda, dx and weights as the reference stores them), so this leg
+    never loads the product library."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
 
-    rihvr = importlib.import_module(PKG)
-    p = rihvr.params_from_config(cfg)
     nz = min(planes, cfg.num_planes)
-    z = rihvr.plane_list(p)[:nz]
+    z = cfg.plane_list()[:nz]
     op = O.OracleParams(W=cfg.W, H=cfg.H, z=z, dx=cfg.dx(), lam=cfg.lam(), l1=cfg.l1(), tv=cfg.tv(),
                         n_tv=cfg.num_tv_iterations, mode=7, faithful=1)
     b64 = b.astype(np.float64)
@@ -221,6 +226,39 @@ def cpu_sample(cfg, b, steps: int, warmup: int, planes: int = 16):
                       f"per step, {steps} steps ({dt:.1f} s)"}
 
 
+def cufft_comparator(cfg, ktimes, reps: int = 5):
+    """cuFFT (torch.fft) on the same planes as the forward operator's FFT
+    passes: a batched FP32 complex 2-D FFT of the Nz planes, out of place,
+    timed with CUDA events.  Beside it the hand-written forward row and column
+    passes per launch (which also apply the transfer function and sum over z)."""
+    import torch
+
+    dev = torch.device("cuda", torch.cuda.current_device())
+    x = torch.randn((cfg.num_planes, cfg.H, cfg.W), dtype=torch.complex64, device=dev)
+    y = torch.empty_like(x)
+    torch.fft.fft2(x, out=y)  # plan creation
+    torch.cuda.synchronize()
+    st = torch.cuda.current_stream(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(reps):
+        torch.fft.fft2(x, out=y)
+    e1.record(st)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    del x, y
+    torch.cuda.empty_cache()
+    ours = None
+    if "fwd_row" in ktimes and "fwd_col" in ktimes:
+        ours = sum(ktimes[k][0] / max(ktimes[k][1], 1) for k in ("fwd_row", "fwd_col"))
+    V = cfg.voxels()
+    return {"what": "torch.fft.fft2 (cuFFT) of the Nz planes, complex64, out of place",
+            "cufft_ms": ms, "cufft_voxels_per_s": V / (ms / 1e3),
+            "ours_forward_row_plus_column_ms": ours,
+            "ours_over_cufft": (ms / ours) if ours else None,
+            "note": "the hand-written passes also multiply by the transfer function and sum over z"}
+
+
 def run_reference(args):
     ws, rank, _ = dist_env()
     if rank != 0:
@@ -228,6 +266,8 @@ def run_reference(args):
     cfg = workload(args.config)
     synth = importlib.import_module(PKG + ".synth")
     _, b = synth.make_hologram(cfg)
+    # the reference's own path is CUDA-only (it needs OpenCV C++, absent here);
+    # its CPU stand-in is the FP64 oracle on the same sample as cpu_baseline
     cb = cpu_sample(cfg, b, args.steps, args.warmup)
     line = {"metric": METRIC, "value": cb["value"], "unit": "voxel-iters/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "impl": "reference",
@@ -239,50 +279,68 @@ def run_reference(args):
 
 
 def run_frames(args):
-    """Batched time series (config 3 shapes): frames of uneven size and plane
-    count, reconstructed frame after frame and then all at once with
-    rihvr_reconstruct_batch on the same contexts.  Prints one JSON line."""
+    """Batched time series (the uneven-series workload): `--frames` frames
+    (default 64) of an advected tracer population (synth.series_frames: H and W
+    from {512, 640, 768, 1024}, Nz 100-400, 200-3000 tracers, a seeded
+    divergence-free velocity field between frames), `--steps` FISTA iterations
+    each.  Frames run in waves whose contexts fit in device memory; each wave
+    is reconstructed frame after frame and then all at once with
+    rihvr_reconstruct_batch on the same contexts (graphs captured by an
+    untimed warm-up call).  Prints one JSON line."""
     import torch
 
     torch.cuda.set_device(0)
     rihvr = importlib.import_module(PKG)
     synth = importlib.import_module(PKG + ".synth")
-    rng = np.random.default_rng(3)
-    n = args.frames
-    cfgs = []
-    for i in range(n):
-        side = int(rng.choice([512, 640, 768, 1024]))
-        cfgs.append(synth.HoloConfig(
-            name=f"series_frame{i}", width=side, height=side, zero_padding=0,
-            num_planes=int(rng.integers(100, 401)), start_plane=2500.0, plane_stepsize=2.0, resolution=1.1,
-            wavelength=0.632, regularization_param=0.15, regularization_TV_param=0.1,
-            num_inverse_iterations=args.steps, num_tv_iterations=5, n_disks=int(rng.integers(200, 3001)),
-            disk_radius=(1.0, 4.0), noise_sigma=0.02, seed=100 + i))
-    holos = [synth.make_hologram(c)[1] for c in cfgs]
-    solvers = [rihvr.SparseCompressiveHolo(rihvr.params_from_config(c, record_objective=0), c.W, c.H)
-               for c in cfgs]
+    n = args.frames if args.frames else 64
+    cfgs = synth.series_frames(n, iterations=args.steps)
+    t_gen = time.perf_counter()
+    holos = [synth.make_hologram(c, device="cuda")[1] for c in cfgs]
+    t_gen = time.perf_counter() - t_gen
+    torch.cuda.empty_cache()
+    budget = 0.75 * torch.cuda.mem_get_info()[0]
     vox = sum(c.voxels() for c in cfgs) * args.steps
-    try:
-        rihvr.reconstruct_batch(solvers, holos)  # warm-up: module load, first launches
-        torch.cuda.synchronize()
-        t0 = time.perf_counter()
-        seq = [s.inverseReconstruct(b) for s, b in zip(solvers, holos)]
-        torch.cuda.synchronize()
-        t_seq = time.perf_counter() - t0
-        t0 = time.perf_counter()
-        bat = rihvr.reconstruct_batch(solvers, holos)
-        torch.cuda.synchronize()
-        t_bat = time.perf_counter() - t0
-    finally:
-        for s in solvers:
-            s.destroy()
-    line = {"metric": "frames reconstructed per second (uneven time series)", "value": n / t_bat, "unit": "frames/s",
-            "higher_is_better": True, "n_gpus": 1, "steps": args.steps, "data": "synthetic",
-            "config": {"workload": "uneven_series", "frames": [[c.W, c.H, c.num_planes] for c in cfgs],
-                       "fista_iterations": args.steps, "tv_iterations": 5},
+    t_seq = t_bat = 0.0
+    waves, seq_obj, bat_obj = [], [], []
+    i = 0
+    while i < n:
+        wave, bytes_ = [], 0
+        while i < n:
+            need = 44 * cfgs[i].voxels() + (256 << 20)  # FP32 volumes, gradient, intermediate, planes
+            if wave and bytes_ + need > budget:
+                break
+            wave.append(i)
+            bytes_ += need
+            i += 1
+        solvers = [rihvr.SparseCompressiveHolo(rihvr.params_from_config(cfgs[j], record_objective=0),
+                                               cfgs[j].W, cfgs[j].H) for j in wave]
+        hs = [holos[j] for j in wave]
+        try:
+            rihvr.reconstruct_batch(solvers, hs)  # warm-up: first launches and graph capture
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            seq = [s_.inverseReconstruct(b_) for s_, b_ in zip(solvers, hs)]
+            torch.cuda.synchronize()
+            t_seq += time.perf_counter() - t0
+            t0 = time.perf_counter()
+            bat = rihvr.reconstruct_batch(solvers, hs)
+            torch.cuda.synchronize()
+            t_bat += time.perf_counter() - t0
+        finally:
+            for s_ in solvers:
+                s_.destroy()
+        waves.append(len(wave))
+        seq_obj += list(seq)
+        bat_obj += list(bat)
+    line = {"metric": "frames reconstructed per second (uneven advected-tracer time series)", "value": n / t_bat,
+            "unit": "frames/s", "higher_is_better": True, "n_gpus": 1, "steps": args.steps, "data": "synthetic",
+            "config": {"workload": f"uneven_series_{n}_frames",
+                       "frames": [[c.W, c.H, c.num_planes, c.n_disks] for c in cfgs],
+                       "fista_iterations": args.steps, "tv_iterations": 5, "waves": waves},
             "batched_s": t_bat, "sequential_s": t_seq, "speedup": t_seq / t_bat,
             "voxel_iters_per_s_batched": vox / t_bat, "voxel_iters_per_s_sequential": vox / t_seq,
-            "objectives_equal": bool(np.array_equal(np.asarray(seq), np.asarray(bat)))}
+            "objectives_equal": bool(np.array_equal(np.asarray(seq_obj), np.asarray(bat_obj))),
+            "hologram_generation_s": t_gen}
     print(json.dumps(line), flush=True)
     return 0
 
@@ -370,7 +428,7 @@ def run_warmstart(args):
     torch.cuda.set_device(0)
     rihvr = importlib.import_module(PKG)
     ws = importlib.import_module(PKG + ".warmstart")
-    seeds = np.arange(300_000, 300_000 + args.frames)
+    seeds = np.arange(300_000, 300_000 + (args.frames if args.frames else 16))
     with rihvr.UNet(ws.PLANES, ws.SIZE, ws.SIZE) as net:
         net.load(ws.WEIGHTS)
         rows = ws.evaluate(net, seeds)
@@ -482,6 +540,8 @@ def run_ours(args):
            "h2d_bytes_per_step": int(b.nbytes) / args.steps, "d2h_bytes_per_step": (int(hout.numel() * 4) + 8) / args.steps,
            "ms": e2e_ms, "what": "set_hologram (H2D from pinned) + K iterations + estimate and objective (D2H)"}
 
+    cufft = cufft_comparator(cfg, ktimes) if ws == 1 else None
+
     tto = None
     if ws == 1 and not args.nz and args.config == "c2" and args.time_to_objective:
         tto = time_to_objective(rihvr, cfg, b, s, storage, stream, hb)
@@ -506,8 +566,8 @@ def run_ours(args):
     if rank == 0:
         cpu = None
         if ws == 1 and not args.no_cpu_baseline:
-            # 192 planes: about 10 s of oracle work on a 16-core host
-            cpu = cpu_sample(cfg, b, steps=2, warmup=1, planes=192)
+            # the same sample as the reference arm: about 10 s of oracle work on a 16-core host
+            cpu = cpu_sample(cfg, b, steps=2, warmup=1)
         line = {
             "metric": METRIC, "value": value, "unit": "voxel-iters/s", "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": max_ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -518,6 +578,7 @@ def run_ours(args):
                        "l2": "inputs larger than L2 (volumes of %.1f GB each)" % (V * sbytes / 1e9),
                        "record_objective": False, "autotune": bool(args.autotune), "launch_shapes": tuning},
             "e2e": e2e, "time_to_objective": tto, "roofline": roofline, "cpu_baseline": cpu,
+            "cufft_comparator": cufft,
             "iteration_roofline": {"bytes_per_voxel_iter": 32 + 4 * sbytes,
                                    "achieved": iter_bytes * args.steps / (max_ms / 1e3) / 1e9, "peak": peak,
                                    "frac": iter_bytes * args.steps / (max_ms / 1e3) / 1e9 / peak},
@@ -540,7 +601,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c2", choices=["c2", "c1", "c5", "series", "segment", "warmstart"])
-    ap.add_argument("--frames", type=int, default=8, help="frames of the uneven series (--config series)")
+    ap.add_argument("--frames", type=int, default=0,
+                    help="frames of the uneven series (--config series, default 64) or of the warm-start set (default 16)")
     ap.add_argument("--storage", default="f32", choices=["f32", "bf16", "f16"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--nz", type=int, default=0, help="override the plane count (profiling cases)")

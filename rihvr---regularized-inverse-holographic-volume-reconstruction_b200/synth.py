@@ -56,6 +56,11 @@ class HoloConfig:
     rod_width: float = 2.0
     noise_sigma: float = 0.01
     seed: int = 0
+    # frame of an advected tracer series (series_frames): when series_seed >= 0
+    # the disks are the first n_disks tracers of that series at frame
+    # series_frame, instead of independent random disks
+    series_seed: int = -1
+    series_frame: int = 0
 
     @property
     def W(self) -> int:
@@ -156,6 +161,79 @@ def _stamp_disk(plane: np.ndarray, cx: float, cy: float, r: float) -> None:
     plane[np.ix_(yy, xx)] = np.maximum(sub, m.astype(plane.dtype))
 
 
+# ---------------------------------------------------------------------------
+# advected tracer series (the batched time-series workload)
+# ---------------------------------------------------------------------------
+SERIES_TRACERS = 3000   # tracers in the series; a frame images the first n_disks
+SERIES_MODES = 8        # Fourier modes of the velocity field
+SERIES_DT = 0.004       # time step between frames, in box lengths per unit velocity
+
+
+def velocity_modes(series_seed: int, modes: int = SERIES_MODES):
+    """A seeded random divergence-free velocity field on the periodic unit cube,
+    u(x) = sum_m -sin(2 pi k_m . x + phi_m) (k_m x b_m) / |k_m|: the curl of the
+    vector potential sum_m b_m cos(2 pi k_m . x + phi_m) / (2 pi |k_m|), so
+    div u = 0 exactly.  Returns (k (m, 3) integer wave vectors, b (m, 3), phi (m,))."""
+    rng = np.random.Generator(np.random.PCG64(1_000_003 + series_seed))
+    k = rng.integers(-3, 4, size=(modes, 3))
+    k[np.all(k == 0, axis=1)] = (1, 0, 0)
+    b = rng.standard_normal((modes, 3))
+    phi = rng.uniform(0, 2 * np.pi, modes)
+    return k.astype(np.float64), b, phi
+
+
+def velocity(pos: np.ndarray, field_) -> np.ndarray:
+    """u at positions (n, 3) in the unit cube."""
+    k, b, phi = field_
+    kb = np.cross(k, b) / np.linalg.norm(k, axis=1)[:, None]  # (m, 3)
+    arg = 2 * np.pi * pos @ k.T + phi[None, :]                 # (n, m)
+    return -np.sin(arg) @ kb
+
+
+def divergence(pos: np.ndarray, field_) -> np.ndarray:
+    """div u at positions (analytic); zero up to rounding for every field here."""
+    k, b, phi = field_
+    kb = np.cross(k, b) / np.linalg.norm(k, axis=1)[:, None]
+    arg = 2 * np.pi * pos @ k.T + phi[None, :]
+    # d/dx_j of -sin(2 pi k.x + phi) kb_j = -2 pi cos(.) k_j kb_j, summed over j
+    return -2 * np.pi * np.cos(arg) @ np.sum(k * kb, axis=1)
+
+
+def tracer_positions(series_seed: int, frame: int, n: int = SERIES_TRACERS) -> np.ndarray:
+    """Tracer positions (n, 3) in the periodic unit cube at `frame`: uniform at
+    frame 0, then advected by velocity_modes(series_seed) with one midpoint
+    (RK2) step of SERIES_DT per frame."""
+    rng = np.random.Generator(np.random.PCG64(2_000_029 + series_seed))
+    pos = rng.random((n, 3))
+    f = velocity_modes(series_seed)
+    for _ in range(frame):
+        mid = pos + 0.5 * SERIES_DT * velocity(pos, f)
+        pos = np.mod(pos + SERIES_DT * velocity(mid, f), 1.0)
+    return pos
+
+
+def series_frames(n_frames: int = 64, series_seed: int = 0, iterations: int = 100, sides=(512, 640, 768, 1024),
+                  planes=(100, 400), tracers=(200, 3000)) -> list:
+    """The uneven time series: frame i has H and W drawn from `sides`, Nz from
+    `planes` (inclusive), dz 2, dx 1.1, lambda 0.632 (length units um), and
+    images the first n_i (drawn from `tracers`) tracers of one advected
+    population, each mapped from the unit cube to its own W x H x Nz box."""
+    rng = np.random.Generator(np.random.PCG64(3_000_017 + series_seed))
+    out = []
+    for i in range(n_frames):
+        h = int(rng.choice(sides))
+        w = int(rng.choice(sides))
+        nz = int(rng.integers(planes[0], planes[1] + 1))
+        nt = int(rng.integers(tracers[0], tracers[1] + 1))
+        out.append(HoloConfig(name=f"series{series_seed}_frame{i:03d}_{w}x{h}x{nz}", width=w, height=h,
+                              zero_padding=0, num_planes=nz, start_plane=2500.0, plane_stepsize=2.0,
+                              resolution=1.1, wavelength=0.632, regularization_param=0.15,
+                              regularization_TV_param=0.1, num_inverse_iterations=iterations, num_tv_iterations=5,
+                              n_disks=nt, disk_radius=(1.0, 4.0), noise_sigma=0.02, seed=10_000 + i,
+                              series_seed=series_seed, series_frame=i))
+    return out
+
+
 def object_masks(cfg: HoloConfig) -> dict:
     """Opaque-object masks per plane index: {z_index: mask (H, W) float64}."""
     rng = np.random.Generator(np.random.PCG64(cfg.seed))
@@ -166,6 +244,14 @@ def object_masks(cfg: HoloConfig) -> dict:
         if k not in masks:
             masks[k] = np.zeros((H, W), np.float64)
         return masks[k]
+
+    if cfg.series_seed >= 0:
+        pos = tracer_positions(cfg.series_seed, cfg.series_frame)[:cfg.n_disks]
+        for x, y, z in pos:
+            r = rng.uniform(*cfg.disk_radius)
+            k = min(int(z * cfg.num_planes), cfg.num_planes - 1)
+            _stamp_disk(plane(k), p + x * cfg.width, p + y * cfg.height, r)
+        return masks
 
     for _ in range(cfg.n_disks):
         r = rng.uniform(*cfg.disk_radius)
@@ -205,6 +291,25 @@ def propagate_objects(cfg: HoloConfig, masks: dict) -> np.ndarray:
     return 1.0 + _ifft2(S)
 
 
+def propagate_objects_torch(cfg: HoloConfig, masks: dict, device) -> np.ndarray:
+    """propagate_objects in FP64 on a torch device (input generation only)."""
+    import torch
+
+    H, W = cfg.H, cfg.W
+    lam, dx = cfg.lam(), cfg.dx()
+    zl = cfg.plane_list()
+    fy = ((((torch.arange(H, device=device, dtype=torch.float64) + H // 2) % H) - H // 2) / H)[:, None]
+    fx = ((((torch.arange(W, device=device, dtype=torch.float64) + W // 2) % W) - W // 2) / W)[None, :]
+    a = (lam / dx) ** 2 * (fx ** 2 + fy ** 2)
+    sm1 = torch.where(a >= 1.0, torch.full_like(a, -1.0), -a / (torch.sqrt(torch.clamp(1.0 - a, min=0.0)) + 1.0))
+    c = 2 * np.pi / lam * sm1
+    S = torch.zeros((H, W), dtype=torch.complex128, device=device)
+    for k in sorted(masks):
+        m = torch.from_numpy(masks[k]).to(device)
+        S += torch.polar(torch.ones_like(c), float(zl[k]) * c) * torch.fft.fft2(-m)
+    return (1.0 + torch.fft.ifft2(S)).cpu().numpy()
+
+
 def translated_frame(b: np.ndarray, k: int) -> np.ndarray:
     """Frame k of a series made by translating frame 0's particle field: the
     hologram of a translated field is the circularly shifted hologram (the
@@ -239,16 +344,20 @@ def preprocess(img: np.ndarray, zero_padding: int) -> np.ndarray:
     return out
 
 
-def make_hologram(cfg: HoloConfig, cache_dir: str | None = None):
-    """Return (uint8 camera image, preprocessed float32 hologram b)."""
+def make_hologram(cfg: HoloConfig, cache_dir: str | None = None, device=None):
+    """Return (uint8 camera image, preprocessed float32 hologram b).  With a
+    torch `device` the propagation runs there in FP64 (faster for large
+    frames; the result can differ from the CPU's in the last bits, so cached
+    files record which was used)."""
     if cache_dir is None:
         cache_dir = os.environ.get("RIHVR_CACHE", "/tmp/rihvr_cache")
-    path = os.path.join(cache_dir, f"{cfg.name}_{cfg.key()}.npz")
+    tag = "" if device is None else "_dev"
+    path = os.path.join(cache_dir, f"{cfg.name}_{cfg.key()}{tag}.npz")
     if os.path.exists(path):
         with np.load(path) as z:
             return z["img"], z["b"]
     masks = object_masks(cfg)
-    U = propagate_objects(cfg, masks)
+    U = propagate_objects(cfg, masks) if device is None else propagate_objects_torch(cfg, masks, device)
     img = camera_image(cfg, U)
     b = preprocess(img, cfg.zero_padding)
     try:
