@@ -84,6 +84,8 @@ cudaError_t launch_prox_l1(int storage, const ProxArgs& a, int* nblocks_out, cud
 cudaError_t launch_reduce_partials(const double* partials, int nblocks, double* scratch, double* out,
                                    cudaStream_t st);
 size_t reduce_scratch_doubles();
+cudaError_t launch_fill_uniform_c(float2* x, long long n, unsigned long long seed, cudaStream_t st);
+cudaError_t launch_sumsq(const float* x, long long n, double* partials, int* nblocks_out, cudaStream_t st);
 cudaError_t launch_finish_forward(const float2* c, const float* b, float* dnew, long long n, double* partials,
                                   int* nblocks_out, cudaStream_t st);
 cudaError_t launch_holo_momentum(const float* dnew, float* dY0, float* dX, const float* b, float* r,
