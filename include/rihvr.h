@@ -54,6 +54,12 @@ enum rihvr_mode {
   RIHVR_MODE_FASTA_FUSED_LASSO_2D = 7  /* L1 + per-plane 2-D TV (the CLI default) */
 };
 
+/* Storage of the three iterate volumes; arithmetic is FP32 in every case.
+ * FP16 keeps the objective within 1e-2 of the FP64 solution (2.6e-4 at the
+ * 1024 x 1024 x 1000 workload).  BF16 does not (2.3e-2 there: its 8-bit
+ * mantissa adds rounding noise to every stored iterate, and the objective gap
+ * grows with its square), so rihvr_create accepts BF16 only with
+ * faithful = 0, where no agreement with the reference is claimed. */
 enum rihvr_storage { RIHVR_STORE_F32 = 0, RIHVR_STORE_BF16 = 1, RIHVR_STORE_F16 = 2 };
 
 /* Solver parameters.  The first block mirrors umnholo::Parameters
@@ -135,7 +141,7 @@ int rihvr_plane_list(const rihvr_params* params, double* z_out);
  * (src/core/sparse_compressive_holo.cu:58-135).  width x height is the padded
  * hologram size.  Each side is even, 16..4096, with prime factors 2, 3, 5 and 7
  * only (the reference needs multiples of 16); square planes of side 32, 48, 64,
- * 128, 256, 384, 512, 768 or 1024 take the fastest FFT passes. */
+ * 128, 256, 384, 512, 640, 768, 1024 or 2304 take the fastest FFT passes. */
 int rihvr_create(const rihvr_params* params, int width, int height, rihvr_ctx** out);
 
 /* SparseCompressiveHolo::destroy (:137-146). */
@@ -193,9 +199,11 @@ int rihvr_batch_last_combined(void);
 
 /* Launch-shape autotuner (no reference counterpart).  Times the candidate
  * shapes of the passes that have a free parameter on this context's own
- * buffers - z-chunks of the adjoint column pass, z-chunks of the forward
- * column pass, runs per plane of the streaming TV prox and streaming versus
- * tiled TV prox - and keeps the fastest.  Results are cached per process for
+ * buffers - the adjoint column pass's algorithm for evenly spaced planes
+ * (transfer function by recurrence or evaluated at every plane) and its
+ * z-chunks, z-chunks of the forward column pass, runs per plane of the
+ * streaming TV prox and streaming versus tiled TV prox - and keeps the
+ * fastest.  Results are cached per process for
  * the plane size, plane count, TV iterations, mode, storage and objective
  * recording, so later contexts of the same shape reuse them.  Safe between
  * iterations (only scratch buffers are written).  Tuned shapes may change the
@@ -206,8 +214,12 @@ int rihvr_autotune(rihvr_ctx* ctx, double* best_ms);
 
 /* The launch shapes in use: z-chunks of the adjoint and forward column passes,
  * runs per plane of the streaming TV prox and the TV kernel (1 tiled,
- * 2 streaming); 0 means the built-in choice.  Any pointer may be NULL. */
-int rihvr_tuning(const rihvr_ctx* ctx, int* adj_chunks, int* fwd_chunks, int* tv_runs, int* tv_kernel);
+ * 2 streaming); 0 means the built-in choice.  adj_recurrence receives 1 when
+ * the adjoint column pass advances the transfer function by a recurrence
+ * over evenly spaced planes (square planes of side 32 to 1024 except 384 and
+ * 768), else 0.  Any pointer may be NULL. */
+int rihvr_tuning(const rihvr_ctx* ctx, int* adj_chunks, int* fwd_chunks, int* tv_runs, int* tv_kernel,
+                 int* adj_recurrence);
 
 /* Restart from x = 0 without changing the hologram. */
 int rihvr_reset(rihvr_ctx* ctx);

@@ -37,7 +37,7 @@ MODE_FASTA_FUSED_LASSO = 6
 MODE_FASTA_FUSED_LASSO_2D = 7
 STORE_F32, STORE_BF16, STORE_F16 = 0, 1, 2
 
-SUPPORTED_SIDES = (32, 48, 64, 128, 256, 384, 512, 768, 1024)
+SUPPORTED_SIDES = (32, 48, 64, 128, 256, 384, 512, 640, 768, 1024, 2304)
 
 
 class RihvrParams(ctypes.Structure):
@@ -183,7 +183,8 @@ def load_library(path: str = LIB_PATH):
     L.rihvr_set_batch_mode.argtypes = [ip]
     L.rihvr_batch_last_combined.argtypes = []
     L.rihvr_autotune.argtypes = [vp, P(ctypes.c_double)]
-    L.rihvr_tuning.argtypes = [vp, P(ctypes.c_int), P(ctypes.c_int), P(ctypes.c_int), P(ctypes.c_int)]
+    L.rihvr_tuning.argtypes = [vp, P(ctypes.c_int), P(ctypes.c_int), P(ctypes.c_int), P(ctypes.c_int),
+                               P(ctypes.c_int)]
     L.rihvr_reset.argtypes = [vp]
     L.rihvr_set_initial_volume.argtypes = [vp, vp, ip]
     L.rihvr_iterate.argtypes = [vp, ip]
@@ -569,9 +570,10 @@ class SparseCompressiveHolo:
 
     def tuning(self) -> dict:
         """Launch shapes in use (rihvr_tuning); 0 = built-in choice."""
-        v = [ctypes.c_int() for _ in range(4)]
+        v = [ctypes.c_int() for _ in range(5)]
         _check(self._L.rihvr_tuning(self._h, *[ctypes.byref(x) for x in v]), "rihvr_tuning")
-        return dict(zip(("adj_chunks", "fwd_chunks", "tv_runs", "tv_kernel"), (x.value for x in v)))
+        return dict(zip(("adj_chunks", "fwd_chunks", "tv_runs", "tv_kernel", "adj_recurrence"),
+                        (x.value for x in v)))
 
     def inverseReconstruct(self, b: np.ndarray | None = None) -> float:
         if b is not None:

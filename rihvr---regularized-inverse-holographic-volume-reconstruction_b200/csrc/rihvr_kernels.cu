@@ -26,7 +26,12 @@
 namespace rihvr {
 
 // ---------------------------------------------------------------------------
-// line configurations: N = N1 * N2, N1 threads per line, N2 elements each
+// line configurations: N = N1 * N2, N1 threads per line, N2 elements each.
+// After the exchange a thread holds M stage-B rows of N1 elements (VS values).
+// Where N1 divides N2 every thread holds N2 / N1 rows; otherwise (side 640 =
+// 20 x 32) the N2 rows are dealt round-robin and a thread's last row exists
+// only when t + N1 (M - 1) < N2 (EXACT false): the missing rows are computed
+// on zeros and never stored.
 // ---------------------------------------------------------------------------
 template <int N>
 struct LineCfg;
@@ -34,7 +39,8 @@ struct LineCfg;
   template <>                                                                            \
   struct LineCfg<NN> {                                                                   \
     static constexpr int N = NN, N1 = NN1, N2 = NN / NN1, M = (NN / NN1) / NN1;          \
-    static constexpr int LD = NN1 + 1;                                                   \
+    static constexpr int LD = NN1 + 1, VS = N2;                                          \
+    static constexpr bool EXACT = true;                                                  \
     static_assert((NN / NN1) % NN1 == 0, "N1 must divide N2");                           \
   };
 RIHVR_LINE(32, 4)
@@ -46,9 +52,31 @@ RIHVR_LINE(384, 8)
 RIHVR_LINE(512, 16)
 RIHVR_LINE(768, 16)
 RIHVR_LINE(1024, 32)
+RIHVR_LINE(2304, 48)  // the 2048 x 2048 hologram padded by 128 on each side
 #undef RIHVR_LINE
+template <>
+struct LineCfg<640> {  // 20 threads a line, 32 elements each; 12 of them take a second stage-B row
+  static constexpr int N = 640, N1 = 20, N2 = 32, M = 2;
+  static constexpr int LD = N1 + 1, VS = M * N1;
+  static constexpr bool EXACT = false;
+};
 
-#define RIHVR_FOR_EACH_SIZE(X) X(32) X(48) X(64) X(128) X(256) X(384) X(512) X(768) X(1024)
+// the first K values of a register array, as an array of K
+template <int K, int L>
+__device__ __forceinline__ float2 (&head(float2 (&a)[L]))[K] {
+  static_assert(K <= L, "prefix longer than the array");
+  return *reinterpret_cast<float2(*)[K]>(&a[0]);
+}
+
+// does stage-B row j of thread t exist (always, for the exact splits)
+template <int N>
+__device__ __forceinline__ bool row_ok(int t, int j) {
+  using C = LineCfg<N>;
+  if constexpr (C::EXACT) return true;
+  else return t + C::N1 * j < C::N2;
+}
+
+#define RIHVR_FOR_EACH_SIZE(X) X(32) X(48) X(64) X(128) X(256) X(384) X(512) X(640) X(768) X(1024) X(2304)
 
 bool line_size_supported(int n) {
   switch (n) {
@@ -85,9 +113,9 @@ static cudaError_t allow_smem(K kernel, size_t bytes) {
   return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
-template <int N1, int N2, bool INV>
-__device__ __forceinline__ void stage_b_dft(float2 (&w)[N2]) {
-  constexpr int M = N2 / N1;
+template <int N1, int VS, bool INV>
+__device__ __forceinline__ void stage_b_dft(float2 (&w)[VS]) {
+  constexpr int M = VS / N1;
 #pragma unroll
   for (int j = 0; j < M; ++j) {
     float2 s[N1];
@@ -108,6 +136,10 @@ template <int N>
 struct RowLayout {
   using C = LineCfg<N>;
   static constexpr int LPB = kRowThreads / C::N1;
+  // lines of 48 threads straddle warps: the block then holds whole lines only
+  // and exchanges through a block barrier instead of a warp one
+  static constexpr bool WARP_LINES = (32 % C::N1) == 0;
+  static constexpr int THREADS = LPB * C::N1;
   static constexpr int base_ls = C::N2 * C::LD;
   // pad the per-line stride so that lines sharing a half-warp hit different banks
   static constexpr int LS = (C::N1 >= 16) ? base_ls : base_ls + (((C::N1 % 16) - (base_ls % 16) + 16) % 16);
@@ -133,32 +165,39 @@ __global__ void __launch_bounds__(kRowThreads) k_rows(const void* __restrict__ i
   using C = LineCfg<N>;
   using Lay = RowLayout<N>;
   constexpr int N1 = C::N1, N2 = C::N2, M = C::M, LD = C::LD;
-  static_assert(32 % N1 == 0, "a line must not straddle warps");
+  static_assert(Lay::WARP_LINES || Lay::THREADS <= kRowThreads, "whole lines per block");
   extern __shared__ __align__(128) float2 sm[];
   const int li = threadIdx.x / N1, t = threadIdx.x % N1;
   long long L = (long long)blockIdx.x * Lay::LPB + li;
   const bool active = L < nlines;
   if (!active) L = nlines - 1;
   const size_t base = (size_t)L * N;
-  float2 v[N2];
+  float2 v[C::VS];
 #pragma unroll
   for (int n2 = 0; n2 < N2; ++n2) v[n2] = load_as<IN>(in, base + t + N1 * n2);
-  reg_fft<N2, INV>(v);
-  line_twiddle<N, N2, INV>(v, t);
+  reg_fft<N2, INV>(head<N2>(v));
+  line_twiddle<N, N2, INV>(head<N2>(v), t);
   float2* sl = sm + li * Lay::LS;
 #pragma unroll
   for (int k2 = 0; k2 < N2; ++k2) sl[k2 * LD + t] = v[k2];
-  __syncwarp();
+  if constexpr (Lay::WARP_LINES) {
+    __syncwarp();
+  } else {
+    __syncthreads();
+  }
 #pragma unroll
-  for (int j = 0; j < M; ++j)
+  for (int j = 0; j < M; ++j) {
+    const bool ok = row_ok<N>(t, j);
 #pragma unroll
-    for (int n1 = 0; n1 < N1; ++n1) v[j * N1 + n1] = sl[(t + N1 * j) * LD + n1];
-  stage_b_dft<N1, N2, INV>(v);
+    for (int n1 = 0; n1 < N1; ++n1) v[j * N1 + n1] = ok ? sl[(t + N1 * j) * LD + n1] : make_float2(0.f, 0.f);
+  }
+  stage_b_dft<N1, C::VS, INV>(v);
   if (active) {
 #pragma unroll
     for (int j = 0; j < M; ++j)
+      if (row_ok<N>(t, j))
 #pragma unroll
-      for (int k1 = 0; k1 < N1; ++k1) out[base + t + N1 * j + N2 * k1] = cscale(v[j * N1 + k1], scale);
+        for (int k1 = 0; k1 < N1; ++k1) out[base + t + N1 * j + N2 * k1] = cscale(v[j * N1 + k1], scale);
   }
 }
 
@@ -169,7 +208,7 @@ static cudaError_t rows_launch(const void* in, float2* out, long long nlines, fl
   if (blocks <= 0) return cudaSuccess;
   cudaError_t e = allow_smem(k_rows<N, INV, IN>, Lay::SMEM_BYTES);
   if (e != cudaSuccess) return e;
-  k_rows<N, INV, IN><<<(unsigned)blocks, kRowThreads, Lay::SMEM_BYTES, st>>>(in, out, nlines, scale);
+  k_rows<N, INV, IN><<<(unsigned)blocks, Lay::THREADS, Lay::SMEM_BYTES, st>>>(in, out, nlines, scale);
   return cudaGetLastError();
 }
 
@@ -217,8 +256,13 @@ struct ColLayout {
   // or more blocks share an SM, so one block's barriers no longer idle the
   // whole SM (measured 10-17 % faster column passes than 256-thread blocks).
   // Sides 384 and 768 measured no gain or a loss and keep 256 threads.
+  // Side 2304 (48 threads a column, 48 elements a thread) takes 4 columns:
+  // 192 threads, so that the forward pass's 255 registers a thread fit.
+  // Side 640 (20 threads a column) takes 8 columns: 160 threads.
   static constexpr int CC = (N == 256 || N == 512 || N == 1024) ? 128 / C::N1
-                                                                 : (C::N1 >= 32 ? 8 : (C::N1 >= 16 ? 16 : 32));
+                            : N == 2304                        ? 4
+                            : N == 640                         ? 8
+                                                               : (C::N1 >= 32 ? 8 : (C::N1 >= 16 ? 16 : 32));
   static constexpr int THREADS = CC * C::N1;
   static constexpr int SMEM_ELEMS = C::N2 * C::LD * CC;
   static constexpr size_t SMEM_BYTES = sizeof(float2) * SMEM_ELEMS;
@@ -227,7 +271,8 @@ struct ColLayout {
   // staging strips in shared memory next to the exchange buffer: two for the
   // forward pass (double-buffered prefetch), one complex + one FP64 strip for
   // the adjoint (spectrum and phase table, constant over z)
-  static constexpr bool STAGE = (N % CC == 0) && (SMEM_BYTES + 2 * sizeof(float2) * STRIP_ELEMS <= 220 * 1024);
+  // (only where two blocks still fit on an SM: side 2304 would take 222 KB)
+  static constexpr bool STAGE = (N % CC == 0) && (SMEM_BYTES + 2 * sizeof(float2) * STRIP_ELEMS <= 113 * 1024);
   static constexpr size_t STAGE_BYTES = SMEM_BYTES + (STAGE ? 2 * sizeof(float2) * STRIP_ELEMS : 0);
 };
 
@@ -309,7 +354,7 @@ constexpr int tma_rows() {
 // Exchange + stage B shared by all column kernels.  On entry v holds the
 // twiddled stage-A output of this thread; on exit the stage-B output.
 template <int N, bool INV>
-__device__ __forceinline__ void col_exchange(float2 (&v)[LineCfg<N>::N2], float2* sm, int c, int t) {
+__device__ __forceinline__ void col_exchange(float2 (&v)[LineCfg<N>::VS], float2* sm, int c, int t) {
   using C = LineCfg<N>;
   using Lay = ColLayout<N>;
   constexpr int N1 = C::N1, N2 = C::N2, M = C::M, LD = C::LD, CC = Lay::CC;
@@ -318,10 +363,13 @@ __device__ __forceinline__ void col_exchange(float2 (&v)[LineCfg<N>::N2], float2
   for (int k2 = 0; k2 < N2; ++k2) sm[(k2 * LD + t) * CC + c] = v[k2];
   __syncthreads();
 #pragma unroll
-  for (int j = 0; j < M; ++j)
+  for (int j = 0; j < M; ++j) {
+    const bool ok = row_ok<N>(t, j);
 #pragma unroll
-    for (int n1 = 0; n1 < N1; ++n1) v[j * N1 + n1] = sm[((t + N1 * j) * LD + n1) * CC + c];
-  stage_b_dft<N1, N2, INV>(v);
+    for (int n1 = 0; n1 < N1; ++n1)
+      v[j * N1 + n1] = ok ? sm[((t + N1 * j) * LD + n1) * CC + c] : make_float2(0.f, 0.f);
+  }
+  stage_b_dft<N1, C::VS, INV>(v);
 }
 
 // The column passes walk many planes with the same thread-to-row assignment,
@@ -331,7 +379,7 @@ __device__ __forceinline__ void col_exchange(float2 (&v)[LineCfg<N>::N2], float2
 // products); shared memory limits the column passes to 8 warps per SM, which
 // leaves the registers free.  Longer lines regenerate them every plane.
 template <int N>
-constexpr bool kHoistTw = LineCfg<N>::N2 <= 32;
+constexpr bool kHoistTw = LineCfg<N>::N2 <= 32 && LineCfg<N>::EXACT;
 
 template <int N, int N2, bool INV>
 __device__ __forceinline__ void apply_twiddles(float2 (&v)[N2], const float2 (&tw)[kHoistTw<N> ? N2 : 1], int t) {
@@ -396,7 +444,7 @@ __global__ void __launch_bounds__(ColLayout<N>::THREADS) k_adj_col(const float2*
   for (int z = zb; z < ze; ++z) {
     const double zz = znext;
     if (z + 1 < ze) znext = zlist[z + 1];  // in flight during this plane
-    float2 v[N2];
+    float2 v[C::VS];
     if constexpr (Lay::STAGE) {
 #pragma unroll
       for (int n2 = 0; n2 < N2; ++n2) {
@@ -416,8 +464,8 @@ __global__ void __launch_bounds__(ColLayout<N>::THREADS) k_adj_col(const float2*
         sched_fence();
       }
     }
-    reg_fft<N2, true>(v);
-    apply_twiddles<N, N2, true>(v, tw, t);
+    reg_fft<N2, true>(head<N2>(v));
+    apply_twiddles<N, N2, true>(head<N2>(v), tw, t);
     // the exchange buffer also holds the previous plane's output tile: its
     // store must have read it (the exchange starts with a barrier)
     if (TMA && threadIdx.x == 0) bulk_wait_read_all();
@@ -426,6 +474,106 @@ __global__ void __launch_bounds__(ColLayout<N>::THREADS) k_adj_col(const float2*
       // plane z's [N][CC] column strip goes out through the TMA from the
       // exchange buffer, as a few bulk stores instead of N2 8-byte stores a thread
       __syncthreads();  // every thread is done reading the exchange
+#pragma unroll
+      for (int j = 0; j < M; ++j)
+        if (row_ok<N>(t, j))
+#pragma unroll
+          for (int k1 = 0; k1 < N1; ++k1) sm[(N1 * j + N2 * k1 + t) * CC + c] = v[j * N1 + k1];
+      fence_smem_async();
+      __syncthreads();
+      if (threadIdx.x == 0) {
+        constexpr int R = tma_rows<N>();
+#pragma unroll 1
+        for (int b = 0; b < N; b += R) tma_store_3d(&umap, sm + b * CC, blockIdx.x * CC, b, z);
+        bulk_commit();
+      }
+    } else if (col_ok) {
+      float2* Uz = U + (size_t)z * HW + (size_t)t * W + x;
+#pragma unroll
+      for (int j = 0; j < M; ++j)
+        if (row_ok<N>(t, j))
+#pragma unroll
+          for (int k1 = 0; k1 < N1; ++k1) Uz[(size_t)(N1 * j + N2 * k1) * W] = v[j * N1 + k1];
+    }
+  }
+  if (TMA && threadIdx.x == 0) bulk_wait_all();
+}
+
+// Transfer function H'_z = exp(i 2 pi u), u = frac(z * cturn), with the
+// accurate sincospi: used where a value seeds many planes (the recurrence
+// below), so its error is not multiplied by the plane count.
+__device__ __forceinline__ float2 transfer_accurate(double z, double cturn, bool conj_) {
+  double u = z * cturn;
+  u -= rint(u);
+  float s, c;
+  sincospif(2.0f * (float)u, &s, &c);
+  return make_float2(c, conj_ ? -s : s);
+}
+
+// Planes between exact re-anchorings of the adjoint recurrence.  FP32
+// rotations drift by about one rounding a step; 16 steps keep that near 1e-6.
+constexpr int kAdjAnchor = 16;
+
+// Adjoint column pass for evenly spaced planes (z_{k+1} - z_k = dz for all k):
+// Y_z = conj(H'_z) Rs advances from plane to plane by the rotation
+// D = conj(H'_dz), one complex product an element, instead of an FP64 phase
+// reduction and a sincos.  Y lives in registers and D in shared memory, which
+// replaces both staged strips of k_adj_col (spectrum and phase table): 66 KB
+// a block at side 1024 instead of 98 KB, so three blocks share an SM.  Every
+// kAdjAnchor planes Y is recomputed exactly from Rs and the FP64 phase table.
+// Lines of up to 32 elements a thread only (the inter-stage twiddles are
+// regenerated each plane to leave registers for Y).
+template <int N, bool TMA>
+__global__ void __launch_bounds__(ColLayout<N>::THREADS, 3)
+    k_adj_col_rec(const float2* __restrict__ Rs, const double* __restrict__ cturn, const double* __restrict__ zlist,
+                  double dz, float2* __restrict__ U, int z0, int z1, int zpb,
+                  const __grid_constant__ CUtensorMap umap) {
+  using C = LineCfg<N>;
+  using Lay = ColLayout<N>;
+  constexpr int N1 = C::N1, N2 = C::N2, M = C::M, CC = Lay::CC;
+  static_assert(N2 <= 32, "the recurrence keeps a line's elements in registers");
+  constexpr int W = N;
+  extern __shared__ __align__(128) float2 sm[];
+  const int c = threadIdx.x % CC, t = threadIdx.x / CC;
+  const int xr = blockIdx.x * CC + c;
+  const bool col_ok = xr < W;
+  const int x = col_ok ? xr : W - 1;
+  const int zb = z0 + blockIdx.y * zpb, ze = min(zb + zpb, z1);
+  if (zb >= ze) return;
+  float2* s_d = sm + Lay::SMEM_ELEMS;  // this thread's rotations, [row][CC] (thread-private slots)
+  const float2* rs = Rs + (size_t)t * W + x;
+  const double* ct = cturn + (size_t)t * W + x;
+  float2 y[N2];
+#pragma unroll
+  for (int n2 = 0; n2 < N2; ++n2) {
+    const double cn = __ldg(ct + (size_t)n2 * N1 * W);
+    s_d[(t + N1 * n2) * CC + c] = transfer_accurate(dz, cn, true);
+    y[n2] = cmul(__ldg(rs + (size_t)n2 * N1 * W), transfer_accurate(zlist[zb], cn, true));
+  }
+#pragma unroll 1
+  for (int z = zb; z < ze; ++z) {
+    if (z > zb) {
+      if ((z - zb) % kAdjAnchor == 0) {
+        const double zz = zlist[z];
+        const float2* rsz = launder(rs);
+        const double* ctz = launder(ct);
+#pragma unroll
+        for (int n2 = 0; n2 < N2; ++n2)
+          y[n2] = cmul(__ldg(rsz + (size_t)n2 * N1 * W), transfer_accurate(zz, __ldg(ctz + (size_t)n2 * N1 * W), true));
+      } else {
+#pragma unroll
+        for (int n2 = 0; n2 < N2; ++n2) y[n2] = cmul(y[n2], s_d[(t + N1 * n2) * CC + c]);
+      }
+    }
+    float2 v[N2];
+#pragma unroll
+    for (int n2 = 0; n2 < N2; ++n2) v[n2] = y[n2];
+    reg_fft<N2, true>(v);
+    line_twiddle<N, N2, true>(v, launder_i(t));
+    if (TMA && threadIdx.x == 0) bulk_wait_read_all();
+    col_exchange<N, true>(v, sm, c, t);
+    if constexpr (TMA) {
+      __syncthreads();
 #pragma unroll
       for (int j = 0; j < M; ++j)
 #pragma unroll
@@ -439,7 +587,7 @@ __global__ void __launch_bounds__(ColLayout<N>::THREADS) k_adj_col(const float2*
         bulk_commit();
       }
     } else if (col_ok) {
-      float2* Uz = U + (size_t)z * HW + (size_t)t * W + x;
+      float2* Uz = U + (size_t)z * ((size_t)N * W) + (size_t)t * W + x;
 #pragma unroll
       for (int j = 0; j < M; ++j)
 #pragma unroll
@@ -479,9 +627,9 @@ __global__ void __launch_bounds__(ColLayout<N>::THREADS) k_fwd_col(const float2*
     if (zb < ze) strip_async<N>(s_t, T + (size_t)zb * HW, blockIdx.x * CC);
     cp_async_commit();
   }
-  float2 acc[N2];
+  float2 acc[C::VS];
 #pragma unroll
-  for (int i = 0; i < N2; ++i) acc[i] = make_float2(0.f, 0.f);
+  for (int i = 0; i < C::VS; ++i) acc[i] = make_float2(0.f, 0.f);
   float2 tw[kHoistTw<N> ? N2 : 1];
   if constexpr (kHoistTw<N>) line_twiddles<N, N2, false>(tw, t);
   double znext = zb < ze ? zlist[zb] : 0.0;
@@ -489,7 +637,7 @@ __global__ void __launch_bounds__(ColLayout<N>::THREADS) k_fwd_col(const float2*
   for (int z = zb; z < ze; ++z) {
     const double zz = znext;
     if (z + 1 < ze) znext = zlist[z + 1];  // in flight during this plane
-    float2 v[N2];
+    float2 v[C::VS];
     if constexpr (Lay::STAGE) {
       cp_async_wait<0>();
       __syncthreads();
@@ -500,8 +648,8 @@ __global__ void __launch_bounds__(ColLayout<N>::THREADS) k_fwd_col(const float2*
 #pragma unroll
       for (int n2 = 0; n2 < N2; ++n2) v[n2] = Tz[(size_t)n2 * N1 * W];
     }
-    reg_fft<N2, false>(v);
-    apply_twiddles<N, N2, false>(v, tw, t);
+    reg_fft<N2, false>(head<N2>(v));
+    apply_twiddles<N, N2, false>(head<N2>(v), tw, t);
     // the exchange's first barrier also orders every thread's reads of s_t
     // before the refill below
     col_exchange<N, false>(v, sm, c, t);
@@ -510,20 +658,23 @@ __global__ void __launch_bounds__(ColLayout<N>::THREADS) k_fwd_col(const float2*
       cp_async_commit();
 #pragma unroll
       for (int j = 0; j < M; ++j)
+        if (row_ok<N>(t, j))
 #pragma unroll
-        for (int k1 = 0; k1 < N1; ++k1) {
-          const float2 h = transfer(zz, s_ct[(N1 * j + N2 * k1 + t) * CC + c], false);
-          cmac<N>(acc[j * N1 + k1], v[j * N1 + k1], h);
-        }
+          for (int k1 = 0; k1 < N1; ++k1) {
+            const float2 h = transfer(zz, s_ct[(N1 * j + N2 * k1 + t) * CC + c], false);
+            cmac<N>(acc[j * N1 + k1], v[j * N1 + k1], h);
+          }
     } else {
       const double* ctz = launder(ct);
 #pragma unroll
-      for (int g = 0; g < N2; g += kPhaseGroup) {
+      for (int g = 0; g < C::VS; g += kPhaseGroup) {
 #pragma unroll
         for (int q = 0; q < kPhaseGroup; ++q) {
           const int j = (g + q) / N1, k1 = (g + q) % N1;
-          const float2 h = transfer(zz, __ldg(ctz + (size_t)(N1 * j + N2 * k1) * W), false);
-          cmac<N>(acc[j * N1 + k1], v[j * N1 + k1], h);
+          if (row_ok<N>(t, j)) {
+            const float2 h = transfer(zz, __ldg(ctz + (size_t)(N1 * j + N2 * k1) * W), false);
+            cmac<N>(acc[j * N1 + k1], v[j * N1 + k1], h);
+          }
         }
         sched_fence();
       }
@@ -534,8 +685,9 @@ __global__ void __launch_bounds__(ColLayout<N>::THREADS) k_fwd_col(const float2*
     float2* Sp = Spart + (size_t)blockIdx.y * HW + (size_t)t * W + x;
 #pragma unroll
     for (int j = 0; j < M; ++j)
+      if (row_ok<N>(t, j))
 #pragma unroll
-      for (int k1 = 0; k1 < N1; ++k1) Sp[(size_t)(N1 * j + N2 * k1) * W] = acc[j * N1 + k1];
+        for (int k1 = 0; k1 < N1; ++k1) Sp[(size_t)(N1 * j + N2 * k1) * W] = acc[j * N1 + k1];
   }
 }
 
@@ -553,18 +705,19 @@ __global__ void __launch_bounds__(ColLayout<N>::THREADS) k_plane_col(const float
   const bool col_ok = xr < W;
   const int x = col_ok ? xr : W - 1;
   const float2* src = in + (size_t)t * W + x;
-  float2 v[N2];
+  float2 v[C::VS];
 #pragma unroll
   for (int n2 = 0; n2 < N2; ++n2) v[n2] = src[(size_t)n2 * N1 * W];
-  reg_fft<N2, INV>(v);
-  line_twiddle<N, N2, INV>(v, t);
+  reg_fft<N2, INV>(head<N2>(v));
+  line_twiddle<N, N2, INV>(head<N2>(v), t);
   col_exchange<N, INV>(v, sm, c, t);
   if (col_ok) {
     float2* dst = out + (size_t)t * W + x;
 #pragma unroll
     for (int j = 0; j < M; ++j)
+      if (row_ok<N>(t, j))
 #pragma unroll
-      for (int k1 = 0; k1 < N1; ++k1) dst[(size_t)(N1 * j + N2 * k1) * W] = cscale(v[j * N1 + k1], scale);
+        for (int k1 = 0; k1 < N1; ++k1) dst[(size_t)(N1 * j + N2 * k1) * W] = cscale(v[j * N1 + k1], scale);
   }
 }
 
@@ -606,12 +759,15 @@ static bool plane_stack_map(CUtensorMap* m, void* base, int n, int nz, int cc, i
 
 template <int N>
 static cudaError_t adj_col_n(const float2* Rs, const double* cturn, const double* zlist, float2* U, int W,
-                             int z0, int z1, cudaStream_t st, int chunks_hint) {
+                             int z0, int z1, cudaStream_t st, int chunks_hint, double dz_uniform) {
   using Lay = ColLayout<N>;
   const int nz = z1 - z0;
   if (nz <= 0) return cudaSuccess;
   const int strips = col_strips<N>(W);
-  const int target = 8 * num_sms();
+  // the recurrence variant: evenly spaced planes, lines of <= 32 elements a thread
+  constexpr bool kRecOk = kHoistTw<N> && (N % Lay::CC == 0);
+  const bool rec = kRecOk && dz_uniform != 0.0 && !std::getenv("RIHVR_ADJ_NO_RECURRENCE");
+  const int target = (rec ? 12 : 8) * num_sms();
   int chunks = chunks_hint > 0 ? chunks_hint : (target + strips - 1) / strips;
   if (chunks > nz) chunks = nz;
   if (chunks < 1) chunks = 1;
@@ -621,6 +777,23 @@ static cudaError_t adj_col_n(const float2* Rs, const double* cturn, const double
   std::memset(&umap, 0, sizeof(umap));
   const bool tma = (W == N) && (N % Lay::CC == 0) && plane_stack_map(&umap, U, N, z1, Lay::CC, tma_rows<N>());
   cudaError_t e;
+  if constexpr (kRecOk) {
+    if (rec) {
+      constexpr size_t smem = Lay::SMEM_BYTES + sizeof(float2) * Lay::STRIP_ELEMS;
+      if (tma) {
+        e = allow_smem(k_adj_col_rec<N, true>, smem);
+        if (e != cudaSuccess) return e;
+        k_adj_col_rec<N, true><<<dim3(strips, chunks), Lay::THREADS, smem, st>>>(Rs, cturn, zlist, dz_uniform, U, z0,
+                                                                                  z1, zpb, umap);
+      } else {
+        e = allow_smem(k_adj_col_rec<N, false>, smem);
+        if (e != cudaSuccess) return e;
+        k_adj_col_rec<N, false><<<dim3(strips, chunks), Lay::THREADS, smem, st>>>(Rs, cturn, zlist, dz_uniform, U,
+                                                                                   z0, z1, zpb, umap);
+      }
+      return cudaGetLastError();
+    }
+  }
   if (tma) {
     e = allow_smem(k_adj_col<N, true>, Lay::STAGE_BYTES);
     if (e != cudaSuccess) return e;
@@ -635,13 +808,26 @@ static cudaError_t adj_col_n(const float2* Rs, const double* cturn, const double
   return cudaGetLastError();
 }
 
+bool adj_recurrence_supported(int W, int H) {
+  if (W != H) return false;
+  switch (H) {
+#define RIHVR_CASE(NN) \
+  case NN:             \
+    return kHoistTw<NN> && (NN % ColLayout<NN>::CC == 0);
+    RIHVR_FOR_EACH_SIZE(RIHVR_CASE)
+#undef RIHVR_CASE
+    default:
+      return false;
+  }
+}
+
 static cudaError_t launch_adj_col_fast(const float2* Rs, const double* cturn, const double* zlist, float2* U, int W,
-                                      int H, int z0, int z1, cudaStream_t st, int chunks_hint) {
+                                      int H, int z0, int z1, cudaStream_t st, int chunks_hint, double dz_uniform) {
   if (W != H) return cudaErrorInvalidValue;
   switch (H) {
 #define RIHVR_CASE(NN) \
   case NN:             \
-    return adj_col_n<NN>(Rs, cturn, zlist, U, W, z0, z1, st, chunks_hint);
+    return adj_col_n<NN>(Rs, cturn, zlist, U, W, z0, z1, st, chunks_hint, dz_uniform);
     RIHVR_FOR_EACH_SIZE(RIHVR_CASE)
 #undef RIHVR_CASE
     default:
@@ -2423,8 +2609,8 @@ cudaError_t launch_rows(int inverse, int in_kind, const void* in, int out_kind, 
 }
 
 cudaError_t launch_adj_col(const float2* Rs, const double* cturn, const double* zlist, float2* U, int W, int H,
-                           int z0, int z1, cudaStream_t st, int chunks_hint) {
-  if (fast_square(W, H)) return launch_adj_col_fast(Rs, cturn, zlist, U, W, H, z0, z1, st, chunks_hint);
+                           int z0, int z1, cudaStream_t st, int chunks_hint, double dz_uniform) {
+  if (fast_square(W, H)) return launch_adj_col_fast(Rs, cturn, zlist, U, W, H, z0, z1, st, chunks_hint, dz_uniform);
   const int nz = z1 - z0;
   if (nz <= 0) return cudaSuccess;
   GPlan p;

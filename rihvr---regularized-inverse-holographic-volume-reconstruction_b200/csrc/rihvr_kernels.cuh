@@ -69,8 +69,13 @@ int segment_volume(int storage, const void* P, const void* Pprev, float beta, in
                    rihvr_segment_info* info, SegWorkspace* ws, cudaStream_t st);
 size_t max_partial_blocks(int W, int H, int Nz);
 
+// square sizes whose adjoint column pass has the recurrence variant
+bool adj_recurrence_supported(int W, int H);
+// dz_uniform != 0: the planes are evenly spaced by dz_uniform (z_{k+1} - z_k,
+// exact in FP64), which lets the square fast sizes advance the transfer
+// function by a recurrence; 0 takes the direct evaluation at every plane.
 cudaError_t launch_adj_col(const float2* Rs, const double* cturn, const double* zlist, float2* U, int W,
-                           int H, int z0, int z1, cudaStream_t st, int chunks_hint = 0);
+                           int H, int z0, int z1, cudaStream_t st, int chunks_hint = 0, double dz_uniform = 0.0);
 cudaError_t launch_rows(int inverse, int in_kind, const void* in, int out_kind, void* out, int W,
                         long long nlines, float scale, cudaStream_t st);
 cudaError_t launch_fwd_col(const float2* T, const double* cturn, const double* zlist, float2* Spart, int W,

@@ -191,6 +191,8 @@ struct rihvr_ctx {
   float* r = nullptr;
   double* cturn = nullptr;
   double* zlist = nullptr;
+  double dz_uniform = 0;  // plane spacing when every z_{k+1} - z_k is the same (FP64), else 0
+  int tune_adj_rec = 1;   // adjoint column pass may advance H'_z by the recurrence (needs dz_uniform)
   double* partials = nullptr;
   unsigned* nonfinite_d = nullptr;  // count of non-finite hologram samples (rihvr_set_hologram)
   size_t partial_cap = 0;
@@ -354,7 +356,8 @@ int reduce_into(rihvr_ctx* c, int nblocks, int slot) {
 int adjoint_volume(rihvr_ctx* c) {
   {
     ProfScope ps(c, K_ADJ_COL);
-    KL(launch_adj_col(c->Rs, c->cturn, c->zlist, c->U, c->W, c->H, 0, c->Nz, c->st, c->tune_adj_chunks));
+    KL(launch_adj_col(c->Rs, c->cturn, c->zlist, c->U, c->W, c->H, 0, c->Nz, c->st, c->tune_adj_chunks,
+                      c->tune_adj_rec ? c->dz_uniform : 0.0));
   }
   {
     ProfScope ps(c, K_ADJ_ROW);
@@ -994,7 +997,7 @@ int copy_in(rihvr_ctx* c, void* dst, const void* src, size_t bytes, int is_devic
 int validate(const rihvr_params* p, int W, int H) {
   if (!p) return fail(RIHVR_ERR_INVALID_ARGUMENT, "params is NULL");
   if (W <= 0 || H <= 0) return fail(RIHVR_ERR_INVALID_ARGUMENT, "width and height must be positive");
-  // Square planes of side 32, 48, 64, 128, 256, 384, 512, 768 or 1024 take the
+  // Square planes of side 32, 48, 64, 128, 256, 384, 512, 640, 768, 1024 or 2304 take the
   // register-resident FFT passes; any other even width and height from 16 to
   // 4096 whose prime factors are 2, 3, 5 and 7 takes the generic passes (the
   // reference needs multiples of 16, :126, 1948).
@@ -1008,6 +1011,14 @@ int validate(const rihvr_params* p, int W, int H) {
   if (p->mode != 5 && p->mode != 6 && p->mode != 7)
     return fail(RIHVR_ERR_UNKNOWN_MODE, "mode must be 5, 6 or 7 (unsupported mode)");
   if (p->storage < 0 || p->storage > 2) return fail(RIHVR_ERR_INVALID_ARGUMENT, "storage must be 0, 1 or 2");
+  // BF16 storage rounds every stored iterate to 8 significant bits; at the
+  // 1024 x 1024 x 1000 workload the objective then ends 2.3e-2 from the FP64
+  // solution, outside the 1e-2 tolerance of reduced-precision storage.  FP16
+  // (11 bits, 2.6e-4 there) meets it, so reference-faithful solves refuse BF16.
+  if (p->storage == STORE_BF16 && p->faithful)
+    return fail(RIHVR_ERR_INVALID_ARGUMENT,
+                "BF16 volume storage misses the 1e-2 objective tolerance of faithful solves; use FP16 (storage 2) "
+                "or faithful = 0");
   if (p->num_tv_iterations < 0 || p->num_tv_iterations > 20)
     return fail(RIHVR_ERR_INVALID_ARGUMENT, "num_tv_iterations must be in 0..20");
   if (!(p->wavelength > 0.f) || !(p->resolution > 0.f))
@@ -1137,6 +1148,10 @@ int rihvr_create(const rihvr_params* params, int width, int height, rihvr_ctx** 
   phase_turns(height, width, (double)params->resolution, (double)params->wavelength, ct);
   std::vector<double> zl((size_t)c->Nz);
   rihvr_plane_list(params, zl.data());
+  // evenly spaced planes (exactly, in FP64) let the adjoint advance H'_z by a recurrence
+  c->dz_uniform = c->Nz > 1 ? zl[1] - zl[0] : 1.0;
+  for (int k = 1; k + 1 < c->Nz && c->dz_uniform != 0; ++k)
+    if (zl[(size_t)k + 1] - zl[(size_t)k] != c->dz_uniform) c->dz_uniform = 0;
   if (cudaMemcpy(c->cturn, ct.data(), sizeof(double) * ct.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemcpy(c->zlist, zl.data(), sizeof(double) * zl.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemsetAsync(c->b, 0, sizeof(float) * c->HW, c->st) != cudaSuccess)
@@ -1200,7 +1215,7 @@ struct TuneKey {
   }
 };
 struct TuneVal {
-  int adj_chunks, fwd_chunks, tv_nseg, tv_kernel;
+  int adj_chunks, fwd_chunks, tv_nseg, tv_kernel, adj_rec;
   double ms;
 };
 std::mutex g_tune_mu;
@@ -1228,21 +1243,28 @@ int autotune_run(rihvr_ctx* c, cudaEvent_t e0, cudaEvent_t e1, TuneVal* out) {
   const int prev_profiling = c->profiling;
   c->profiling = false;
   float best;
-  // 1. z-chunks of the adjoint column pass
-  int best_adj = 0;
+  // 1. the adjoint column pass: transfer function by recurrence over evenly
+  //    spaced planes or evaluated at every plane, and its z-chunks
+  int best_adj = 0, best_rec = c->dz_uniform != 0 ? 1 : 0;
   float t_adj = 1e30f;
-  for (int ch : {0, 2, 4, 8, 16, 32}) {
-    if (ch > c->Nz) continue;
-    RC(time_min(c, e0, e1, [&]() -> int {
-      KL(launch_adj_col(c->Rs, c->cturn, c->zlist, c->U, c->W, c->H, 0, c->Nz, c->st, ch));
-      return RIHVR_OK;
-    }, &best));
-    if (best < t_adj * 0.98f) {
-      t_adj = best;
-      best_adj = ch;
+  for (int rec : {1, 0}) {
+    if (rec && (c->dz_uniform == 0 || !adj_recurrence_supported(c->W, c->H))) continue;
+    for (int ch : {0, 2, 4, 8, 16, 32}) {
+      if (ch > c->Nz) continue;
+      RC(time_min(c, e0, e1, [&]() -> int {
+        KL(launch_adj_col(c->Rs, c->cturn, c->zlist, c->U, c->W, c->H, 0, c->Nz, c->st, ch,
+                          rec ? c->dz_uniform : 0.0));
+        return RIHVR_OK;
+      }, &best));
+      if (best < t_adj * 0.98f) {
+        t_adj = best;
+        best_adj = ch;
+        best_rec = rec;
+      }
     }
   }
   c->tune_adj_chunks = best_adj;
+  c->tune_adj_rec = best_rec;
   // a valid gradient volume for the prox candidates
   KL(launch_rows(1, ELEM_C32, c->U, ELEM_C32, c->G, c->W, (long long)c->Nz * c->H, 1.0f, c->st));
   // 2. 2-D TV prox: streaming with 1..8 runs per plane or the built-in count, or tiled
@@ -1286,7 +1308,7 @@ int autotune_run(rihvr_ctx* c, cudaEvent_t e0, cudaEvent_t e1, TuneVal* out) {
   }
   c->nchunks = best_fwd;
   c->profiling = prev_profiling;
-  *out = TuneVal{c->tune_adj_chunks, c->nchunks, c->tune_tv_nseg, c->tune_tv_kernel,
+  *out = TuneVal{c->tune_adj_chunks, c->nchunks, c->tune_tv_nseg, c->tune_tv_kernel, c->tune_adj_rec,
                  (double)t_adj + (double)t_tv + (double)t_fwd};
   return RIHVR_OK;
 }
@@ -1295,9 +1317,12 @@ int autotune_run(rihvr_ctx* c, cudaEvent_t e0, cudaEvent_t e1, TuneVal* out) {
 
 extern "C" {
 
-int rihvr_tuning(const rihvr_ctx* c, int* adj_chunks, int* fwd_chunks, int* tv_runs, int* tv_kernel) {
+int rihvr_tuning(const rihvr_ctx* c, int* adj_chunks, int* fwd_chunks, int* tv_runs, int* tv_kernel,
+                 int* adj_recurrence) {
   if (!c) return fail(RIHVR_ERR_INVALID_ARGUMENT, "NULL context");
   if (adj_chunks) *adj_chunks = c->tune_adj_chunks;
+  if (adj_recurrence)
+    *adj_recurrence = (c->tune_adj_rec && c->dz_uniform != 0 && adj_recurrence_supported(c->W, c->H)) ? 1 : 0;
   if (fwd_chunks) *fwd_chunks = c->nchunks;
   if (tv_runs) *tv_runs = c->tune_tv_nseg;
   if (tv_kernel) *tv_kernel = c->tune_tv_kernel;
@@ -1317,6 +1342,7 @@ int rihvr_autotune(rihvr_ctx* c, double* best_ms) {
       c->nchunks = it->second.fwd_chunks;
       c->tune_tv_nseg = it->second.tv_nseg;
       c->tune_tv_kernel = it->second.tv_kernel;
+      c->tune_adj_rec = it->second.adj_rec;
       c->tuned = true;
       if (best_ms) *best_ms = it->second.ms;
       return RIHVR_OK;

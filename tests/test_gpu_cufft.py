@@ -30,7 +30,7 @@ def setup(rihvr, side, nz):
     return p, op, H
 
 
-@pytest.mark.parametrize("side,nz", [(256, 4), (384, 3), (1024, 2), (640, 2)])
+@pytest.mark.parametrize("side,nz", [(256, 4), (384, 3), (1024, 2), (640, 2), (2304, 2)])
 def test_operators_as_accurate_as_cufft(rihvr, side, nz):
     import torch
 

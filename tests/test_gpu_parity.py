@@ -52,7 +52,7 @@ def rand_volume(rng, nz, side, scale=0.05):
 
 
 @pytest.mark.parametrize("side,nz", [(32, 3), (48, 4), (64, 5), (128, 4), (256, 2), (384, 3), (512, 2), (768, 2),
-                                     (1024, 2)])
+                                     (1024, 2), (2304, 2), (640, 3)])
 def test_forward_matches_oracle(rihvr, side, nz):
     p = make(rihvr, side, nz)
     rng = np.random.default_rng(side + nz)
@@ -64,7 +64,7 @@ def test_forward_matches_oracle(rihvr, side, nz):
 
 
 @pytest.mark.parametrize("side,nz", [(32, 3), (48, 4), (64, 5), (128, 2), (256, 2), (384, 3), (512, 2), (768, 2),
-                                     (1024, 2)])
+                                     (1024, 2), (2304, 3), (640, 5)])
 def test_adjoint_matches_oracle(rihvr, side, nz):
     p = make(rihvr, side, nz)
     rng = np.random.default_rng(7 * side + nz)
@@ -136,6 +136,7 @@ p.start_plane, p.plane_stepsize, p.num_planes = 100.0, 40.0, nz
 p.wavelength, p.resolution, p.zero_padding = 0.632, 2.0, 0
 p.regularization_param, p.regularization_TV_param, p.num_tv_iterations = 0.01, 0.02, ntv
 p.storage = st
+p.faithful = int(st != 1)  # BF16 storage only with faithful = 0
 rng = np.random.default_rng(11)
 x = (0.05 * (rng.standard_normal((nz, side, side)) + 1j * rng.standard_normal((nz, side, side)))).astype(np.complex64)
 r = rng.standard_normal((side, side)).astype(np.float32)
@@ -225,10 +226,11 @@ def test_objective_recording_does_not_change_the_solve(rihvr, synthmod, cache_di
 
 @pytest.mark.parametrize("storage", [1, 2])
 def test_reduced_precision_storage(rihvr, synthmod, cache_dir, storage):
+    """FP16 in faithful mode; BF16 only with faithful = 0 (refused otherwise)."""
     side, nz, n = 64, 6, 20
     cfg = synthmod.small_config(W=side, H=side, Nz=nz, seed=4)
     _, b = synthmod.make_hologram(cfg, cache_dir=cache_dir)
-    p = rihvr.params_from_config(cfg, storage=storage)
+    p = rihvr.params_from_config(cfg, storage=storage, faithful=0 if storage == 1 else 1)
     log, X, f, terms, est = run_gpu(rihvr, p, side, b, n)
     olog, OX, _, _, _ = O.solve(oparams(rihvr, p, side), b.astype(np.float64), n)
     assert abs(f - olog["f_x"][-1]) / abs(olog["f_x"][-1]) < TOL_LOW

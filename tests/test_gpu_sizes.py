@@ -35,7 +35,8 @@ def oparams(rihvr, p, W, H):
                           faithful=p.faithful, t0=p.initial_step)
 
 
-SIZES = [(640, 640, 2), (96, 64, 3), (64, 96, 3), (48, 80, 2), (210, 100, 2), (1536, 16, 2), (2304, 2304, 1)]
+SIZES = [(1280, 1280, 1), (96, 64, 3), (64, 96, 3), (48, 80, 2), (210, 100, 2), (1536, 16, 2), (2560, 2560, 1),
+         (640, 512, 2)]
 
 
 @pytest.mark.parametrize("W,H,nz", SIZES)
