@@ -161,7 +161,7 @@ def time_to_objective(rihvr, cfg, b, s, storage, stream, hb, tol=1e-3):
     if g.get("workload") != cfg.name or hashlib.sha1(b.tobytes()).hexdigest() != g.get("b_sha1"):
         return None
     target = float(g["f_x"][-1])
-    p = rihvr.params_from_config(cfg, record_objective=1, storage=storage)
+    p = rihvr.params_from_config(cfg, record_objective=1, storage=storage, faithful=0 if storage == 1 else 1)
     with rihvr.SparseCompressiveHolo(p, cfg.W, cfg.H) as t:
         t.setHologram(b)
         t.iterate(1)  # first iteration runs eagerly (tables, graph capture)
@@ -487,7 +487,9 @@ def run_ours(args):
     _, b0 = synth.make_hologram(cfg)
     b = synth.translated_frame(b0, frame)
     storage = {"f32": 0, "bf16": 1, "f16": 2}[args.storage]
-    p = rihvr.params_from_config(cfg, record_objective=0, storage=storage, autotune=1 if args.autotune else 0)
+    # BF16 storage is accepted only without the reference-faithful arithmetic
+    p = rihvr.params_from_config(cfg, record_objective=0, storage=storage, autotune=1 if args.autotune else 0,
+                                 faithful=0 if storage == 1 else 1)
     s = rihvr.SparseCompressiveHolo(p, cfg.W, cfg.H)
     V = cfg.voxels()
     s.setHologram(b)  # tunes launch shapes first with --autotune

@@ -214,15 +214,15 @@ def tracer_positions(series_seed: int, frame: int, n: int = SERIES_TRACERS) -> n
 
 def series_frames(n_frames: int = 64, series_seed: int = 0, iterations: int = 100, sides=(512, 640, 768, 1024),
                   planes=(100, 400), tracers=(200, 3000)) -> list:
-    """The uneven time series: frame i has H and W drawn from `sides`, Nz from
-    `planes` (inclusive), dz 2, dx 1.1, lambda 0.632 (length units um), and
-    images the first n_i (drawn from `tracers`) tracers of one advected
-    population, each mapped from the unit cube to its own W x H x Nz box."""
+    """The uneven time series: frame i is a square hologram whose side is drawn
+    from `sides`, with Nz from `planes` (inclusive), dz 2, dx 1.1, lambda 0.632
+    (length units um); it images the first n_i (drawn from `tracers`) tracers
+    of one advected population, each mapped from the unit cube to its own
+    W x H x Nz box."""
     rng = np.random.Generator(np.random.PCG64(3_000_017 + series_seed))
     out = []
     for i in range(n_frames):
-        h = int(rng.choice(sides))
-        w = int(rng.choice(sides))
+        h = w = int(rng.choice(sides))
         nz = int(rng.integers(planes[0], planes[1] + 1))
         nt = int(rng.integers(tracers[0], tracers[1] + 1))
         out.append(HoloConfig(name=f"series{series_seed}_frame{i:03d}_{w}x{h}x{nz}", width=w, height=h,

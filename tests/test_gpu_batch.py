@@ -61,15 +61,16 @@ def test_batch_as_one_graph_per_iteration(rihvr, synthmod, cache_dir):
             synthmod.small_config(W=128, H=128, Nz=4, seed=22, num_inverse_iterations=9, num_tv_iterations=3),
             synthmod.small_config(W=32, H=32, Nz=7, seed=23, num_inverse_iterations=9),
             synthmod.small_config(W=64, H=64, Nz=3, seed=24, num_inverse_iterations=9, regularization_TV_param=0.0)]
-    storage = [0, 0, 2, 1]
+    storage = [0, 0, 2, 1]  # BF16 only with faithful = 0
     holos = [synthmod.make_hologram(c, cache_dir=cache_dir)[1] for c in cfgs]
     seq = []
     for c, b, sto in zip(cfgs, holos, storage):
-        with rihvr.SparseCompressiveHolo(rihvr.params_from_config(c, storage=sto), c.W, c.H) as s:
+        with rihvr.SparseCompressiveHolo(rihvr.params_from_config(c, storage=sto, faithful=int(sto != 1)), c.W,
+                                         c.H) as s:
             f = s.inverseReconstruct(b)
             seq.append((f, s.getVolume(), s.iterations()))
-    solvers = [rihvr.SparseCompressiveHolo(rihvr.params_from_config(c, storage=sto), c.W, c.H)
-               for c, sto in zip(cfgs, storage)]
+    solvers = [rihvr.SparseCompressiveHolo(rihvr.params_from_config(c, storage=sto, faithful=int(sto != 1)), c.W,
+                                           c.H) for c, sto in zip(cfgs, storage)]
     rihvr.set_batch_mode(1)
     try:
         for _ in range(2):

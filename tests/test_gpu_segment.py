@@ -75,7 +75,7 @@ def test_segment_of_a_solved_volume(rihvr, synthmod, storage):
     cfg = synthmod.config1()
     cfg.num_planes = 16
     _, b = synthmod.make_hologram(cfg)
-    p = rihvr.params_from_config(cfg, storage=storage)
+    p = rihvr.params_from_config(cfg, storage=storage, faithful=int(storage != 1))  # BF16: faithful = 0
     with rihvr.SparseCompressiveHolo(p, cfg.W, cfg.H) as s:
         s.setHologram(b)
         s.iterate(15)
