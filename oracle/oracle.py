@@ -4,8 +4,9 @@ TEST INFRASTRUCTURE ONLY: imported by ``tests/``, ``__graft_entry__.smoke()``
 and the ``cpu_baseline`` / ``--impl reference`` legs of ``bench.py`` as the
 checker and the CPU baseline.  The product path never imports this module.
 
-Parity status: unpinned (the reference ships no golden data for this path and
-cannot be compiled here); the oracle is pinned against numpy.fft and against
+Parity status: pinned to the reference's own CUDA kernels, built unchanged by
+``oracle/build_ref.py`` and driven by ``oracle/ref_harness.cu``
+(``tests/test_gpu_ref_pin.py``); also checked against numpy.fft and
 mathematical known answers in ``tests/test_oracle.py``.
 """
 from __future__ import annotations

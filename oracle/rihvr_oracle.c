@@ -7,12 +7,15 @@
  * also the timed CPU baseline ("port": the reference has no CPU path and its
  * CUDA build needs OpenCV C++, which is absent).
  *
- * Parity status: unpinned.  The reference ships no golden vectors, fixtures
- * or test bodies for this path (its Test/ suites are declared but not
- * shipped) and cannot be compiled here, so this restatement is checked
- * against numpy.fft and against mathematical known answers (adjoint
+ * Parity status: pinned to the reference's own kernels.  The reference ships
+ * no golden vectors, fixtures or test bodies for this path, and cannot be
+ * built whole here (OpenCV C++ is absent), but its hot-path CUDA kernels
+ * compile alone: oracle/build_ref.py builds them, unchanged, behind the
+ * harness oracle/ref_harness.cu, and tests/test_gpu_ref_pin.py checks every
+ * operation of this file and its whole FISTA loop against them on a GPU.  It
+ * is also checked against numpy.fft and mathematical known answers (adjoint
  * identity, unit-modulus transfer function, TV fixed points, shrink on
- * scalars) instead of against the reference's own outputs.
+ * scalars).
  *
  * Everything is double precision complex.  Every function below cites the
  * reference function it restates (paths relative to the RIHVR source tree).
