@@ -199,9 +199,9 @@ int rihvr_batch_last_combined(void);
 
 /* Launch-shape autotuner (no reference counterpart).  Times the candidate
  * shapes of the passes that have a free parameter on this context's own
- * buffers - the adjoint column pass's algorithm for evenly spaced planes
- * (transfer function by recurrence or evaluated at every plane) and its
- * z-chunks, z-chunks of the forward column pass, runs per plane of the
+ * buffers - the column passes' algorithms for evenly spaced planes
+ * (transfer function by recurrence or Horner's scheme, or evaluated at every
+ * plane) and their z-chunks, runs per plane of the
  * streaming TV prox and streaming versus tiled TV prox - and keeps the
  * fastest.  Results are cached per process for
  * the plane size, plane count, TV iterations, mode, storage and objective
@@ -217,9 +217,11 @@ int rihvr_autotune(rihvr_ctx* ctx, double* best_ms);
  * 2 streaming); 0 means the built-in choice.  adj_recurrence receives 1 when
  * the adjoint column pass advances the transfer function by a recurrence
  * over evenly spaced planes (square planes of side 32 to 1024 except 384 and
- * 768), else 0.  Any pointer may be NULL. */
+ * 768), else 0.  fwd_horner receives 1 when the forward column pass sums over
+ * evenly spaced planes by Horner's scheme (square planes of side 32 to 512 and
+ * 1024), else 0.  Any pointer may be NULL. */
 int rihvr_tuning(const rihvr_ctx* ctx, int* adj_chunks, int* fwd_chunks, int* tv_runs, int* tv_kernel,
-                 int* adj_recurrence);
+                 int* adj_recurrence, int* fwd_horner);
 
 /* Restart from x = 0 without changing the hologram. */
 int rihvr_reset(rihvr_ctx* ctx);

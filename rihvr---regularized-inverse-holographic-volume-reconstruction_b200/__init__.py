@@ -184,7 +184,7 @@ def load_library(path: str = LIB_PATH):
     L.rihvr_batch_last_combined.argtypes = []
     L.rihvr_autotune.argtypes = [vp, P(ctypes.c_double)]
     L.rihvr_tuning.argtypes = [vp, P(ctypes.c_int), P(ctypes.c_int), P(ctypes.c_int), P(ctypes.c_int),
-                               P(ctypes.c_int)]
+                               P(ctypes.c_int), P(ctypes.c_int)]
     L.rihvr_reset.argtypes = [vp]
     L.rihvr_set_initial_volume.argtypes = [vp, vp, ip]
     L.rihvr_iterate.argtypes = [vp, ip]
@@ -570,9 +570,9 @@ class SparseCompressiveHolo:
 
     def tuning(self) -> dict:
         """Launch shapes in use (rihvr_tuning); 0 = built-in choice."""
-        v = [ctypes.c_int() for _ in range(5)]
+        v = [ctypes.c_int() for _ in range(6)]
         _check(self._L.rihvr_tuning(self._h, *[ctypes.byref(x) for x in v]), "rihvr_tuning")
-        return dict(zip(("adj_chunks", "fwd_chunks", "tv_runs", "tv_kernel", "adj_recurrence"),
+        return dict(zip(("adj_chunks", "fwd_chunks", "tv_runs", "tv_kernel", "adj_recurrence", "fwd_horner"),
                         (x.value for x in v)))
 
     def inverseReconstruct(self, b: np.ndarray | None = None) -> float:

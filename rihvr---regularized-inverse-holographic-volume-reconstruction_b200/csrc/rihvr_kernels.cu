@@ -691,6 +691,92 @@ __global__ void __launch_bounds__(ColLayout<N>::THREADS) k_fwd_col(const float2*
   }
 }
 
+// Forward column pass for evenly spaced planes, by Horner's scheme: with
+// H'_z = H'_{zb} D^(z - zb) and D = H'_dz,
+//   sum_{z in [zb, ze)} H'_z V_z = H'_{zb} (((V_{ze-1} D + V_{ze-2}) D + ...) D + V_{zb}),
+// so each plane costs one complex multiply-add by D (held in shared memory in
+// place of the FP64 phase-table strip) instead of an FP64 phase reduction, a
+// sincos and a multiply-add; H'_{zb} is applied once, exactly, at the end.  The
+// planes go in descending order.  D^k carries the rounding of D k times (about
+// k x 6e-8 in phase), which stays near 1e-5 for the longest z-chunks used.
+template <int N>
+__global__ void __launch_bounds__(ColLayout<N>::THREADS) k_fwd_col_horner(const float2* __restrict__ T,
+                                                                          const double* __restrict__ cturn,
+                                                                          const double* __restrict__ zlist, double dz,
+                                                                          float2* __restrict__ Spart, int z0, int z1,
+                                                                          int zpb) {
+  using C = LineCfg<N>;
+  using Lay = ColLayout<N>;
+  constexpr int N1 = C::N1, N2 = C::N2, M = C::M, CC = Lay::CC;
+  static_assert(Lay::STAGE && C::EXACT, "staged square sizes only");
+  constexpr int W = N;
+  extern __shared__ __align__(128) float2 sm[];
+  const int c = threadIdx.x % CC, t = threadIdx.x / CC;
+  const int xr = blockIdx.x * CC + c;
+  const bool col_ok = xr < W;
+  const int x = col_ok ? xr : W - 1;
+  const int zb = z0 + blockIdx.y * zpb, ze = min(zb + zpb, z1);
+  constexpr size_t HW = (size_t)N * W;
+  const double* ct = cturn + (size_t)t * W + x;
+  float2* const s_t = sm + Lay::SMEM_ELEMS;       // one strip of T
+  float2* const s_d = s_t + Lay::STRIP_ELEMS;     // this thread's rotations D, stage-B layout
+  if (zb < ze) strip_async<N>(s_t, T + (size_t)(ze - 1) * HW, blockIdx.x * CC);
+  cp_async_commit();
+#pragma unroll
+  for (int j = 0; j < M; ++j)
+#pragma unroll
+    for (int k1 = 0; k1 < N1; ++k1)
+      s_d[(N1 * j + N2 * k1 + t) * CC + c] = transfer_accurate(dz, __ldg(ct + (size_t)(N1 * j + N2 * k1) * W), false);
+  float2 acc[N2];
+#pragma unroll
+  for (int i = 0; i < N2; ++i) acc[i] = make_float2(0.f, 0.f);
+  float2 tw[kHoistTw<N> ? N2 : 1];
+  if constexpr (kHoistTw<N>) line_twiddles<N, N2, false>(tw, t);
+#pragma unroll 1
+  for (int z = ze - 1; z >= zb; --z) {
+    cp_async_wait<0>();
+    __syncthreads();
+    float2 v[N2];
+#pragma unroll
+    for (int n2 = 0; n2 < N2; ++n2) v[n2] = s_t[(t + N1 * n2) * CC + c];
+    reg_fft<N2, false>(v);
+    apply_twiddles<N, N2, false>(v, tw, t);
+    // the exchange's first barrier orders every thread's reads of s_t before the refill
+    col_exchange<N, false>(v, sm, c, t);
+    if (z - 1 >= zb) strip_async<N>(s_t, T + (size_t)(z - 1) * HW, blockIdx.x * CC);
+    cp_async_commit();
+#pragma unroll
+    for (int j = 0; j < M; ++j)
+#pragma unroll
+      for (int k1 = 0; k1 < N1; ++k1) {
+        const float2 d = s_d[(N1 * j + N2 * k1 + t) * CC + c];
+        float2& a = acc[j * N1 + k1];
+        const float2 u = v[j * N1 + k1];
+        const float ax = a.x;
+        a.x = fmaf(ax, d.x, fmaf(-a.y, d.y, u.x));
+        a.y = fmaf(ax, d.y, fmaf(a.y, d.x, u.y));
+      }
+  }
+  cp_async_wait<0>();
+  if (col_ok && zb < ze) {
+    const double zz = zlist[zb];
+    float2* Sp = Spart + (size_t)blockIdx.y * HW + (size_t)t * W + x;
+#pragma unroll
+    for (int j = 0; j < M; ++j)
+#pragma unroll
+      for (int k1 = 0; k1 < N1; ++k1) {
+        const float2 h = transfer_accurate(zz, __ldg(ct + (size_t)(N1 * j + N2 * k1) * W), false);
+        Sp[(size_t)(N1 * j + N2 * k1) * W] = cmul(acc[j * N1 + k1], h);
+      }
+  } else if (col_ok) {
+    float2* Sp = Spart + (size_t)blockIdx.y * HW + (size_t)t * W + x;
+#pragma unroll
+    for (int j = 0; j < M; ++j)
+#pragma unroll
+      for (int k1 = 0; k1 < N1; ++k1) Sp[(size_t)(N1 * j + N2 * k1) * W] = make_float2(0.f, 0.f);
+  }
+}
+
 // Plain column DFT of one (square) plane.
 template <int N, bool INV>
 __global__ void __launch_bounds__(ColLayout<N>::THREADS) k_plane_col(const float2* __restrict__ in,
@@ -858,30 +944,53 @@ static int fwd_col_chunks_fast(int W, int H, int Nz) {
 
 template <int N>
 static cudaError_t fwd_col_n(const float2* T, const double* cturn, const double* zlist, float2* Spart, int W,
-                             int z0, int z1, int nchunks, cudaStream_t st) {
+                             int z0, int z1, int nchunks, cudaStream_t st, double dz_uniform) {
   using Lay = ColLayout<N>;
   const int nz = z1 - z0;
   if (nz <= 0) return cudaSuccess;
   const int strips = col_strips<N>(W);
   const int zpb = (nz + nchunks - 1) / nchunks;
   const int chunks = (nz + zpb - 1) / zpb;
-  cudaError_t e = allow_smem(k_fwd_col<N>, Lay::STAGE_BYTES);
-  if (e != cudaSuccess) return e;
+  cudaError_t e;
   if (chunks < nchunks) {  // unused chunk slots must read as zero
     e = cudaMemsetAsync(Spart + (size_t)chunks * N * W, 0, sizeof(float2) * (size_t)(nchunks - chunks) * N * W, st);
     if (e != cudaSuccess) return e;
   }
+  if constexpr (Lay::STAGE && LineCfg<N>::EXACT) {
+    if (dz_uniform != 0.0) {
+      e = allow_smem(k_fwd_col_horner<N>, Lay::STAGE_BYTES);
+      if (e != cudaSuccess) return e;
+      k_fwd_col_horner<N><<<dim3(strips, chunks), Lay::THREADS, Lay::STAGE_BYTES, st>>>(T, cturn, zlist, dz_uniform,
+                                                                                         Spart, z0, z1, zpb);
+      return cudaGetLastError();
+    }
+  }
+  e = allow_smem(k_fwd_col<N>, Lay::STAGE_BYTES);
+  if (e != cudaSuccess) return e;
   k_fwd_col<N><<<dim3(strips, chunks), Lay::THREADS, Lay::STAGE_BYTES, st>>>(T, cturn, zlist, Spart, z0, z1, zpb);
   return cudaGetLastError();
 }
 
+bool fwd_horner_supported(int W, int H) {
+  if (W != H) return false;
+  switch (H) {
+#define RIHVR_CASE(NN) \
+  case NN:             \
+    return ColLayout<NN>::STAGE && LineCfg<NN>::EXACT;
+    RIHVR_FOR_EACH_SIZE(RIHVR_CASE)
+#undef RIHVR_CASE
+    default:
+      return false;
+  }
+}
+
 static cudaError_t launch_fwd_col_fast(const float2* T, const double* cturn, const double* zlist, float2* Spart,
-                                      int W, int H, int z0, int z1, int nchunks, cudaStream_t st) {
+                                      int W, int H, int z0, int z1, int nchunks, cudaStream_t st, double dz_uniform) {
   if (W != H) return cudaErrorInvalidValue;
   switch (H) {
 #define RIHVR_CASE(NN) \
   case NN:             \
-    return fwd_col_n<NN>(T, cturn, zlist, Spart, W, z0, z1, nchunks, st);
+    return fwd_col_n<NN>(T, cturn, zlist, Spart, W, z0, z1, nchunks, st, dz_uniform);
     RIHVR_FOR_EACH_SIZE(RIHVR_CASE)
 #undef RIHVR_CASE
     default:
@@ -2633,8 +2742,8 @@ cudaError_t launch_adj_col(const float2* Rs, const double* cturn, const double* 
 }
 
 cudaError_t launch_fwd_col(const float2* T, const double* cturn, const double* zlist, float2* Spart, int W, int H,
-                           int z0, int z1, int nchunks, cudaStream_t st) {
-  if (fast_square(W, H)) return launch_fwd_col_fast(T, cturn, zlist, Spart, W, H, z0, z1, nchunks, st);
+                           int z0, int z1, int nchunks, cudaStream_t st, double dz_uniform) {
+  if (fast_square(W, H)) return launch_fwd_col_fast(T, cturn, zlist, Spart, W, H, z0, z1, nchunks, st, dz_uniform);
   const int nz = z1 - z0;
   if (nz <= 0) return cudaSuccess;
   GPlan p;

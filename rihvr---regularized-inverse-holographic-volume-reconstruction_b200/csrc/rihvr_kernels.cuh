@@ -78,8 +78,11 @@ cudaError_t launch_adj_col(const float2* Rs, const double* cturn, const double* 
                            int H, int z0, int z1, cudaStream_t st, int chunks_hint = 0, double dz_uniform = 0.0);
 cudaError_t launch_rows(int inverse, int in_kind, const void* in, int out_kind, void* out, int W,
                         long long nlines, float scale, cudaStream_t st);
+// dz_uniform != 0 (evenly spaced planes): square staged sizes sum over z by
+// Horner's scheme with the rotation H'_dz (fwd_horner_supported)
 cudaError_t launch_fwd_col(const float2* T, const double* cturn, const double* zlist, float2* Spart, int W,
-                           int H, int z0, int z1, int nchunks, cudaStream_t st);
+                           int H, int z0, int z1, int nchunks, cudaStream_t st, double dz_uniform = 0.0);
+bool fwd_horner_supported(int W, int H);
 int fwd_col_chunks(int W, int H, int Nz);
 cudaError_t launch_plane_col(int inverse, const float2* in, float2* out, int W, int H, float scale,
                              cudaStream_t st);

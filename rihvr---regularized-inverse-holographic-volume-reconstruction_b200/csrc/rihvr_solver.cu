@@ -193,6 +193,7 @@ struct rihvr_ctx {
   double* zlist = nullptr;
   double dz_uniform = 0;  // plane spacing when every z_{k+1} - z_k is the same (FP64), else 0
   int tune_adj_rec = 1;   // adjoint column pass may advance H'_z by the recurrence (needs dz_uniform)
+  int tune_fwd_horner = 1;  // forward column pass may sum over z by Horner's scheme (needs dz_uniform)
   double* partials = nullptr;
   unsigned* nonfinite_d = nullptr;  // count of non-finite hologram samples (rihvr_set_hologram)
   size_t partial_cap = 0;
@@ -374,7 +375,8 @@ int forward_volume(rihvr_ctx* c, int kind, const void* vol) {
   }
   {
     ProfScope ps(c, K_FWD_COL);
-    KL(launch_fwd_col(c->U, c->cturn, c->zlist, c->Spart, c->W, c->H, 0, c->Nz, c->nchunks, c->st));
+    KL(launch_fwd_col(c->U, c->cturn, c->zlist, c->Spart, c->W, c->H, 0, c->Nz, c->nchunks, c->st,
+                      c->tune_fwd_horner ? c->dz_uniform : 0.0));
   }
   ProfScope ps(c, K_PLANE);
   KL(launch_sum_chunks(c->Spart, c->nchunks, c->S, (long long)c->HW, c->st));
@@ -1215,7 +1217,7 @@ struct TuneKey {
   }
 };
 struct TuneVal {
-  int adj_chunks, fwd_chunks, tv_nseg, tv_kernel, adj_rec;
+  int adj_chunks, fwd_chunks, tv_nseg, tv_kernel, adj_rec, fwd_horner;
   double ms;
 };
 std::mutex g_tune_mu;
@@ -1291,25 +1293,33 @@ int autotune_run(rihvr_ctx* c, cudaEvent_t e0, cudaEvent_t e1, TuneVal* out) {
     c->tune_tv_kernel = bk;
     c->tune_tv_nseg = bn;
   }
-  // 3. z-chunks of the forward column pass (with the sum of the partial spectra)
-  int best_fwd = c->nchunks;
+  // 3. the forward column pass: z-sum by Horner's scheme over evenly spaced
+  //    planes or with the transfer function at every plane, and its z-chunks
+  //    (with the sum of the partial spectra)
+  int best_fwd = c->nchunks, best_horner = 0;
   float t_fwd = 1e30f;
-  for (int ch : {c->nchunks, 1, 2, 4, 8, 16}) {
-    if (ch > c->Nz || ch > kMaxFwdChunks) continue;
-    RC(time_min(c, e0, e1, [&]() -> int {
-      KL(launch_fwd_col(c->U, c->cturn, c->zlist, c->Spart, c->W, c->H, 0, c->Nz, ch, c->st));
-      KL(launch_sum_chunks(c->Spart, ch, c->S, (long long)c->HW, c->st));
-      return RIHVR_OK;
-    }, &best));
-    if (best < t_fwd * 0.98f) {
-      t_fwd = best;
-      best_fwd = ch;
+  for (int hor : {1, 0}) {
+    if (hor && (c->dz_uniform == 0 || !fwd_horner_supported(c->W, c->H))) continue;
+    for (int ch : {c->nchunks, 1, 2, 4, 8, 16}) {
+      if (ch > c->Nz || ch > kMaxFwdChunks) continue;
+      RC(time_min(c, e0, e1, [&]() -> int {
+        KL(launch_fwd_col(c->U, c->cturn, c->zlist, c->Spart, c->W, c->H, 0, c->Nz, ch, c->st,
+                          hor ? c->dz_uniform : 0.0));
+        KL(launch_sum_chunks(c->Spart, ch, c->S, (long long)c->HW, c->st));
+        return RIHVR_OK;
+      }, &best));
+      if (best < t_fwd * 0.98f) {
+        t_fwd = best;
+        best_fwd = ch;
+        best_horner = hor;
+      }
     }
   }
   c->nchunks = best_fwd;
+  c->tune_fwd_horner = best_horner;
   c->profiling = prev_profiling;
   *out = TuneVal{c->tune_adj_chunks, c->nchunks, c->tune_tv_nseg, c->tune_tv_kernel, c->tune_adj_rec,
-                 (double)t_adj + (double)t_tv + (double)t_fwd};
+                 c->tune_fwd_horner, (double)t_adj + (double)t_tv + (double)t_fwd};
   return RIHVR_OK;
 }
 
@@ -1318,11 +1328,13 @@ int autotune_run(rihvr_ctx* c, cudaEvent_t e0, cudaEvent_t e1, TuneVal* out) {
 extern "C" {
 
 int rihvr_tuning(const rihvr_ctx* c, int* adj_chunks, int* fwd_chunks, int* tv_runs, int* tv_kernel,
-                 int* adj_recurrence) {
+                 int* adj_recurrence, int* fwd_horner) {
   if (!c) return fail(RIHVR_ERR_INVALID_ARGUMENT, "NULL context");
   if (adj_chunks) *adj_chunks = c->tune_adj_chunks;
   if (adj_recurrence)
     *adj_recurrence = (c->tune_adj_rec && c->dz_uniform != 0 && adj_recurrence_supported(c->W, c->H)) ? 1 : 0;
+  if (fwd_horner)
+    *fwd_horner = (c->tune_fwd_horner && c->dz_uniform != 0 && fwd_horner_supported(c->W, c->H)) ? 1 : 0;
   if (fwd_chunks) *fwd_chunks = c->nchunks;
   if (tv_runs) *tv_runs = c->tune_tv_nseg;
   if (tv_kernel) *tv_kernel = c->tune_tv_kernel;
@@ -1343,6 +1355,7 @@ int rihvr_autotune(rihvr_ctx* c, double* best_ms) {
       c->tune_tv_nseg = it->second.tv_nseg;
       c->tune_tv_kernel = it->second.tv_kernel;
       c->tune_adj_rec = it->second.adj_rec;
+      c->tune_fwd_horner = it->second.fwd_horner;
       c->tuned = true;
       if (best_ms) *best_ms = it->second.ms;
       return RIHVR_OK;

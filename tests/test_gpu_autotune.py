@@ -23,7 +23,7 @@ def test_autotune_keeps_the_solution(rihvr, synthmod, cache_dir):
     (l0, x0, t0), (l1, x1, t1) = runs[0], runs[1]
     # evenly spaced planes at a recurrence size: the untuned adjoint uses the recurrence
     assert t0 == {"adj_chunks": 0, "fwd_chunks": t0["fwd_chunks"], "tv_runs": 0, "tv_kernel": 0,
-                  "adj_recurrence": 1}
+                  "adj_recurrence": 1, "fwd_horner": 1}
     assert t1["tv_kernel"] in (0, 1, 2) and 1 <= t1["fwd_chunks"] <= 16 and t1["adj_recurrence"] in (0, 1)
     assert np.array_equal(l0["backtracks"], l1["backtracks"])
     assert np.array_equal(l0["restarted"], l1["restarted"])
@@ -59,10 +59,11 @@ def test_adjoint_recurrence_only_for_evenly_spaced_planes(rihvr):
         p.start_plane, p.plane_stepsize, p.num_planes = z0, dz, nz
         p.wavelength, p.resolution, p.zero_padding = 0.632, 2.0, 0
         with rihvr.SparseCompressiveHolo(p, side, side) as s:
-            return s.tuning()["adj_recurrence"]
+            t = s.tuning()
+            return t["adj_recurrence"], t["fwd_horner"]
 
-    assert tuned(2500.0, 2.0) == 1
+    assert tuned(2500.0, 2.0) == (1, 1)
     z = np.float32(100.0) + np.arange(6, dtype=np.float32) * np.float32(0.1)
     assert len(set(np.diff(z.astype(np.float64)))) > 1  # uneven in FP64
-    assert tuned(100.0, 0.1) == 0
-    assert tuned(2500.0, 2.0, side=384) == 0  # 48 elements a thread: no recurrence variant
+    assert tuned(100.0, 0.1) == (0, 0)
+    assert tuned(2500.0, 2.0, side=384) == (0, 0)  # 48 elements a thread: neither variant
