@@ -214,10 +214,11 @@ int rihvr_autotune(rihvr_ctx* ctx, double* best_ms);
 
 /* The launch shapes in use: z-chunks of the adjoint and forward column passes,
  * runs per plane of the streaming TV prox and the TV kernel (1 tiled,
- * 2 streaming); 0 means the built-in choice.  adj_recurrence receives 1 when
- * the adjoint column pass advances the transfer function by a recurrence
- * over evenly spaced planes (square planes of side 32 to 1024 except 384 and
- * 768), else 0.  fwd_horner receives 1 when the forward column pass sums over
+ * 2 streaming); 0 means the built-in choice.  adj_recurrence receives the
+ * adjoint column pass's variant for evenly spaced planes (square planes of side
+ * 32 to 1024 except 384, 640 and 768): 0 transfer function evaluated at every
+ * plane, 1 advanced by a recurrence with the inter-stage twiddles regenerated
+ * each plane, 2 the recurrence with the twiddles kept in registers.  fwd_horner receives 1 when the forward column pass sums over
  * evenly spaced planes by Horner's scheme (square planes of side 32 to 512 and
  * 1024), else 0.  Any pointer may be NULL. */
 int rihvr_tuning(const rihvr_ctx* ctx, int* adj_chunks, int* fwd_chunks, int* tv_runs, int* tv_kernel,

@@ -30,11 +30,11 @@ CUDA_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr
 HOST_CXX = shutil.which("g++") or "g++"
 
 LIB_SOURCES = ["rihvr_kernels.cu", "rihvr_solver.cu", "rihvr_params.cpp", "rihvr_noalloc.cu", "rihvr_image.cpp",
-               "rihvr_segment.cu", "rihvr_unet.cu"]
+               "rihvr_segment.cu", "rihvr_unet.cu", "rihvr_unet_tc.cu"]
 CLI_SOURCES = ["sparse_inverse_recon.cpp", "sparse_segmentation.cpp"]
 # executable -> its sources (linked against the library)
 EXECUTABLES = {CLI: ["sparse_inverse_recon.cpp"], SEG_CLI: ["sparse_segmentation.cpp"]}
-HEADERS = ["rihvr_device.cuh", "rihvr_kernels.cuh", "rihvr_image.h"]
+HEADERS = ["rihvr_device.cuh", "rihvr_kernels.cuh", "rihvr_image.h", "rihvr_unet_tc.cuh"]
 
 
 def _mtime(p: str) -> float:

@@ -523,8 +523,13 @@ constexpr int kAdjAnchor = 16;
 // kAdjAnchor planes Y is recomputed exactly from Rs and the FP64 phase table.
 // Lines of up to 32 elements a thread only (the inter-stage twiddles are
 // regenerated each plane to leave registers for Y).
-template <int N, bool TMA>
-__global__ void __launch_bounds__(ColLayout<N>::THREADS, 3)
+//
+// HOIST keeps the inter-stage twiddles in registers as k_adj_col does (fewer
+// instructions a plane, two blocks an SM); without it they are regenerated
+// each plane and three blocks fit.  The autotuner picks one of the two or the
+// direct evaluation.
+template <int N, bool TMA, bool HOIST>
+__global__ void __launch_bounds__(ColLayout<N>::THREADS, HOIST ? 2 : 3)
     k_adj_col_rec(const float2* __restrict__ Rs, const double* __restrict__ cturn, const double* __restrict__ zlist,
                   double dz, float2* __restrict__ U, int z0, int z1, int zpb,
                   const __grid_constant__ CUtensorMap umap) {
@@ -543,6 +548,8 @@ __global__ void __launch_bounds__(ColLayout<N>::THREADS, 3)
   float2* s_d = sm + Lay::SMEM_ELEMS;  // this thread's rotations, [row][CC] (thread-private slots)
   const float2* rs = Rs + (size_t)t * W + x;
   const double* ct = cturn + (size_t)t * W + x;
+  float2 tw[HOIST ? N2 : 1];
+  if constexpr (HOIST) line_twiddles<N, N2, true>(tw, t);
   float2 y[N2];
 #pragma unroll
   for (int n2 = 0; n2 < N2; ++n2) {
@@ -569,7 +576,12 @@ __global__ void __launch_bounds__(ColLayout<N>::THREADS, 3)
 #pragma unroll
     for (int n2 = 0; n2 < N2; ++n2) v[n2] = y[n2];
     reg_fft<N2, true>(v);
-    line_twiddle<N, N2, true>(v, launder_i(t));
+    if constexpr (HOIST) {
+#pragma unroll
+      for (int k = 1; k < N2; ++k) v[k] = cmul(v[k], tw[k]);
+    } else {
+      line_twiddle<N, N2, true>(v, launder_i(t));
+    }
     if (TMA && threadIdx.x == 0) bulk_wait_read_all();
     col_exchange<N, true>(v, sm, c, t);
     if constexpr (TMA) {
@@ -845,15 +857,16 @@ static bool plane_stack_map(CUtensorMap* m, void* base, int n, int nz, int cc, i
 
 template <int N>
 static cudaError_t adj_col_n(const float2* Rs, const double* cturn, const double* zlist, float2* U, int W,
-                             int z0, int z1, cudaStream_t st, int chunks_hint, double dz_uniform) {
+                             int z0, int z1, cudaStream_t st, int chunks_hint, double dz_uniform, int rec_mode) {
   using Lay = ColLayout<N>;
   const int nz = z1 - z0;
   if (nz <= 0) return cudaSuccess;
   const int strips = col_strips<N>(W);
-  // the recurrence variant: evenly spaced planes, lines of <= 32 elements a thread
+  // the recurrence variants: evenly spaced planes, lines of <= 32 elements a
+  // thread; `rec_mode` 1 regenerates the twiddles each plane, 2 keeps them
   constexpr bool kRecOk = kHoistTw<N> && (N % Lay::CC == 0);
-  const bool rec = kRecOk && dz_uniform != 0.0 && !std::getenv("RIHVR_ADJ_NO_RECURRENCE");
-  const int target = (rec ? 12 : 8) * num_sms();
+  const bool rec = kRecOk && dz_uniform != 0.0 && rec_mode != 0;
+  const int target = (rec && rec_mode == 1 ? 12 : 8) * num_sms();
   int chunks = chunks_hint > 0 ? chunks_hint : (target + strips - 1) / strips;
   if (chunks > nz) chunks = nz;
   if (chunks < 1) chunks = 1;
@@ -866,18 +879,14 @@ static cudaError_t adj_col_n(const float2* Rs, const double* cturn, const double
   if constexpr (kRecOk) {
     if (rec) {
       constexpr size_t smem = Lay::SMEM_BYTES + sizeof(float2) * Lay::STRIP_ELEMS;
-      if (tma) {
-        e = allow_smem(k_adj_col_rec<N, true>, smem);
-        if (e != cudaSuccess) return e;
-        k_adj_col_rec<N, true><<<dim3(strips, chunks), Lay::THREADS, smem, st>>>(Rs, cturn, zlist, dz_uniform, U, z0,
-                                                                                  z1, zpb, umap);
-      } else {
-        e = allow_smem(k_adj_col_rec<N, false>, smem);
-        if (e != cudaSuccess) return e;
-        k_adj_col_rec<N, false><<<dim3(strips, chunks), Lay::THREADS, smem, st>>>(Rs, cturn, zlist, dz_uniform, U,
-                                                                                   z0, z1, zpb, umap);
-      }
-      return cudaGetLastError();
+      auto go = [&](auto kern) -> cudaError_t {
+        cudaError_t e2 = allow_smem(kern, smem);
+        if (e2 != cudaSuccess) return e2;
+        kern<<<dim3(strips, chunks), Lay::THREADS, smem, st>>>(Rs, cturn, zlist, dz_uniform, U, z0, z1, zpb, umap);
+        return cudaGetLastError();
+      };
+      if (rec_mode == 2) return tma ? go(k_adj_col_rec<N, true, true>) : go(k_adj_col_rec<N, false, true>);
+      return tma ? go(k_adj_col_rec<N, true, false>) : go(k_adj_col_rec<N, false, false>);
     }
   }
   if (tma) {
@@ -908,12 +917,13 @@ bool adj_recurrence_supported(int W, int H) {
 }
 
 static cudaError_t launch_adj_col_fast(const float2* Rs, const double* cturn, const double* zlist, float2* U, int W,
-                                      int H, int z0, int z1, cudaStream_t st, int chunks_hint, double dz_uniform) {
+                                      int H, int z0, int z1, cudaStream_t st, int chunks_hint, double dz_uniform,
+                                      int rec_mode) {
   if (W != H) return cudaErrorInvalidValue;
   switch (H) {
 #define RIHVR_CASE(NN) \
   case NN:             \
-    return adj_col_n<NN>(Rs, cturn, zlist, U, W, z0, z1, st, chunks_hint, dz_uniform);
+    return adj_col_n<NN>(Rs, cturn, zlist, U, W, z0, z1, st, chunks_hint, dz_uniform, rec_mode);
     RIHVR_FOR_EACH_SIZE(RIHVR_CASE)
 #undef RIHVR_CASE
     default:
@@ -2718,8 +2728,9 @@ cudaError_t launch_rows(int inverse, int in_kind, const void* in, int out_kind, 
 }
 
 cudaError_t launch_adj_col(const float2* Rs, const double* cturn, const double* zlist, float2* U, int W, int H,
-                           int z0, int z1, cudaStream_t st, int chunks_hint, double dz_uniform) {
-  if (fast_square(W, H)) return launch_adj_col_fast(Rs, cturn, zlist, U, W, H, z0, z1, st, chunks_hint, dz_uniform);
+                           int z0, int z1, cudaStream_t st, int chunks_hint, double dz_uniform, int rec_mode) {
+  if (fast_square(W, H))
+    return launch_adj_col_fast(Rs, cturn, zlist, U, W, H, z0, z1, st, chunks_hint, dz_uniform, rec_mode);
   const int nz = z1 - z0;
   if (nz <= 0) return cudaSuccess;
   GPlan p;

@@ -73,9 +73,12 @@ size_t max_partial_blocks(int W, int H, int Nz);
 bool adj_recurrence_supported(int W, int H);
 // dz_uniform != 0: the planes are evenly spaced by dz_uniform (z_{k+1} - z_k,
 // exact in FP64), which lets the square fast sizes advance the transfer
-// function by a recurrence; 0 takes the direct evaluation at every plane.
+// function by a recurrence (rec_mode 1: twiddles regenerated each plane, three
+// blocks an SM; 2: twiddles kept in registers, two blocks an SM); rec_mode 0
+// or dz_uniform 0 takes the direct evaluation at every plane.
 cudaError_t launch_adj_col(const float2* Rs, const double* cturn, const double* zlist, float2* U, int W,
-                           int H, int z0, int z1, cudaStream_t st, int chunks_hint = 0, double dz_uniform = 0.0);
+                           int H, int z0, int z1, cudaStream_t st, int chunks_hint = 0, double dz_uniform = 0.0,
+                           int rec_mode = 0);
 cudaError_t launch_rows(int inverse, int in_kind, const void* in, int out_kind, void* out, int W,
                         long long nlines, float scale, cudaStream_t st);
 // dz_uniform != 0 (evenly spaced planes): square staged sizes sum over z by

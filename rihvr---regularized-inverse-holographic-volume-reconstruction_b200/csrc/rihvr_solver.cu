@@ -16,6 +16,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <initializer_list>
 #include <map>
 #include <mutex>
 #include <tuple>
@@ -192,8 +193,13 @@ struct rihvr_ctx {
   double* cturn = nullptr;
   double* zlist = nullptr;
   double dz_uniform = 0;  // plane spacing when every z_{k+1} - z_k is the same (FP64), else 0
-  int tune_adj_rec = 1;   // adjoint column pass may advance H'_z by the recurrence (needs dz_uniform)
-  int tune_fwd_horner = 1;  // forward column pass may sum over z by Horner's scheme (needs dz_uniform)
+  // column-pass variants for evenly spaced planes (need dz_uniform): the
+  // adjoint's transfer function by recurrence (1: twiddles regenerated each
+  // plane, 2: twiddles kept) or direct (0); the forward's z-sum by Horner's
+  // scheme (1) or direct (0).  Autotuned; RIHVR_ADJ_COL and RIHVR_FWD_COL
+  // select one by name.
+  int tune_adj_rec = 0;
+  int tune_fwd_horner = 1;
   double* partials = nullptr;
   unsigned* nonfinite_d = nullptr;  // count of non-finite hologram samples (rihvr_set_hologram)
   size_t partial_cap = 0;
@@ -340,6 +346,19 @@ struct ProfScope {
 // --- plane-level helpers ----------------------------------------------------
 
 // Rs = FFT2(r) / (W H)  (SparseGradient::reconstruct, sparse_gradient.cu:47-75)
+// A variant chosen by name in the environment variable `var` (its index in
+// `names`), else `tuned`.
+int env_variant(const char* var, std::initializer_list<const char*> names, int tuned) {
+  const char* v = std::getenv(var);
+  if (!v) return tuned;
+  int i = 0;
+  for (const char* n : names) {
+    if (std::strcmp(v, n) == 0) return i;
+    ++i;
+  }
+  return tuned;
+}
+
 int residual_spectrum(rihvr_ctx* c) {
   ProfScope ps(c, K_PLANE);
   KL(launch_rows(0, ELEM_R32, c->r, ELEM_C32, c->pc1, c->W, c->H, 1.0f, c->st));
@@ -357,8 +376,9 @@ int reduce_into(rihvr_ctx* c, int nblocks, int slot) {
 int adjoint_volume(rihvr_ctx* c) {
   {
     ProfScope ps(c, K_ADJ_COL);
+    const int rec = env_variant("RIHVR_ADJ_COL", {"direct", "recurrence", "recurrence_hoisted"}, c->tune_adj_rec);
     KL(launch_adj_col(c->Rs, c->cturn, c->zlist, c->U, c->W, c->H, 0, c->Nz, c->st, c->tune_adj_chunks,
-                      c->tune_adj_rec ? c->dz_uniform : 0.0));
+                      rec ? c->dz_uniform : 0.0, rec));
   }
   {
     ProfScope ps(c, K_ADJ_ROW);
@@ -375,8 +395,9 @@ int forward_volume(rihvr_ctx* c, int kind, const void* vol) {
   }
   {
     ProfScope ps(c, K_FWD_COL);
+    const int hor = env_variant("RIHVR_FWD_COL", {"direct", "horner"}, c->tune_fwd_horner);
     KL(launch_fwd_col(c->U, c->cturn, c->zlist, c->Spart, c->W, c->H, 0, c->Nz, c->nchunks, c->st,
-                      c->tune_fwd_horner ? c->dz_uniform : 0.0));
+                      hor ? c->dz_uniform : 0.0));
   }
   ProfScope ps(c, K_PLANE);
   KL(launch_sum_chunks(c->Spart, c->nchunks, c->S, (long long)c->HW, c->st));
@@ -1247,15 +1268,15 @@ int autotune_run(rihvr_ctx* c, cudaEvent_t e0, cudaEvent_t e1, TuneVal* out) {
   float best;
   // 1. the adjoint column pass: transfer function by recurrence over evenly
   //    spaced planes or evaluated at every plane, and its z-chunks
-  int best_adj = 0, best_rec = c->dz_uniform != 0 ? 1 : 0;
+  int best_adj = 0, best_rec = 0;
   float t_adj = 1e30f;
-  for (int rec : {1, 0}) {
+  for (int rec : {0, 2, 1}) {
     if (rec && (c->dz_uniform == 0 || !adj_recurrence_supported(c->W, c->H))) continue;
     for (int ch : {0, 2, 4, 8, 16, 32}) {
       if (ch > c->Nz) continue;
       RC(time_min(c, e0, e1, [&]() -> int {
         KL(launch_adj_col(c->Rs, c->cturn, c->zlist, c->U, c->W, c->H, 0, c->Nz, c->st, ch,
-                          rec ? c->dz_uniform : 0.0));
+                          rec ? c->dz_uniform : 0.0, rec));
         return RIHVR_OK;
       }, &best));
       if (best < t_adj * 0.98f) {
@@ -1332,7 +1353,7 @@ int rihvr_tuning(const rihvr_ctx* c, int* adj_chunks, int* fwd_chunks, int* tv_r
   if (!c) return fail(RIHVR_ERR_INVALID_ARGUMENT, "NULL context");
   if (adj_chunks) *adj_chunks = c->tune_adj_chunks;
   if (adj_recurrence)
-    *adj_recurrence = (c->tune_adj_rec && c->dz_uniform != 0 && adj_recurrence_supported(c->W, c->H)) ? 1 : 0;
+    *adj_recurrence = (c->dz_uniform != 0 && adj_recurrence_supported(c->W, c->H)) ? c->tune_adj_rec : 0;
   if (fwd_horner)
     *fwd_horner = (c->tune_fwd_horner && c->dz_uniform != 0 && fwd_horner_supported(c->W, c->H)) ? 1 : 0;
   if (fwd_chunks) *fwd_chunks = c->nchunks;

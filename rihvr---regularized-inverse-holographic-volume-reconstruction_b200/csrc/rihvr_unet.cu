@@ -17,8 +17,11 @@
 //   output x0 = g * alpha * xbp (alpha a learned scalar)
 // Loss: sum |x0 - x*|^2 / sum |x*|^2 against the plain-FISTA solution x*.
 //
-// The 3x3x3 convolutions are implicit GEMMs on the tensor cores
-// (mma.sync m16n8k16, BF16 operands, FP32 accumulation): a block computes 64
+// The 3x3x3 convolutions are implicit GEMMs on the tensor cores.  Layers
+// whose width is a multiple of 128 run on the 5th-generation tensor cores
+// (tcgen05.mma with accumulators in tensor memory, rihvr_unet_tc.cu); the
+// others on the warp-level instruction (mma.sync m16n8k16, BF16 operands,
+// FP32 accumulation): a block computes 64
 // output voxels x all output channels; the K loop runs over the 27 taps and
 // 16-channel slices, staging a 64 x 16 activation tile (zero outside the
 // volume, converted to BF16) and a 16 x Cout weight tile in shared memory.
@@ -32,6 +35,7 @@
 #include <cmath>
 #include <cstdint>
 #include <new>
+#include <cstdlib>
 #include <cstring>
 #include <random>
 #include <string>
@@ -39,6 +43,7 @@
 
 #include "../../include/rihvr.h"
 #include "rihvr_kernels.cuh"
+#include "rihvr_unet_tc.cuh"
 
 namespace rihvr {
 namespace unet {
@@ -221,9 +226,21 @@ cudaError_t conv3_launch(const float* X, int Cin, const __nv_bfloat16* Wt, int C
   return cudaGetLastError();
 }
 
-// output channels co0 .. co0 + Cn - 1 (Cn 16, 32, 48 or 64)
+// the tcgen05 path is used where it applies unless RIHVR_UNET_MMA=sync
+bool use_tcgen05() {
+  static const bool on = [] {
+    const char* e = std::getenv("RIHVR_UNET_MMA");
+    return !(e && std::strcmp(e, "sync") == 0);
+  }();
+  return on;
+}
+
+// output channels co0 .. co0 + Cn - 1 (Cn 16, 32, 48 or 64); `err` receives 1
+// if a tcgen05 launch's bounded wait ran out
 cudaError_t conv3(const float* X, int Cin, const __nv_bfloat16* Wt, int Cout, int co0, int Cn, const float* bias,
-                  float* Y, Vol v, int relu, int mirror, cudaStream_t st) {
+                  float* Y, Vol v, int relu, int mirror, int* err, cudaStream_t st) {
+  if (use_tcgen05() && conv3_tc_supported(v.W, Cin, Cn))
+    return conv3_tc(X, Cin, Wt, Cout, co0, Cn, bias, Y, v.D, v.H, v.W, relu, mirror, err, st);
   switch (Cn) {
     case 16: return conv3_launch<2, 4>(X, Cin, Wt, Cout, co0, bias, Y, v, relu, mirror, st);
     case 32: return conv3_launch<4, 4>(X, Cin, Wt, Cout, co0, bias, Y, v, relu, mirror, st);
@@ -582,6 +599,7 @@ struct rihvr_unet {
   float *B1a = nullptr, *B1b = nullptr, *S1 = nullptr, *C1 = nullptr, *P1 = nullptr;
   float *D2a = nullptr, *D2b = nullptr, *P2 = nullptr;
   double* sums = nullptr;   // [0] sum |xbp|^2, [1] sum |x*|^2, [2] loss
+  int* tc_err = nullptr;    // set by a tcgen05 convolution whose bounded wait ran out
   float* rms = nullptr;
   float2* x0tmp = nullptr;  // prediction during training
   cudaStream_t st = nullptr;
@@ -607,7 +625,7 @@ int ualloc(rihvr_unet* u, T** p, size_t count) {
 int conv_fwd(rihvr_unet* u, int li, const float* X, float* Y) {
   const Conv& L = u->layers[li];
   const Vol v = u->lv[L.level];
-  UCK(conv3(X, L.cin, u->wb + u->wb_off[li], L.cout, 0, L.cout, u->w + L.b_off, Y, v, 1, 0, u->st));
+  UCK(conv3(X, L.cin, u->wb + u->wb_off[li], L.cout, 0, L.cout, u->w + L.b_off, Y, v, 1, 0, u->tc_err, u->st));
   ++u->launches;
   return RIHVR_OK;
 }
@@ -626,7 +644,7 @@ int conv_back(rihvr_unet* u, int li, const float* X, float* dY, float* dX) {
   // the data gradient: output channels of the transposed weights in windows of 64
   for (int co0 = 0; dX && co0 < L.cin; co0 += 64) {
     UCK(conv3(dY, L.cout, u->wt + u->wb_off[li], L.cin, co0, std::min(64, L.cin - co0), nullptr, dX, v, 0, 1,
-              u->st));
+              u->tc_err, u->st));
     ++u->launches;
   }
   UCK(cudaGetLastError());
@@ -701,6 +719,18 @@ int check_net(const rihvr_unet* u) {
   return RIHVR_OK;
 }
 
+// after a synchronisation: did a tcgen05 convolution give up waiting?  (the
+// flag is cleared for the next call)
+int check_tc(rihvr_unet* u) {
+  int e = 0;
+  UCK(cudaMemcpy(&e, u->tc_err, sizeof(int), cudaMemcpyDeviceToHost));
+  if (e) {
+    UCK(cudaMemset(u->tc_err, 0, sizeof(int)));
+    return unet_fail(RIHVR_ERR_CUDA, "a tensor-core convolution timed out waiting for its MMAs");
+  }
+  return RIHVR_OK;
+}
+
 }  // namespace
 
 namespace rihvr {
@@ -709,7 +739,10 @@ namespace rihvr {
 int unet_predict_on(rihvr_unet* u, const float2* xbp, float scale, float2* x0, cudaStream_t st) {
   if (!u || !xbp || !x0) return unet_fail(RIHVR_ERR_INVALID_ARGUMENT, "NULL argument");
   u->st = st;
-  return forward(u, xbp, nullptr, x0, scale);
+  const int rc = forward(u, xbp, nullptr, x0, scale);
+  if (rc != RIHVR_OK) return rc;
+  UCK(cudaStreamSynchronize(st));
+  return check_tc(u);
 }
 void unet_dims(const rihvr_unet* u, int* D, int* H, int* W) {
   *D = u->lv[0].D;
@@ -778,6 +811,7 @@ int rihvr_unet_create(int depth, int height, int width, unsigned long long seed,
   A(&u->P2, n2 * 32);
   A(&u->rms, 1);
   if (rc == RIHVR_OK) rc = ualloc(u, &u->sums, 3);
+  if (rc == RIHVR_OK) rc = ualloc(u, &u->tc_err, 1);
   if (rc == RIHVR_OK) rc = ualloc(u, &u->x0tmp, (size_t)n0);
   if (rc != RIHVR_OK) return bail(rc);
   // He-normal weights (fan-in 27 x real input channels; only channel 0 of the
@@ -798,7 +832,8 @@ int rihvr_unet_create(int depth, int height, int width, unsigned long long seed,
   h[u->head_off + 17] = 1.f;
   if (cudaMemcpy(u->w, h.data(), sizeof(float) * u->nparam, cudaMemcpyHostToDevice) != cudaSuccess ||
       cudaMemset(u->m, 0, sizeof(float) * u->nparam) != cudaSuccess ||
-      cudaMemset(u->s, 0, sizeof(float) * u->nparam) != cudaSuccess)
+      cudaMemset(u->s, 0, sizeof(float) * u->nparam) != cudaSuccess ||
+      cudaMemset(u->tc_err, 0, sizeof(int)) != cudaSuccess)
     return bail(unet_fail(RIHVR_ERR_CUDA, "initial copies failed"));
   u->st = nullptr;
   if ((rc = refresh_bf16(u)) != RIHVR_OK) return bail(rc);
@@ -840,7 +875,7 @@ int rihvr_unet_predict(rihvr_unet* u, const float* xbp, float* x0) {
   const int rc = forward(u, reinterpret_cast<const float2*>(xbp), nullptr, reinterpret_cast<float2*>(x0));
   if (rc != RIHVR_OK) return rc;
   UCK(cudaStreamSynchronize(nullptr));
-  return RIHVR_OK;
+  return check_tc(u);
 }
 
 int rihvr_unet_gradients(rihvr_unet* u, const float* xbp, const float* xstar, float* grad_out, double* loss) {
@@ -855,7 +890,7 @@ int rihvr_unet_gradients(rihvr_unet* u, const float* xbp, const float* xstar, fl
   double h[3];
   UCK(cudaMemcpy(h, u->sums, sizeof(h), cudaMemcpyDeviceToHost));
   if (loss) *loss = h[2];
-  return RIHVR_OK;
+  return check_tc(u);
 }
 
 int rihvr_unet_train_step(rihvr_unet* u, const float* xbp, const float* xstar, float lr, double* loss) {

@@ -21,10 +21,10 @@ def test_autotune_keeps_the_solution(rihvr, synthmod, cache_dir):
             s.iterate(10)
             runs[tune] = (s.iterations(), s.getVolume(), tun)
     (l0, x0, t0), (l1, x1, t1) = runs[0], runs[1]
-    # evenly spaced planes at a recurrence size: the untuned adjoint uses the recurrence
+    # evenly spaced planes: the untuned adjoint evaluates directly, the forward uses Horner's scheme
     assert t0 == {"adj_chunks": 0, "fwd_chunks": t0["fwd_chunks"], "tv_runs": 0, "tv_kernel": 0,
-                  "adj_recurrence": 1, "fwd_horner": 1}
-    assert t1["tv_kernel"] in (0, 1, 2) and 1 <= t1["fwd_chunks"] <= 16 and t1["adj_recurrence"] in (0, 1)
+                  "adj_recurrence": 0, "fwd_horner": 1}
+    assert t1["tv_kernel"] in (0, 1, 2) and 1 <= t1["fwd_chunks"] <= 16 and t1["adj_recurrence"] in (0, 1, 2)
     assert np.array_equal(l0["backtracks"], l1["backtracks"])
     assert np.array_equal(l0["restarted"], l1["restarted"])
     assert np.max(np.abs(l0["f_x"] - l1["f_x"]) / np.abs(l0["f_x"])) < 1e-5
@@ -51,9 +51,10 @@ def test_autotune_cache(rihvr, synthmod, cache_dir):
     assert second < first
 
 
-def test_adjoint_recurrence_only_for_evenly_spaced_planes(rihvr):
-    """The recurrence needs z_{k+1} - z_k equal for every k (in FP64, from the
-    float plane list): dz = 0.1 gives uneven float positions, dz = 2 even ones."""
+def test_column_variants_only_for_evenly_spaced_planes(rihvr):
+    """The recurrence and Horner variants need z_{k+1} - z_k equal for every k
+    (in FP64, from the float plane list): dz = 0.1 gives uneven float
+    positions, dz = 2 even ones."""
     def tuned(z0, dz, side=128, nz=6):
         p = rihvr.default_params()
         p.start_plane, p.plane_stepsize, p.num_planes = z0, dz, nz
@@ -62,7 +63,7 @@ def test_adjoint_recurrence_only_for_evenly_spaced_planes(rihvr):
             t = s.tuning()
             return t["adj_recurrence"], t["fwd_horner"]
 
-    assert tuned(2500.0, 2.0) == (1, 1)
+    assert tuned(2500.0, 2.0) == (0, 1)  # untuned: direct adjoint, Horner forward
     z = np.float32(100.0) + np.arange(6, dtype=np.float32) * np.float32(0.1)
     assert len(set(np.diff(z.astype(np.float64)))) > 1  # uneven in FP64
     assert tuned(100.0, 0.1) == (0, 0)

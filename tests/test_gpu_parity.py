@@ -105,6 +105,10 @@ def test_prox_step_matches_oracle(rihvr, mode, faithful):
     assert rel(out, ref) < TOL_F32
     assert abs(sums[0] - rsums[0]) < 1e-4 * max(abs(rsums[0]), 1e-6 * abs(rsums[1]) + 1e-12)
     assert abs(sums[1] - rsums[1]) < 1e-4 * abs(rsums[1])
+    # the restart statistic against y0 = x: with the reference's weights (faithful) it is
+    # a weighted -|p - x|^2, bounded by twice the plain one
+    assert abs(sums[2] - rsums[2]) < 2e-4 * abs(rsums[1])
+    assert rsums[2] < 0
 
 
 @pytest.mark.parametrize("side,nz,n_tv", [(32, 3, 5), (128, 3, 1), (128, 2, 2), (384, 2, 3), (256, 2, 6),
@@ -268,3 +272,26 @@ def test_errors_are_status_codes(rihvr):
         s.setHologram(np.zeros((64, 64), np.float32))
         s.iterate(2)  # a zero hologram is a valid (trivial) problem
         assert np.all(s.getVolume() == 0)
+
+
+@pytest.mark.parametrize("side,nz", [(1024, 20), (512, 37), (256, 50), (64, 19)])
+@pytest.mark.parametrize("adj,fwd", [("direct", "direct"), ("recurrence", "horner"),
+                                     ("recurrence_hoisted", "horner")])
+def test_column_pass_variants_match_oracle(rihvr, monkeypatch, side, nz, adj, fwd):
+    """Every column-pass variant for evenly spaced planes (selected by name,
+    as the autotuner would pick them) against the FP64 oracle: the adjoint's
+    recurrence (re-anchored every 16 planes) and the forward's Horner sum, on
+    enough planes to cross several anchors and z-chunks."""
+    monkeypatch.setenv("RIHVR_ADJ_COL", adj)
+    monkeypatch.setenv("RIHVR_FWD_COL", fwd)
+    p = make(rihvr, side, nz)
+    p.start_plane, p.plane_stepsize = 2500.0, 2.0  # evenly spaced in float
+    rng = np.random.default_rng(side * 3 + nz)
+    vol = rand_volume(rng, nz, side)
+    r = rng.standard_normal((side, side)).astype(np.float32)
+    with rihvr.SparseCompressiveHolo(p, side, side) as s:
+        d = s.forward(vol)
+        g = s.adjoint(r)
+    op = oparams(rihvr, p, side)
+    assert rel(d, O.forward(op, vol.astype(np.complex128))) < TOL_F32
+    assert rel(g, O.adjoint(op, r.astype(np.float64))) < TOL_F32
