@@ -121,6 +121,9 @@ typedef struct rihvr_file_params {
   int segment_min_area;            /* 5009 */
   double segment_min_intensity;    /* 5010 */
   int segment_close_size;          /* 5011 */
+  int background_start;            /* 1003 (-1: unset) */
+  int background_end;              /* 1004 (-1: unset) */
+  int use_median_background;       /* 7006 */
 } rihvr_file_params;
 
 typedef struct rihvr_ctx rihvr_ctx;
@@ -162,6 +165,45 @@ int rihvr_debug_fail_allocations_after(int n);
  * reference only prints a warning per bad sample, check_isnan_mdata,
  * sparse_compressive_holo.cu:9-35, and goes on to a solve full of NaNs). */
 int rihvr_set_hologram(rihvr_ctx* ctx, const float* b, int is_device);
+
+/* The driver's preprocessing (main_sparse_inverse.cu:106-124, as
+ * rihvr_preprocess) on the GPU, straight into the context's hologram: the raw
+ * width x height camera frame travels as stored, `bits` per sample (8:
+ * uint8, 16: uint16, 32: floats holding 8/16-bit sample values), and so does
+ * `background` (same type and size; used when files->remove_background).  The
+ * crop comes from `files` (NULL: whole frame, no background) and the padding
+ * from the context's zero_padding; cropped size + 2 * padding must equal the
+ * context's width and height.  The result equals rihvr_preprocess's bit for
+ * bit.  RIHVR_ERR_INVALID_DATA for a frame of zero mean or float samples that
+ * are not integers in [0, 65535]; the context then keeps its state. */
+int rihvr_set_hologram_frame(rihvr_ctx* ctx, const void* frame, int bits, int width, int height,
+                             const void* background, const rihvr_file_params* files, int is_device);
+/* The context's hologram b (height x width floats), as set. */
+int rihvr_get_hologram(rihvr_ctx* ctx, float* out, int is_device);
+
+/* Background generation (src/core/main_create_background.cu), on the GPU.
+ * `frames`: count frames of width x height samples, `bits` as for
+ * rihvr_set_hologram_frame, one after another, host or device memory
+ * (is_device, which also applies to the outputs).  Backgrounds are floats on
+ * the samples' scale (0-255 for 8-bit frames).
+ * rihvr_background_mean: HoloSequence::useBackgroundSubtraction
+ * (holo_sequence.cu:309-447): background = (sum of the frames in order, FP32)
+ * * fl(1/count); stats (may be NULL) = alpha, beta, minimum, average as
+ * background_stats.txt lists them: alpha = mean of the frames' means of
+ * frame - background minus 5 times the mean of their standard deviations,
+ * beta = 255 / (10 * mean standard deviation), minimum = 0, average = mean of
+ * the background.  The caller picks the frames (the reference's selection is
+ * in the create-background program). */
+int rihvr_background_mean(const void* frames, int bits, int width, int height, int count, int is_device,
+                          float* background, double* stats);
+/* median_background_calc (main_create_background.cu:103-193): count >= 5
+ * frames in, count - 2 backgrounds out (background_0000 .. of the frames'
+ * numbering), each the per-pixel median of the five frames the reference's
+ * five-frame stack holds at that point (rihvr_background_median5_frames
+ * lists them, 5 per background). */
+int rihvr_background_median5(const void* frames, int bits, int width, int height, int count, int is_device,
+                             float* backgrounds);
+int rihvr_background_median5_frames(int count, int* frame_indices);
 
 /* SparseCompressiveHolo::inverseReconstruct(Hologram, mode) (:173-633): runs
  * num_inverse_iterations from x = 0.  final_objective (may be NULL) receives
@@ -304,12 +346,16 @@ int rihvr_prox_step(rihvr_ctx* ctx, const float* x, const float* residual, doubl
 /* Image I/O and preprocessing of the hologram frame (the OpenCV parts of
  * Hologram on the reconstruction path).
  * rihvr_read_image: Hologram::read (hologram.cu:139-199) - 8/16-bit grayscale
- * or RGB TIFF (uncompressed, PackBits, LZW, horizontal predictor) or binary
- * PGM; values as stored.  Call with pixels == NULL to get the size, then with
- * a width*height buffer and the same width/height. */
+ * or RGB TIFF (uncompressed, PackBits, LZW, horizontal predictor), 8/16-bit
+ * grayscale or 8-bit RGB PNG, or binary PGM; values as stored.  Call with
+ * pixels == NULL to get the size, then with a width*height buffer and the same
+ * width/height. */
 int rihvr_read_image(const char* path, float* pixels, int* width, int* height, int* bits);
 /* cv::imwrite of an 8-bit grayscale image: baseline uncompressed TIFF. */
 int rihvr_write_tiff8(const char* path, const unsigned char* pixels, int width, int height);
+/* cv::imwrite of an 8-bit grayscale image as PNG (the backgrounds'
+ * format, main_create_background.cu:154, 249). */
+int rihvr_write_png8(const char* path, const unsigned char* pixels, int width, int height);
 /* The preprocessing of main_sparse_inverse.cu:106-124: /255 (hologram.cu:
  * 401-439); I/mean - 1 (:332-358) or, when files->remove_background, (I - B) /
  * max(sqrt(B), 0.1) (:1365-1432); crop to files' ROI (:768-887); zero padding

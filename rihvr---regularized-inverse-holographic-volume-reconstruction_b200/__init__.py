@@ -91,6 +91,9 @@ class FileParams(ctypes.Structure):
         ("segment_min_area", ctypes.c_int),
         ("segment_min_intensity", ctypes.c_double),
         ("segment_close_size", ctypes.c_int),
+        ("background_start", ctypes.c_int),
+        ("background_end", ctypes.c_int),
+        ("use_median_background", ctypes.c_int),
     ]
 
 
@@ -135,7 +138,9 @@ EXPORTED = (
     "rihvr_iteration_count", "rihvr_objective", "rihvr_get_iterations", "rihvr_get_plane", "rihvr_get_volume",
     "rihvr_get_estimate", "rihvr_get_residual", "rihvr_forward", "rihvr_adjoint", "rihvr_prox_step",
     "rihvr_adjoint_noalloc", "rihvr_sparsity", "rihvr_initial_estimate", "rihvr_lipschitz",
-    "rihvr_read_image", "rihvr_write_tiff8", "rihvr_preprocess", "rihvr_io_error",
+    "rihvr_set_hologram_frame", "rihvr_get_hologram", "rihvr_background_mean", "rihvr_background_median5",
+    "rihvr_background_median5_frames",
+    "rihvr_read_image", "rihvr_write_tiff8", "rihvr_write_png8", "rihvr_preprocess", "rihvr_io_error",
     "rihvr_segment_params_default", "rihvr_segment", "rihvr_segment_intensity", "rihvr_write_centroids",
     "rihvr_unet_create", "rihvr_unet_destroy", "rihvr_unet_param_count", "rihvr_unet_get_params",
     "rihvr_unet_set_params", "rihvr_unet_predict", "rihvr_unet_gradients", "rihvr_unet_train_step",
@@ -178,6 +183,11 @@ def load_library(path: str = LIB_PATH):
     L.rihvr_debug_fail_allocations_after.argtypes = [ip]
     L.rihvr_destroy.restype = None
     L.rihvr_set_hologram.argtypes = [vp, vp, ip]
+    L.rihvr_set_hologram_frame.argtypes = [vp, vp, ip, ip, ip, vp, P(FileParams), ip]
+    L.rihvr_get_hologram.argtypes = [vp, vp, ip]
+    L.rihvr_background_mean.argtypes = [vp, ip, ip, ip, ip, ip, vp, P(ctypes.c_double)]
+    L.rihvr_background_median5.argtypes = [vp, ip, ip, ip, ip, ip, vp]
+    L.rihvr_background_median5_frames.argtypes = [ip, P(ctypes.c_int)]
     L.rihvr_reconstruct.argtypes = [vp, P(ctypes.c_double)]
     L.rihvr_reconstruct_batch.argtypes = [P(vp), ip, P(vp), ip, P(ctypes.c_double), P(ctypes.c_int)]
     L.rihvr_set_batch_mode.argtypes = [ip]
@@ -204,6 +214,7 @@ def load_library(path: str = LIB_PATH):
     L.rihvr_lipschitz.argtypes = [vp, ip, ctypes.c_ulonglong, P(ctypes.c_double), vp]
     L.rihvr_read_image.argtypes = [ctypes.c_char_p, vp, P(ctypes.c_int), P(ctypes.c_int), P(ctypes.c_int)]
     L.rihvr_write_tiff8.argtypes = [ctypes.c_char_p, vp, ip, ip]
+    L.rihvr_write_png8.argtypes = [ctypes.c_char_p, vp, ip, ip]
     L.rihvr_preprocess.argtypes = [vp, ip, ip, vp, P(FileParams), ip, vp, P(ctypes.c_int), P(ctypes.c_int)]
     L.rihvr_io_error.restype = ctypes.c_char_p
     L.rihvr_segment_params_default.argtypes = [P(SegmentParams)]
@@ -475,6 +486,79 @@ def write_tiff8(path: str, img: np.ndarray):
               "rihvr_write_tiff8")
 
 
+def write_png8(path: str, img: np.ndarray):
+    img = np.ascontiguousarray(img, dtype=np.uint8)
+    _io_check(load_library().rihvr_write_png8(path.encode(), _ptr(img), img.shape[1], img.shape[0]),
+              "rihvr_write_png8")
+
+
+_SAMPLE_BITS = {np.dtype(np.uint8): 8, np.dtype(np.uint16): 16, np.dtype(np.float32): 32}
+
+
+def _frames_arg(frames):
+    """(pointer, bits, is_device, keep-alive) for camera frames: a numpy array
+    of uint8, uint16 or float32 samples, or a CUDA tensor of those types."""
+    try:
+        import torch
+    except ImportError:  # pragma: no cover - torch is part of the image
+        torch = None
+    if torch is not None and isinstance(frames, torch.Tensor):
+        t = frames.contiguous()
+        bits = {torch.uint8: 8, torch.uint16: 16, torch.float32: 32}.get(t.dtype)
+        if bits is None or not t.is_cuda:
+            raise ValueError("frames must be a CUDA tensor of uint8, uint16 or float32")
+        return ctypes.c_void_p(t.data_ptr()), bits, 1, t
+    a = np.asarray(frames)
+    if a.dtype not in _SAMPLE_BITS:
+        a = a.astype(np.float32)
+    a = np.ascontiguousarray(a)
+    return _ptr(a), _SAMPLE_BITS[a.dtype], 0, a
+
+
+def median5_frames(count: int) -> np.ndarray:
+    """The five frames behind each median background (count - 2 rows)."""
+    out = np.empty((count - 2, 5), np.int32)
+    _check(load_library().rihvr_background_median5_frames(int(count), out.ctypes.data_as(
+        ctypes.POINTER(ctypes.c_int))), "rihvr_background_median5_frames")
+    return out
+
+
+def background_mean(frames):
+    """Mean background of frames [count, H, W] (HoloSequence::
+    useBackgroundSubtraction) on the GPU: (background float32 [H, W],
+    stats dict alpha, beta, minimum, average)."""
+    ptr, bits, dev, keep = _frames_arg(frames)
+    k, h, w = keep.shape
+    stats = (ctypes.c_double * 4)()
+    if dev:
+        import torch
+
+        out = torch.empty((h, w), dtype=torch.float32, device=keep.device)
+        optr = ctypes.c_void_p(out.data_ptr())
+    else:
+        out = np.empty((h, w), np.float32)
+        optr = _ptr(out)
+    _check(load_library().rihvr_background_mean(ptr, bits, w, h, k, dev, optr, stats), "rihvr_background_mean")
+    return out, dict(zip(("alpha", "beta", "minimum", "average"), stats[:]))
+
+
+def background_median5(frames):
+    """Running median-of-five backgrounds (median_background_calc) of frames
+    [count, H, W] on the GPU: float32 [count - 2, H, W]."""
+    ptr, bits, dev, keep = _frames_arg(frames)
+    k, h, w = keep.shape
+    if dev:
+        import torch
+
+        out = torch.empty((max(k - 2, 0), h, w), dtype=torch.float32, device=keep.device)
+        optr = ctypes.c_void_p(out.data_ptr())
+    else:
+        out = np.empty((max(k - 2, 0), h, w), np.float32)
+        optr = _ptr(out)
+    _check(load_library().rihvr_background_median5(ptr, bits, w, h, k, dev, optr), "rihvr_background_median5")
+    return out
+
+
 def preprocess(holo: np.ndarray, zero_padding: int, background: np.ndarray | None = None,
                files: FileParams | None = None) -> np.ndarray:
     """The reference preprocessing (rescale, normalise or background divide,
@@ -552,6 +636,32 @@ class SparseCompressiveHolo:
         if b.shape != (self.height, self.width):
             raise ValueError(f"hologram shape {b.shape} != {(self.height, self.width)}")
         _check(self._L.rihvr_set_hologram(self._h, _ptr(b), 0), "rihvr_set_hologram")
+
+    def setHologramFrame(self, frame, background=None, files: FileParams | None = None):
+        """The driver's preprocessing on the GPU (rihvr_set_hologram_frame):
+        `frame` is the raw camera frame [H0, W0] (uint8, uint16 or float32
+        samples; numpy or CUDA tensor), `background` one of the same kind;
+        crop from `files`, padding from the parameters."""
+        ptr, bits, dev, keep = _frames_arg(frame)
+        bptr, bkeep = None, None
+        if background is not None:
+            bptr, bbits, bdev, bkeep = _frames_arg(background)
+            if (bbits, bdev, bkeep.shape) != (bits, dev, keep.shape):
+                raise ValueError("background must match the frame's type, place and shape")
+            if files is None:
+                files = FileParams()
+                files.remove_background = 1
+                files.roi_size = -1
+                files.roi_x = files.roi_y = -1
+        h0, w0 = keep.shape
+        _check(self._L.rihvr_set_hologram_frame(self._h, ptr, bits, w0, h0, bptr,
+                                                ctypes.byref(files) if files is not None else None, dev),
+               "rihvr_set_hologram_frame")
+
+    def getHologram(self) -> np.ndarray:
+        out = np.empty((self.height, self.width), np.float32)
+        _check(self._L.rihvr_get_hologram(self._h, _ptr(out), 0), "rihvr_get_hologram")
+        return out
 
     def setInitialVolume(self, x0: np.ndarray):
         """Warm start (rihvr_set_initial_volume): continue FISTA from x0

@@ -1,5 +1,6 @@
 """In-tree build of the native library (``librihvr_b200.so``) and the
-``sparse-inverse-recon`` command-line driver, for sm_100a only.
+``sparse-inverse-recon``, ``sparse-segmentation`` and ``create-background``
+command-line programs, for sm_100a only.
 
     python build.py            # incremental
     python build.py --force    # rebuild everything
@@ -19,6 +20,7 @@ BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "librihvr_b200.so")
 CLI = os.path.join(HERE, "sparse-inverse-recon")
 SEG_CLI = os.path.join(HERE, "sparse-segmentation")
+BG_CLI = os.path.join(HERE, "create-background")
 INCLUDE = os.path.abspath(os.path.join(HERE, "..", "include"))
 
 NVCC = os.environ.get("NVCC", shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc")
@@ -30,11 +32,12 @@ CUDA_FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr
 HOST_CXX = shutil.which("g++") or "g++"
 
 LIB_SOURCES = ["rihvr_kernels.cu", "rihvr_solver.cu", "rihvr_params.cpp", "rihvr_noalloc.cu", "rihvr_image.cpp",
-               "rihvr_segment.cu", "rihvr_unet.cu", "rihvr_unet_tc.cu"]
-CLI_SOURCES = ["sparse_inverse_recon.cpp", "sparse_segmentation.cpp"]
+               "rihvr_segment.cu", "rihvr_unet.cu", "rihvr_unet_tc.cu", "rihvr_frame.cu"]
+CLI_SOURCES = ["sparse_inverse_recon.cpp", "sparse_segmentation.cpp", "create_background.cpp"]
 # executable -> its sources (linked against the library)
-EXECUTABLES = {CLI: ["sparse_inverse_recon.cpp"], SEG_CLI: ["sparse_segmentation.cpp"]}
-HEADERS = ["rihvr_device.cuh", "rihvr_kernels.cuh", "rihvr_image.h", "rihvr_unet_tc.cuh"]
+EXECUTABLES = {CLI: ["sparse_inverse_recon.cpp"], SEG_CLI: ["sparse_segmentation.cpp"],
+               BG_CLI: ["create_background.cpp"]}
+HEADERS = ["rihvr_device.cuh", "rihvr_kernels.cuh", "rihvr_image.h", "rihvr_unet_tc.cuh", "rihvr_frame.cuh"]
 
 
 def _mtime(p: str) -> float:
@@ -69,7 +72,7 @@ def build(force: bool = False, verbose: bool = False) -> str:
         objs = dict(zip(srcs, ex.map(lambda s: _compile(s, force, verbose), srcs)))
     lib_objs = [objs[s] for s in LIB_SOURCES]
     if force or _mtime(LIB) < max(_mtime(o) for o in lib_objs):
-        cmd = [NVCC, "-ccbin", HOST_CXX] + ARCH + ["-shared", "-o", LIB] + lib_objs + ["-lcudart"]
+        cmd = [NVCC, "-ccbin", HOST_CXX] + ARCH + ["-shared", "-o", LIB] + lib_objs + ["-lcudart", "-lz"]
         if verbose:
             print(" ".join(cmd), flush=True)
         subprocess.run(cmd, check=True)

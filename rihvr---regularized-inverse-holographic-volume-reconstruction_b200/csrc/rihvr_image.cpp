@@ -3,8 +3,12 @@
 
 #include "rihvr.h"
 
+#include <zlib.h>
+
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <fstream>
 #include <iterator>
@@ -19,6 +23,11 @@ bool read_file(const std::string& path, std::vector<uint8_t>& buf) {
   buf.assign(std::istreambuf_iterator<char>(f), std::istreambuf_iterator<char>());
   return true;
 }
+
+// cvtColor(BGR2GRAY) of 8-bit samples: 0.299 R + 0.587 G + 0.114 B in 15-bit
+// fixed point, rounded (the OpenCV 4 coefficients; equal to cv2 4.13 on all
+// 2^24 colours)
+int gray8(int r, int g, int b) { return (r * 9798 + g * 19235 + b * 3735 + (1 << 14)) >> 15; }
 
 struct Tiff {
   const std::vector<uint8_t>& d;
@@ -205,8 +214,8 @@ bool read_tiff(const std::vector<uint8_t>& buf, Image& img, std::string& err) {
       s[c] = bps == 8 ? raw[k] : (t.le ? (raw[2 * k] | (raw[2 * k + 1] << 8)) : ((raw[2 * k] << 8) | raw[2 * k + 1]));
     }
     double g = s[0];
-    if (spp == 3) {  // imread gives BGR; BGR2GRAY weights on R, G, B
-      g = bps == 8 ? (double)(((int)s[0] * 4899 + (int)s[1] * 9617 + (int)s[2] * 1868 + (1 << 13)) >> 14)
+    if (spp == 3) {  // imread gives BGR; cvtColor(BGR2GRAY) weights R, G, B
+      g = bps == 8 ? (double)gray8((int)s[0], (int)s[1], (int)s[2])
                    : std::nearbyint(0.299 * s[0] + 0.587 * s[1] + 0.114 * s[2]);
     }
     if (photo == 0) g = maxv - g;
@@ -242,6 +251,94 @@ bool read_pnm(const std::vector<uint8_t>& buf, Image& img, std::string& err) {
   return true;
 }
 
+uint32_t be32(const uint8_t* p) { return ((uint32_t)p[0] << 24) | ((uint32_t)p[1] << 16) | ((uint32_t)p[2] << 8) | p[3]; }
+
+// PNG (ISO/IEC 15948): non-interlaced 8/16-bit grayscale or 8-bit RGB, as
+// Hologram::read accepts after imread (hologram.cu:146-183: CV_8U, CV_16U,
+// and CV_8UC3 converted to gray).
+bool read_png(const std::vector<uint8_t>& buf, Image& img, std::string& err) {
+  size_t p = 8;
+  uint32_t W = 0, H = 0;
+  int depth = 0, color = -1, interlace = 0;
+  std::vector<uint8_t> z;
+  bool end = false;
+  while (!end) {
+    if (p + 12 > buf.size()) return err = "truncated PNG", false;
+    const uint32_t len = be32(&buf[p]);
+    const uint8_t* type = &buf[p + 4];
+    const uint8_t* data = &buf[p + 8];
+    if (len > buf.size() - p - 12) return err = "truncated PNG chunk", false;
+    if (crc32(crc32(0L, Z_NULL, 0), type, len + 4) != be32(data + len)) return err = "PNG chunk CRC mismatch", false;
+    if (!std::memcmp(type, "IHDR", 4)) {
+      if (len != 13) return err = "bad PNG header", false;
+      W = be32(data);
+      H = be32(data + 4);
+      depth = data[8];
+      color = data[9];
+      interlace = data[12];
+    } else if (!std::memcmp(type, "IDAT", 4)) {
+      z.insert(z.end(), data, data + len);
+    } else if (!std::memcmp(type, "IEND", 4)) {
+      end = true;
+    }
+    p += 12 + (size_t)len;
+  }
+  if (!W || !H) return err = "missing PNG header", false;
+  if (interlace) return err = "interlaced PNG is not supported", false;
+  int ch;
+  if (color == 0 && (depth == 8 || depth == 16)) ch = 1;
+  else if (color == 2 && depth == 8) ch = 3;
+  else return err = "unsupported PNG type (color " + std::to_string(color) + ", depth " + std::to_string(depth) +
+                    "): 8/16-bit grayscale or 8-bit RGB", false;
+  const size_t bpp = (size_t)ch * (depth / 8), row = (size_t)W * bpp;
+  std::vector<uint8_t> raw((row + 1) * H);
+  uLongf got = (uLongf)raw.size();
+  if (uncompress(raw.data(), &got, z.data(), (uLong)z.size()) != Z_OK || got != raw.size())
+    return err = "corrupt PNG image data", false;
+  // undo the per-row filters in place (filter byte, then the row)
+  std::vector<uint8_t> px(row * H);
+  for (size_t y = 0; y < H; ++y) {
+    const int f = raw[y * (row + 1)];
+    const uint8_t* s = &raw[y * (row + 1) + 1];
+    uint8_t* o = &px[y * row];
+    const uint8_t* up = y ? &px[(y - 1) * row] : nullptr;
+    for (size_t i = 0; i < row; ++i) {
+      const int a = i >= bpp ? o[i - bpp] : 0, b = up ? up[i] : 0, c = (up && i >= bpp) ? up[i - bpp] : 0;
+      int v;
+      switch (f) {
+        case 0: v = s[i]; break;
+        case 1: v = s[i] + a; break;
+        case 2: v = s[i] + b; break;
+        case 3: v = s[i] + ((a + b) >> 1); break;
+        case 4: {
+          const int q = a + b - c, pa = std::abs(q - a), pb = std::abs(q - b), pc = std::abs(q - c);
+          v = s[i] + ((pa <= pb && pa <= pc) ? a : (pb <= pc ? b : c));
+          break;
+        }
+        default: return err = "bad PNG filter type", false;
+      }
+      o[i] = (uint8_t)v;
+    }
+  }
+  img.width = (int)W;
+  img.height = (int)H;
+  img.bits = depth;
+  img.pixels.resize((size_t)W * H);
+  for (size_t i = 0; i < (size_t)W * H; ++i) {
+    if (ch == 3) {  // R, G, B in the file
+      const uint8_t* q = &px[3 * i];
+      img.pixels[i] = (float)gray8(q[0], q[1], q[2]);
+    } else {
+      img.pixels[i] = depth == 8 ? px[i] : (float)((px[2 * i] << 8) | px[2 * i + 1]);
+    }
+  }
+  return true;
+}
+
+void put_be32(std::vector<uint8_t>& b, uint32_t v) {
+  for (int k = 3; k >= 0; --k) b.push_back((v >> (8 * k)) & 0xff);
+}
+
 void put16(std::vector<uint8_t>& b, uint16_t v) {
   b.push_back(v & 0xff);
   b.push_back(v >> 8);
@@ -256,7 +353,41 @@ bool read_image(const std::string& path, Image& out, std::string& err) {
   std::vector<uint8_t> buf;
   if (!read_file(path, buf)) return err = "cannot read " + path, false;
   if (buf.size() >= 2 && buf[0] == 'P' && buf[1] == '5') return read_pnm(buf, out, err);
+  static const uint8_t kPng[8] = {0x89, 'P', 'N', 'G', '\r', '\n', 0x1a, '\n'};
+  if (buf.size() >= 8 && !std::memcmp(buf.data(), kPng, 8)) return read_png(buf, out, err);
   return read_tiff(buf, out, err);
+}
+
+bool write_png8(const std::string& path, const uint8_t* pixels, int width, int height, std::string& err) {
+  const size_t row = (size_t)width;
+  std::vector<uint8_t> raw((row + 1) * height);
+  for (int y = 0; y < height; ++y) {
+    raw[y * (row + 1)] = 0;  // no filter
+    std::memcpy(&raw[y * (row + 1) + 1], pixels + (size_t)y * row, row);
+  }
+  uLongf zn = compressBound((uLong)raw.size());
+  std::vector<uint8_t> z(zn);
+  if (compress2(z.data(), &zn, raw.data(), (uLong)raw.size(), 1) != Z_OK) return err = "PNG compression failed", false;
+  z.resize(zn);
+  std::vector<uint8_t> b = {0x89, 'P', 'N', 'G', '\r', '\n', 0x1a, '\n'};
+  auto chunk = [&](const char* type, const std::vector<uint8_t>& data) {
+    put_be32(b, (uint32_t)data.size());
+    const size_t t0 = b.size();
+    b.insert(b.end(), type, type + 4);
+    b.insert(b.end(), data.begin(), data.end());
+    put_be32(b, (uint32_t)crc32(crc32(0L, Z_NULL, 0), &b[t0], (uInt)(data.size() + 4)));
+  };
+  std::vector<uint8_t> ihdr;
+  put_be32(ihdr, (uint32_t)width);
+  put_be32(ihdr, (uint32_t)height);
+  ihdr.insert(ihdr.end(), {8, 0, 0, 0, 0});  // 8-bit grayscale, deflate, no interlace
+  chunk("IHDR", ihdr);
+  chunk("IDAT", z);
+  chunk("IEND", {});
+  std::ofstream f(path, std::ios::binary);
+  if (!f) return err = "cannot open " + path, false;
+  f.write(reinterpret_cast<const char*>(b.data()), (std::streamsize)b.size());
+  return (bool)f || (err = "write failed: " + path, false);
 }
 
 bool write_tiff8(const std::string& path, const uint8_t* pixels, int width, int height, std::string& err) {
@@ -291,6 +422,24 @@ bool write_tiff8(const std::string& path, const uint8_t* pixels, int width, int 
   return (bool)f || (err = "write failed: " + path, false);
 }
 
+bool exact_unit_mean(const float* v, size_t n, double* mean) {
+  unsigned __int128 acc = 0;
+  for (size_t i = 0; i < n; ++i) {
+    const float x = v[i];
+    if (!(x >= 0.f && x <= 65535.f && x == std::floor(x))) return false;
+    const float q = x / 255.0f;
+    acc += (unsigned long long)(q * 2147483648.0f);  // q * 2^31, an integer below 2^40
+  }
+  *mean = unit_mean_from_sum((unsigned long long)acc, (unsigned long long)(acc >> 64), n);
+  return true;
+}
+
+double unit_mean_from_sum(unsigned long long lo, unsigned long long hi, size_t n) {
+  const unsigned __int128 s = ((unsigned __int128)hi << 64) | lo;
+  // one rounding to double, exact scaling by 2^-31, one rounding of the quotient
+  return std::ldexp((double)s, -31) / (double)n;
+}
+
 uint8_t to_u8(double v) {
   if (!(v > 0)) return 0;  // NaN and negatives
   if (v >= 255) return 255;
@@ -301,8 +450,8 @@ bool preprocess(const Image& holo, const Image* bg, const Preprocess& pp, std::v
                 int& height, std::string& err) {
   const int W0 = holo.width, H0 = holo.height;
   const size_t n0 = (size_t)W0 * H0;
-  // float32 arithmetic throughout (OpenCV's CV_32F matrices); the mean is
-  // accumulated in double as cv::mean does
+  // float32 arithmetic throughout (OpenCV's CV_32F matrices); the mean in
+  // double as cv::mean gives it
   std::vector<float> f(n0);
   for (size_t i = 0; i < n0; ++i) f[i] = holo.pixels[i] / 255.0f;  // rescale (hologram.cu:401-439), 16-bit too
   if (pp.remove_background) {
@@ -315,38 +464,20 @@ bool preprocess(const Image& holo, const Image* bg, const Preprocess& pp, std::v
       f[i] = (f[i] - B) / sb;
     }
   } else {
-    // I / mean - 1  (hologram.cu:332-358)
+    // I / mean - 1  (hologram.cu:332-358).  cv::mean sums in double; here the
+    // sum is exact (then rounded once) for camera samples, so that the device
+    // path gives the same mean; other float inputs are summed in order.
     double m = 0;
-    for (size_t i = 0; i < n0; ++i) m += f[i];
-    m /= (double)n0;
+    if (!exact_unit_mean(holo.pixels.data(), n0, &m)) {
+      for (size_t i = 0; i < n0; ++i) m += f[i];
+      m /= (double)n0;
+    }
     if (!(m != 0)) return err = "hologram mean is zero", false;
     const float mf = (float)m;
     for (size_t i = 0; i < n0; ++i) f[i] = f[i] / mf - 1.0f;
   }
-  // crop (hologram.cu:768-887): a rectangle, or a square around a centre,
-  // clamped into the image; pixels outside the image read as zero
-  int rx, ry, rw, rh;
-  if (pp.roi_rect_w > 0 && pp.roi_rect_h > 0) {
-    rx = pp.roi_rect_x;
-    ry = pp.roi_rect_y;
-    rw = pp.roi_rect_w;
-    rh = pp.roi_rect_h;
-  } else if (pp.roi_size >= 1) {
-    const int size = pp.roi_size;
-    rx = pp.roi_x - size / 2;
-    ry = pp.roi_y - size / 2;
-    rw = rh = size;
-    if (rx < 0) rx = 0;
-    if (ry < 0) ry = 0;
-    if (rx + size > W0) rx = W0 - size;
-    if (ry + size > H0) ry = H0 - size;
-    if (W0 < size) { rx = 0; rw = W0; }
-    if (H0 < size) { ry = 0; rh = H0; }
-  } else {
-    rx = ry = 0;
-    rw = W0;
-    rh = H0;
-  }
+  const CropRect cr = crop_rect(pp, W0, H0);
+  const int rx = cr.x, ry = cr.y, rw = cr.w, rh = cr.h;
   const int p = pp.zero_padding;
   width = rw + 2 * p;
   height = rh + 2 * p;
@@ -388,6 +519,11 @@ int rihvr_read_image(const char* path, float* pixels, int* width, int* height, i
 int rihvr_write_tiff8(const char* path, const unsigned char* pixels, int width, int height) {
   if (!path || !pixels || width <= 0 || height <= 0) return RIHVR_ERR_INVALID_ARGUMENT;
   return rihvr_io::write_tiff8(path, pixels, width, height, g_io_error) ? RIHVR_OK : RIHVR_ERR_BAD_FILENAME;
+}
+
+int rihvr_write_png8(const char* path, const unsigned char* pixels, int width, int height) {
+  if (!path || !pixels || width <= 0 || height <= 0) return RIHVR_ERR_INVALID_ARGUMENT;
+  return rihvr_io::write_png8(path, pixels, width, height, g_io_error) ? RIHVR_OK : RIHVR_ERR_BAD_FILENAME;
 }
 
 int rihvr_preprocess(const float* holo, int width, int height, const float* background,

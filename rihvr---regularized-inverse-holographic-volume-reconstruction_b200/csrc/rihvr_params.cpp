@@ -61,6 +61,7 @@ int rihvr_read_param_file(const char* path, rihvr_params* p, rihvr_file_params* 
   f->segment_min_area = 2;                  // segmentation defaults (holo_ui.cpp:44-46)
   f->segment_min_intensity = 1.0;
   f->segment_close_size = 3;
+  f->background_start = f->background_end = -1;  // holo_ui.cpp:28-29
   bool set_full_filename = false;
   char buff[8192];
   char description[8192];
@@ -80,7 +81,8 @@ int rihvr_read_param_file(const char* path, rihvr_params* p, rihvr_file_params* 
     switch (id) {
       case 1001: f->image_count = (int)value; break;
       case 1002: f->start_image = (int)value; break;
-      case 1003: case 1004: break;  // background frame range (background generation, out of scope)
+      case 1003: f->background_start = (int)value; break;
+      case 1004: f->background_end = (int)value; break;
       case 2001: copy_str(f->image_filename, char_value); set_full_filename = true; break;
       case 2002: copy_str(f->image_path, char_value); break;
       case 2003: copy_str(f->image_formatted_name, char_value); break;
@@ -114,7 +116,8 @@ int rihvr_read_param_file(const char* path, rihvr_params* p, rihvr_file_params* 
       case 6005: p->num_tv_iterations = (int)value; break;
       case 7001: flag(&f->output_planes); break;
       case 7005: flag(&f->output_steps); break;
-      case 7002: case 7003: case 7004: case 7006: break;  // other pipelines' switches
+      case 7006: flag(&f->use_median_background); break;
+      case 7002: case 7003: case 7004: break;  // other pipelines' switches
       default:
         // the reference prints and stops reading (:475-480); report it instead
         g_param_error = std::string("unknown or unsupported parameter line: ") + buff;

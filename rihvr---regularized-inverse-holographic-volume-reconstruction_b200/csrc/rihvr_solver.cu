@@ -27,6 +27,7 @@
 #include <vector>
 
 #include "../../include/rihvr.h"
+#include "rihvr_frame.cuh"
 #include "rihvr_kernels.cuh"
 
 using namespace rihvr;
@@ -228,6 +229,7 @@ struct rihvr_ctx {
   DevRec* dlog_h = nullptr;          // pinned
   bool warm = false;                 // one iteration ran eagerly (attributes, tables)
   SegWorkspace* seg_ws = nullptr;    // segmentation buffers, grown on first use
+  FrameWorkspace* frame_ws = nullptr;  // raw-frame uploads (rihvr_set_hologram_frame), grown on first use
   // launch shapes chosen by the autotuner (0 = built-in choice)
   int tune_adj_chunks = 0, tune_tv_nseg = 0, tune_tv_kernel = 0;
   bool tuned = false;
@@ -1188,6 +1190,7 @@ void rihvr_destroy(rihvr_ctx* c) {
   if (c->st) cudaStreamSynchronize(c->st);
   drop_graphs(c);
   if (c->seg_ws) seg_workspace_destroy(c->seg_ws);
+  frame_workspace_free(c->frame_ws);
   for (void* p : c->allocs) cudaFree(p);
   if (c->sums_h) cudaFreeHost(c->sums_h);
   if (c->scal_h) cudaFreeHost(c->scal_h);
@@ -1223,6 +1226,27 @@ int rihvr_set_hologram(rihvr_ctx* c, const float* b, int is_device) {
   RC(state_reset(c));
   if (c->p.autotune && !c->tuned) RC(rihvr_autotune(c, nullptr));
   return RIHVR_OK;
+}
+
+int rihvr_set_hologram_frame(rihvr_ctx* c, const void* frame, int bits, int width, int height,
+                             const void* background, const rihvr_file_params* files, int is_device) {
+  if (!c || !frame) return fail(RIHVR_ERR_INVALID_ARGUMENT, "NULL argument");
+  const float* staged = nullptr;
+  // the frame is preprocessed into the workspace; the context's hologram and
+  // state change only when that succeeded
+  RC(frame_to_hologram(&c->frame_ws, frame, bits, width, height, background, files, c->p.zero_padding, c->W, c->H,
+                       is_device, c->st, &staged, &c->launches));
+  RC(copy_in(c, c->b, staged, sizeof(float) * c->HW, 1));
+  c->have_holo = true;
+  RC(state_reset(c));
+  if (c->p.autotune && !c->tuned) RC(rihvr_autotune(c, nullptr));
+  return RIHVR_OK;
+}
+
+int rihvr_get_hologram(rihvr_ctx* c, float* out, int is_device) {
+  if (!c || !out) return fail(RIHVR_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (!c->have_holo) return fail(RIHVR_ERR_MISSING_DATA, "no hologram set");
+  return copy_out(c, out, c->b, sizeof(float) * c->HW, is_device);
 }
 
 }  // extern "C"

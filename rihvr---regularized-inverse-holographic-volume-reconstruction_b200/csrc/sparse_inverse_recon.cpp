@@ -242,8 +242,9 @@ int run(int argc, char** argv) {
   std::string err;
   if (!rihvr_io::read_image(read_name, holo, err)) return fail_msg(err), -1;
   if (files.remove_background && !rihvr_io::read_image(files.background_filename, bg, err)) return fail_msg(err), -1;
+  // the raw frame goes to the GPU as stored and is preprocessed there
+  // (rihvr_set_hologram_frame); the size follows from the crop and padding
   rihvr_io::Preprocess pp;
-  pp.remove_background = files.remove_background;
   pp.roi_x = files.roi_x;
   pp.roi_y = files.roi_y;
   pp.roi_size = files.roi_size;
@@ -251,12 +252,11 @@ int run(int argc, char** argv) {
   pp.roi_rect_y = files.roi_rect_y;
   pp.roi_rect_w = files.roi_rect_w;
   pp.roi_rect_h = files.roi_rect_h;
-  pp.zero_padding = p.zero_padding;
-  std::vector<float> b;
-  int W, H;
-  if (!rihvr_io::preprocess(holo, files.remove_background ? &bg : nullptr, pp, b, W, H, err)) return fail_msg(err), -1;
+  if (files.remove_background && (bg.width != holo.width || bg.height != holo.height))
+    return fail_msg("background must match the hologram size"), -1;
+  const rihvr_io::CropRect cr = rihvr_io::crop_rect(pp, holo.width, holo.height);
+  const int W = cr.w + 2 * p.zero_padding, H = cr.h + 2 * p.zero_padding;
   const std::string out = files.output_path;
-  if (!write_minmax(out + "/enh.tif", b, W, H)) return -1;
 
   rihvr_ctx* ctx = nullptr;
   rc = rihvr_create(&p, W, H, &ctx);
@@ -265,7 +265,29 @@ int run(int argc, char** argv) {
     rihvr_destroy(ctx);
     return code;
   };
-  if (rihvr_set_hologram(ctx, b.data(), 0) != RIHVR_OK) return fail_msg(rihvr_last_error()), done(-1);
+  {
+    // 8- and 16-bit frames travel as such; anything else as float samples
+    const int bits = (holo.bits == 8 || holo.bits == 16) && (!files.remove_background || bg.bits == holo.bits)
+                         ? holo.bits : 32;
+    std::vector<unsigned char> fb, bb;
+    auto pack = [&](const rihvr_io::Image& im, std::vector<unsigned char>& dst) {
+      const size_t n = im.pixels.size();
+      dst.resize(n * (bits / 8));
+      for (size_t i = 0; i < n; ++i) {
+        if (bits == 8) dst[i] = (unsigned char)im.pixels[i];
+        else if (bits == 16) reinterpret_cast<unsigned short*>(dst.data())[i] = (unsigned short)im.pixels[i];
+        else reinterpret_cast<float*>(dst.data())[i] = im.pixels[i];
+      }
+    };
+    pack(holo, fb);
+    if (files.remove_background) pack(bg, bb);
+    if (rihvr_set_hologram_frame(ctx, fb.data(), bits, holo.width, holo.height,
+                                 files.remove_background ? bb.data() : nullptr, &files, 0) != RIHVR_OK)
+      return fail_msg(rihvr_last_error()), done(-1);
+  }
+  std::vector<float> b((size_t)W * H);
+  if (rihvr_get_hologram(ctx, b.data(), 0) != RIHVR_OK) return fail_msg(rihvr_last_error()), done(-1);
+  if (!write_minmax(out + "/enh.tif", b, W, H)) return done(-1);
   // calcInitialObjectiveFunction's images (sparse_compressive_holo.cu:2901-2966), limits +-0.25
   std::vector<float> est(b.size()), res(b.size());
   if (rihvr_initial_estimate(ctx, est.data(), 0) != RIHVR_OK) return fail_msg(rihvr_last_error()), done(-1);
