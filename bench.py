@@ -13,6 +13,7 @@ frame (preprocessed on the GPU) to host results.
     python bench.py --config series    # uneven time series, batched vs frame by frame
     python bench.py --config segment   # particle segmentation of the reconstructed volume
     python bench.py --config warmstart --frames 16   # learned warm start against FISTA from zero
+    python bench.py --config warmstart4              # the same at 512x512x200 on 256 held-out holograms
 """
 from __future__ import annotations
 
@@ -459,6 +460,58 @@ def run_warmstart(args):
     return 0
 
 
+def run_warmstart4(args):
+    """The learned warm start on its specified configuration, 512x512x200
+    (500-3000 disks and rods, noise 0.005-0.03): the network trained at
+    128x128x32 (fully convolutional, same optics) applied to held-out
+    holograms of that size; iterations and device time to plain FISTA's
+    100-iteration objective within 1e-3, with and without it, and the
+    network's inference time at that size.  Prints one JSON line."""
+    import torch
+
+    torch.cuda.set_device(0)
+    rihvr = importlib.import_module(PKG)
+    ws = importlib.import_module(PKG + ".warmstart")
+    n = args.frames if args.frames else 256
+    seeds = np.arange(400_000, 400_000 + n)
+    S, Z = ws.C4_SIZE, ws.C4_PLANES
+    with rihvr.UNet(Z, S, S) as net:
+        net.load(ws.WEIGHTS)
+        t0 = time.perf_counter()
+        rows = ws.evaluate(net, seeds, size=S, planes=Z, sampler=ws.config4_sample, device="cuda")
+        eval_s = time.perf_counter() - t0
+        cfg = ws.config4_sample(int(seeds[0]))
+        synth = importlib.import_module(PKG + ".synth")
+        _, b = synth.make_hologram(cfg, device="cuda")
+        with rihvr.SparseCompressiveHolo(rihvr.params_from_config(cfg, record_objective=0), S, S) as s:
+            s.setHologram(b)
+            xbp = torch.from_numpy(s.backpropagate()).cuda()
+        for _ in range(3):
+            net.predict(xbp)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(args.steps):
+            net.predict(xbp)
+        e1.record()
+        e1.synchronize()
+        infer_ms = e0.elapsed_time(e1) / args.steps
+    s_ = ws.summary(rows)
+    vox = Z * S * S
+    flops = 0
+    for cin, cout, lvl in [(16, 16, 0), (16, 16, 0), (16, 32, 1), (32, 32, 1), (32, 64, 2), (64, 64, 2),
+                           (96, 32, 1), (32, 32, 1), (48, 16, 0), (16, 16, 0)]:
+        flops += 2 * 27 * cin * cout * vox // (8 ** lvl)
+    line = {"metric": "iterations and device ms to plain FISTA's 100-iteration objective (1e-3), warm start vs zero",
+            "value": s_["mean_iters_warm"], "unit": "iterations", "higher_is_better": False, "n_gpus": 1,
+            "data": "synthetic", "config": {"workload": f"warmstart_{S}x{S}x{Z}", "holograms": len(rows),
+                                             "weights": os.path.basename(ws.WEIGHTS)},
+            "summary": s_, "inference_ms": infer_ms, "inference_tflops": flops / (infer_ms * 1e-3) / 1e12,
+            "conv_flops": flops, "eval_s": eval_s, "rows": rows}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_ours(args):
     ws, rank, local = dist_env()
     import torch
@@ -607,9 +660,10 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="c2", choices=["c2", "c1", "c5", "series", "segment", "warmstart"])
+    ap.add_argument("--config", default="c2", choices=["c2", "c1", "c5", "series", "segment", "warmstart", "warmstart4"])
     ap.add_argument("--frames", type=int, default=0,
-                    help="frames of the uneven series (--config series, default 64) or of the warm-start set (default 16)")
+                    help="frames of the uneven series (--config series, default 64) or of the warm-start set "
+                         "(default 16; 256 for warmstart4)")
     ap.add_argument("--storage", default="f32", choices=["f32", "bf16", "f16"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--nz", type=int, default=0, help="override the plane count (profiling cases)")
@@ -628,6 +682,8 @@ def main():
         return run_segment(args)
     if args.config == "warmstart":
         return run_warmstart(args)
+    if args.config == "warmstart4":
+        return run_warmstart4(args)
     return run_ours(args)
 
 

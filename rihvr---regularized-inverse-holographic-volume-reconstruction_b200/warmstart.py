@@ -57,6 +57,24 @@ def sample_config(seed: int, size: int = SIZE, planes: int = PLANES, iterations:
         noise_sigma=float(rng.uniform(0.005, 0.03)), seed=seed)
 
 
+# The configuration the warm start is specified on: 512 x 512 x 200 voxels
+# with the same optics, 500-3000 particles (half disks of radius 1-4 px, half
+# rods 10-60 px long), camera noise sigma 0.005-0.03.
+C4_SIZE, C4_PLANES = 512, 200
+
+
+def config4_sample(seed: int, size: int = C4_SIZE, planes: int = C4_PLANES, iterations: int = 100):
+    synth = _synth()
+    rng = np.random.default_rng(seed + 2_000_003)
+    n = int(rng.integers(500, 3001))
+    return synth.HoloConfig(
+        name=f"warmstart_c4_{size}x{size}x{planes}_s{seed}", width=size, height=size, zero_padding=0,
+        num_planes=planes, start_plane=1000.0, plane_stepsize=2.0, resolution=1.1, wavelength=0.632,
+        regularization_param=0.15, regularization_TV_param=0.1, num_inverse_iterations=iterations,
+        num_tv_iterations=5, n_disks=n // 2, disk_radius=(1.0, 4.0), n_rods=n - n // 2, rod_length=(10.0, 60.0),
+        rod_width=2.0, noise_sigma=float(rng.uniform(0.005, 0.03)), seed=seed)
+
+
 def make_set(seeds, size: int = SIZE, planes: int = PLANES, iterations: int = 100, log=None):
     """[(b, xbp, x*)] with xbp and x* as CUDA complex64 tensors."""
     import torch
@@ -99,23 +117,27 @@ def _iters_to(f, target, tol=1e-3):
     return int(hit[0]) + 1 if len(hit) else None
 
 
-def evaluate(net, seeds, size: int = SIZE, planes: int = PLANES, iterations: int = 100, tol: float = 1e-3):
+def evaluate(net, seeds, size: int = SIZE, planes: int = PLANES, iterations: int = 100, tol: float = 1e-3,
+             sampler=None, device=None):
     """Per held-out hologram: plain FISTA's final objective (the target), the
     iterations plain FISTA and the warm start need to come within tol of it,
     and the device time of both solves to that point (the warm start's
-    including the network)."""
+    including the network).  `sampler(seed, size, planes, iterations)` makes
+    the holograms' configurations (sample_config by default); `device`
+    synthesises them there."""
     import torch
 
     rihvr = _pkg()
     synth = _synth()
-    cfg0 = sample_config(int(seeds[0]), size, planes, iterations)
+    sampler = sampler or sample_config
+    cfg0 = sampler(int(seeds[0]), size, planes, iterations)
     rows = []
     rec = rihvr.params_from_config(cfg0, record_objective=1)
     fast = rihvr.params_from_config(cfg0, record_objective=0)
     with rihvr.SparseCompressiveHolo(rec, size, size) as s, rihvr.SparseCompressiveHolo(fast, size, size) as t:
         for sd in seeds:
-            cfg = sample_config(int(sd), size, planes, iterations)
-            _, b = synth.make_hologram(cfg)
+            cfg = sampler(int(sd), size, planes, iterations)
+            _, b = synth.make_hologram(cfg, device=device)
             s.setHologram(b)
             s.iterate(iterations)
             fp = s.iterations()["f_x"]
