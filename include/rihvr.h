@@ -468,6 +468,12 @@ int rihvr_unet_gradients(rihvr_unet* net, const float* xbp, const float* xstar, 
 /* one Adam step (beta 0.9 / 0.999) on that loss */
 int rihvr_unet_train_step(rihvr_unet* net, const float* xbp, const float* xstar, float lr, double* loss);
 long long rihvr_unet_launch_count(const rihvr_unet* net);
+/* Activation precision rihvr_unet_predict (and rihvr_warm_start) use at the
+ * network's size: 16 when every level's width is a multiple of 128 (widths
+ * that are multiples of 512) - BF16 activations between tcgen05
+ * convolutions fed by TMA, the head fused into the last one - else 32 (FP32
+ * activations, the training path).  RIHVR_UNET_MMA=sync forces 32. */
+int rihvr_unet_activation_bits(rihvr_unet* net);
 /* xbp = t A^H b of the context's hologram (t its initial step); leaves the
  * solve reset to x = 0. */
 int rihvr_backpropagate(rihvr_ctx* ctx, float* xbp_out, int is_device);

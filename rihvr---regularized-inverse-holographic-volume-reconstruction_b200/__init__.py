@@ -144,7 +144,7 @@ EXPORTED = (
     "rihvr_segment_params_default", "rihvr_segment", "rihvr_segment_intensity", "rihvr_write_centroids",
     "rihvr_unet_create", "rihvr_unet_destroy", "rihvr_unet_param_count", "rihvr_unet_get_params",
     "rihvr_unet_set_params", "rihvr_unet_predict", "rihvr_unet_gradients", "rihvr_unet_train_step",
-    "rihvr_unet_launch_count", "rihvr_backpropagate", "rihvr_warm_start",
+    "rihvr_unet_launch_count", "rihvr_unet_activation_bits", "rihvr_backpropagate", "rihvr_warm_start",
     "rihvr_set_profiling", "rihvr_kernel_times", "rihvr_get_stream", "rihvr_launch_count", "rihvr_device_bytes",
     "rihvr_status_string", "rihvr_last_error",
 )
@@ -234,6 +234,7 @@ def load_library(path: str = LIB_PATH):
     L.rihvr_unet_train_step.argtypes = [vp, vp, vp, ctypes.c_float, P(ctypes.c_double)]
     L.rihvr_unet_launch_count.argtypes = [vp]
     L.rihvr_unet_launch_count.restype = ctypes.c_longlong
+    L.rihvr_unet_activation_bits.argtypes = [vp]
     L.rihvr_backpropagate.argtypes = [vp, vp, ip]
     L.rihvr_warm_start.argtypes = [vp, vp]
     L.rihvr_initial_estimate.argtypes = [vp, vp, ip]
@@ -397,6 +398,11 @@ class UNet:
         if p.size != self.param_count():
             raise ValueError(f"{p.size} parameters, the network has {self.param_count()}")
         _check(self._L.rihvr_unet_set_params(self._h, _ptr(p)), "rihvr_unet_set_params")
+
+    def activation_bits(self) -> int:
+        """16 when predict runs with BF16 activations (tcgen05 at every
+        level), 32 on the FP32 path."""
+        return int(self._L.rihvr_unet_activation_bits(self._h))
 
     def predict(self, xbp):
         import torch

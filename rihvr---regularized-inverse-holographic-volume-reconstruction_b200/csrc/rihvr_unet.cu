@@ -535,6 +535,81 @@ __global__ void k_weights_bf16(const float* __restrict__ w, int Cout, int Cin, _
   }
 }
 
+// ---- inference with BF16 activations (channels-last, 8 channels = 16 bytes)
+
+__device__ __forceinline__ unsigned short bf16_bits(float v) {
+  const __nv_bfloat16 b = __float2bfloat16_rn(v);
+  return *reinterpret_cast<const unsigned short*>(&b);
+}
+
+// input channel 0 = |xbp| / rms (the FP32 value k_input writes, rounded as
+// the convolutions round their operands), channels 1..15 = 0
+__global__ void k_input_bf16(const float2* __restrict__ xbp, long long n, const float* __restrict__ rms,
+                             __nv_bfloat16* __restrict__ X) {
+  const float inv = 1.f / fmaxf(rms[0], 1e-30f);
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const float2 a = xbp[i];
+    uint4* d = reinterpret_cast<uint4*>(X + i * 16);
+    d[0] = make_uint4((unsigned)bf16_bits(sqrtf(a.x * a.x + a.y * a.y) * inv), 0u, 0u, 0u);
+    d[1] = make_uint4(0u, 0u, 0u, 0u);
+  }
+}
+
+__device__ __forceinline__ void bf16x8_add(float (&acc)[8], uint4 q) {
+  const unsigned u[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+  for (int j = 0; j < 4; ++j) {
+    acc[2 * j] += __uint_as_float(u[j] << 16);
+    acc[2 * j + 1] += __uint_as_float(u[j] & 0xFFFF0000u);
+  }
+}
+
+// 2x2x2 average pool, 8 channels a thread: FP32 sum of the 8 children in the
+// order of k_pool, times 1/8, rounded to BF16
+__global__ void k_pool_bf16(const __nv_bfloat16* __restrict__ X, __nv_bfloat16* __restrict__ Y, Vol c, int C) {
+  const int G = C / 8;
+  const long long n = c.n() * G;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+    const int g = (int)(e % G);
+    const long long vv = e / G;
+    const int x = (int)(vv % c.W), y = (int)((vv / c.W) % c.H), z = (int)(vv / ((long long)c.W * c.H));
+    const int W2 = 2 * c.W, H2 = 2 * c.H;
+    float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const long long src = (((long long)(2 * z + (q >> 2)) * H2 + 2 * y + ((q >> 1) & 1)) * W2) + 2 * x + (q & 1);
+      bf16x8_add(acc, *reinterpret_cast<const uint4*>(X + src * C + g * 8));
+    }
+    uint4 o;
+    o.x = (unsigned)bf16_bits(acc[0] * 0.125f) | ((unsigned)bf16_bits(acc[1] * 0.125f) << 16);
+    o.y = (unsigned)bf16_bits(acc[2] * 0.125f) | ((unsigned)bf16_bits(acc[3] * 0.125f) << 16);
+    o.z = (unsigned)bf16_bits(acc[4] * 0.125f) | ((unsigned)bf16_bits(acc[5] * 0.125f) << 16);
+    o.w = (unsigned)bf16_bits(acc[6] * 0.125f) | ((unsigned)bf16_bits(acc[7] * 0.125f) << 16);
+    *reinterpret_cast<uint4*>(Y + vv * C + g * 8) = o;
+  }
+}
+
+// nearest x2 upsampling of U (Cu channels) and concatenation with S (Cs), 8
+// channels a thread
+__global__ void k_up_concat_bf16(const __nv_bfloat16* __restrict__ U, int Cu, const __nv_bfloat16* __restrict__ S,
+                                 int Cs, __nv_bfloat16* __restrict__ Y, Vol f) {
+  const int C = Cu + Cs, G = C / 8;
+  const long long n = f.n() * G;
+  for (long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x; e < n; e += (long long)gridDim.x * blockDim.x) {
+    const int g = (int)(e % G);
+    const long long vv = e / G;
+    uint4 v;
+    if (g * 8 >= Cu) {
+      v = *reinterpret_cast<const uint4*>(S + vv * Cs + g * 8 - Cu);
+    } else {
+      const int x = (int)(vv % f.W), y = (int)((vv / f.W) % f.H), z = (int)(vv / ((long long)f.W * f.H));
+      const long long src = (((long long)(z >> 1) * (f.H >> 1)) + (y >> 1)) * (f.W >> 1) + (x >> 1);
+      v = *reinterpret_cast<const uint4*>(U + src * Cu + g * 8);
+    }
+    *reinterpret_cast<uint4*>(Y + vv * C + g * 8) = v;
+  }
+}
+
 }  // namespace unet
 }  // namespace rihvr
 
@@ -598,6 +673,17 @@ struct rihvr_unet {
   float *A0a = nullptr, *A0b = nullptr, *S0 = nullptr, *C0 = nullptr;
   float *B1a = nullptr, *B1b = nullptr, *S1 = nullptr, *C1 = nullptr, *P1 = nullptr;
   float *D2a = nullptr, *D2b = nullptr, *P2 = nullptr;
+  // inference with BF16 activations (predict on widths that are multiples of
+  // 512, where every level runs on tcgen05): weights in the bulk-copy layout,
+  // activations allocated on first use, one TMA tensor map per layer input
+  __nv_bfloat16* wtc = nullptr;
+  size_t wtc_off[kNumConv] = {};
+  bool bf_ready = false;
+  bool bf_failed = false;  // the tensor maps could not be made: predict keeps the FP32 path
+  __nv_bfloat16 *b_in0 = nullptr, *b_a0 = nullptr, *b_a1 = nullptr, *b_c1 = nullptr;  // level 0
+  __nv_bfloat16 *b_p1 = nullptr, *b_a2 = nullptr, *b_a3 = nullptr, *b_c2 = nullptr, *b_a7 = nullptr;  // level 1
+  __nv_bfloat16 *b_p2 = nullptr, *b_a4 = nullptr, *b_a5 = nullptr;  // level 2
+  TcMap maps[kNumConv];
   double* sums = nullptr;   // [0] sum |xbp|^2, [1] sum |x*|^2, [2] loss
   int* tc_err = nullptr;    // set by a tcgen05 convolution whose bounded wait ran out
   float* rms = nullptr;
@@ -656,7 +742,8 @@ int refresh_bf16(rihvr_unet* u) {
     const Conv& L = u->layers[i];
     k_weights_bf16<<<blocks_for((long long)L.cout * 27 * L.cin), 256, 0, u->st>>>(
         u->w + L.w_off, L.cout, L.cin, u->wb + u->wb_off[i], u->wt + u->wb_off[i]);
-    ++u->launches;
+    UCK(tc_weights(u->w + L.w_off, L.cout, L.cin, u->wtc + u->wtc_off[i], u->st));
+    u->launches += 2;
   }
   UCK(cudaGetLastError());
   return RIHVR_OK;
@@ -714,6 +801,108 @@ int backward(rihvr_unet* u, const float2* xbp, const float2* xs) {
   return RIHVR_OK;
 }
 
+// The BF16-activation path applies where every level's width is a multiple
+// of 128 (tcgen05) and the tensor-map encoder is there; RIHVR_UNET_MMA=sync
+// keeps the FP32 path everywhere.
+bool bf16_path(const rihvr_unet* u) {
+  if (!use_tcgen05() || u->bf_failed) return false;
+  for (int i = 0; i < kNumConv; ++i) {
+    const Conv& L = u->layers[i];
+    const Vol v = u->lv[L.level];
+    if (!conv3_tc_bf16_supported(v.D, v.H, v.W, L.cin, L.cout)) return false;
+  }
+  return true;
+}
+
+// activations and tensor maps of the BF16 path, on first use
+int bf16_prepare(rihvr_unet* u) {
+  if (u->bf_ready) return RIHVR_OK;
+  const long long n0 = u->lv[0].n(), n1 = u->lv[1].n(), n2 = u->lv[2].n();
+  int rc = RIHVR_OK;
+  auto A = [&](__nv_bfloat16** p, size_t n) {
+    if (rc == RIHVR_OK) rc = ualloc(u, p, n);
+  };
+  A(&u->b_in0, n0 * 16);
+  A(&u->b_a0, n0 * 16);
+  A(&u->b_a1, n0 * 16);
+  A(&u->b_c1, n0 * 48);
+  A(&u->b_p1, n1 * 16);
+  A(&u->b_a2, n1 * 32);
+  A(&u->b_a3, n1 * 32);
+  A(&u->b_c2, n1 * 96);
+  A(&u->b_a7, n1 * 32);
+  A(&u->b_p2, n2 * 32);
+  A(&u->b_a4, n2 * 64);
+  A(&u->b_a5, n2 * 64);
+  if (rc != RIHVR_OK) return rc;
+  // layer inputs: enc1 in0, a0; enc2 p1, a2; bottom p2, a4; dec2 c2, a6 (= a2);
+  // dec1 c1, a8 (= a0)
+  const __nv_bfloat16* in[kNumConv] = {u->b_in0, u->b_a0, u->b_p1, u->b_a2, u->b_p2,
+                                       u->b_a4, u->b_c2, u->b_a2, u->b_c1, u->b_a0};
+  for (int i = 0; i < kNumConv; ++i) {
+    const Conv& L = u->layers[i];
+    const Vol v = u->lv[L.level];
+    if (!tc_map_encode(&u->maps[i], in[i], L.cin, v.D, v.H, v.W)) {
+      u->bf_failed = true;
+      return RIHVR_OK;
+    }
+  }
+  u->bf_ready = true;
+  return RIHVR_OK;
+}
+
+int conv_bf16(rihvr_unet* u, int li, __nv_bfloat16* Y, const TcHead* head = nullptr) {
+  const Conv& L = u->layers[li];
+  const Vol v = u->lv[L.level];
+  UCK(conv3_tc_bf16(u->maps[li], L.cin, u->wtc + u->wtc_off[li], u->w + L.b_off, L.cout, Y, v.D, v.H, v.W, head,
+                    u->tc_err, u->st));
+  ++u->launches;
+  return RIHVR_OK;
+}
+
+// x0 = g alpha scale xbp with BF16 activations between the layers: the
+// convolution operands are the BF16 values the FP32 path rounds them to, so
+// the two paths differ only where the 2x2x2 pools average (BF16 inputs here,
+// FP32 there); the head works on the last layer's FP32 values
+int forward_bf16(rihvr_unet* u, const float2* xbp, float2* x0, float scale) {
+  int rc = bf16_prepare(u);
+  if (rc != RIHVR_OK) return rc;
+  const long long n0 = u->lv[0].n(), n1 = u->lv[1].n(), n2 = u->lv[2].n();
+  UCK(cudaMemsetAsync(u->sums, 0, 3 * sizeof(double), u->st));
+  k_sumsq<<<blocks_for(n0), 256, 0, u->st>>>(xbp, nullptr, n0, u->sums);
+  k_rms<<<1, 1, 0, u->st>>>(u->sums, n0, u->rms);
+  k_input_bf16<<<blocks_for(n0), 256, 0, u->st>>>(xbp, n0, u->rms, u->b_in0);
+  u->launches += 3;
+  if ((rc = conv_bf16(u, 0, u->b_a0)) || (rc = conv_bf16(u, 1, u->b_a1))) return rc;
+  k_pool_bf16<<<blocks_for(n1 * 2), 256, 0, u->st>>>(u->b_a1, u->b_p1, u->lv[1], 16);
+  if ((rc = conv_bf16(u, 2, u->b_a2)) || (rc = conv_bf16(u, 3, u->b_a3))) return rc;
+  k_pool_bf16<<<blocks_for(n2 * 4), 256, 0, u->st>>>(u->b_a3, u->b_p2, u->lv[2], 32);
+  if ((rc = conv_bf16(u, 4, u->b_a4)) || (rc = conv_bf16(u, 5, u->b_a5))) return rc;
+  k_up_concat_bf16<<<blocks_for(n1 * 12), 256, 0, u->st>>>(u->b_a5, 64, u->b_a3, 32, u->b_c2, u->lv[1]);
+  if ((rc = conv_bf16(u, 6, u->b_a2)) || (rc = conv_bf16(u, 7, u->b_a7))) return rc;
+  k_up_concat_bf16<<<blocks_for(n0 * 6), 256, 0, u->st>>>(u->b_a7, 32, u->b_a1, 16, u->b_c1, u->lv[0]);
+  if ((rc = conv_bf16(u, 8, u->b_a0))) return rc;
+  TcHead hd;
+  hd.w = u->w + u->head_off;
+  hd.xbp = xbp;
+  hd.scale = scale;
+  hd.x0 = x0;
+  if ((rc = conv_bf16(u, 9, nullptr, &hd))) return rc;
+  u->launches += 4;
+  UCK(cudaGetLastError());
+  return RIHVR_OK;
+}
+
+// prediction: the BF16 path where it applies, else the FP32 forward pass
+int predict(rihvr_unet* u, const float2* xbp, float2* x0, float scale) {
+  if (bf16_path(u)) {
+    const int rc = bf16_prepare(u);
+    if (rc != RIHVR_OK) return rc;
+    if (!u->bf_failed) return forward_bf16(u, xbp, x0, scale);
+  }
+  return forward(u, xbp, nullptr, x0, scale);
+}
+
 int check_net(const rihvr_unet* u) {
   if (!u) return unet_fail(RIHVR_ERR_INVALID_ARGUMENT, "NULL network");
   return RIHVR_OK;
@@ -739,7 +928,7 @@ namespace rihvr {
 int unet_predict_on(rihvr_unet* u, const float2* xbp, float scale, float2* x0, cudaStream_t st) {
   if (!u || !xbp || !x0) return unet_fail(RIHVR_ERR_INVALID_ARGUMENT, "NULL argument");
   u->st = st;
-  const int rc = forward(u, xbp, nullptr, x0, scale);
+  const int rc = predict(u, xbp, x0, scale);
   if (rc != RIHVR_OK) return rc;
   UCK(cudaStreamSynchronize(st));
   return check_tc(u);
@@ -775,6 +964,7 @@ int rihvr_unet_create(int depth, int height, int width, unsigned long long seed,
     u->layers[i].b_off = off;
     off += (size_t)kLayers[i].cout;
     u->wb_off[i] = boff;
+    u->wtc_off[i] = boff;  // same sizes: Cout x 27 x Cin
     boff += (size_t)kLayers[i].cout * 27 * kLayers[i].cin;
   }
   u->head_off = off;
@@ -790,6 +980,7 @@ int rihvr_unet_create(int depth, int height, int width, unsigned long long seed,
   A(&u->s, u->nparam);
   if (rc == RIHVR_OK) rc = ualloc(u, &u->wb, boff);
   if (rc == RIHVR_OK) rc = ualloc(u, &u->wt, boff);
+  if (rc == RIHVR_OK) rc = ualloc(u, &u->wtc, boff);
   for (int i = 0; i < kNumConv; ++i) A(&u->act[i], (size_t)u->lv[kLayers[i].level].n() * kLayers[i].cout);
   A(&u->in0, n0 * 16);
   A(&u->p1, n1 * 16);
@@ -872,7 +1063,7 @@ int rihvr_unet_set_params(rihvr_unet* u, const float* in) {
 int rihvr_unet_predict(rihvr_unet* u, const float* xbp, float* x0) {
   if (check_net(u) || !xbp || !x0) return unet_fail(RIHVR_ERR_INVALID_ARGUMENT, "NULL argument");
   u->st = nullptr;
-  const int rc = forward(u, reinterpret_cast<const float2*>(xbp), nullptr, reinterpret_cast<float2*>(x0));
+  const int rc = predict(u, reinterpret_cast<const float2*>(xbp), reinterpret_cast<float2*>(x0), 1.f);
   if (rc != RIHVR_OK) return rc;
   UCK(cudaStreamSynchronize(nullptr));
   return check_tc(u);
@@ -909,5 +1100,11 @@ int rihvr_unet_train_step(rihvr_unet* u, const float* xbp, const float* xstar, f
 }
 
 long long rihvr_unet_launch_count(const rihvr_unet* u) { return u ? u->launches : 0; }
+
+int rihvr_unet_activation_bits(rihvr_unet* u) {
+  if (check_net(u)) return 0;
+  if (bf16_path(u) && bf16_prepare(u) == RIHVR_OK && !u->bf_failed) return 16;
+  return 32;
+}
 
 }  // extern "C"

@@ -21,10 +21,13 @@
 // 32w..32w+31 of each row), adds the bias, applies the ReLU and stores FP32
 // channels-last.  Output values match the mma.sync kernel up to the order of
 // the FP32 accumulation.
+#include <cuda.h>  // CUtensorMap and its enums; the encoder is resolved at run time
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
+#include <cstring>
 
 #include "rihvr_unet_tc.cuh"
 
@@ -276,7 +279,293 @@ cudaError_t tc_launch(const float* X, int Cin, const __nv_bfloat16* Wt, int Cout
   return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------
+// Inference form with BF16 activations.  The block, tile and MMA sequence are
+// those above; what changes is how the operands arrive and leave:
+//   A: two TMA tensor loads per 16-channel slice (channels 0-7 and 8-15, box
+//      8 channels x 130 x (kTcYT + 2) x 3 of the channels-last BF16 input),
+//      which land in exactly the two-plane layout the descriptors read; the
+//      halo outside the volume is the TMA's zero fill;
+//   B: one bulk copy of the slice's weights, kept in global memory already in
+//      the [plane][tap][co][8 channels] order;
+//   both complete on one mbarrier (transaction bytes), issued and awaited by
+//   the thread that issues the MMAs, so no other thread touches them;
+//   output: bias and ReLU in FP32, rounded to BF16 and stored channels-last,
+//   or, for the last layer (HEAD), the 1x1x1 head, sigmoid and
+//   x0 = g alpha scale xbp computed from the FP32 values in the epilogue.
+// Every wait is bounded; a wait that runs out sets *err.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+  asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}" ::"r"(bar),
+               "r"(bytes)
+               : "memory");
+}
+
+// TMA load of a 4-D box (coordinates innermost first; the first, a channel
+// index, is a multiple of 8, i.e. 16 bytes) into shared memory, completing
+// on the mbarrier.  No multicast.
+__device__ __forceinline__ void tma_load_4d(uint32_t dst, const CUtensorMap* map, int c0, int c1, int c2, int c3,
+                                            uint32_t bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
+      "%5}], [%6];" ::"r"(dst),
+      "l"(reinterpret_cast<unsigned long long>(map)), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(bar)
+      : "memory");
+}
+
+// bulk copy of `bytes` (a multiple of 16, both addresses 16-byte aligned)
+__device__ __forceinline__ void bulk_load(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+               "l"(src), "r"(bytes), "r"(bar)
+               : "memory");
+}
+
+constexpr uint32_t kTcBoxBytes = 8u * 2u * kTcHalo;  // one channel plane of the halo (the TMA box)
+// planes start 1024 bytes apart, so that every TMA destination is aligned
+constexpr uint32_t kTcPlaneBytes = (kTcBoxBytes + 1023u) / 1024u * 1024u;
+
+template <int CN>
+constexpr size_t tcb_smem() {
+  return (size_t)2 * kTcPlaneBytes + (size_t)2 * 27 * CN * 16 + 32;
+}
+
+template <int CN, bool HEAD>
+__global__ void __launch_bounds__(kTcThreads) k_conv3_tc_bf16(const __grid_constant__ CUtensorMap xmap, int Cin,
+                                                              const __nv_bfloat16* __restrict__ Wp,
+                                                              const float* __restrict__ bias,
+                                                              __nv_bfloat16* __restrict__ Y, int D, int H, int W,
+                                                              TcHead hd, int* __restrict__ err) {
+  static_assert(CN % 16 == 0 && CN >= 16 && CN <= 64, "N of the MMA");
+  static_assert(!HEAD || CN == 16, "the head takes 16 channels");
+  constexpr uint32_t NCOLS = tmem_cols<CN>();
+  constexpr uint32_t BBYTES = 2u * 27u * CN * 16u;
+  extern __shared__ __align__(1024) unsigned char tsm[];
+  unsigned char* A0 = tsm;                   // channels 0-7 of the halo, 16 B a voxel
+  unsigned char* A1 = A0 + kTcPlaneBytes;    // channels 8-15
+  unsigned char* B0 = A1 + kTcPlaneBytes;    // [2][27 * CN] x 16 B
+  uint64_t* bars = reinterpret_cast<uint64_t*>(B0 + BBYTES);  // [0] operands landed, [1] MMAs done
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 2);
+  int* s_state = reinterpret_cast<int*>(tslot + 1);  // [0] ok, [1] parity of the last commit
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int nbx = W / kTcX, nby = (H + kTcYT - 1) / kTcYT;
+  const int bx = blockIdx.x % nbx, by = (blockIdx.x / nbx) % nby, z0 = blockIdx.x / (nbx * nby);
+  const int x0 = bx * kTcX, y0 = by * kTcYT;
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(saddr(tslot)),
+                 "r"(NCOLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(saddr(bars)) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(saddr(bars + 1)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tbase = *tslot;
+  const uint32_t bar_full = saddr(bars), bar_mma = saddr(bars + 1);
+
+  if (tid == 0) {
+    const uint32_t idesc = instr_desc(CN);
+    const uint32_t a0 = saddr(A0), b0 = saddr(B0);
+    const int nslice = Cin / 16;
+    uint32_t pf = 0, pm = 0;
+    bool ok = true;
+    int committed = 0;  // commits not yet awaited
+    for (int s = 0; s < nslice; ++s) {
+      if (s > 0) {  // the previous slice's MMAs have read the operands
+        ok = mbar_wait(bar_mma, pm);
+        pm ^= 1u;
+        committed = 0;
+        if (!ok) break;
+      }
+      mbar_expect_tx(bar_full, 2u * kTcBoxBytes + BBYTES);
+      tma_load_4d(a0, &xmap, 16 * s, x0 - 1, y0 - 1, z0 - 1, bar_full);
+      tma_load_4d(a0 + kTcPlaneBytes, &xmap, 16 * s + 8, x0 - 1, y0 - 1, z0 - 1, bar_full);
+      bulk_load(b0, Wp + (size_t)s * (BBYTES / 2), BBYTES, bar_full);
+      ok = mbar_wait(bar_full, pf);
+      pf ^= 1u;
+      if (!ok) {
+        mbar_wait(bar_full, pf ^ 1u);  // a last bounded chance for the copies in flight
+        break;
+      }
+      asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+      for (int k = 0; k < 27; ++k) {
+        int dz, dy, dx;
+        tap_off(k, &dz, &dy, &dx);
+        const uint64_t bd = smem_desc(b0 + (uint32_t)(k * CN * 16), 27 * CN * 16, 128);
+#pragma unroll
+        for (int m = 0; m < kTcYT; ++m) {
+          const int h = ((1 + dz) * kTcHY + (m + 1 + dy)) * kTcHX + (1 + dx);
+          const uint64_t ad = smem_desc(a0 + (uint32_t)(h * 16), kTcPlaneBytes, 128);
+          mma_bf16_ss(tbase + (uint32_t)(m * CN), ad, bd, idesc, (s > 0 || k > 0) ? 1u : 0u);
+        }
+      }
+      mma_commit(bar_mma);
+      committed = 1;
+    }
+    if (!ok) {
+      atomicExch(err, 1);
+      if (committed) mbar_wait(bar_mma, pm);  // let committed MMAs finish before the memory is released
+    }
+    s_state[0] = ok ? 1 : 0;
+    s_state[1] = (int)pm;
+  }
+  __syncthreads();
+  bool ok = s_state[0] != 0;
+  if (ok) {
+    ok = mbar_wait(bar_mma, (uint32_t)s_state[1]);
+    if (!ok) atomicExch(err, 1);
+  }
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  if (ok) {
+    const int xx = x0 + warp * 32 + lane;
+#pragma unroll 1
+    for (int m = 0; m < kTcYT; ++m) {
+      const int yy = y0 + m;
+      const long long vox = ((long long)z0 * H + yy) * W + xx;
+      float zsum = 0.f;
+      if constexpr (HEAD) zsum = hd.w[16];
+#pragma unroll
+      for (int c16 = 0; c16 < CN / 16; ++c16) {
+        float v[16];
+        // every lane of the warp takes part in the load, also for rows past H
+        tmem_ld16(tbase + ((uint32_t)(warp * 32) << 16) + (uint32_t)(m * CN + c16 * 16), v);
+#pragma unroll
+        for (int j = 0; j < 16; ++j) v[j] = fmaxf(v[j] + bias[c16 * 16 + j], 0.f);
+        if constexpr (HEAD) {
+#pragma unroll
+          for (int j = 0; j < 16; ++j) zsum += hd.w[j] * v[j];
+        } else if (yy < H) {
+          uint4 o0, o1;
+          o0.x = pack2(v[0], v[1]);
+          o0.y = pack2(v[2], v[3]);
+          o0.z = pack2(v[4], v[5]);
+          o0.w = pack2(v[6], v[7]);
+          o1.x = pack2(v[8], v[9]);
+          o1.y = pack2(v[10], v[11]);
+          o1.z = pack2(v[12], v[13]);
+          o1.w = pack2(v[14], v[15]);
+          uint4* dst = reinterpret_cast<uint4*>(Y + vox * CN + c16 * 16);
+          dst[0] = o0;
+          dst[1] = o1;
+        }
+      }
+      if constexpr (HEAD) {
+        if (yy < H) {
+          const float g = 1.f / (1.f + expf(-zsum));
+          const float alpha = hd.w[17] * hd.scale;
+          const float2 a = hd.xbp[vox];
+          hd.x0[vox] = make_float2(g * alpha * a.x, g * alpha * a.y);
+        }
+      }
+    }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(NCOLS) : "memory");
+  }
+}
+
+// cuTensorMapEncodeTiled, resolved once through the runtime
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+EncodeTiledFn encode_tiled() {
+  static const EncodeTiledFn fn = [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess)
+      p = nullptr;
+    return reinterpret_cast<EncodeTiledFn>(p);
+  }();
+  return fn;
+}
+
+template <int CN, bool HEAD>
+cudaError_t tcb_launch(const TcMap& m, int Cin, const __nv_bfloat16* Wp, const float* bias, __nv_bfloat16* Y, int D,
+                       int H, int W, const TcHead& hd, int* err, cudaStream_t st) {
+  constexpr size_t smem = tcb_smem<CN>();
+  static bool opted = false;
+  if (!opted) {
+    const cudaError_t e = cudaFuncSetAttribute(k_conv3_tc_bf16<CN, HEAD>,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    opted = true;
+  }
+  CUtensorMap map;
+  static_assert(sizeof(map) == sizeof(m.bytes), "tensor map size");
+  std::memcpy(&map, m.bytes, sizeof(map));
+  const unsigned blocks = (unsigned)((W / kTcX) * ((H + kTcYT - 1) / kTcYT) * D);
+  k_conv3_tc_bf16<CN, HEAD><<<blocks, kTcThreads, smem, st>>>(map, Cin, Wp, bias, Y, D, H, W, hd, err);
+  return cudaGetLastError();
+}
+
+// Wp[s][p][k][co][8] = bf16(w[co][k][16 s + 8 p + j]) for one layer
+__global__ void k_weights_tc(const float* __restrict__ w, int Cout, int Cin, __nv_bfloat16* __restrict__ wp) {
+  const long long n = (long long)Cout * 27 * Cin;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const int ci = (int)(i % Cin), k = (int)((i / Cin) % 27), co = (int)(i / (27LL * Cin));
+    const int s = ci >> 4, p = (ci >> 3) & 1, j = ci & 7;
+    wp[((((long long)s * 2 + p) * 27 + k) * Cout + co) * 8 + j] = __float2bfloat16_rn(w[i]);
+  }
+}
+
 }  // namespace
+
+bool tc_map_encode(TcMap* m, const __nv_bfloat16* X, int C, int D, int H, int W) {
+  const EncodeTiledFn enc = encode_tiled();
+  if (!enc || !X || (reinterpret_cast<uintptr_t>(X) & 15) != 0 || C % 16 != 0) return false;
+  CUtensorMap map;
+  std::memset(&map, 0, sizeof(map));
+  const cuuint64_t dims[4] = {(cuuint64_t)C, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)D};
+  const cuuint64_t strides[3] = {(cuuint64_t)C * 2, (cuuint64_t)W * C * 2, (cuuint64_t)H * W * C * 2};
+  const cuuint32_t box[4] = {8, (cuuint32_t)kTcHX, (cuuint32_t)kTcHY, (cuuint32_t)kTcHZ};
+  const cuuint32_t estr[4] = {1, 1, 1, 1};
+  if (enc(&map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<__nv_bfloat16*>(X), dims, strides, box, estr,
+          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return false;
+  static_assert(sizeof(map) == sizeof(m->bytes), "tensor map size");
+  std::memcpy(m->bytes, &map, sizeof(map));
+  return true;
+}
+
+bool conv3_tc_bf16_supported(int D, int H, int W, int Cin, int Cout) {
+  return W % kTcX == 0 && Cin % 16 == 0 && (Cout == 16 || Cout == 32 || Cout == 48 || Cout == 64) && D >= 1 &&
+         H >= 1 && encode_tiled() != nullptr;
+}
+
+size_t tc_weights_elems(int Cout, int Cin) { return (size_t)Cout * 27 * Cin; }
+
+cudaError_t tc_weights(const float* w, int Cout, int Cin, __nv_bfloat16* wp, cudaStream_t st) {
+  const long long n = (long long)Cout * 27 * Cin;
+  const int blocks = (int)std::min<long long>((n + 255) / 256, 1184);
+  k_weights_tc<<<blocks, 256, 0, st>>>(w, Cout, Cin, wp);
+  return cudaGetLastError();
+}
+
+cudaError_t conv3_tc_bf16(const TcMap& xmap, int Cin, const __nv_bfloat16* Wp, const float* bias, int Cout,
+                          __nv_bfloat16* Y, int D, int H, int W, const TcHead* head, int* err, cudaStream_t st) {
+  if (!conv3_tc_bf16_supported(D, H, W, Cin, Cout)) return cudaErrorInvalidValue;
+  const TcHead hd = head ? *head : TcHead{};
+  if (head) {
+    if (Cout != 16) return cudaErrorInvalidValue;
+    return tcb_launch<16, true>(xmap, Cin, Wp, bias, Y, D, H, W, hd, err, st);
+  }
+  switch (Cout) {
+    case 16: return tcb_launch<16, false>(xmap, Cin, Wp, bias, Y, D, H, W, hd, err, st);
+    case 32: return tcb_launch<32, false>(xmap, Cin, Wp, bias, Y, D, H, W, hd, err, st);
+    case 48: return tcb_launch<48, false>(xmap, Cin, Wp, bias, Y, D, H, W, hd, err, st);
+    default: return tcb_launch<64, false>(xmap, Cin, Wp, bias, Y, D, H, W, hd, err, st);
+  }
+}
 
 bool conv3_tc_supported(int W, int Cin, int Cn) {
   return W % kTcX == 0 && Cin % 16 == 0 && (Cn == 16 || Cn == 32 || Cn == 48 || Cn == 64);

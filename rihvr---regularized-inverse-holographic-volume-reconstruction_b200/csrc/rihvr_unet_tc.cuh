@@ -17,5 +17,26 @@ bool conv3_tc_supported(int W, int Cin, int Cn);
 cudaError_t conv3_tc(const float* X, int Cin, const __nv_bfloat16* Wt, int Cout, int co0, int Cn, const float* bias,
                      float* Y, int D, int H, int W, int relu, int mirror, int* err, cudaStream_t st);
 
+// Inference form with BF16 activations (channels-last, C a multiple of 16):
+// the input arrives by TMA through a tensor map made by tc_map_encode, the
+// weights by a bulk copy from the layout tc_weights writes, the output is
+// BF16 with bias and ReLU, or (head != NULL, Cout 16) the head's
+// x0 = sigmoid(w . relu(y) + b) alpha scale xbp.
+struct TcMap {
+  alignas(64) unsigned char bytes[128];  // a CUtensorMap
+};
+struct TcHead {
+  const float* w = nullptr;      // 16 weights, bias, alpha
+  const float2* xbp = nullptr;
+  float scale = 1.f;
+  float2* x0 = nullptr;
+};
+bool tc_map_encode(TcMap* m, const __nv_bfloat16* X, int C, int D, int H, int W);
+bool conv3_tc_bf16_supported(int D, int H, int W, int Cin, int Cout);
+size_t tc_weights_elems(int Cout, int Cin);
+cudaError_t tc_weights(const float* w, int Cout, int Cin, __nv_bfloat16* wp, cudaStream_t st);
+cudaError_t conv3_tc_bf16(const TcMap& xmap, int Cin, const __nv_bfloat16* Wp, const float* bias, int Cout,
+                          __nv_bfloat16* Y, int D, int H, int W, const TcHead* head, int* err, cudaStream_t st);
+
 }  // namespace unet
 }  // namespace rihvr

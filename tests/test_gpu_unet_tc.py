@@ -2,7 +2,9 @@
 accumulators in tensor memory, layers whose width is a multiple of 128)
 against the FP64 numpy reference and against the warp-level mma.sync kernels
 (RIHVR_UNET_MMA=sync, in a separate process: the choice is read once per
-process)."""
+process); and the inference path with BF16 activations (widths that are
+multiples of 512: TMA-fed tcgen05 convolutions at every level, the head fused
+into the last)."""
 import os
 import subprocess
 import sys
@@ -92,3 +94,36 @@ def test_tcgen05_matches_mma_sync(tmp_path):
     assert rel(a["x0"], b["x0"]) < 1e-4
     assert abs(float(a["loss"]) - float(b["loss"])) < 1e-4 * abs(float(b["loss"]))
     assert rel(a["grad"], b["grad"]) < 1e-3
+
+
+def test_bf16_inference_path_matches_reference(rihvr):
+    """Width 512: predict runs with BF16 activations.  Against the reference
+    that rounds the stored activations as that path does (BF16 operands and
+    FP32 accumulation are the only other difference: 2e-3), and against the
+    FP32-activation reference (the pools then average unrounded values:
+    1e-2)."""
+    shape = (16, 32, 512)
+    params = U.init_params(21).astype(np.float32)
+    xbp, _ = sample(22, shape)
+    with rihvr.UNet(*shape) as net:
+        net.set_params(params)
+        assert net.activation_bits() == 16
+        x0 = net.predict(xbp).cpu().numpy()
+        x0b = net.predict(xbp).cpu().numpy()
+    assert np.array_equal(x0, x0b)  # deterministic
+    p64, a64 = params.astype(np.float64), xbp.astype(np.complex128)
+    U.emulate_bf16(True)
+    try:
+        rs, _ = U.forward(p64, a64, store_bf16=True)
+        rf, _ = U.forward(p64, a64)
+    finally:
+        U.emulate_bf16(False)
+    assert rel(x0, rs) < 2e-3
+    assert rel(x0, rf) < 1e-2
+
+
+def test_small_widths_keep_fp32_activations(rihvr):
+    with rihvr.UNet(8, 16, 128) as net:
+        assert net.activation_bits() == 32
+    with rihvr.UNet(8, 16, 256) as net:
+        assert net.activation_bits() == 32

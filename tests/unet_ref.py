@@ -107,25 +107,30 @@ def net_input(xbp):
     return X
 
 
-def forward(params, xbp):
+def forward(params, xbp, store_bf16=False):
+    """x0 and the intermediate tensors.  `store_bf16` models the inference
+    path with BF16 activations: every stored activation (input, layer
+    outputs but the last, pooled tensors) is rounded to BF16; the pools
+    average the rounded values."""
     Ws, bs, head, _ = unpack(params)
     c = {}
     relu = lambda z: np.maximum(z, 0.0)
-    c["in"] = net_input(xbp)
+    st = bf16 if store_bf16 else (lambda v: v)
+    c["in"] = st(net_input(xbp))
     a = [None] * 10
-    a[0] = relu(conv_fwd(c["in"], Ws[0], bs[0]))
-    a[1] = relu(conv_fwd(a[0], Ws[1], bs[1]))
-    c["p1"] = pool(a[1])
-    a[2] = relu(conv_fwd(c["p1"], Ws[2], bs[2]))
-    a[3] = relu(conv_fwd(a[2], Ws[3], bs[3]))
-    c["p2"] = pool(a[3])
-    a[4] = relu(conv_fwd(c["p2"], Ws[4], bs[4]))
-    a[5] = relu(conv_fwd(a[4], Ws[5], bs[5]))
+    a[0] = st(relu(conv_fwd(c["in"], Ws[0], bs[0])))
+    a[1] = st(relu(conv_fwd(a[0], Ws[1], bs[1])))
+    c["p1"] = st(pool(a[1]))
+    a[2] = st(relu(conv_fwd(c["p1"], Ws[2], bs[2])))
+    a[3] = st(relu(conv_fwd(a[2], Ws[3], bs[3])))
+    c["p2"] = st(pool(a[3]))
+    a[4] = st(relu(conv_fwd(c["p2"], Ws[4], bs[4])))
+    a[5] = st(relu(conv_fwd(a[4], Ws[5], bs[5])))
     c["c2"] = np.concatenate([up(a[5]), a[3]], axis=-1)
-    a[6] = relu(conv_fwd(c["c2"], Ws[6], bs[6]))
-    a[7] = relu(conv_fwd(a[6], Ws[7], bs[7]))
+    a[6] = st(relu(conv_fwd(c["c2"], Ws[6], bs[6])))
+    a[7] = st(relu(conv_fwd(a[6], Ws[7], bs[7])))
     c["c1"] = np.concatenate([up(a[7]), a[1]], axis=-1)
-    a[8] = relu(conv_fwd(c["c1"], Ws[8], bs[8]))
+    a[8] = st(relu(conv_fwd(c["c1"], Ws[8], bs[8])))
     a[9] = relu(conv_fwd(a[8], Ws[9], bs[9]))
     z = a[9] @ head[:16] + head[16]
     g = 1.0 / (1.0 + np.exp(-z))
