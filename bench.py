@@ -462,8 +462,9 @@ def run_warmstart(args):
 
 def run_warmstart4(args):
     """The learned warm start on its specified configuration, 512x512x200
-    (500-3000 disks and rods, noise 0.005-0.03): the network trained at
-    128x128x32 (fully convolutional, same optics) applied to held-out
+    (500-3000 disks and rods, noise 0.005-0.03): the network trained on
+    full-depth crops of that configuration (or, without those weights, the
+    one trained at 128x128x32; it is fully convolutional) applied to held-out
     holograms of that size; iterations and device time to plain FISTA's
     100-iteration objective within 1e-3, with and without it, and the
     network's inference time at that size.  Prints one JSON line."""
@@ -475,8 +476,9 @@ def run_warmstart4(args):
     n = args.frames if args.frames else 256
     seeds = np.arange(400_000, 400_000 + n)
     S, Z = ws.C4_SIZE, ws.C4_PLANES
+    weights = ws.C4_WEIGHTS if os.path.exists(ws.C4_WEIGHTS) else ws.WEIGHTS
     with rihvr.UNet(Z, S, S) as net:
-        net.load(ws.WEIGHTS)
+        net.load(weights)
         t0 = time.perf_counter()
         rows = ws.evaluate(net, seeds, size=S, planes=Z, sampler=ws.config4_sample, device="cuda")
         eval_s = time.perf_counter() - t0
@@ -486,6 +488,7 @@ def run_warmstart4(args):
         with rihvr.SparseCompressiveHolo(rihvr.params_from_config(cfg, record_objective=0), S, S) as s:
             s.setHologram(b)
             xbp = torch.from_numpy(s.backpropagate()).cuda()
+        act_bits = net.activation_bits()
         for _ in range(3):
             net.predict(xbp)
         torch.cuda.synchronize()
@@ -505,7 +508,8 @@ def run_warmstart4(args):
     line = {"metric": "iterations and device ms to plain FISTA's 100-iteration objective (1e-3), warm start vs zero",
             "value": s_["mean_iters_warm"], "unit": "iterations", "higher_is_better": False, "n_gpus": 1,
             "data": "synthetic", "config": {"workload": f"warmstart_{S}x{S}x{Z}", "holograms": len(rows),
-                                             "weights": os.path.basename(ws.WEIGHTS)},
+                                             "weights": os.path.basename(weights),
+                                             "activation_bits": act_bits},
             "summary": s_, "inference_ms": infer_ms, "inference_tflops": flops / (infer_ms * 1e-3) / 1e12,
             "conv_flops": flops, "eval_s": eval_s, "rows": rows}
     print(json.dumps(line), flush=True)

@@ -12,6 +12,7 @@ the iterations each needs to come within 1e-3 (relative) of plain FISTA's
 final objective.
 
     python warmstart.py train --out weights.npy [--samples 1024 --epochs 50]
+    python warmstart.py train4 [--holograms 256 --crops 4 --epochs 8]   # 512x512x200, full-depth crops
     python warmstart.py evaluate --weights weights.npy [--samples 16]
 """
 from __future__ import annotations
@@ -95,6 +96,49 @@ def make_set(seeds, size: int = SIZE, planes: int = PLANES, iterations: int = 10
             out.append((b, xbp, xs))
             if log and (i + 1) % 32 == 0:
                 log(f"  {i + 1}/{len(seeds)} samples")
+    return out
+
+
+# Training on the 512 x 512 x 200 configuration: full-depth crops of
+# C4_CROP x C4_CROP pixels.  A crop keeps every plane, so its back-propagated
+# field holds the same depth range and its RMS (by which the network divides
+# its input) is close to the whole volume's.
+C4_CROP = 128
+C4_WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)),
+                          f"warmstart_unet_c4_{C4_PLANES}x{C4_CROP}x{C4_CROP}.npy")
+
+
+def make_set_c4(seeds, crops: int = 4, iterations: int = 100, log=None, seed: int = 0):
+    """[(None, xbp crop, x* crop)] from 512 x 512 x 200 holograms, `crops`
+    random full-depth crops of each, as CUDA complex64 tensors; the volumes
+    stay on the device."""
+    import ctypes
+
+    import torch
+
+    rihvr = _pkg()
+    synth = _synth()
+    rng = np.random.default_rng(seed)
+    S, Z, c = C4_SIZE, C4_PLANES, C4_CROP
+    cfg0 = config4_sample(int(seeds[0]))
+    p = rihvr.params_from_config(cfg0, record_objective=0)
+    out = []
+    xbp = torch.empty((Z, S, S), dtype=torch.complex64, device="cuda")
+    xs = torch.empty_like(xbp)
+    L = rihvr.load_library()
+    with rihvr.SparseCompressiveHolo(p, S, S) as sol:
+        for i, sd in enumerate(seeds):
+            _, b = synth.make_hologram(config4_sample(int(sd), iterations=iterations), device="cuda")
+            sol.setHologram(b)
+            rihvr._check(L.rihvr_backpropagate(sol._h, ctypes.c_void_p(xbp.data_ptr()), 1), "rihvr_backpropagate")
+            sol.iterate(iterations)
+            rihvr._check(L.rihvr_get_volume(sol._h, ctypes.c_void_p(xs.data_ptr()), 1), "rihvr_get_volume")
+            torch.cuda.synchronize()
+            for _ in range(crops):
+                y0, x0 = (int(v) for v in rng.integers(0, S - c + 1, 2))
+                out.append((None, xbp[:, y0:y0 + c, x0:x0 + c].contiguous(), xs[:, y0:y0 + c, x0:x0 + c].contiguous()))
+            if log and (i + 1) % 16 == 0:
+                log(f"  {i + 1}/{len(seeds)} holograms")
     return out
 
 
@@ -187,12 +231,39 @@ def main(argv=None):
     tr.add_argument("--epochs", type=int, default=50)
     tr.add_argument("--lr", type=float, default=1e-3)
     tr.add_argument("--eval", type=int, default=8)
+    t4 = sub.add_parser("train4", help="train on full-depth crops of 512x512x200 holograms")
+    t4.add_argument("--out", default=C4_WEIGHTS)
+    t4.add_argument("--holograms", type=int, default=256)
+    t4.add_argument("--crops", type=int, default=4)
+    t4.add_argument("--epochs", type=int, default=8)
+    t4.add_argument("--lr", type=float, default=1e-3)
+    t4.add_argument("--init", default=WEIGHTS, help="starting weights ('' for a fresh network)")
+    t4.add_argument("--eval", type=int, default=16)
     ev = sub.add_parser("evaluate")
     ev.add_argument("--weights", default=WEIGHTS)
     ev.add_argument("--samples", type=int, default=16)
     a = ap.parse_args(argv)
     rihvr = _pkg()
     log = lambda m: print(m, flush=True)
+    if a.cmd == "train4":
+        t0 = time.perf_counter()
+        data = make_set_c4(np.arange(500_000, 500_000 + a.holograms), a.crops, log=log)
+        t1 = time.perf_counter()
+        log(f"training set: {len(data)} crops of {a.holograms} holograms in {t1 - t0:.1f} s")
+        with rihvr.UNet(C4_PLANES, C4_CROP, C4_CROP, seed=0) as net:
+            if a.init:
+                net.load(a.init)
+            hist = train(net, data, a.epochs, a.lr, log=log)
+            net.save(a.out)
+        t2 = time.perf_counter()
+        del data
+        with rihvr.UNet(C4_PLANES, C4_SIZE, C4_SIZE) as big:
+            big.load(a.out)
+            rows = evaluate(big, np.arange(400_000, 400_000 + a.eval), size=C4_SIZE, planes=C4_PLANES,
+                            sampler=config4_sample, device="cuda")
+        print(json.dumps({"train_s": t2 - t1, "data_s": t1 - t0, "losses": hist, "eval": summary(rows),
+                          "rows": rows}), flush=True)
+        return 0
     with rihvr.UNet(PLANES, SIZE, SIZE, seed=0) as net:
         if a.cmd == "train":
             t0 = time.perf_counter()
