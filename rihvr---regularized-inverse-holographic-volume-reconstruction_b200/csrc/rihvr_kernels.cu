@@ -499,6 +499,48 @@ __global__ void __launch_bounds__(ColLayout<N>::THREADS) k_adj_col(const float2*
   if (TMA && threadIdx.x == 0) bulk_wait_all();
 }
 
+// Inter-stage twiddles as a per-block table in shared memory, for column
+// kernels that run three blocks an SM: w^(t k) for the N1 thread rows t and
+// the N2 elements k of a line, the same values (same FP32 expression) that
+// line_twiddles keeps in registers, so results are bit-identical to the
+// register-resident form while 2 N2 registers a thread are freed.  Rows are
+// padded to an even length (16-byte aligned pairs) that spreads the 8 rows a
+// warp reads over all 32 banks.
+template <int N>
+struct TwTable {
+  using C = LineCfg<N>;
+  static constexpr int LDT = C::N2 + 2;  // float2 per row
+  static constexpr int ELEMS = C::N1 * LDT;
+  static constexpr size_t BYTES = sizeof(float2) * ELEMS;
+};
+
+template <int N, bool INV>
+__device__ __forceinline__ void tw_table_build(float2* tab) {
+  using C = LineCfg<N>;
+  constexpr int N2 = C::N2, LDT = TwTable<N>::LDT;
+  const float sgn = INV ? 2.0f : -2.0f;
+  for (int i = threadIdx.x; i < C::N1 * N2; i += ColLayout<N>::THREADS) {
+    const int t = i / N2, k = i - t * N2;
+    float s, c;
+    sincospif(sgn * (float)((t * k) % N) / (float)N, &s, &c);
+    tab[t * LDT + k] = make_float2(c, s);
+  }
+}
+
+// v[k] *= w^(t k), k >= 1, from the table (pairs of twiddles per 16-byte load)
+template <int N>
+__device__ __forceinline__ void tw_table_apply(float2 (&v)[LineCfg<N>::N2], const float2* tab, int t) {
+  constexpr int N2 = LineCfg<N>::N2;
+  static_assert(N2 % 2 == 0, "twiddle pairs");
+  const float4* row = reinterpret_cast<const float4*>(tab + t * TwTable<N>::LDT);
+#pragma unroll
+  for (int k = 0; k < N2; k += 2) {
+    const float4 q = row[k / 2];
+    if (k > 0) v[k] = cmul(v[k], make_float2(q.x, q.y));
+    v[k + 1] = cmul(v[k + 1], make_float2(q.z, q.w));
+  }
+}
+
 // Transfer function H'_z = exp(i 2 pi u), u = frac(z * cturn), with the
 // accurate sincospi: used where a value seeds many planes (the recurrence
 // below), so its error is not multiplied by the plane count.
@@ -524,15 +566,17 @@ constexpr int kAdjAnchor = 16;
 // Lines of up to 32 elements a thread only (the inter-stage twiddles are
 // regenerated each plane to leave registers for Y).
 //
-// HOIST keeps the inter-stage twiddles in registers as k_adj_col does (fewer
-// instructions a plane, two blocks an SM); without it they are regenerated
-// each plane and three blocks fit.  The autotuner picks one of the two or the
-// direct evaluation.
-template <int N, bool TMA, bool HOIST>
-__global__ void __launch_bounds__(ColLayout<N>::THREADS, HOIST ? 2 : 3)
+// TWM selects the inter-stage twiddles: 1 keeps them in registers as k_adj_col
+// does (fewest instructions a plane, two blocks an SM); 0 regenerates them
+// each plane (three blocks fit, twice the instructions); 2 reads them from a
+// per-block shared table (one 16-byte load per two elements, three blocks an
+// SM).  The autotuner picks one of these or the direct evaluation.
+template <int N, bool TMA, int TWM>
+__global__ void __launch_bounds__(ColLayout<N>::THREADS, TWM == 1 ? 2 : 3)
     k_adj_col_rec(const float2* __restrict__ Rs, const double* __restrict__ cturn, const double* __restrict__ zlist,
                   double dz, float2* __restrict__ U, int z0, int z1, int zpb,
                   const __grid_constant__ CUtensorMap umap) {
+  constexpr bool HOIST = TWM == 1;
   using C = LineCfg<N>;
   using Lay = ColLayout<N>;
   constexpr int N1 = C::N1, N2 = C::N2, M = C::M, CC = Lay::CC;
@@ -546,10 +590,15 @@ __global__ void __launch_bounds__(ColLayout<N>::THREADS, HOIST ? 2 : 3)
   const int zb = z0 + blockIdx.y * zpb, ze = min(zb + zpb, z1);
   if (zb >= ze) return;
   float2* s_d = sm + Lay::SMEM_ELEMS;  // this thread's rotations, [row][CC] (thread-private slots)
+  float2* s_tw = s_d + Lay::STRIP_ELEMS;  // twiddle table (TWM 2)
   const float2* rs = Rs + (size_t)t * W + x;
   const double* ct = cturn + (size_t)t * W + x;
   float2 tw[HOIST ? N2 : 1];
   if constexpr (HOIST) line_twiddles<N, N2, true>(tw, t);
+  if constexpr (TWM == 2) {
+    tw_table_build<N, true>(s_tw);
+    __syncthreads();
+  }
   float2 y[N2];
 #pragma unroll
   for (int n2 = 0; n2 < N2; ++n2) {
@@ -579,6 +628,8 @@ __global__ void __launch_bounds__(ColLayout<N>::THREADS, HOIST ? 2 : 3)
     if constexpr (HOIST) {
 #pragma unroll
       for (int k = 1; k < N2; ++k) v[k] = cmul(v[k], tw[k]);
+    } else if constexpr (TWM == 2) {
+      tw_table_apply<N>(v, s_tw, t);
     } else {
       line_twiddle<N, N2, true>(v, launder_i(t));
     }
@@ -789,6 +840,186 @@ __global__ void __launch_bounds__(ColLayout<N>::THREADS) k_fwd_col_horner(const 
   }
 }
 
+// The same Horner sum with three blocks an SM instead of two.  Shared memory
+// per block drops from three column strips to two plus the twiddle table: T
+// lands in the exchange buffer itself, and plane z-1's strip is requested as
+// soon as every thread has read plane z's exchange, so its load overlaps the
+// second DFT stage and the multiply-add (and the other blocks' work).  The
+// inter-stage twiddles come from the per-block table, which frees the
+// registers the third block needs.  Same arithmetic, same bits as
+// k_fwd_col_horner.
+template <int N>
+constexpr size_t horner1_smem() {
+  using Lay = ColLayout<N>;
+  constexpr size_t buf = Lay::SMEM_ELEMS > Lay::STRIP_ELEMS ? (size_t)Lay::SMEM_ELEMS : Lay::STRIP_ELEMS;
+  return sizeof(float2) * (buf + Lay::STRIP_ELEMS) + TwTable<N>::BYTES + 16;  // + the mbarrier
+}
+
+// Bounded waits of the TMA-fed column passes that ran out since the last read
+// (col_wait_timeouts).  None is expected: a wait covers one strip copy.
+__device__ unsigned g_col_wait_timeouts;
+constexpr unsigned kColMaxSpins = 1u << 26;
+
+__device__ __forceinline__ void col_mbar_expect_tx(unsigned bar, unsigned bytes) {
+  asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}" ::"r"(bar),
+               "r"(bytes)
+               : "memory");
+}
+
+// wait for phase `parity` of the mbarrier, at most kColMaxSpins tries; false when the bound ran out
+__device__ __forceinline__ bool col_mbar_wait(unsigned bar, unsigned parity) {
+  for (unsigned i = 0; i < kColMaxSpins; ++i) {
+    unsigned ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.b32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    if (ok) return true;
+  }
+  return false;
+}
+
+// TMA load of a [rows][CC] box of 8-byte elements (x, row, plane) into shared
+// memory, completing on the mbarrier.  No multicast; x * 8 bytes is a multiple
+// of 16 and every coordinate lies inside the tensor.
+__device__ __forceinline__ void tma_load_3d(void* smem, const CUtensorMap* map, int x, int y, int z, unsigned bar) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], "
+      "[%5];" ::"r"(d),
+      "l"(reinterpret_cast<unsigned long long>(map)), "r"(x), "r"(y), "r"(z), "r"(bar)
+      : "memory");
+}
+
+// With TMA, one thread loads each plane's strip as tma_rows<N>-row boxes that
+// complete on an mbarrier, instead of every thread issuing 16-byte cp.async
+// pieces.  Every wait on the mbarrier is bounded: when one runs out, the block
+// counts it in g_col_wait_timeouts (read back by col_wait_timeouts), gives the
+// copy in flight one more bounded wait and leaves without writing its sums.
+template <int N, bool TMA>
+__global__ void __launch_bounds__(ColLayout<N>::THREADS, 3)
+    k_fwd_col_horner1(const float2* __restrict__ T, const double* __restrict__ cturn,
+                      const double* __restrict__ zlist, double dz, float2* __restrict__ Spart, int z0, int z1,
+                      int zpb, const __grid_constant__ CUtensorMap tmap) {
+  using C = LineCfg<N>;
+  using Lay = ColLayout<N>;
+  constexpr int N1 = C::N1, N2 = C::N2, M = C::M, LD = C::LD, CC = Lay::CC;
+  static_assert(Lay::STAGE && C::EXACT && kHoistTw<N>, "staged square sizes of up to 32 elements a thread");
+  constexpr int W = N;
+  constexpr size_t BUF = Lay::SMEM_ELEMS > Lay::STRIP_ELEMS ? (size_t)Lay::SMEM_ELEMS : Lay::STRIP_ELEMS;
+  extern __shared__ __align__(128) float2 sm[];
+  const int c = threadIdx.x % CC, t = threadIdx.x / CC;
+  const int xr = blockIdx.x * CC + c;
+  const bool col_ok = xr < W;
+  const int x = col_ok ? xr : W - 1;
+  const int zb = z0 + blockIdx.y * zpb, ze = min(zb + zpb, z1);
+  constexpr size_t HW = (size_t)N * W;
+  const double* ct = cturn + (size_t)t * W + x;
+  float2* const s_d = sm + BUF;                  // this thread's rotations D, stage-B layout
+  float2* const s_tw = s_d + Lay::STRIP_ELEMS;   // twiddle table
+  uint64_t* const bar = reinterpret_cast<uint64_t*>(s_tw + TwTable<N>::ELEMS);
+  const unsigned sbar = (unsigned)__cvta_generic_to_shared(bar);
+  unsigned phase = 0;
+  constexpr int R = tma_rows<N>();
+  constexpr unsigned kStripBytes = (unsigned)(sizeof(float2) * Lay::STRIP_ELEMS);
+  // plane z's strip into the buffer: by TMA (thread 0) or cp.async (all threads)
+  auto request = [&](int z) {
+    if constexpr (TMA) {
+      if (threadIdx.x == 0) {
+        fence_smem_async();  // the block's reads of the buffer come before the copy's writes
+        col_mbar_expect_tx(sbar, kStripBytes);
+#pragma unroll 1
+        for (int b = 0; b < N; b += R) tma_load_3d(sm + b * CC, &tmap, blockIdx.x * CC, b, z, sbar);
+      }
+    } else {
+      strip_async<N>(sm, T + (size_t)z * HW, blockIdx.x * CC);
+      cp_async_commit();
+    }
+  };
+  if constexpr (TMA) {
+    if (threadIdx.x == 0) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(sbar) : "memory");
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+  }
+  if (zb < ze) request(ze - 1);
+  tw_table_build<N, false>(s_tw);
+#pragma unroll
+  for (int j = 0; j < M; ++j)
+#pragma unroll
+    for (int k1 = 0; k1 < N1; ++k1)
+      s_d[(N1 * j + N2 * k1 + t) * CC + c] = transfer_accurate(dz, __ldg(ct + (size_t)(N1 * j + N2 * k1) * W), false);
+  float2 acc[N2];
+#pragma unroll
+  for (int i = 0; i < N2; ++i) acc[i] = make_float2(0.f, 0.f);
+#pragma unroll 1
+  for (int z = ze - 1; z >= zb; --z) {
+    if constexpr (TMA) {
+      const bool ok = col_mbar_wait(sbar, phase);
+      if (__syncthreads_or(!ok)) {  // a wait ran out: count it, let the copy land, leave
+        if (threadIdx.x == 0) {
+          atomicAdd(&g_col_wait_timeouts, 1u);
+          col_mbar_wait(sbar, phase);
+        }
+        return;
+      }
+      phase ^= 1u;
+    } else {
+      cp_async_wait<0>();
+      __syncthreads();  // plane z's strip (and, the first time, the table) is visible
+    }
+    float2 v[N2];
+#pragma unroll
+    for (int n2 = 0; n2 < N2; ++n2) v[n2] = sm[(t + N1 * n2) * CC + c];
+    reg_fft<N2, false>(v);
+    tw_table_apply<N>(v, s_tw, t);
+    __syncthreads();  // every thread has read the strip: the buffer becomes the exchange
+#pragma unroll
+    for (int k2 = 0; k2 < N2; ++k2) sm[(k2 * LD + t) * CC + c] = v[k2];
+    __syncthreads();
+#pragma unroll
+    for (int j = 0; j < M; ++j)
+#pragma unroll
+      for (int n1 = 0; n1 < N1; ++n1) v[j * N1 + n1] = sm[((t + N1 * j) * LD + n1) * CC + c];
+    __syncthreads();  // every thread has read the exchange: refill with plane z-1
+    if (z - 1 >= zb) request(z - 1);
+    stage_b_dft<N1, C::VS, false>(v);
+#pragma unroll
+    for (int j = 0; j < M; ++j)
+#pragma unroll
+      for (int k1 = 0; k1 < N1; ++k1) {
+        const float2 d = s_d[(N1 * j + N2 * k1 + t) * CC + c];
+        float2& a = acc[j * N1 + k1];
+        const float2 u = v[j * N1 + k1];
+        const float ax = a.x;
+        a.x = fmaf(ax, d.x, fmaf(-a.y, d.y, u.x));
+        a.y = fmaf(ax, d.y, fmaf(a.y, d.x, u.y));
+      }
+  }
+  if constexpr (!TMA) cp_async_wait<0>();
+  if (col_ok && zb < ze) {
+    const double zz = zlist[zb];
+    float2* Sp = Spart + (size_t)blockIdx.y * HW + (size_t)t * W + x;
+#pragma unroll
+    for (int j = 0; j < M; ++j)
+#pragma unroll
+      for (int k1 = 0; k1 < N1; ++k1) {
+        const float2 h = transfer_accurate(zz, __ldg(ct + (size_t)(N1 * j + N2 * k1) * W), false);
+        Sp[(size_t)(N1 * j + N2 * k1) * W] = cmul(acc[j * N1 + k1], h);
+      }
+  } else if (col_ok) {
+    float2* Sp = Spart + (size_t)blockIdx.y * HW + (size_t)t * W + x;
+#pragma unroll
+    for (int j = 0; j < M; ++j)
+#pragma unroll
+      for (int k1 = 0; k1 < N1; ++k1) Sp[(size_t)(N1 * j + N2 * k1) * W] = make_float2(0.f, 0.f);
+  }
+}
+
 // Plain column DFT of one (square) plane.
 template <int N, bool INV>
 __global__ void __launch_bounds__(ColLayout<N>::THREADS) k_plane_col(const float2* __restrict__ in,
@@ -866,7 +1097,7 @@ static cudaError_t adj_col_n(const float2* Rs, const double* cturn, const double
   // thread; `rec_mode` 1 regenerates the twiddles each plane, 2 keeps them
   constexpr bool kRecOk = kHoistTw<N> && (N % Lay::CC == 0);
   const bool rec = kRecOk && dz_uniform != 0.0 && rec_mode != 0;
-  const int target = (rec && rec_mode == 1 ? 12 : 8) * num_sms();
+  const int target = (rec && (rec_mode == 1 || rec_mode == 3) ? 12 : 8) * num_sms();
   int chunks = chunks_hint > 0 ? chunks_hint : (target + strips - 1) / strips;
   if (chunks > nz) chunks = nz;
   if (chunks < 1) chunks = 1;
@@ -878,15 +1109,17 @@ static cudaError_t adj_col_n(const float2* Rs, const double* cturn, const double
   cudaError_t e;
   if constexpr (kRecOk) {
     if (rec) {
-      constexpr size_t smem = Lay::SMEM_BYTES + sizeof(float2) * Lay::STRIP_ELEMS;
+      // the twiddle table follows the rotation strip (rec_mode 3)
+      const size_t smem = Lay::SMEM_BYTES + sizeof(float2) * Lay::STRIP_ELEMS + (rec_mode == 3 ? TwTable<N>::BYTES : 0);
       auto go = [&](auto kern) -> cudaError_t {
         cudaError_t e2 = allow_smem(kern, smem);
         if (e2 != cudaSuccess) return e2;
         kern<<<dim3(strips, chunks), Lay::THREADS, smem, st>>>(Rs, cturn, zlist, dz_uniform, U, z0, z1, zpb, umap);
         return cudaGetLastError();
       };
-      if (rec_mode == 2) return tma ? go(k_adj_col_rec<N, true, true>) : go(k_adj_col_rec<N, false, true>);
-      return tma ? go(k_adj_col_rec<N, true, false>) : go(k_adj_col_rec<N, false, false>);
+      if (rec_mode == 3) return tma ? go(k_adj_col_rec<N, true, 2>) : go(k_adj_col_rec<N, false, 2>);
+      if (rec_mode == 2) return tma ? go(k_adj_col_rec<N, true, 1>) : go(k_adj_col_rec<N, false, 1>);
+      return tma ? go(k_adj_col_rec<N, true, 0>) : go(k_adj_col_rec<N, false, 0>);
     }
   }
   if (tma) {
@@ -954,7 +1187,7 @@ static int fwd_col_chunks_fast(int W, int H, int Nz) {
 
 template <int N>
 static cudaError_t fwd_col_n(const float2* T, const double* cturn, const double* zlist, float2* Spart, int W,
-                             int z0, int z1, int nchunks, cudaStream_t st, double dz_uniform) {
+                             int z0, int z1, int nchunks, cudaStream_t st, double dz_uniform, int horner_mode) {
   using Lay = ColLayout<N>;
   const int nz = z1 - z0;
   if (nz <= 0) return cudaSuccess;
@@ -965,6 +1198,23 @@ static cudaError_t fwd_col_n(const float2* T, const double* cturn, const double*
   if (chunks < nchunks) {  // unused chunk slots must read as zero
     e = cudaMemsetAsync(Spart + (size_t)chunks * N * W, 0, sizeof(float2) * (size_t)(nchunks - chunks) * N * W, st);
     if (e != cudaSuccess) return e;
+  }
+  if constexpr (Lay::STAGE && LineCfg<N>::EXACT && kHoistTw<N>) {
+    if (dz_uniform != 0.0 && (horner_mode == 2 || horner_mode == 3)) {
+      constexpr size_t smem = horner1_smem<N>();
+      CUtensorMap tmap;
+      std::memset(&tmap, 0, sizeof(tmap));
+      // mode 3: TMA strip loads where the map can be made (square planes, column blocks that tile the row)
+      const bool tma = horner_mode == 3 && W == N && (N % Lay::CC == 0) &&
+                       plane_stack_map(&tmap, const_cast<float2*>(T), N, z1, Lay::CC, tma_rows<N>());
+      auto go = [&](auto kern) -> cudaError_t {
+        cudaError_t e2 = allow_smem(kern, smem);
+        if (e2 != cudaSuccess) return e2;
+        kern<<<dim3(strips, chunks), Lay::THREADS, smem, st>>>(T, cturn, zlist, dz_uniform, Spart, z0, z1, zpb, tmap);
+        return cudaGetLastError();
+      };
+      return tma ? go(k_fwd_col_horner1<N, true>) : go(k_fwd_col_horner1<N, false>);
+    }
   }
   if constexpr (Lay::STAGE && LineCfg<N>::EXACT) {
     if (dz_uniform != 0.0) {
@@ -981,12 +1231,12 @@ static cudaError_t fwd_col_n(const float2* T, const double* cturn, const double*
   return cudaGetLastError();
 }
 
-bool fwd_horner_supported(int W, int H) {
+bool fwd_horner_supported(int W, int H, int horner_mode) {
   if (W != H) return false;
   switch (H) {
 #define RIHVR_CASE(NN) \
   case NN:             \
-    return ColLayout<NN>::STAGE && LineCfg<NN>::EXACT;
+    return ColLayout<NN>::STAGE && LineCfg<NN>::EXACT && (horner_mode < 2 || kHoistTw<NN>);
     RIHVR_FOR_EACH_SIZE(RIHVR_CASE)
 #undef RIHVR_CASE
     default:
@@ -995,12 +1245,13 @@ bool fwd_horner_supported(int W, int H) {
 }
 
 static cudaError_t launch_fwd_col_fast(const float2* T, const double* cturn, const double* zlist, float2* Spart,
-                                      int W, int H, int z0, int z1, int nchunks, cudaStream_t st, double dz_uniform) {
+                                      int W, int H, int z0, int z1, int nchunks, cudaStream_t st, double dz_uniform,
+                                      int horner_mode) {
   if (W != H) return cudaErrorInvalidValue;
   switch (H) {
 #define RIHVR_CASE(NN) \
   case NN:             \
-    return fwd_col_n<NN>(T, cturn, zlist, Spart, W, z0, z1, nchunks, st, dz_uniform);
+    return fwd_col_n<NN>(T, cturn, zlist, Spart, W, z0, z1, nchunks, st, dz_uniform, horner_mode);
     RIHVR_FOR_EACH_SIZE(RIHVR_CASE)
 #undef RIHVR_CASE
     default:
@@ -2752,9 +3003,20 @@ cudaError_t launch_adj_col(const float2* Rs, const double* cturn, const double* 
   return cudaGetLastError();
 }
 
+cudaError_t col_wait_timeouts(cudaStream_t st, unsigned* count) {
+  unsigned zero = 0;
+  cudaError_t e = cudaMemcpyFromSymbolAsync(count, g_col_wait_timeouts, sizeof(unsigned), 0, cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e == cudaSuccess && *count) e = cudaMemcpyToSymbolAsync(g_col_wait_timeouts, &zero, sizeof(unsigned), 0,
+                                                              cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess && *count) e = cudaStreamSynchronize(st);
+  return e;
+}
+
 cudaError_t launch_fwd_col(const float2* T, const double* cturn, const double* zlist, float2* Spart, int W, int H,
-                           int z0, int z1, int nchunks, cudaStream_t st, double dz_uniform) {
-  if (fast_square(W, H)) return launch_fwd_col_fast(T, cturn, zlist, Spart, W, H, z0, z1, nchunks, st, dz_uniform);
+                           int z0, int z1, int nchunks, cudaStream_t st, double dz_uniform, int horner_mode) {
+  if (fast_square(W, H))
+    return launch_fwd_col_fast(T, cturn, zlist, Spart, W, H, z0, z1, nchunks, st, dz_uniform, horner_mode);
   const int nz = z1 - z0;
   if (nz <= 0) return cudaSuccess;
   GPlan p;

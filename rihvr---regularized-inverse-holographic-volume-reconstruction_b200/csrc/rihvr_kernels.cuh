@@ -74,18 +74,27 @@ bool adj_recurrence_supported(int W, int H);
 // dz_uniform != 0: the planes are evenly spaced by dz_uniform (z_{k+1} - z_k,
 // exact in FP64), which lets the square fast sizes advance the transfer
 // function by a recurrence (rec_mode 1: twiddles regenerated each plane, three
-// blocks an SM; 2: twiddles kept in registers, two blocks an SM); rec_mode 0
-// or dz_uniform 0 takes the direct evaluation at every plane.
+// blocks an SM; 2: twiddles kept in registers, two blocks an SM; 3: twiddles
+// from a per-block shared table, three blocks an SM); rec_mode 0 or
+// dz_uniform 0 takes the direct evaluation at every plane.
 cudaError_t launch_adj_col(const float2* Rs, const double* cturn, const double* zlist, float2* U, int W,
                            int H, int z0, int z1, cudaStream_t st, int chunks_hint = 0, double dz_uniform = 0.0,
                            int rec_mode = 0);
 cudaError_t launch_rows(int inverse, int in_kind, const void* in, int out_kind, void* out, int W,
                         long long nlines, float scale, cudaStream_t st);
 // dz_uniform != 0 (evenly spaced planes): square staged sizes sum over z by
-// Horner's scheme with the rotation H'_dz (fwd_horner_supported)
+// Horner's scheme with the rotation H'_dz (fwd_horner_supported); horner_mode
+// 1 stages T in its own double buffer (two blocks an SM), 2 in the exchange
+// buffer with the twiddles in a shared table (three blocks an SM), 3 the same
+// with each strip loaded by TMA (bounded mbarrier waits, col_wait_timeouts).
 cudaError_t launch_fwd_col(const float2* T, const double* cturn, const double* zlist, float2* Spart, int W,
-                           int H, int z0, int z1, int nchunks, cudaStream_t st, double dz_uniform = 0.0);
-bool fwd_horner_supported(int W, int H);
+                           int H, int z0, int z1, int nchunks, cudaStream_t st, double dz_uniform = 0.0,
+                           int horner_mode = 1);
+bool fwd_horner_supported(int W, int H, int horner_mode = 1);
+// Bounded waits of the TMA-fed column passes that ran out since the last call
+// (synchronises the stream; clears the count).  Nonzero means a forward sum
+// was left incomplete.
+cudaError_t col_wait_timeouts(cudaStream_t st, unsigned* count);
 int fwd_col_chunks(int W, int H, int Nz);
 cudaError_t launch_plane_col(int inverse, const float2* in, float2* out, int W, int H, float scale,
                              cudaStream_t st);

@@ -378,7 +378,8 @@ int reduce_into(rihvr_ctx* c, int nblocks, int slot) {
 int adjoint_volume(rihvr_ctx* c) {
   {
     ProfScope ps(c, K_ADJ_COL);
-    const int rec = env_variant("RIHVR_ADJ_COL", {"direct", "recurrence", "recurrence_hoisted"}, c->tune_adj_rec);
+    const int rec = env_variant("RIHVR_ADJ_COL", {"direct", "recurrence", "recurrence_hoisted", "recurrence_table"},
+                                c->tune_adj_rec);
     KL(launch_adj_col(c->Rs, c->cturn, c->zlist, c->U, c->W, c->H, 0, c->Nz, c->st, c->tune_adj_chunks,
                       rec ? c->dz_uniform : 0.0, rec));
   }
@@ -397,9 +398,10 @@ int forward_volume(rihvr_ctx* c, int kind, const void* vol) {
   }
   {
     ProfScope ps(c, K_FWD_COL);
-    const int hor = env_variant("RIHVR_FWD_COL", {"direct", "horner"}, c->tune_fwd_horner);
+    const int hor = env_variant("RIHVR_FWD_COL", {"direct", "horner", "horner_onebuf", "horner_tma"},
+                                c->tune_fwd_horner);
     KL(launch_fwd_col(c->U, c->cturn, c->zlist, c->Spart, c->W, c->H, 0, c->Nz, c->nchunks, c->st,
-                      hor ? c->dz_uniform : 0.0));
+                      hor ? c->dz_uniform : 0.0, hor));
   }
   ProfScope ps(c, K_PLANE);
   KL(launch_sum_chunks(c->Spart, c->nchunks, c->S, (long long)c->HW, c->st));
@@ -1001,11 +1003,22 @@ int eager_start(rihvr_ctx* c, int n, int* ran) {
   return RIHVR_OK;
 }
 
+// The TMA-fed forward column pass bounds its waits; a wait that ran out left a
+// forward sum incomplete, which is reported here instead of a wrong result.
+int check_col_waits(rihvr_ctx* c) {
+  unsigned n = 0;
+  CK(col_wait_timeouts(c->st, &n));
+  if (n)
+    return fail(RIHVR_ERR_CUDA, std::to_string(n) + " bounded wait(s) of the forward column pass ran out");
+  return RIHVR_OK;
+}
+
 int run_iterations(rihvr_ctx* c, int n) {
   if (!c->have_holo) return fail(RIHVR_ERR_MISSING_DATA, "no hologram set");
   int i = 0;
   RC(eager_start(c, n, &i));
-  return run_iterations_from(c, i, n);
+  RC(run_iterations_from(c, i, n));
+  return check_col_waits(c);
 }
 
 int copy_out(rihvr_ctx* c, void* dst, const void* src, size_t bytes, int is_device) {
@@ -1294,7 +1307,7 @@ int autotune_run(rihvr_ctx* c, cudaEvent_t e0, cudaEvent_t e1, TuneVal* out) {
   //    spaced planes or evaluated at every plane, and its z-chunks
   int best_adj = 0, best_rec = 0;
   float t_adj = 1e30f;
-  for (int rec : {0, 2, 1}) {
+  for (int rec : {0, 2, 1, 3}) {
     if (rec && (c->dz_uniform == 0 || !adj_recurrence_supported(c->W, c->H))) continue;
     for (int ch : {0, 2, 4, 8, 16, 32}) {
       if (ch > c->Nz) continue;
@@ -1343,13 +1356,13 @@ int autotune_run(rihvr_ctx* c, cudaEvent_t e0, cudaEvent_t e1, TuneVal* out) {
   //    (with the sum of the partial spectra)
   int best_fwd = c->nchunks, best_horner = 0;
   float t_fwd = 1e30f;
-  for (int hor : {1, 0}) {
-    if (hor && (c->dz_uniform == 0 || !fwd_horner_supported(c->W, c->H))) continue;
+  for (int hor : {1, 2, 3, 0}) {
+    if (hor && (c->dz_uniform == 0 || !fwd_horner_supported(c->W, c->H, hor))) continue;
     for (int ch : {c->nchunks, 1, 2, 4, 8, 16}) {
       if (ch > c->Nz || ch > kMaxFwdChunks) continue;
       RC(time_min(c, e0, e1, [&]() -> int {
         KL(launch_fwd_col(c->U, c->cturn, c->zlist, c->Spart, c->W, c->H, 0, c->Nz, ch, c->st,
-                          hor ? c->dz_uniform : 0.0));
+                          hor ? c->dz_uniform : 0.0, hor));
         KL(launch_sum_chunks(c->Spart, ch, c->S, (long long)c->HW, c->st));
         return RIHVR_OK;
       }, &best));
@@ -1379,7 +1392,9 @@ int rihvr_tuning(const rihvr_ctx* c, int* adj_chunks, int* fwd_chunks, int* tv_r
   if (adj_recurrence)
     *adj_recurrence = (c->dz_uniform != 0 && adj_recurrence_supported(c->W, c->H)) ? c->tune_adj_rec : 0;
   if (fwd_horner)
-    *fwd_horner = (c->tune_fwd_horner && c->dz_uniform != 0 && fwd_horner_supported(c->W, c->H)) ? 1 : 0;
+    *fwd_horner = (c->tune_fwd_horner && c->dz_uniform != 0 && fwd_horner_supported(c->W, c->H, c->tune_fwd_horner))
+                      ? c->tune_fwd_horner
+                      : 0;
   if (fwd_chunks) *fwd_chunks = c->nchunks;
   if (tv_runs) *tv_runs = c->tune_tv_nseg;
   if (tv_kernel) *tv_kernel = c->tune_tv_kernel;
@@ -1754,6 +1769,7 @@ int rihvr_forward(rihvr_ctx* c, const float* volume, float* holo_out, int is_dev
   if (!c || !volume || !holo_out) return fail(RIHVR_ERR_INVALID_ARGUMENT, "NULL argument");
   RC(copy_in(c, c->G, volume, sizeof(float2) * c->V, is_device));
   RC(forward_volume(c, ELEM_C32, c->G));
+  RC(check_col_waits(c));
   return copy_out(c, holo_out, c->dnew, sizeof(float) * c->HW, is_device);
 }
 

@@ -276,7 +276,8 @@ def test_errors_are_status_codes(rihvr):
 
 @pytest.mark.parametrize("side,nz", [(1024, 20), (512, 37), (256, 50), (64, 19)])
 @pytest.mark.parametrize("adj,fwd", [("direct", "direct"), ("recurrence", "horner"),
-                                     ("recurrence_hoisted", "horner")])
+                                     ("recurrence_hoisted", "horner"), ("recurrence_table", "horner_onebuf"),
+                                     ("recurrence_hoisted", "horner_tma")])
 def test_column_pass_variants_match_oracle(rihvr, monkeypatch, side, nz, adj, fwd):
     """Every column-pass variant for evenly spaced planes (selected by name,
     as the autotuner would pick them) against the FP64 oracle: the adjoint's
@@ -295,3 +296,30 @@ def test_column_pass_variants_match_oracle(rihvr, monkeypatch, side, nz, adj, fw
     op = oparams(rihvr, p, side)
     assert rel(d, O.forward(op, vol.astype(np.complex128))) < TOL_F32
     assert rel(g, O.adjoint(op, r.astype(np.float64))) < TOL_F32
+
+
+@pytest.mark.parametrize("side,nz", [(1024, 20), (512, 37), (256, 50), (64, 19)])
+def test_table_twiddle_variants_bits_equal_register_forms(rihvr, monkeypatch, side, nz):
+    """The three-blocks-an-SM column passes (twiddles from a shared table; the
+    forward pass's strip staged in the exchange buffer, by cp.async or by TMA)
+    compute the same FP32
+    operations as the register-resident forms.  The forward sums are
+    bit-equal.  The adjoint's default z-chunks differ between the two (more
+    blocks resident, more chunks), and the recurrence re-anchors every 16
+    planes from each chunk's first plane, so its last bits may differ."""
+    p = make(rihvr, side, nz)
+    p.start_plane, p.plane_stepsize = 2500.0, 2.0
+    rng = np.random.default_rng(side * 5 + nz)
+    vol = rand_volume(rng, nz, side)
+    r = rng.standard_normal((side, side)).astype(np.float32)
+    out = []
+    for adj, fwd in (("recurrence_hoisted", "horner"), ("recurrence_table", "horner_onebuf"),
+                     ("recurrence_table", "horner_tma")):
+        monkeypatch.setenv("RIHVR_ADJ_COL", adj)
+        monkeypatch.setenv("RIHVR_FWD_COL", fwd)
+        with rihvr.SparseCompressiveHolo(p, side, side) as s:
+            out.append((s.forward(vol), s.adjoint(r)))
+    (d0, g0), (d1, g1), (d2, _) = out
+    assert np.array_equal(d0, d1)
+    assert np.array_equal(d0, d2)
+    assert rel(g1, g0) < 2e-6
