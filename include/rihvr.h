@@ -220,8 +220,14 @@ int rihvr_reconstruct(rihvr_ctx* ctx, double* final_objective);
  * (rihvr_set_batch_mode), frames that share a device and iteration count run
  * the iterations after the first as ONE graph launch per iteration for all
  * frames: each frame's iteration (its attempts, backtracking test and
- * momentum step, decided on the device) is a branch of the same graph.
- * Either way the results are those of the sequential calls, bit for bit.  The
+ * momentum step, decided on the device) is a branch of the same graph.  In
+ * batch mode 2, frames that share a device run all their iterations after the
+ * first as ONE graph launch (up to 256 iterations a frame per launch): each
+ * frame is a branch that loops on the device at its own pace, with its own
+ * iteration count; the graph of the last mode-2 call is kept, and a call on
+ * the same contexts (none re-tuned or destroyed since) launches it without
+ * capturing again.  Either way the results are those of the sequential calls,
+ * bit for bit.  The
  * contexts must be distinct and may differ in size and parameters.
  * final_objectives and statuses (n entries each) may be NULL; statuses[i]
  * receives frame i's status.  Returns the first nonzero status in frame order. */
@@ -229,14 +235,15 @@ int rihvr_reconstruct_batch(rihvr_ctx* const* ctxs, int n, const float* const* h
                             double* final_objectives, int* statuses);
 
 /* Process-wide batch mode: 0 = one host thread and stream per frame
- * (default), 1 = one graph launch per iteration for all frames.  Mode 1 pays
- * a graph build per call and keeps the frames in step at every iteration; it
- * measured slower than mode 0 on every frame set tried.  Returns
+ * (default), 1 = one graph launch per iteration for all frames, 2 = one graph
+ * launch for the whole solves of all frames.  Modes 1 and 2 pay a graph build
+ * per call; mode 1 also keeps the frames in step at every iteration.  Returns
  * RIHVR_ERR_INVALID_ARGUMENT for other values. */
 int rihvr_set_batch_mode(int mode);
 
 /* 1 when the last rihvr_reconstruct_batch call on this host thread ran its
- * frames as one graph launch per iteration, else 0. */
+ * frames as one graph launch per iteration, 2 when it ran their whole solves
+ * as one graph launch, else 0. */
 int rihvr_batch_last_combined(void);
 
 /* Launch-shape autotuner (no reference counterpart).  Times the candidate

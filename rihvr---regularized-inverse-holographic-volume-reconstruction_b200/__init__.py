@@ -458,14 +458,16 @@ def reconstruct_batch(solvers, holograms):
 
 def set_batch_mode(mode: int):
     """rihvr_set_batch_mode: 0 = one host thread and stream per frame
-    (default), 1 = one graph launch per iteration for all frames."""
+    (default), 1 = one graph launch per iteration for all frames, 2 = one graph
+    launch for the whole solves of all frames."""
     _check(load_library().rihvr_set_batch_mode(int(mode)), "rihvr_set_batch_mode")
 
 
-def batch_last_combined() -> bool:
-    """Whether the last reconstruct_batch on this thread ran its frames as one
-    graph launch per iteration (rihvr_batch_last_combined)."""
-    return bool(load_library().rihvr_batch_last_combined())
+def batch_last_combined() -> int:
+    """How the last reconstruct_batch on this thread ran its frames
+    (rihvr_batch_last_combined): 1 one graph launch per iteration, 2 one graph
+    launch for the whole solves, 0 one loop per frame."""
+    return int(load_library().rihvr_batch_last_combined())
 
 
 def _io_check(rc: int, where: str):

@@ -1097,7 +1097,7 @@ static cudaError_t adj_col_n(const float2* Rs, const double* cturn, const double
   // thread; `rec_mode` 1 regenerates the twiddles each plane, 2 keeps them
   constexpr bool kRecOk = kHoistTw<N> && (N % Lay::CC == 0);
   const bool rec = kRecOk && dz_uniform != 0.0 && rec_mode != 0;
-  const int target = (rec && (rec_mode == 1 || rec_mode == 3) ? 12 : 8) * num_sms();
+  const int target = (rec && rec_mode != 2 ? 12 : 8) * num_sms();
   int chunks = chunks_hint > 0 ? chunks_hint : (target + strips - 1) / strips;
   if (chunks > nz) chunks = nz;
   if (chunks < 1) chunks = 1;
@@ -1110,7 +1110,8 @@ static cudaError_t adj_col_n(const float2* Rs, const double* cturn, const double
   if constexpr (kRecOk) {
     if (rec) {
       // the twiddle table follows the rotation strip (rec_mode 3)
-      const size_t smem = Lay::SMEM_BYTES + sizeof(float2) * Lay::STRIP_ELEMS + (rec_mode == 3 ? TwTable<N>::BYTES : 0);
+      const size_t smem =
+          Lay::SMEM_BYTES + sizeof(float2) * Lay::STRIP_ELEMS + (rec_mode == 3 ? TwTable<N>::BYTES : 0);
       auto go = [&](auto kern) -> cudaError_t {
         cudaError_t e2 = allow_smem(kern, smem);
         if (e2 != cudaSuccess) return e2;

@@ -18,6 +18,7 @@
 #include <cstring>
 #include <initializer_list>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <tuple>
 #include <new>
@@ -251,6 +252,8 @@ struct rihvr_ctx {
   size_t ev_used = 0;
   size_t bytes = 0;
   long long launches = 0;  // kernels launched by this context
+  unsigned long long uid = 0;  // unique for the process (a reused address gets a new one)
+  unsigned graph_gen = 0;      // advanced whenever the context's captured graphs are dropped
   std::vector<void*> allocs;
 };
 
@@ -544,6 +547,7 @@ int enqueue_momentum(rihvr_ctx* c) {
 }
 
 void drop_graphs(rihvr_ctx* c) {
+  ++c->graph_gen;
   for (auto& row : c->g_att)
     for (auto& g : row)
       if (g) {
@@ -850,6 +854,229 @@ int run_iterations_batch(rihvr_ctx* const* cs, int nc, int n, const BatchGraphs&
   return RIHVR_OK;
 }
 
+// Whole solves as one graph launch (batch mode 2).  Every frame is a branch of
+// one graph: a kernel that sets the frame's loop condition from its device
+// loop state, then a WHILE node whose body selects the iteration capture for
+// the frame's current rotation position with a SWITCH node (three bodies,
+// each the sequence capture_iteration records, with its own WHILE node of
+// backtracking attempts) and advances the loop state.  Each frame loops on the
+// device at its own pace, with its own iteration count; the host launches the
+// graph once for up to kDevLogCap iterations of every frame.  Every body is
+// the sequence build_iter_graph captures, so the iterates are those of
+// run_iterations_dev, bit for bit.
+struct LoopCtl {
+  int remaining;  // iterations still to run in this launch
+  int slot;       // position of P_k in the rotation
+};
+
+__global__ void k_loop_init(const LoopCtl* L, cudaGraphConditionalHandle hw) {
+  cudaGraphSetConditional(hw, L->remaining > 0 ? 1u : 0u);
+}
+__global__ void k_loop_select(const LoopCtl* L, cudaGraphConditionalHandle hs) {
+  cudaGraphSetConditional(hs, (unsigned)L->slot);
+}
+__global__ void k_loop_step(LoopCtl* L, cudaGraphConditionalHandle hw) {
+  L->remaining -= 1;
+  L->slot = L->slot == 2 ? 0 : L->slot + 1;  // rotate(): the new P_k is the old P_{k+1}
+  cudaGraphSetConditional(hw, L->remaining > 0 ? 1u : 0u);
+}
+
+struct SolveGraph {
+  cudaGraphExec_t g = nullptr;
+  LoopCtl* L_d = nullptr;  // one per frame
+  LoopCtl* L_h = nullptr;  // pinned staging
+  std::vector<int> n_main, n_body;
+  SolveGraph() = default;
+  SolveGraph(const SolveGraph&) = delete;
+  SolveGraph& operator=(const SolveGraph&) = delete;
+  ~SolveGraph() {
+    if (g) cudaGraphExecDestroy(g);
+    if (L_d) cudaFree(L_d);
+    if (L_h) cudaFreeHost(L_h);
+  }
+};
+
+// capture `enqueue` (kernel launches on c->st) into graph g after `deps`;
+// `tail` receives the capture's last nodes
+template <typename F>
+int capture_into(rihvr_ctx* c, cudaGraph_t g, const std::vector<cudaGraphNode_t>& deps,
+                 std::vector<cudaGraphNode_t>* tail, F enqueue) {
+  CK(cudaStreamBeginCaptureToGraph(c->st, g, deps.empty() ? nullptr : deps.data(), nullptr, deps.size(),
+                                   cudaStreamCaptureModeThreadLocal));
+  const int rc = enqueue();
+  cudaStreamCaptureStatus status;
+  const cudaGraphNode_t* d = nullptr;
+  size_t nd = 0;
+  const cudaError_t e = cudaStreamGetCaptureInfo(c->st, &status, nullptr, nullptr, &d, &nd);
+  if (tail) tail->assign(d, d + (e == cudaSuccess ? nd : 0));
+  cudaGraph_t cap = nullptr;
+  const cudaError_t e2 = cudaStreamEndCapture(c->st, &cap);
+  if (rc != RIHVR_OK) return rc;
+  CK(e);
+  CK(e2);
+  return RIHVR_OK;
+}
+
+int build_solve_graph(rihvr_ctx* const* cs, int n, SolveGraph& S) {
+  S.n_main.assign(n, 0);
+  S.n_body.assign(n, 0);
+  CK(cudaMalloc(&S.L_d, sizeof(LoopCtl) * n));
+  CK(cudaMallocHost(&S.L_h, sizeof(LoopCtl) * n));
+  GraphGuard guard;
+  CK(cudaGraphCreate(&guard.g, 0));
+  for (int i = 0; i < n; ++i) {
+    rihvr_ctx* c = cs[i];
+    LoopCtl* L = S.L_d + i;
+    cudaGraphConditionalHandle hw, hs;
+    CK(cudaGraphConditionalHandleCreate(&hw, guard.g, 0, 0));
+    std::vector<cudaGraphNode_t> tail;
+    RC(capture_into(c, guard.g, {}, &tail, [&]() -> int {
+      CK((k_loop_init<<<1, 1, 0, c->st>>>(L, hw), cudaGetLastError()));
+      return RIHVR_OK;
+    }));
+    cudaGraphNodeParams wp = {};
+    wp.type = cudaGraphNodeTypeConditional;
+    wp.conditional.handle = hw;
+    wp.conditional.type = cudaGraphCondTypeWhile;
+    wp.conditional.size = 1;
+    cudaGraphNode_t wnode;
+    CK(cudaGraphAddNode(&wnode, guard.g, tail.data(), tail.size(), &wp));
+    cudaGraph_t body = wp.conditional.phGraph_out[0];
+    CK(cudaGraphConditionalHandleCreate(&hs, body, 0, 0));
+    RC(capture_into(c, body, {}, &tail, [&]() -> int {
+      CK((k_loop_select<<<1, 1, 0, c->st>>>(L, hs), cudaGetLastError()));
+      return RIHVR_OK;
+    }));
+    cudaGraphNodeParams sp = {};
+    sp.type = cudaGraphNodeTypeConditional;
+    sp.conditional.handle = hs;
+    sp.conditional.type = cudaGraphCondTypeSwitch;
+    sp.conditional.size = 3;
+    cudaGraphNode_t snode;
+    CK(cudaGraphAddNode(&snode, body, tail.data(), tail.size(), &sp));
+    const int p0 = c->iPrev, c0 = c->iCur, n0 = c->iNew;
+    for (int slot = 0; slot < 3; ++slot) {
+      c->iCur = slot;
+      c->iPrev = (slot + 2) % 3;
+      c->iNew = (slot + 1) % 3;
+      const int rc = capture_iteration(c, sp.conditional.phGraph_out[slot], &S.n_main[i], &S.n_body[i]);
+      c->iPrev = p0;
+      c->iCur = c0;
+      c->iNew = n0;
+      if (rc != RIHVR_OK) return rc;
+    }
+    RC(capture_into(c, body, {snode}, nullptr, [&]() -> int {
+      CK((k_loop_step<<<1, 1, 0, c->st>>>(L, hw), cudaGetLastError()));
+      return RIHVR_OK;
+    }));
+  }
+  CK(cudaGraphInstantiate(&S.g, guard.g, 0));
+  return RIHVR_OK;
+}
+
+// The last solve graph built, kept for the next batch call on the same
+// contexts: its key is every context's uid and graph generation, in order, so
+// a context that was re-tuned (its graphs dropped) or destroyed never reuses
+// it; rihvr_destroy releases it when one of its contexts goes.
+struct SolveCache {
+  std::mutex mu;
+  std::vector<std::pair<unsigned long long, unsigned>> key;
+  std::unique_ptr<SolveGraph> S;
+};
+SolveCache& solve_cache() {
+  static SolveCache* cache = new SolveCache;  // never destroyed: no CUDA calls at process exit
+  return *cache;
+}
+
+std::vector<std::pair<unsigned long long, unsigned>> solve_key(rihvr_ctx* const* cs, int n) {
+  std::vector<std::pair<unsigned long long, unsigned>> k(n);
+  for (int i = 0; i < n; ++i) k[i] = {cs[i]->uid, cs[i]->graph_gen};
+  return k;
+}
+
+// the cached solve graph for these contexts (removed from the cache while in
+// use), or a newly built one; null on failure
+std::unique_ptr<SolveGraph> take_solve_graph(rihvr_ctx* const* cs, int n) {
+  const auto key = solve_key(cs, n);
+  {
+    SolveCache& sc = solve_cache();
+    std::lock_guard<std::mutex> lk(sc.mu);
+    if (sc.S && sc.key == key) {
+      sc.key.clear();
+      return std::move(sc.S);
+    }
+  }
+  std::unique_ptr<SolveGraph> S(new (std::nothrow) SolveGraph);
+  if (!S || build_solve_graph(cs, n, *S) != RIHVR_OK) return nullptr;
+  return S;
+}
+
+void keep_solve_graph(rihvr_ctx* const* cs, int n, std::unique_ptr<SolveGraph> S) {
+  SolveCache& sc = solve_cache();
+  std::lock_guard<std::mutex> lk(sc.mu);
+  sc.key = solve_key(cs, n);
+  sc.S = std::move(S);  // the previous one, if any, is released here
+}
+
+// a context is going away: drop a cached solve graph that runs it
+void forget_solve_graph(const rihvr_ctx* c) {
+  SolveCache& sc = solve_cache();
+  std::lock_guard<std::mutex> lk(sc.mu);
+  for (const auto& k : sc.key)
+    if (k.first == c->uid) {
+      sc.S.reset();
+      sc.key.clear();
+      return;
+    }
+}
+
+// iters[i] iterations of every context through the solve graph, at most
+// kDevLogCap a launch, on the first context's stream (the other streams are
+// ordered before and after it).  The contexts share a device.
+int run_solves_graph(rihvr_ctx* const* cs, int nc, const std::vector<int>& iters, const SolveGraph& S) {
+  cudaStream_t st = cs[0]->st;
+  EventGuard ev;
+  CK(cudaEventCreateWithFlags(&ev.e, cudaEventDisableTiming));
+  for (int i = 1; i < nc; ++i) {
+    CK(cudaEventRecord(ev.e, cs[i]->st));
+    CK(cudaStreamWaitEvent(st, ev.e, 0));
+  }
+  std::vector<int> done(nc, 0);
+  for (;;) {
+    bool any = false;
+    std::vector<int> m(nc, 0);
+    for (int i = 0; i < nc; ++i) {
+      m[i] = std::min(iters[i] - done[i], kDevLogCap);
+      any = any || m[i] > 0;
+    }
+    if (!any) break;
+    for (int i = 0; i < nc; ++i) {
+      S.L_h[i].remaining = m[i];
+      S.L_h[i].slot = cs[i]->iCur;
+      stage_ctl(cs[i]);
+      CK(cudaMemcpyAsync(cs[i]->ctl_d, cs[i]->ctl_h, sizeof(IterCtl), cudaMemcpyHostToDevice, st));
+    }
+    CK(cudaMemcpyAsync(S.L_d, S.L_h, sizeof(LoopCtl) * nc, cudaMemcpyHostToDevice, st));
+    CK(cudaGraphLaunch(S.g, st));
+    for (int i = 0; i < nc; ++i) {
+      CK(cudaMemcpyAsync(cs[i]->ctl_h, cs[i]->ctl_d, sizeof(IterCtl), cudaMemcpyDeviceToHost, st));
+      if (m[i] > 0)
+        CK(cudaMemcpyAsync(cs[i]->dlog_h, cs[i]->dlog_d, sizeof(DevRec) * m[i], cudaMemcpyDeviceToHost, st));
+    }
+    CK(cudaStreamSynchronize(st));
+    for (int i = 0; i < nc; ++i) {
+      if (m[i] == 0) continue;
+      cs[i]->launches += 1 + (long long)m[i] * (S.n_main[i] + 2);  // + the loop kernels
+      take_ctl(cs[i], m[i], S.n_body[i]);
+      for (int k = 0; k < m[i]; ++k) rotate(cs[i]);
+      done[i] += m[i];
+    }
+  }
+  CK(cudaEventRecord(ev.e, st));
+  for (int i = 1; i < nc; ++i) CK(cudaStreamWaitEvent(cs[i]->st, ev.e, 0));
+  return RIHVR_OK;
+}
+
 // RIHVR_ITER_LOOP=host selects the host-synchronised loop (one_iteration)
 // instead, for comparison; both give the same iterates bit for bit.
 bool dev_loop_enabled() {
@@ -862,7 +1089,8 @@ bool dev_loop_enabled() {
 
 // How rihvr_reconstruct_batch runs the iterations after the first
 // (rihvr_set_batch_mode): 0 = each frame's own device loop on its own host
-// thread and stream, 1 = one graph launch per iteration for all frames.
+// thread and stream, 1 = one graph launch per iteration for all frames,
+// 2 = one graph launch for the whole solves of all frames.
 std::atomic<int> g_batch_mode{0};
 
 // whether the last rihvr_reconstruct_batch call on this host thread ran its
@@ -1127,6 +1355,8 @@ int rihvr_create(const rihvr_params* params, int width, int height, rihvr_ctx** 
   }
   rihvr_ctx* c = new (std::nothrow) rihvr_ctx();
   if (!c) return fail(RIHVR_ERR_OUT_OF_MEMORY, "host allocation failed");
+  static std::atomic<unsigned long long> next_uid{1};
+  c->uid = next_uid.fetch_add(1);
   c->p = *params;
   c->W = width;
   c->H = height;
@@ -1201,6 +1431,7 @@ int rihvr_create(const rihvr_params* params, int width, int height, rihvr_ctx** 
 void rihvr_destroy(rihvr_ctx* c) {
   if (!c) return;
   if (c->st) cudaStreamSynchronize(c->st);
+  forget_solve_graph(c);
   drop_graphs(c);
   if (c->seg_ws) seg_workspace_destroy(c->seg_ws);
   frame_workspace_free(c->frame_ws);
@@ -1508,16 +1739,38 @@ int rihvr_reconstruct_batch(rihvr_ctx* const* ctxs, int n, const float* const* h
   });
   // the remaining iterations: in batch mode 1, one graph launch per iteration
   // for all frames when they share a device, run the device-decided loop and
-  // are at the same point; else each frame's own loop on its own thread
-  bool combined = n > 1 && g_batch_mode.load() == 1;
+  // are at the same point; in batch mode 2, one graph launch for the whole
+  // solves of all frames that share a device and run the device-decided loop
+  // (any iteration counts); else each frame's own loop on its own thread
+  const int bmode = g_batch_mode.load();
+  bool combined = n > 1 && bmode != 0;
   const int rest = ctxs[0]->p.num_inverse_iterations - ran[0];
+  std::vector<int> rests(n, 0);
+  bool any_rest = false;
   for (int i = 0; i < n && combined; ++i) {
     const rihvr_ctx* c = ctxs[i];
-    combined = st[i] == RIHVR_OK && use_dev_loop(c) && c->device == ctxs[0]->device &&
-               c->p.num_inverse_iterations - ran[i] == rest && c->iCur == ctxs[0]->iCur;
+    rests[i] = c->p.num_inverse_iterations - ran[i];
+    any_rest = any_rest || rests[i] > 0;
+    combined = st[i] == RIHVR_OK && use_dev_loop(c) && c->device == ctxs[0]->device;
+    if (bmode == 1) combined = combined && rests[i] == rest && c->iCur == ctxs[0]->iCur;
   }
-  combined = combined && rest > 0;
-  if (combined) {
+  combined = combined && (bmode == 2 ? any_rest : rest > 0);
+  if (combined && bmode == 2) {
+    std::unique_ptr<SolveGraph> S;
+    if (cudaSetDevice(ctxs[0]->device) == cudaSuccess) S = take_solve_graph(ctxs, n);
+    if (S) {
+      const int rc = run_solves_graph(ctxs, n, rests, *S);
+      for (int i = 0; i < n; ++i) {
+        st[i] = rc;
+        if (rc != RIHVR_OK) msg[i] = g_last_error;
+      }
+      if (rc == RIHVR_OK) keep_solve_graph(ctxs, n, std::move(S));
+      g_batch_combined = 2;
+    } else {
+      cudaGetLastError();
+      combined = false;
+    }
+  } else if (combined) {
     BatchGraphs B;
     if (cudaSetDevice(ctxs[0]->device) == cudaSuccess && build_batch_graphs(ctxs, n, B) == RIHVR_OK) {
       const int rc = run_iterations_batch(ctxs, n, rest, B);
@@ -1552,7 +1805,7 @@ int rihvr_reconstruct_batch(rihvr_ctx* const* ctxs, int n, const float* const* h
 }
 
 int rihvr_set_batch_mode(int mode) {
-  if (mode != 0 && mode != 1) return fail(RIHVR_ERR_INVALID_ARGUMENT, "batch mode must be 0 or 1");
+  if (mode < 0 || mode > 2) return fail(RIHVR_ERR_INVALID_ARGUMENT, "batch mode must be 0, 1 or 2");
   g_batch_mode.store(mode);
   return RIHVR_OK;
 }

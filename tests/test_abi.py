@@ -129,12 +129,13 @@ def test_batch_validates_before_touching_contexts(rihvr):
 
 
 def test_batch_mode_setting(rihvr):
-    """rihvr_set_batch_mode takes 0 or 1 only; a rejected batch ran no frame
-    as one graph per iteration."""
+    """rihvr_set_batch_mode takes 0, 1 or 2 only; a rejected batch ran no
+    frame as a combined graph."""
     L = rihvr.load_library()
-    assert L.rihvr_set_batch_mode(2) == rihvr.ERR_INVALID_ARGUMENT
+    assert L.rihvr_set_batch_mode(3) == rihvr.ERR_INVALID_ARGUMENT
     assert L.rihvr_set_batch_mode(-1) == rihvr.ERR_INVALID_ARGUMENT
     assert L.rihvr_set_batch_mode(1) == rihvr.OK
     assert L.rihvr_reconstruct_batch(None, 1, None, 0, None, None) == rihvr.ERR_INVALID_ARGUMENT
     assert L.rihvr_batch_last_combined() == 0
+    assert L.rihvr_set_batch_mode(2) == rihvr.OK
     assert L.rihvr_set_batch_mode(0) == rihvr.OK
