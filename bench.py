@@ -46,6 +46,18 @@ def peaks():
         return FALLBACK_HBM_GBS, "fallback"
 
 
+FALLBACK_BF16_TFLOPS = 1590.0
+
+
+def bf16_peak():
+    """Dense BF16 tensor-core peak (burst) in TFLOP/s and where it came from."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["bf16_tflops"]), "measured (burst)"
+    except Exception:
+        return FALLBACK_BF16_TFLOPS, "fallback"
+
+
 def dist_env():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -533,6 +545,58 @@ def run_warmstart4(args):
     return 0
 
 
+UNET_LAYERS = [(16, 16, 0), (16, 16, 0), (16, 32, 1), (32, 32, 1), (32, 64, 2), (64, 64, 2), (96, 32, 1),
+               (32, 32, 1), (48, 16, 0), (16, 16, 0)]  # (in, out channels, level) of the 3x3x3 convolutions
+
+
+def run_unet(args):
+    """The warm-start network's inference alone (rihvr_unet_predict: input
+    normalisation, ten 3x3x3 convolutions on tcgen05 with BF16 activations,
+    pooling, upsampling, the head fused into the last layer) on a
+    `--nz` x 512 x 512 volume (default 200 planes, the warm start's
+    configuration) of random complex values, with the weights trained there.
+    A step is one inference; CUDA events on the network's stream.  Prints one
+    JSON line with the tensor-core throughput of the convolutions."""
+    import torch
+
+    torch.cuda.set_device(0)
+    rihvr = importlib.import_module(PKG)
+    ws = importlib.import_module(PKG + ".warmstart")
+    Z, S = (args.nz or ws.C4_PLANES), ws.C4_SIZE
+    weights = ws.C4_WEIGHTS if os.path.exists(ws.C4_WEIGHTS) else ws.WEIGHTS
+    g = torch.Generator(device="cuda").manual_seed(7)
+    xbp = torch.complex(torch.randn((Z, S, S), device="cuda", generator=g),
+                        torch.randn((Z, S, S), device="cuda", generator=g))
+    with rihvr.UNet(Z, S, S) as net:
+        net.load(weights)
+        bits = net.activation_bits()
+        for _ in range(max(3, args.warmup)):
+            net.predict(xbp)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with ClockSampler(0) as clk:
+            e0.record()
+            for _ in range(args.steps):
+                net.predict(xbp)
+            e1.record()
+            e1.synchronize()
+        ms = e0.elapsed_time(e1) / args.steps
+    vox = Z * S * S
+    flops = sum(2 * 27 * ci * co * vox // (8 ** lv) for ci, co, lv in UNET_LAYERS)
+    tf = flops / (ms * 1e-3) / 1e12
+    peak, src = bf16_peak()
+    line = {"metric": "warm-start network inference, TFLOP/s of the 3x3x3 convolutions", "value": tf,
+            "unit": "TFLOP/s", "higher_is_better": True, "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms, "dtype": "bf16", "data": "synthetic",
+            "config": {"workload": f"unet_inference_{Z}x{S}x{S}", "weights": os.path.basename(weights),
+                       "activation_bits": bits},
+            "roofline": {"bound": "tensor", "achieved": tf, "peak": peak, "unit": "TFLOP/s",
+                         "frac": tf / peak, "peak_source": src},
+            "conv_flops": flops, "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_ours(args):
     ws, rank, local = dist_env()
     import torch
@@ -681,7 +745,8 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="c2", choices=["c2", "c1", "c5", "series", "segment", "warmstart", "warmstart4"])
+    ap.add_argument("--config", default="c2",
+                    choices=["c2", "c1", "c5", "series", "segment", "warmstart", "warmstart4", "unet"])
     ap.add_argument("--frames", type=int, default=0,
                     help="frames of the uneven series (--config series, default 64) or of the warm-start set "
                          "(default 16; 256 for warmstart4)")
@@ -705,6 +770,8 @@ def main():
         return run_warmstart(args)
     if args.config == "warmstart4":
         return run_warmstart4(args)
+    if args.config == "unet":
+        return run_unet(args)
     return run_ours(args)
 
 
