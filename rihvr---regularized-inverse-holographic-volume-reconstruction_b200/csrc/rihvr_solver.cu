@@ -197,11 +197,12 @@ struct rihvr_ctx {
   double dz_uniform = 0;  // plane spacing when every z_{k+1} - z_k is the same (FP64), else 0
   // column-pass variants for evenly spaced planes (need dz_uniform): the
   // adjoint's transfer function by recurrence (1: twiddles regenerated each
-  // plane, 2: twiddles kept) or direct (0); the forward's z-sum by Horner's
-  // scheme (1) or direct (0).  Autotuned; RIHVR_ADJ_COL and RIHVR_FWD_COL
-  // select one by name.
+  // plane, 2: twiddles kept, 3: twiddles from a shared table) or direct (0);
+  // the forward's z-sum by Horner's scheme (1: two blocks an SM; 2, 3: three
+  // blocks an SM, the strip copied by cp.async or TMA) or direct (0).
+  // Autotuned; RIHVR_ADJ_COL and RIHVR_FWD_COL select one by name.
   int tune_adj_rec = 0;
-  int tune_fwd_horner = 1;
+  int tune_fwd_horner = 3;  // TMA-fed Horner pass; sizes without it take the two-block form (1)
   double* partials = nullptr;
   unsigned* nonfinite_d = nullptr;  // count of non-finite hologram samples (rihvr_set_hologram)
   size_t partial_cap = 0;
@@ -1623,8 +1624,10 @@ int rihvr_tuning(const rihvr_ctx* c, int* adj_chunks, int* fwd_chunks, int* tv_r
   if (adj_recurrence)
     *adj_recurrence = (c->dz_uniform != 0 && adj_recurrence_supported(c->W, c->H)) ? c->tune_adj_rec : 0;
   if (fwd_horner)
-    *fwd_horner = (c->tune_fwd_horner && c->dz_uniform != 0 && fwd_horner_supported(c->W, c->H, c->tune_fwd_horner))
-                      ? c->tune_fwd_horner
+    // the variant that runs: a three-block form (2, 3) falls back to the
+    // two-block form (1) at sizes that do not have it
+    *fwd_horner = (c->tune_fwd_horner && c->dz_uniform != 0 && fwd_horner_supported(c->W, c->H, 1))
+                      ? (fwd_horner_supported(c->W, c->H, c->tune_fwd_horner) ? c->tune_fwd_horner : 1)
                       : 0;
   if (fwd_chunks) *fwd_chunks = c->nchunks;
   if (tv_runs) *tv_runs = c->tune_tv_nseg;

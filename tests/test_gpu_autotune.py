@@ -23,7 +23,7 @@ def test_autotune_keeps_the_solution(rihvr, synthmod, cache_dir):
     (l0, x0, t0), (l1, x1, t1) = runs[0], runs[1]
     # evenly spaced planes: the untuned adjoint evaluates directly, the forward uses Horner's scheme
     assert t0 == {"adj_chunks": 0, "fwd_chunks": t0["fwd_chunks"], "tv_runs": 0, "tv_kernel": 0,
-                  "adj_recurrence": 0, "fwd_horner": 1}
+                  "adj_recurrence": 0, "fwd_horner": 3}
     assert t1["tv_kernel"] in (0, 1, 2) and 1 <= t1["fwd_chunks"] <= 16 and t1["adj_recurrence"] in (0, 1, 2, 3)
     assert t1["fwd_horner"] in (0, 1, 2, 3)
     assert np.array_equal(l0["backtracks"], l1["backtracks"])
@@ -64,7 +64,7 @@ def test_column_variants_only_for_evenly_spaced_planes(rihvr):
             t = s.tuning()
             return t["adj_recurrence"], t["fwd_horner"]
 
-    assert tuned(2500.0, 2.0) == (0, 1)  # untuned: direct adjoint, Horner forward
+    assert tuned(2500.0, 2.0) == (0, 3)  # untuned: direct adjoint, TMA-fed Horner forward
     z = np.float32(100.0) + np.arange(6, dtype=np.float32) * np.float32(0.1)
     assert len(set(np.diff(z.astype(np.float64)))) > 1  # uneven in FP64
     assert tuned(100.0, 0.1) == (0, 0)
