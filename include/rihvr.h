@@ -263,7 +263,8 @@ int rihvr_autotune(rihvr_ctx* ctx, double* best_ms);
 
 /* The launch shapes in use: z-chunks of the adjoint and forward column passes,
  * runs per plane of the streaming TV prox and the TV kernel (1 tiled,
- * 2 streaming); 0 means the built-in choice.  adj_recurrence receives the
+ * 2 streaming in 2-warp blocks, 3 streaming in 4-warp blocks); 0 means the
+ * built-in choice.  adj_recurrence receives the
  * adjoint column pass's variant for evenly spaced planes (square planes of side
  * 32 to 1024 except 384, 640 and 768): 0 transfer function evaluated at every
  * plane, 1 advanced by a recurrence with the inter-stage twiddles regenerated

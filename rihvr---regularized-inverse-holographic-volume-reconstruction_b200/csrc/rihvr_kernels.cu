@@ -2094,33 +2094,50 @@ static TvsGrid tvs_grid(int W, int H, int Nz, int VW, int warps_per_sm, int warm
   return g;
 }
 
-template <typename ST, int NTV, bool NORMS>
-static cudaError_t strip_launch_n(const ProxArgs& a, int* nblocks_out, cudaStream_t st) {
+// Warps a block of the streaming prox: 2 (built in), or 4 when the tuning
+// asks for it (tv_kernel 3) and the 8-row ring applies (n_tv <= 5), where
+// three 4-warp blocks (12 warps) share an SM at up to 168 registers.
+template <int NTV, bool NORMS, int NW>
+constexpr int tvw_minb_nw() {
+  return NW == 2 ? tvw_minb<NTV, NORMS>() : 3;
+}
+
+template <typename ST, int NTV, bool NORMS, int NW>
+static cudaError_t strip_launch_nw(const ProxArgs& a, int* nblocks_out, cudaStream_t st) {
   using Sh = TvwShape<NTV, 2>;
-  cudaError_t e = allow_smem(k_prox_tv2d_strip<ST, NTV, NORMS>, Sh::SMEM);
+  constexpr int MINB = tvw_minb_nw<NTV, NORMS, NW>();
+  constexpr size_t SMEM = Sh::SMEM / Sh::NW * NW;  // one ring a warp
+  auto kern = k_prox_tv2d_strip<ST, NTV, NORMS, 2, NW, MINB>;
+  cudaError_t e = allow_smem(kern, SMEM);
   if (e != cudaSuccess) return e;
   // resident blocks per SM, for the choice of runs per plane
-  static const int resident = [] {
+  static const int resident = [kern] {
     int b = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, k_prox_tv2d_strip<ST, NTV, NORMS>, 32 * Sh::NW, Sh::SMEM) !=
-            cudaSuccess ||
-        b <= 0) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b, kern, 32 * NW, SMEM) != cudaSuccess || b <= 0) {
       cudaGetLastError();
-      b = tvw_minb<NTV, NORMS>();
+      b = MINB;
     }
     return b;
   }();
-  TvsGrid g = tvs_grid(a.W, a.H, a.Nz, Sh::VW, Sh::NW * resident, 2 * Sh::h + 3);
+  TvsGrid g = tvs_grid(a.W, a.H, a.Nz, Sh::VW, NW * resident, 2 * Sh::h + 3);
   if (a.tv_nseg > 0) {  // tuned number of runs per plane
     g.seg_len = (a.H + min(a.tv_nseg, a.H) - 1) / min(a.tv_nseg, a.H);
     g.nseg = (a.H + g.seg_len - 1) / g.seg_len;
   }
   const long long runs = (long long)g.nstrips * g.nseg * a.Nz;
-  const long long blocks = (runs + Sh::NW - 1) / Sh::NW;
+  const long long blocks = (runs + NW - 1) / NW;
   if (blocks > 0x7fffffffLL || blocks > a.partial_cap) return cudaErrorInvalidConfiguration;
   *nblocks_out = (int)blocks;
-  k_prox_tv2d_strip<ST, NTV, NORMS><<<(unsigned)blocks, 32 * Sh::NW, Sh::SMEM, st>>>(a, g);
+  kern<<<(unsigned)blocks, 32 * NW, SMEM, st>>>(a, g);
   return cudaGetLastError();
+}
+
+template <typename ST, int NTV, bool NORMS>
+static cudaError_t strip_launch_n(const ProxArgs& a, int* nblocks_out, cudaStream_t st) {
+  if constexpr (TvwShape<NTV, 2>::D == 8) {
+    if (a.tv_kernel == 3) return strip_launch_nw<ST, NTV, NORMS, 4>(a, nblocks_out, st);
+  }
+  return strip_launch_nw<ST, NTV, NORMS, 2>(a, nblocks_out, st);
 }
 
 template <typename ST, int NTV>
@@ -2147,12 +2164,20 @@ static cudaError_t strip_dispatch(const ProxArgs& a, int* nb, cudaStream_t st) {
 }
 constexpr int kStripNtvMax = 10;
 
-// RIHVR_TV_KERNEL=tiles forces the tiled kernel (comparison and fallback);
-// read once per process.
+// RIHVR_TV_KERNEL=tiles forces the tiled kernel (comparison and fallback),
+// RIHVR_TV_KERNEL=strip4 the streaming kernel in 4-warp blocks; read once per
+// process.
 static bool tv_stream_enabled() {
   static const bool on = [] {
     const char* v = std::getenv("RIHVR_TV_KERNEL");
     return !(v && std::strcmp(v, "tiles") == 0);
+  }();
+  return on;
+}
+static bool tv_strip4_forced() {
+  static const bool on = [] {
+    const char* v = std::getenv("RIHVR_TV_KERNEL");
+    return v && std::strcmp(v, "strip4") == 0;
   }();
   return on;
 }
@@ -2178,10 +2203,12 @@ size_t max_partial_blocks(int W, int H, int Nz) {
 cudaError_t launch_prox_tv2d(int storage, const ProxArgs& a, int* nblocks_out, cudaStream_t st) {
   if (a.n_tv < 0 || a.n_tv > 20) return cudaErrorInvalidValue;
   if (a.n_tv >= 1 && a.n_tv <= kStripNtvMax && a.tv_kernel != 1 && tv_stream_enabled()) {
+    ProxArgs b = a;
+    if (tv_strip4_forced()) b.tv_kernel = 3;
     switch (storage) {
-      case STORE_BF16: return strip_dispatch<__nv_bfloat162>(a, nblocks_out, st);
-      case STORE_F16: return strip_dispatch<__half2>(a, nblocks_out, st);
-      default: return strip_dispatch<float2>(a, nblocks_out, st);
+      case STORE_BF16: return strip_dispatch<__nv_bfloat162>(b, nblocks_out, st);
+      case STORE_F16: return strip_dispatch<__half2>(b, nblocks_out, st);
+      default: return strip_dispatch<float2>(b, nblocks_out, st);
     }
   }
   dim3 g;

@@ -40,7 +40,8 @@ struct ProxArgs {
   double* partials;   // [blocks][kNumSums]
   long long partial_cap = 0;  // blocks partials holds; a launch needing more is refused
   // tuning knobs (0 = built-in choice): runs per plane of the streaming 2-D TV
-  // prox, and the 2-D TV kernel (1 tiled, 2 streaming)
+  // prox, and the 2-D TV kernel (1 tiled, 2 streaming in 2-warp blocks,
+  // 3 streaming in 4-warp blocks where the 8-row ring applies, n_tv <= 5)
   int tv_nseg = 0;
   int tv_kernel = 0;
   // device copy of (beta, t, mu, s, thr); when set, the 2-D TV and L1 prox

@@ -1559,10 +1559,11 @@ int autotune_run(rihvr_ctx* c, cudaEvent_t e0, cudaEvent_t e1, TuneVal* out) {
   c->tune_adj_rec = best_rec;
   // a valid gradient volume for the prox candidates
   KL(launch_rows(1, ELEM_C32, c->U, ELEM_C32, c->G, c->W, (long long)c->Nz * c->H, 1.0f, c->st));
-  // 2. 2-D TV prox: streaming with 1..8 runs per plane or the built-in count, or tiled
+  // 2. 2-D TV prox: streaming in 2- or 4-warp blocks with 1..8 runs per
+  //    plane or the built-in count, or tiled
   float t_tv = 0.f;
   if (c->mode == 7 && c->p.num_tv_iterations >= 1 && c->p.regularization_TV_param > 0.f) {
-    const int cand[6][2] = {{0, 0}, {2, 1}, {2, 2}, {2, 4}, {2, 8}, {1, 0}};
+    const int cand[9][2] = {{0, 0}, {2, 1}, {2, 2}, {2, 4}, {2, 8}, {3, 0}, {3, 2}, {3, 4}, {1, 0}};
     t_tv = 1e30f;
     int bk = 0, bn = 0;
     for (const auto& cd : cand) {

@@ -24,7 +24,7 @@ def test_autotune_keeps_the_solution(rihvr, synthmod, cache_dir):
     # evenly spaced planes: the untuned adjoint evaluates directly, the forward uses Horner's scheme
     assert t0 == {"adj_chunks": 0, "fwd_chunks": t0["fwd_chunks"], "tv_runs": 0, "tv_kernel": 0,
                   "adj_recurrence": 0, "fwd_horner": 3}
-    assert t1["tv_kernel"] in (0, 1, 2) and 1 <= t1["fwd_chunks"] <= 16 and t1["adj_recurrence"] in (0, 1, 2, 3)
+    assert t1["tv_kernel"] in (0, 1, 2, 3) and 1 <= t1["fwd_chunks"] <= 16 and t1["adj_recurrence"] in (0, 1, 2, 3)
     assert t1["fwd_horner"] in (0, 1, 2, 3)
     assert np.array_equal(l0["backtracks"], l1["backtracks"])
     assert np.array_equal(l0["restarted"], l1["restarted"])

@@ -153,8 +153,8 @@ np.save(sys.argv[7], out)
 @pytest.mark.parametrize("side,nz,ntv,storage", [(1024, 3, 5, 0), (384, 4, 3, 0), (768, 2, 6, 1), (256, 3, 4, 2),
                                                  (512, 2, 10, 2), (640, 2, 8, 0)])
 def test_streaming_prox_bits_equal_tiled(rihvr, tmp_path, side, nz, ntv, storage):
-    """The streaming TV prox reproduces the tiled kernel's P_new bit for bit
-    (run lengths odd and even, every storage type)."""
+    """The streaming TV prox, in 2- and 4-warp blocks, reproduces the tiled
+    kernel's P_new bit for bit (run lengths odd and even, every storage type)."""
     import subprocess
     import sys
 
@@ -163,17 +163,18 @@ def test_streaming_prox_bits_equal_tiled(rihvr, tmp_path, side, nz, ntv, storage
     script = tmp_path / "prox.py"
     script.write_text(_TILES_SCRIPT)
     outs = {}
-    for kern in ("tiles", "strip"):
+    for kern in ("tiles", "strip", "strip4"):
         env = dict(os.environ)
         env.pop("RIHVR_TV_KERNEL", None)
-        if kern == "tiles":
-            env["RIHVR_TV_KERNEL"] = "tiles"
+        if kern != "strip":
+            env["RIHVR_TV_KERNEL"] = kern
         f = tmp_path / f"{kern}.npy"
         r = subprocess.run([sys.executable, str(script), ROOT, PKG_NAME, str(side), str(nz), str(ntv), str(storage),
                             str(f)], env=env, capture_output=True, text=True, timeout=600)
         assert r.returncode == 0, r.stderr[-2000:]
         outs[kern] = np.load(f)
     assert np.array_equal(outs["tiles"].view(np.uint32), outs["strip"].view(np.uint32))
+    assert np.array_equal(outs["tiles"].view(np.uint32), outs["strip4"].view(np.uint32))
 
 
 def run_gpu(rihvr, p, side, b, n):
