@@ -514,6 +514,14 @@ struct TwTable {
   static constexpr size_t BYTES = sizeof(float2) * ELEMS;
 };
 
+// Blocks an SM the table-twiddle column kernels are compiled for: three for
+// lines of up to 32 elements a thread; one for 48 (sides 384, 768 and 2304),
+// whose lines alone take most of the register file.
+template <int N>
+constexpr int col3_minb() {
+  return LineCfg<N>::N2 <= 32 ? 3 : 1;
+}
+
 template <int N, bool INV>
 __device__ __forceinline__ void tw_table_build(float2* tab) {
   using C = LineCfg<N>;
@@ -572,7 +580,7 @@ constexpr int kAdjAnchor = 16;
 // per-block shared table (one 16-byte load per two elements, three blocks an
 // SM).  The autotuner picks one of these or the direct evaluation.
 template <int N, bool TMA, int TWM>
-__global__ void __launch_bounds__(ColLayout<N>::THREADS, TWM == 1 ? 2 : 3)
+__global__ void __launch_bounds__(ColLayout<N>::THREADS, TWM == 1 ? 2 : col3_minb<N>())
     k_adj_col_rec(const float2* __restrict__ Rs, const double* __restrict__ cturn, const double* __restrict__ zlist,
                   double dz, float2* __restrict__ U, int z0, int z1, int zpb,
                   const __grid_constant__ CUtensorMap umap) {
@@ -580,7 +588,7 @@ __global__ void __launch_bounds__(ColLayout<N>::THREADS, TWM == 1 ? 2 : 3)
   using C = LineCfg<N>;
   using Lay = ColLayout<N>;
   constexpr int N1 = C::N1, N2 = C::N2, M = C::M, CC = Lay::CC;
-  static_assert(N2 <= 32, "the recurrence keeps a line's elements in registers");
+  static_assert(N2 <= (TWM == 2 ? 48 : 32), "the recurrence keeps a line's elements in registers");
   constexpr int W = N;
   extern __shared__ __align__(128) float2 sm[];
   const int c = threadIdx.x % CC, t = threadIdx.x / CC;
@@ -855,6 +863,14 @@ constexpr size_t horner1_smem() {
   return sizeof(float2) * (buf + Lay::STRIP_ELEMS) + TwTable<N>::BYTES + 16;  // + the mbarrier
 }
 
+// Square sizes that have the table-twiddle forms (k_fwd_col_horner1, and
+// k_adj_col_rec with TWM 2): whole lines a thread (N1 | N2), column blocks
+// that tile the row, up to 48 elements a thread, and the exchange buffer,
+// the rotation strip and the table within the 227 KB a block may take.
+template <int N>
+constexpr bool kTableCols = LineCfg<N>::EXACT && (N % ColLayout<N>::CC == 0) && LineCfg<N>::N2 <= 48 &&
+                            LineCfg<N>::N2 % 2 == 0 && horner1_smem<N>() <= 227 * 1024;
+
 // Bounded waits of the TMA-fed column passes that ran out since the last read
 // (col_wait_timeouts).  None is expected: a wait covers one strip copy.
 __device__ unsigned g_col_wait_timeouts;
@@ -900,14 +916,14 @@ __device__ __forceinline__ void tma_load_3d(void* smem, const CUtensorMap* map, 
 // counts it in g_col_wait_timeouts (read back by col_wait_timeouts), gives the
 // copy in flight one more bounded wait and leaves without writing its sums.
 template <int N, bool TMA>
-__global__ void __launch_bounds__(ColLayout<N>::THREADS, 3)
+__global__ void __launch_bounds__(ColLayout<N>::THREADS, col3_minb<N>())
     k_fwd_col_horner1(const float2* __restrict__ T, const double* __restrict__ cturn,
                       const double* __restrict__ zlist, double dz, float2* __restrict__ Spart, int z0, int z1,
                       int zpb, const __grid_constant__ CUtensorMap tmap) {
   using C = LineCfg<N>;
   using Lay = ColLayout<N>;
   constexpr int N1 = C::N1, N2 = C::N2, M = C::M, LD = C::LD, CC = Lay::CC;
-  static_assert(Lay::STAGE && C::EXACT && kHoistTw<N>, "staged square sizes of up to 32 elements a thread");
+  static_assert(C::EXACT && N % CC == 0 && N2 <= 48, "square sizes of up to 48 elements a thread");
   constexpr int W = N;
   constexpr size_t BUF = Lay::SMEM_ELEMS > Lay::STRIP_ELEMS ? (size_t)Lay::SMEM_ELEMS : Lay::STRIP_ELEMS;
   extern __shared__ __align__(128) float2 sm[];
@@ -1094,9 +1110,10 @@ static cudaError_t adj_col_n(const float2* Rs, const double* cturn, const double
   if (nz <= 0) return cudaSuccess;
   const int strips = col_strips<N>(W);
   // the recurrence variants: evenly spaced planes, lines of <= 32 elements a
-  // thread; `rec_mode` 1 regenerates the twiddles each plane, 2 keeps them
+  // thread; `rec_mode` 1 regenerates the twiddles each plane, 2 keeps them;
+  // 3 reads them from a shared table (lines of up to 48 elements)
   constexpr bool kRecOk = kHoistTw<N> && (N % Lay::CC == 0);
-  const bool rec = kRecOk && dz_uniform != 0.0 && rec_mode != 0;
+  const bool rec = dz_uniform != 0.0 && ((kRecOk && rec_mode != 0) || (kTableCols<N> && rec_mode == 3));
   const int target = (rec && rec_mode != 2 ? 12 : 8) * num_sms();
   int chunks = chunks_hint > 0 ? chunks_hint : (target + strips - 1) / strips;
   if (chunks > nz) chunks = nz;
@@ -1107,7 +1124,7 @@ static cudaError_t adj_col_n(const float2* Rs, const double* cturn, const double
   std::memset(&umap, 0, sizeof(umap));
   const bool tma = (W == N) && (N % Lay::CC == 0) && plane_stack_map(&umap, U, N, z1, Lay::CC, tma_rows<N>());
   cudaError_t e;
-  if constexpr (kRecOk) {
+  if constexpr (kRecOk || kTableCols<N>) {
     if (rec) {
       // the twiddle table follows the rotation strip (rec_mode 3)
       const size_t smem =
@@ -1118,9 +1135,13 @@ static cudaError_t adj_col_n(const float2* Rs, const double* cturn, const double
         kern<<<dim3(strips, chunks), Lay::THREADS, smem, st>>>(Rs, cturn, zlist, dz_uniform, U, z0, z1, zpb, umap);
         return cudaGetLastError();
       };
-      if (rec_mode == 3) return tma ? go(k_adj_col_rec<N, true, 2>) : go(k_adj_col_rec<N, false, 2>);
-      if (rec_mode == 2) return tma ? go(k_adj_col_rec<N, true, 1>) : go(k_adj_col_rec<N, false, 1>);
-      return tma ? go(k_adj_col_rec<N, true, 0>) : go(k_adj_col_rec<N, false, 0>);
+      if constexpr (kTableCols<N>) {
+        if (rec_mode == 3) return tma ? go(k_adj_col_rec<N, true, 2>) : go(k_adj_col_rec<N, false, 2>);
+      }
+      if constexpr (kRecOk) {
+        if (rec_mode == 2) return tma ? go(k_adj_col_rec<N, true, 1>) : go(k_adj_col_rec<N, false, 1>);
+        return tma ? go(k_adj_col_rec<N, true, 0>) : go(k_adj_col_rec<N, false, 0>);
+      }
     }
   }
   if (tma) {
@@ -1137,12 +1158,12 @@ static cudaError_t adj_col_n(const float2* Rs, const double* cturn, const double
   return cudaGetLastError();
 }
 
-bool adj_recurrence_supported(int W, int H) {
+bool adj_recurrence_supported(int W, int H, int rec_mode) {
   if (W != H) return false;
   switch (H) {
 #define RIHVR_CASE(NN) \
   case NN:             \
-    return kHoistTw<NN> && (NN % ColLayout<NN>::CC == 0);
+    return rec_mode == 3 ? kTableCols<NN> : (kHoistTw<NN> && (NN % ColLayout<NN>::CC == 0));
     RIHVR_FOR_EACH_SIZE(RIHVR_CASE)
 #undef RIHVR_CASE
     default:
@@ -1200,7 +1221,7 @@ static cudaError_t fwd_col_n(const float2* T, const double* cturn, const double*
     e = cudaMemsetAsync(Spart + (size_t)chunks * N * W, 0, sizeof(float2) * (size_t)(nchunks - chunks) * N * W, st);
     if (e != cudaSuccess) return e;
   }
-  if constexpr (Lay::STAGE && LineCfg<N>::EXACT && kHoistTw<N>) {
+  if constexpr (kTableCols<N>) {
     if (dz_uniform != 0.0 && (horner_mode == 2 || horner_mode == 3)) {
       constexpr size_t smem = horner1_smem<N>();
       CUtensorMap tmap;
@@ -1237,7 +1258,7 @@ bool fwd_horner_supported(int W, int H, int horner_mode) {
   switch (H) {
 #define RIHVR_CASE(NN) \
   case NN:             \
-    return ColLayout<NN>::STAGE && LineCfg<NN>::EXACT && (horner_mode < 2 || kHoistTw<NN>);
+    return horner_mode >= 2 ? kTableCols<NN> : (ColLayout<NN>::STAGE && LineCfg<NN>::EXACT);
     RIHVR_FOR_EACH_SIZE(RIHVR_CASE)
 #undef RIHVR_CASE
     default:

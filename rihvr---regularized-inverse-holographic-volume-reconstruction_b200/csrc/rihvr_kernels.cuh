@@ -71,7 +71,7 @@ int segment_volume(int storage, const void* P, const void* Pprev, float beta, in
 size_t max_partial_blocks(int W, int H, int Nz);
 
 // square sizes whose adjoint column pass has the recurrence variant
-bool adj_recurrence_supported(int W, int H);
+bool adj_recurrence_supported(int W, int H, int rec_mode = 2);
 // dz_uniform != 0: the planes are evenly spaced by dz_uniform (z_{k+1} - z_k,
 // exact in FP64), which lets the square fast sizes advance the transfer
 // function by a recurrence (rec_mode 1: twiddles regenerated each plane, three

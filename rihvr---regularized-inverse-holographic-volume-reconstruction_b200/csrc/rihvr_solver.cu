@@ -1540,7 +1540,7 @@ int autotune_run(rihvr_ctx* c, cudaEvent_t e0, cudaEvent_t e1, TuneVal* out) {
   int best_adj = 0, best_rec = 0;
   float t_adj = 1e30f;
   for (int rec : {0, 2, 1, 3}) {
-    if (rec && (c->dz_uniform == 0 || !adj_recurrence_supported(c->W, c->H))) continue;
+    if (rec && (c->dz_uniform == 0 || !adj_recurrence_supported(c->W, c->H, rec))) continue;
     for (int ch : {0, 2, 4, 8, 16, 32}) {
       if (ch > c->Nz) continue;
       RC(time_min(c, e0, e1, [&]() -> int {
@@ -1623,13 +1623,18 @@ int rihvr_tuning(const rihvr_ctx* c, int* adj_chunks, int* fwd_chunks, int* tv_r
   if (!c) return fail(RIHVR_ERR_INVALID_ARGUMENT, "NULL context");
   if (adj_chunks) *adj_chunks = c->tune_adj_chunks;
   if (adj_recurrence)
-    *adj_recurrence = (c->dz_uniform != 0 && adj_recurrence_supported(c->W, c->H)) ? c->tune_adj_rec : 0;
-  if (fwd_horner)
-    // the variant that runs: a three-block form (2, 3) falls back to the
-    // two-block form (1) at sizes that do not have it
-    *fwd_horner = (c->tune_fwd_horner && c->dz_uniform != 0 && fwd_horner_supported(c->W, c->H, 1))
-                      ? (fwd_horner_supported(c->W, c->H, c->tune_fwd_horner) ? c->tune_fwd_horner : 1)
-                      : 0;
+    *adj_recurrence =
+        (c->tune_adj_rec && c->dz_uniform != 0 && adj_recurrence_supported(c->W, c->H, c->tune_adj_rec))
+            ? c->tune_adj_rec
+            : 0;
+  if (fwd_horner) {
+    // the variant that runs: a table-twiddle form (2, 3) falls back to the
+    // two-block form (1), and that to the direct pass (0), at sizes without it
+    const int hm = c->dz_uniform == 0 ? 0 : c->tune_fwd_horner;
+    *fwd_horner = (hm >= 2 && fwd_horner_supported(c->W, c->H, hm)) ? hm
+                  : (hm >= 1 && fwd_horner_supported(c->W, c->H, 1)) ? 1
+                                                                     : 0;
+  }
   if (fwd_chunks) *fwd_chunks = c->nchunks;
   if (tv_runs) *tv_runs = c->tune_tv_nseg;
   if (tv_kernel) *tv_kernel = c->tune_tv_kernel;

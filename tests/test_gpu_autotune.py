@@ -68,4 +68,4 @@ def test_column_variants_only_for_evenly_spaced_planes(rihvr):
     z = np.float32(100.0) + np.arange(6, dtype=np.float32) * np.float32(0.1)
     assert len(set(np.diff(z.astype(np.float64)))) > 1  # uneven in FP64
     assert tuned(100.0, 0.1) == (0, 0)
-    assert tuned(2500.0, 2.0, side=384) == (0, 0)  # 48 elements a thread: neither variant
+    assert tuned(2500.0, 2.0, side=384) == (0, 3)  # 48 elements a thread: the table-twiddle forms only

@@ -201,11 +201,13 @@ def test_solve_matches_oracle(rihvr, synthmod, cache_dir, mode, faithful, t0):
     olog, OX, OP, oest, f0 = O.solve(op, b.astype(np.float64), n, forced_bt=log["backtracks"],
                                      forced_rs=log["restarted"])
     free, _, _, _, _ = O.solve(op, b.astype(np.float64), n, want_volumes=False)
-    agree = np.mean((free["backtracks"] == log["backtracks"]) & (free["restarted"] == log["restarted"]))
-    assert agree >= 0.9, (free["backtracks"], log["backtracks"], free["restarted"], log["restarted"])
+    # every decision of the oracle's own run equals the GPU's (measured: all
+    # five cases, objective gap <= 7.5e-7, volume <= 8.4e-7)
+    assert np.array_equal(free["backtracks"], log["backtracks"]), (free["backtracks"], log["backtracks"])
+    assert np.array_equal(free["restarted"], log["restarted"]), (free["restarted"], log["restarted"])
     gap = np.abs(log["f_x"] - olog["f_x"]) / np.abs(olog["f_x"])
     assert gap.max() < TOL_F32, gap
-    assert rel(X, OX) < TOL_F32 * 10
+    assert rel(X, OX) < TOL_F32
     assert abs(f - olog["f_x"][-1]) / abs(olog["f_x"][-1]) < TOL_F32
     assert rel(est, oest) < TOL_F32
 
@@ -243,7 +245,10 @@ def test_reduced_precision_storage(rihvr, synthmod, cache_dir, storage):
 
 
 def test_c1_workload_matches_oracle_fixture(rihvr, synthmod):
-    """384x384x40, 100 FISTA / 5 TV iterations against the committed oracle run."""
+    """384x384x40, 100 FISTA / 5 TV iterations against the committed oracle
+    run: the same backtracking and restart decisions at every iteration, the
+    objective within 1e-4 at every iteration, the per-plane L1 norms and
+    cropped volume values within 1e-4 (measured: 3.7e-7, 1.8e-6, 5.2e-6)."""
     g = np.load(GOLD_C1)
     cfg = synthmod.config1()
     _, b = synthmod.make_hologram(cfg)
@@ -251,14 +256,13 @@ def test_c1_workload_matches_oracle_fixture(rihvr, synthmod):
     p = rihvr.params_from_config(cfg)
     log, X, f, terms, est = run_gpu(rihvr, p, cfg.W, b, cfg.num_inverse_iterations)
     assert np.array_equal(log["backtracks"], g["backtracks"])
-    assert np.mean(log["restarted"] == g["restarted"]) >= 0.95
+    assert np.array_equal(log["restarted"], g["restarted"])
     gap = np.abs(log["f_x"] - g["f_x"]) / np.abs(g["f_x"])
-    assert gap[-1] < TOL_F32, gap[-1]
-    assert gap.max() < 10 * TOL_F32, gap.max()
+    assert gap.max() < TOL_F32, gap.max()
     l1 = np.abs(X).sum(axis=(1, 2))
-    assert np.abs(l1 - g["plane_l1"]).sum() / g["plane_l1"].sum() < 1e-3
+    assert np.abs(l1 - g["plane_l1"]).sum() / g["plane_l1"].sum() < TOL_F32
     crops = X[list(g["crop_planes"])][..., 160:224, 160:224]
-    assert rel(crops, g["crops"]) < 1e-2
+    assert rel(crops, g["crops"]) < TOL_F32
 
 
 def test_errors_are_status_codes(rihvr):
@@ -275,7 +279,7 @@ def test_errors_are_status_codes(rihvr):
         assert np.all(s.getVolume() == 0)
 
 
-@pytest.mark.parametrize("side,nz", [(1024, 20), (512, 37), (256, 50), (64, 19)])
+@pytest.mark.parametrize("side,nz", [(1024, 20), (512, 37), (256, 50), (64, 19), (768, 20), (384, 18), (2304, 3)])
 @pytest.mark.parametrize("adj,fwd", [("direct", "direct"), ("recurrence", "horner"),
                                      ("recurrence_hoisted", "horner"), ("recurrence_table", "horner_onebuf"),
                                      ("recurrence_hoisted", "horner_tma")])
@@ -283,7 +287,9 @@ def test_column_pass_variants_match_oracle(rihvr, monkeypatch, side, nz, adj, fw
     """Every column-pass variant for evenly spaced planes (selected by name,
     as the autotuner would pick them) against the FP64 oracle: the adjoint's
     recurrence (re-anchored every 16 planes) and the forward's Horner sum, on
-    enough planes to cross several anchors and z-chunks."""
+    enough planes to cross several anchors and z-chunks.  Sides 384, 768 and
+    2304 (48 elements a thread) have only the table-twiddle forms; a variant a
+    size does not have runs the direct pass."""
     monkeypatch.setenv("RIHVR_ADJ_COL", adj)
     monkeypatch.setenv("RIHVR_FWD_COL", fwd)
     p = make(rihvr, side, nz)
