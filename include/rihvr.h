@@ -263,19 +263,20 @@ int rihvr_autotune(rihvr_ctx* ctx, double* best_ms);
 
 /* The launch shapes in use: z-chunks of the adjoint and forward column passes,
  * runs per plane of the streaming TV prox and the TV kernel (1 tiled,
- * 2 streaming in 2-warp blocks, 3 streaming in 4-warp blocks); 0 means the
- * built-in choice.  adj_recurrence receives the
+ * 2 streaming in 2-warp blocks, 3 streaming in 4-warp blocks, 4 streaming in
+ * one launch where 6-10 TV iterations would take two); 0 means the built-in
+ * choice.  adj_recurrence receives the
  * adjoint column pass's variant for evenly spaced planes (square planes of side
- * 32 to 1024 except 384, 640 and 768): 0 transfer function evaluated at every
+ * 32 to 2304 except 640): 0 transfer function evaluated at every
  * plane, 1 advanced by a recurrence with the inter-stage twiddles regenerated
- * each plane, 2 the recurrence with the twiddles kept in registers, 3 the
- * recurrence with the twiddles read from a per-block shared table.  fwd_horner
- * receives the forward column pass's variant: 1 when it sums over evenly
- * spaced planes by Horner's scheme (square planes of side 32 to 512 and 1024)
- * with its input strip double-buffered, 2 for the same sum with the strip
- * staged in the exchange buffer and a shared twiddle table (sides of up to 32
- * elements a thread), 3 for that form with the strip loaded by TMA, else 0.
- * Any pointer may be NULL. */
+ * each plane, 2 the recurrence with the twiddles kept in registers (these two
+ * up to side 1024, except 384 and 768), 3 the recurrence with the twiddles
+ * read from a per-block shared table.  fwd_horner receives the forward column
+ * pass's variant: 1 when it sums over evenly spaced planes by Horner's scheme
+ * (square planes of side 32 to 512 and 1024) with its input strip
+ * double-buffered, 2 for the same sum with the strip staged in the exchange
+ * buffer and a shared twiddle table (also sides 384, 768 and 2304), 3 for
+ * that form with the strip loaded by TMA, else 0.  Any pointer may be NULL. */
 int rihvr_tuning(const rihvr_ctx* ctx, int* adj_chunks, int* fwd_chunks, int* tv_runs, int* tv_kernel,
                  int* adj_recurrence, int* fwd_horner);
 

@@ -1882,16 +1882,19 @@ __device__ __forceinline__ void store_run(ST* p, const float2 (&v)[CPL]) {
 }
 
 template <typename ST, int NTV, bool NORMS, int CPL = 2, int NW = TvwShape<NTV, CPL>::NW,
-          int MINB = tvw_minb<NTV, NORMS>(), int UNR = 4, int PADTO = 4>
+          int MINB = tvw_minb<NTV, NORMS>(), int UNR = 4, int PADTO = 4, int PART = 0>
 __global__ void __launch_bounds__(32 * NW, MINB) k_prox_tv2d_strip(ProxArgs a0, TvsGrid gr) {
   const ProxArgs a = resolve_scalars(a0);
   using Sh = TvwShape<NTV, CPL>;
   constexpr int h = Sh::h, HX = Sh::HX, VW = Sh::VW, D = Sh::D, RM = D - 1, F4 = Sh::F4;
   constexpr int QS = F4 * 32;     // float4 between the arrays of a slot
   constexpr int SL = 3 * QS;      // float4 per slot
+  static_assert(PART == 0 || CPL == 2, "the two-part forms move a lane's two columns as one float4");
   extern __shared__ float4 tvw_ring[];
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   float4* ring = tvw_ring + (size_t)w * SL * D + lane;
+  // second part: 2 rows of the stored duals (gx pair, gy pair) after the warps' rings
+  float4* gring = tvw_ring + (size_t)NW * SL * D + (size_t)w * 2 * 32 * 2 + lane;
   const int W = a.W, H = a.H;
   const long long work = (long long)blockIdx.x * NW + w;
   const long long nwork = (long long)gr.nstrips * gr.nseg * a.Nz;
@@ -1932,6 +1935,17 @@ __global__ void __launch_bounds__(32 * NW, MINB) k_prox_tv2d_strip(ProxArgs a0, 
 
     // Ring slots are read as rows above r0 - h before any copy lands there;
     // those rows only feed rows above r0, which are not written.
+    // the first part's duals on row `off` (second part): a 2-row ring, so
+    // the copy for the next step is issued once this step has read its rows
+    auto request_g = [&](size_t off, int step) {
+      if constexpr (PART == 2) {
+        float4* gslot = gring + (step & 1) * 2 * 32;
+        cp_async_run<float2, CPL>(gslot, a.gdx + plane + off);
+        cp_async_run<float2, CPL>(gslot + 32, a.gdy + plane + off);
+        cp_async_commit();
+      }
+    };
+    size_t goff = 0;  // row offset of the last main-ring request
     auto request = [&](int slot) {
       const size_t off = (size_t)lrow * W + gc;
       float4* e = ring + slot * SL;
@@ -1939,9 +1953,11 @@ __global__ void __launch_bounds__(32 * NW, MINB) k_prox_tv2d_strip(ProxArgs a0, 
       cp_async_run<float2, CPL>(e + QS, G + off);
       cp_async_run<ST, CPL>(e + 2 * QS, P + off);
       cp_async_commit();
+      goff = off;
       lrow = (lrow + 1 == H) ? 0 : lrow + 1;
     };
     request(0);
+    request_g(goff, 0);
 
     float2 gX[NTV][CPL], gY[NTV][CPL], yU[NTV][CPL];
 #pragma unroll
@@ -1975,16 +1991,36 @@ __global__ void __launch_bounds__(32 * NW, MINB) k_prox_tv2d_strip(ProxArgs a0, 
       if (i + 1 < nsteps) request((i + 1) & RM);
 
       float2 ny[CPL];   // gy of the iteration before, on the row below
-      // iteration 1 on row j-1: g^0 = 0, so the estimate is xh itself
+      // iteration 1 on row j-1: g^0 = 0, so the estimate is xh itself; in the
+      // second part g^0 is the first part's dual, loaded with the rows
       {
-        float2 y[CPL], yl[CPL];
+        float2 y[CPL], yl[CPL], g0x[CPL], g0y[CPL];
         ring_vals<float2, CPL>(ring + ((i - 1) & RM) * SL, y);
+        if constexpr (PART == 2) {
+          float2 g1y[CPL], gxr[CPL];
+          const float4* gp = gring + ((i - 1) & 1) * 2 * 32;  // row j-1
+          const float4* gq = gring + (i & 1) * 2 * 32;        // row j
+          ring_vals<float2, CPL>(gp, g0x);
+          ring_vals<float2, CPL>(gp + 32, g0y);
+          ring_vals<float2, CPL>(gq + 32, g1y);
+#pragma unroll
+          for (int c = 0; c < CPL - 1; ++c) gxr[c] = g0x[c + 1];
+          gxr[CPL - 1] = shfl_down2(g0x[0]);
+#pragma unroll
+          for (int c = 0; c < CPL; ++c) y[c] = tv_estimate(y[c], g0x[c], gxr[c], g0y[c], g1y[c], nmu);
+          // row j-1's values have been used, so its slot is free: the next
+          // step's row goes there
+          if (i + 1 < nsteps) request_g(goff, i + 1);
+        } else {
+#pragma unroll
+          for (int c = 0; c < CPL; ++c) g0x[c] = g0y[c] = z2;
+        }
         yl[0] = shfl_up2(y[CPL - 1]);
 #pragma unroll
         for (int c = 1; c < CPL; ++c) yl[c] = y[c - 1];
 #pragma unroll
         for (int c = 0; c < CPL; ++c) {
-          float2 gx = z2, gy = z2;
+          float2 gx = g0x[c], gy = g0y[c];
           tv_dual(gx, gy, y[c], yl[c], yU[0][c], s2);
           yU[0][c] = y[c];
           ny[c] = gy;
@@ -2025,6 +2061,14 @@ __global__ void __launch_bounds__(32 * NW, MINB) k_prox_tv2d_strip(ProxArgs a0, 
               gY[L][c] = gy;
               y[c] = ogx;
               yl[c] = ogy;
+            }
+          } else if constexpr (PART == 1) {
+            // first part: (y, yl) hold this kernel's last dual on row j - h; it
+            // goes to memory for the second part instead of the estimate
+            if (i >= 2 * h + pad && lane_ok) {
+              const size_t eo = plane + (size_t)orow * W + gc;
+              *reinterpret_cast<float4*>(a.gdx + eo) = make_float4(y[0].x, y[0].y, y[1].x, y[1].y);
+              *reinterpret_cast<float4*>(a.gdy + eo) = make_float4(yl[0].x, yl[0].y, yl[1].x, yl[1].y);
             }
           } else {
             // final stage: p = shrink(estimate) on row j - h, then the sums
@@ -2088,7 +2132,7 @@ __global__ void __launch_bounds__(32 * NW, MINB) k_prox_tv2d_strip(ProxArgs a0, 
 #pragma unroll
     for (int k = 0; k < NS; ++k) dacc[k] += (double)acc[k];
   }
-  block_write_sums<32 * NW>(dacc, a.partials, blockIdx.x);
+  if constexpr (PART != 1) block_write_sums<32 * NW>(dacc, a.partials, blockIdx.x);
 }
 
 // Runs per plane: enough warps for several full waves, while keeping the
@@ -2123,12 +2167,13 @@ constexpr int tvw_minb_nw() {
   return NW == 2 ? tvw_minb<NTV, NORMS>() : 3;
 }
 
-template <typename ST, int NTV, bool NORMS, int NW>
+template <typename ST, int NTV, bool NORMS, int NW, int PART = 0>
 static cudaError_t strip_launch_nw(const ProxArgs& a, int* nblocks_out, cudaStream_t st) {
   using Sh = TvwShape<NTV, 2>;
   constexpr int MINB = tvw_minb_nw<NTV, NORMS, NW>();
-  constexpr size_t SMEM = Sh::SMEM / Sh::NW * NW;  // one ring a warp
-  auto kern = k_prox_tv2d_strip<ST, NTV, NORMS, 2, NW, MINB>;
+  // one ring a warp, and for the second part a 4-row ring of the stored duals
+  constexpr size_t SMEM = Sh::SMEM / Sh::NW * NW + (PART == 2 ? (size_t)NW * 2 * 32 * 2 * sizeof(float4) : 0);
+  auto kern = k_prox_tv2d_strip<ST, NTV, NORMS, 2, NW, MINB, 4, 4, PART>;
   cudaError_t e = allow_smem(kern, SMEM);
   if (e != cudaSuccess) return e;
   // resident blocks per SM, for the choice of runs per plane
@@ -2167,8 +2212,36 @@ static cudaError_t strip_launch(const ProxArgs& a, int* nblocks_out, cudaStream_
                       : strip_launch_n<ST, NTV, false>(a, nblocks_out, st);
 }
 
+// n_tv = K1 + K2 Chambolle iterations as two streaming launches: the first
+// runs iterations 1..K1 and stores the dual (gx, gy) of every voxel (gx in
+// a.gdx, gy in a.gdy, FP32 complex); the second starts from that dual, runs
+// iterations K1+1..n_tv, the estimate, the shrink and the sums.  Each launch
+// needs an x halo of K + 1 columns instead of n_tv + 1 and the 8-row ring, so
+// at n_tv = 10 a 64-column strip keeps 52 valid columns instead of 40 and 16
+// warps share an SM instead of 8.  The arithmetic is the single pass's, in the
+// same order, and the dual goes through memory unrounded, so P_new has the
+// same bits; only the second launch writes block partials.
+template <typename ST, int K1, int K2>
+static cudaError_t strip_launch_split(const ProxArgs& a, int* nblocks_out, cudaStream_t st) {
+  int nb1 = 0;
+  cudaError_t e = strip_launch_nw<ST, K1, false, 2, 1>(a, &nb1, st);
+  if (e != cudaSuccess) return e;
+  return a.want_norms ? strip_launch_nw<ST, K2, true, 2, 2>(a, nblocks_out, st)
+                      : strip_launch_nw<ST, K2, false, 2, 2>(a, nblocks_out, st);
+}
+
 template <typename ST>
 static cudaError_t strip_dispatch(const ProxArgs& a, int* nb, cudaStream_t st) {
+  if (a.gdx && a.gdy && a.tv_kernel != 4) {  // two launches for more than 5 iterations
+    switch (a.n_tv) {
+      case 6: return strip_launch_split<ST, 3, 3>(a, nb, st);
+      case 7: return strip_launch_split<ST, 3, 4>(a, nb, st);
+      case 8: return strip_launch_split<ST, 4, 4>(a, nb, st);
+      case 9: return strip_launch_split<ST, 4, 5>(a, nb, st);
+      case 10: return strip_launch_split<ST, 5, 5>(a, nb, st);
+      default: break;
+    }
+  }
   switch (a.n_tv) {
     case 1: return strip_launch<ST, 1>(a, nb, st);
     case 2: return strip_launch<ST, 2>(a, nb, st);
@@ -2185,9 +2258,8 @@ static cudaError_t strip_dispatch(const ProxArgs& a, int* nb, cudaStream_t st) {
 }
 constexpr int kStripNtvMax = 10;
 
-// RIHVR_TV_KERNEL=tiles forces the tiled kernel (comparison and fallback),
-// RIHVR_TV_KERNEL=strip4 the streaming kernel in 4-warp blocks; read once per
-// process.
+// RIHVR_TV_KERNEL=tiles forces the tiled kernel (comparison and fallback);
+// read once per process.
 static bool tv_stream_enabled() {
   static const bool on = [] {
     const char* v = std::getenv("RIHVR_TV_KERNEL");
@@ -2195,12 +2267,16 @@ static bool tv_stream_enabled() {
   }();
   return on;
 }
-static bool tv_strip4_forced() {
-  static const bool on = [] {
+// RIHVR_TV_KERNEL=strip4 (4-warp blocks) or strip1 (one launch for 6-10
+// iterations) as tv_kernel 3 or 4; 0 when unset
+static int tv_kernel_forced() {
+  static const int k = [] {
     const char* v = std::getenv("RIHVR_TV_KERNEL");
-    return v && std::strcmp(v, "strip4") == 0;
+    if (v && std::strcmp(v, "strip4") == 0) return 3;
+    if (v && std::strcmp(v, "strip1") == 0) return 4;
+    return 0;
   }();
-  return on;
+  return k;
 }
 
 static void tv_grid(const ProxArgs& a, dim3* g) {
@@ -2225,7 +2301,7 @@ cudaError_t launch_prox_tv2d(int storage, const ProxArgs& a, int* nblocks_out, c
   if (a.n_tv < 0 || a.n_tv > 20) return cudaErrorInvalidValue;
   if (a.n_tv >= 1 && a.n_tv <= kStripNtvMax && a.tv_kernel != 1 && tv_stream_enabled()) {
     ProxArgs b = a;
-    if (tv_strip4_forced()) b.tv_kernel = 3;
+    if (tv_kernel_forced()) b.tv_kernel = tv_kernel_forced();
     switch (storage) {
       case STORE_BF16: return strip_dispatch<__nv_bfloat162>(b, nblocks_out, st);
       case STORE_F16: return strip_dispatch<__half2>(b, nblocks_out, st);

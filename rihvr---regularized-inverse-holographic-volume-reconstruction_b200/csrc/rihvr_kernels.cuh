@@ -41,9 +41,14 @@ struct ProxArgs {
   long long partial_cap = 0;  // blocks partials holds; a launch needing more is refused
   // tuning knobs (0 = built-in choice): runs per plane of the streaming 2-D TV
   // prox, and the 2-D TV kernel (1 tiled, 2 streaming in 2-warp blocks,
-  // 3 streaming in 4-warp blocks where the 8-row ring applies, n_tv <= 5)
+  // 3 streaming in 4-warp blocks where the 8-row ring applies, n_tv <= 5,
+  // 4 streaming in one launch where two would be taken, 6 <= n_tv <= 10)
   int tv_nseg = 0;
   int tv_kernel = 0;
+  // dual of the first of two streaming launches (6 <= n_tv <= 10): gx and gy
+  // of every voxel, FP32 complex; null = one launch
+  float2* gdx = nullptr;
+  float2* gdy = nullptr;
   // device copy of (beta, t, mu, s, thr); when set, the 2-D TV and L1 prox
   // kernels read these instead of the values above, so that a captured
   // launch picks up each attempt's step and momentum

@@ -182,6 +182,7 @@ struct rihvr_ctx {
   int iPrev = 0, iCur = 1, iNew = 2;
   float2* G = nullptr;    // gradient volume
   float2* U = nullptr;    // column/row intermediate volume
+  float2* gdy = nullptr;  // gy of the two-launch TV prox (6-10 iterations; gx goes to U)
   float2* Spart = nullptr;
   float2* S = nullptr;
   float2* pc1 = nullptr;
@@ -438,6 +439,10 @@ ProxArgs prox_args(rihvr_ctx* c, double t, bool device_scalars = false) {
   a.partial_cap = (long long)c->partial_cap;
   a.tv_nseg = c->tune_tv_nseg;
   a.tv_kernel = c->tune_tv_kernel;
+  if (c->gdy) {
+    a.gdx = c->U;
+    a.gdy = c->gdy;
+  }
   // proximalFusedLasso2d shrinks only if l1 > 0 (:3715)
   if (c->mode == 7 && !(c->p.regularization_param > 0.f)) a.thr = 0.f;
   if (device_scalars && c->mode != 6) a.dscal = c->scal_d;
@@ -1392,6 +1397,10 @@ int rihvr_create(const rihvr_params* params, int width, int height, rihvr_ctx** 
   if (rc == RIHVR_OK) rc = dalloc_t(c, &c->r, c->HW);
   if (rc == RIHVR_OK) rc = dalloc_t(c, &c->cturn, c->HW);
   if (rc == RIHVR_OK) rc = dalloc_t(c, &c->zlist, (size_t)c->Nz);
+  // 6-10 TV iterations run as two streaming launches whose dual goes through
+  // memory: gx in U (free during the prox) and gy in one more volume
+  if (c->mode == 7 && c->p.num_tv_iterations >= 6 && c->p.num_tv_iterations <= 10 && rc == RIHVR_OK)
+    rc = dalloc_t(c, &c->gdy, c->V);
   if (c->mode == 6) {
     if (rc == RIHVR_OK) rc = dalloc_t(c, &c->X1, c->V);
     if (rc == RIHVR_OK) rc = dalloc_t(c, &c->gx, c->V);
@@ -1560,10 +1569,11 @@ int autotune_run(rihvr_ctx* c, cudaEvent_t e0, cudaEvent_t e1, TuneVal* out) {
   // a valid gradient volume for the prox candidates
   KL(launch_rows(1, ELEM_C32, c->U, ELEM_C32, c->G, c->W, (long long)c->Nz * c->H, 1.0f, c->st));
   // 2. 2-D TV prox: streaming in 2- or 4-warp blocks with 1..8 runs per
-  //    plane or the built-in count, or tiled
+  //    plane or the built-in count, in one launch or two (6-10 iterations),
+  //    or tiled
   float t_tv = 0.f;
   if (c->mode == 7 && c->p.num_tv_iterations >= 1 && c->p.regularization_TV_param > 0.f) {
-    const int cand[9][2] = {{0, 0}, {2, 1}, {2, 2}, {2, 4}, {2, 8}, {3, 0}, {3, 2}, {3, 4}, {1, 0}};
+    const int cand[11][2] = {{0, 0}, {2, 1}, {2, 2}, {2, 4}, {2, 8}, {3, 0}, {3, 2}, {3, 4}, {4, 0}, {4, 2}, {1, 0}};
     t_tv = 1e30f;
     int bk = 0, bn = 0;
     for (const auto& cd : cand) {

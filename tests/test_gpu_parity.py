@@ -151,10 +151,12 @@ np.save(sys.argv[7], out)
 
 
 @pytest.mark.parametrize("side,nz,ntv,storage", [(1024, 3, 5, 0), (384, 4, 3, 0), (768, 2, 6, 1), (256, 3, 4, 2),
-                                                 (512, 2, 10, 2), (640, 2, 8, 0)])
+                                                 (512, 2, 10, 2), (640, 2, 8, 0), (1024, 2, 7, 0), (2304, 1, 9, 2)])
 def test_streaming_prox_bits_equal_tiled(rihvr, tmp_path, side, nz, ntv, storage):
-    """The streaming TV prox, in 2- and 4-warp blocks, reproduces the tiled
-    kernel's P_new bit for bit (run lengths odd and even, every storage type)."""
+    """The streaming TV prox, in 2- and 4-warp blocks, and for 6-10 TV
+    iterations in two launches (the default, its dual stored between them)
+    or one, reproduces the tiled kernel's P_new bit for bit (run lengths odd
+    and even, every storage type)."""
     import subprocess
     import sys
 
@@ -163,7 +165,7 @@ def test_streaming_prox_bits_equal_tiled(rihvr, tmp_path, side, nz, ntv, storage
     script = tmp_path / "prox.py"
     script.write_text(_TILES_SCRIPT)
     outs = {}
-    for kern in ("tiles", "strip", "strip4"):
+    for kern in ("tiles", "strip", "strip4", "strip1"):
         env = dict(os.environ)
         env.pop("RIHVR_TV_KERNEL", None)
         if kern != "strip":
@@ -175,6 +177,7 @@ def test_streaming_prox_bits_equal_tiled(rihvr, tmp_path, side, nz, ntv, storage
         outs[kern] = np.load(f)
     assert np.array_equal(outs["tiles"].view(np.uint32), outs["strip"].view(np.uint32))
     assert np.array_equal(outs["tiles"].view(np.uint32), outs["strip4"].view(np.uint32))
+    assert np.array_equal(outs["tiles"].view(np.uint32), outs["strip1"].view(np.uint32))
 
 
 def run_gpu(rihvr, p, side, b, n):
