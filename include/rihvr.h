@@ -315,6 +315,18 @@ int rihvr_get_plane(rihvr_ctx* ctx, int z, float* out, int is_device);
 /* The whole momentum point volume, complex interleaved Nz x height x width. */
 int rihvr_get_volume(rihvr_ctx* ctx, float* out, int is_device);
 
+/* The momentum point volume without a copy out: *dev_ptr receives a device
+ * pointer to it (complex interleaved FP32, Nz x height x width, on the
+ * context's device), *dtype 0 (FP32 complex).  The volume is materialised in
+ * the context's intermediate buffer and the call synchronises the context's
+ * stream, so the pointer may be read on any stream once it returns; it stays
+ * valid until the next call on the context and must not be written or freed.
+ * For GPU consumers of the volume (segmentation, export) in the caller's own
+ * kernels.  (rihvr_get_volume_ptr of the replacement interface in the
+ * reference's hot-path survey; the reference returns planes only,
+ * getPlane, sparse_compressive_holo.h:92.) */
+int rihvr_get_volume_ptr(rihvr_ctx* ctx, const void** dev_ptr, int* dtype);
+
 /* Estimated hologram A x (estimate_final.tif, :621-622) and residual
  * A x - b (residual_final.tif, :623-624), height x width floats. */
 int rihvr_get_estimate(rihvr_ctx* ctx, float* out, int is_device);

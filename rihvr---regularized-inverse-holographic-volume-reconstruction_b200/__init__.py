@@ -136,6 +136,7 @@ EXPORTED = (
     "rihvr_iterate",
     "rihvr_iterate_timed",
     "rihvr_iteration_count", "rihvr_objective", "rihvr_get_iterations", "rihvr_get_plane", "rihvr_get_volume",
+    "rihvr_get_volume_ptr",
     "rihvr_get_estimate", "rihvr_get_residual", "rihvr_forward", "rihvr_adjoint", "rihvr_prox_step",
     "rihvr_adjoint_noalloc", "rihvr_sparsity", "rihvr_initial_estimate", "rihvr_lipschitz",
     "rihvr_set_hologram_frame", "rihvr_get_hologram", "rihvr_background_mean", "rihvr_background_median5",
@@ -206,6 +207,7 @@ def load_library(path: str = LIB_PATH):
         getattr(L, n).argtypes = [vp, ip, vp, ip]
     for n in ("rihvr_get_volume", "rihvr_get_estimate", "rihvr_get_residual"):
         getattr(L, n).argtypes = [vp, vp, ip]
+    L.rihvr_get_volume_ptr.argtypes = [vp, P(vp), P(ctypes.c_int)]
     L.rihvr_forward.argtypes = [vp, vp, vp, ip]
     L.rihvr_adjoint.argtypes = [vp, vp, vp, ip]
     L.rihvr_prox_step.argtypes = [vp, vp, vp, dp, vp, P(ctypes.c_double), ip]
@@ -753,6 +755,24 @@ class SparseCompressiveHolo:
         out = np.empty((self.depth, self.height, self.width), np.complex64)
         _check(self._L.rihvr_get_volume(self._h, _ptr(out), 0), "rihvr_get_volume")
         return out
+
+    def volume_device(self):
+        """The momentum point volume in device memory, without a copy
+        (rihvr_get_volume_ptr): a torch complex64 CUDA tensor of shape
+        (depth, height, width) viewing the context's buffer, valid until the
+        next call on this solver."""
+        import torch
+
+        ptr, dtype = ctypes.c_void_p(), ctypes.c_int()
+        _check(self._L.rihvr_get_volume_ptr(self._h, ctypes.byref(ptr), ctypes.byref(dtype)), "rihvr_get_volume_ptr")
+        if dtype.value != 0:
+            raise RihvrError(ERR_UNSUPPORTED_SIZE, "unexpected volume type")
+
+        class _DeviceView:  # the CUDA array interface torch reads
+            __cuda_array_interface__ = {"shape": (self.depth, self.height, self.width), "typestr": "<c8",
+                                        "data": (ptr.value, True), "version": 3}
+
+        return torch.as_tensor(_DeviceView(), device="cuda")
 
     def getEstimate(self) -> np.ndarray:
         out = np.empty((self.height, self.width), np.float32)

@@ -1963,6 +1963,16 @@ int rihvr_get_volume(rihvr_ctx* c, float* out, int is_device) {
   return copy_out(c, out, c->U, sizeof(float2) * c->V, is_device);
 }
 
+int rihvr_get_volume_ptr(rihvr_ctx* c, const void** dev_ptr, int* dtype) {
+  if (!c || !dev_ptr) return fail(RIHVR_ERR_INVALID_ARGUMENT, "NULL argument");
+  KL(launch_materialize_x(c->storage, c->vol[c->iCur], c->vol[c->iPrev], (float)c->beta, c->U, (long long)c->V,
+                          c->st));
+  CK(cudaStreamSynchronize(c->st));
+  *dev_ptr = c->U;
+  if (dtype) *dtype = 0;
+  return RIHVR_OK;
+}
+
 int rihvr_segment(rihvr_ctx* c, const rihvr_segment_params* sp, rihvr_object* objects, int max_objects,
                   int* num_objects, rihvr_segment_info* info) {
   if (!c) return fail(RIHVR_ERR_INVALID_ARGUMENT, "NULL context");

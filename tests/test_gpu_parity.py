@@ -333,3 +333,21 @@ def test_table_twiddle_variants_bits_equal_register_forms(rihvr, monkeypatch, si
     assert np.array_equal(d0, d1)
     assert np.array_equal(d0, d2)
     assert rel(g1, g0) < 2e-6
+
+
+def test_volume_device_pointer_is_the_volume(rihvr, synthmod, cache_dir):
+    """rihvr_get_volume_ptr hands out the momentum-point volume in device
+    memory: the same values rihvr_get_volume copies out, for FP32 and FP16
+    storage."""
+    cfg = synthmod.small_config(W=64, H=64, Nz=5, seed=7)
+    _, b = synthmod.make_hologram(cfg, cache_dir=cache_dir)
+    for storage in (0, 2):
+        p = rihvr.params_from_config(cfg, storage=storage)
+        with rihvr.SparseCompressiveHolo(p, cfg.W, cfg.H) as s:
+            s.setHologram(b)
+            s.iterate(6)
+            X = s.getVolume()
+            V = s.volume_device().cpu().numpy()
+        assert V.shape == X.shape
+        assert np.array_equal(V, X)
+        assert np.abs(X).max() > 0
