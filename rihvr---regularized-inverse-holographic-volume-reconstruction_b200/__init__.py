@@ -768,9 +768,9 @@ class SparseCompressiveHolo:
         if dtype.value != 0:
             raise RihvrError(ERR_UNSUPPORTED_SIZE, "unexpected volume type")
 
-        class _DeviceView:  # the CUDA array interface torch reads
+        class _DeviceView:  # the CUDA array interface torch reads (torch wants the read-only flag clear)
             __cuda_array_interface__ = {"shape": (self.depth, self.height, self.width), "typestr": "<c8",
-                                        "data": (ptr.value, True), "version": 3}
+                                        "data": (ptr.value, False), "version": 3}
 
         return torch.as_tensor(_DeviceView(), device="cuda")
 
