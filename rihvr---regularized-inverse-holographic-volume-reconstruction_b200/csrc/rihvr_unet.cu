@@ -226,6 +226,16 @@ cudaError_t conv3_launch(const float* X, int Cin, const __nv_bfloat16* Wt, int C
   return cudaGetLastError();
 }
 
+// the z-walking form of the BF16 convolutions, where a layer qualifies,
+// unless RIHVR_UNET_ZWALK=0
+bool use_zwalk() {
+  static const bool on = [] {
+    const char* e = std::getenv("RIHVR_UNET_ZWALK");
+    return !(e && std::strcmp(e, "0") == 0);
+  }();
+  return on;
+}
+
 // the tcgen05 path is used where it applies unless RIHVR_UNET_MMA=sync
 bool use_tcgen05() {
   static const bool on = [] {
@@ -684,6 +694,8 @@ struct rihvr_unet {
   __nv_bfloat16 *b_p1 = nullptr, *b_a2 = nullptr, *b_a3 = nullptr, *b_c2 = nullptr, *b_a7 = nullptr;  // level 1
   __nv_bfloat16 *b_p2 = nullptr, *b_a4 = nullptr, *b_a5 = nullptr;  // level 2
   TcMap maps[kNumConv];
+  TcMap zmaps[kNumConv];  // the z-walking form's maps, where a layer takes it
+  bool zwalk[kNumConv] = {};
   double* sums = nullptr;   // [0] sum |xbp|^2, [1] sum |x*|^2, [2] loss
   int* tc_err = nullptr;    // set by a tcgen05 convolution whose bounded wait ran out
   float* rms = nullptr;
@@ -846,6 +858,8 @@ int bf16_prepare(rihvr_unet* u) {
       u->bf_failed = true;
       return RIHVR_OK;
     }
+    u->zwalk[i] = use_zwalk() && tcz_supported(v.W, L.cin, L.cout) &&
+                  tc_zmap_encode(&u->zmaps[i], in[i], L.cin, v.D, v.H, v.W, tcz_rows(L.cin) + 2);
   }
   u->bf_ready = true;
   return RIHVR_OK;
@@ -854,8 +868,12 @@ int bf16_prepare(rihvr_unet* u) {
 int conv_bf16(rihvr_unet* u, int li, __nv_bfloat16* Y, const TcHead* head = nullptr) {
   const Conv& L = u->layers[li];
   const Vol v = u->lv[L.level];
-  UCK(conv3_tc_bf16(u->maps[li], L.cin, u->wtc + u->wtc_off[li], u->w + L.b_off, L.cout, Y, v.D, v.H, v.W, head,
-                    u->tc_err, u->st));
+  if (u->zwalk[li])
+    UCK(conv3_tcz(u->zmaps[li], L.cin, u->wtc + u->wtc_off[li], u->w + L.b_off, L.cout, Y, v.D, v.H, v.W, head,
+                  u->tc_err, u->st));
+  else
+    UCK(conv3_tc_bf16(u->maps[li], L.cin, u->wtc + u->wtc_off[li], u->w + L.b_off, L.cout, Y, v.D, v.H, v.W, head,
+                      u->tc_err, u->st));
   ++u->launches;
   return RIHVR_OK;
 }

@@ -27,6 +27,7 @@
 
 #include <algorithm>
 #include <cstdint>
+#include <cstdlib>
 #include <cstring>
 
 #include "rihvr_unet_tc.cuh"
@@ -110,10 +111,27 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
   for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r[j]);
 }
 
-__device__ __forceinline__ void tap_off(int k, int* dz, int* dy, int* dx) {
-  *dz = k / 9 - 1;
-  *dy = (k / 3) % 3 - 1;
-  *dx = k % 3 - 1;
+
+// The 27 x YT MMAs of one 16-channel slice, fully unrolled: ad[dz + 1] is the
+// A descriptor of the slab (or halo plane) a tap reads at z offset dz, bd the
+// descriptor of the slice's first tap; a tap's shifted window and weights
+// are fixed offsets into those (descriptor start addresses count 16-byte units
+// in their low 14 bits, and every offset stays inside the 228 KB of shared
+// memory, so adding to the descriptor adds to the address).
+template <int CN, int YT, int HY, bool MIRROR>
+__device__ __forceinline__ void issue_slice(uint32_t tbase, const uint64_t (&ad)[3], uint64_t bd, uint32_t idesc,
+                                            bool accumulate) {
+#pragma unroll
+  for (int k = 0; k < 27; ++k) {
+    const int kk = MIRROR ? 26 - k : k;
+    const int dz = kk / 9 - 1, dy = (kk / 3) % 3 - 1, dx = kk % 3 - 1;
+    const uint64_t b = bd + (uint64_t)(k * CN);  // k * CN * 16 bytes
+#pragma unroll
+    for (int m = 0; m < YT; ++m) {
+      const uint64_t a = ad[dz + 1] + (uint64_t)((m + 1 + dy) * kTcHX + (1 + dx));
+      mma_bf16_ss(tbase + (uint32_t)(m * CN), a, b, idesc, (accumulate || k > 0) ? 1u : 0u);
+    }
+  }
 }
 
 template <int CN>
@@ -200,17 +218,11 @@ __global__ void __launch_bounds__(kTcThreads) k_conv3_tc(const float* __restrict
     if (tid == 0) {
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       const uint32_t a0 = saddr(A0), b0 = saddr(B0);
-      for (int k = 0; k < 27; ++k) {
-        int dz, dy, dx;
-        tap_off(mirror ? 26 - k : k, &dz, &dy, &dx);
-        const uint64_t bd = smem_desc(b0 + (uint32_t)(k * CN * 16), b_lbo, 128);
-#pragma unroll
-        for (int m = 0; m < kTcYT; ++m) {
-          const int h = ((1 + dz) * kTcHY + (m + 1 + dy)) * kTcHX + (1 + dx);
-          const uint64_t ad = smem_desc(a0 + (uint32_t)(h * 16), a_lbo, 128);
-          mma_bf16_ss(tbase + (uint32_t)(m * CN), ad, bd, idesc, (s > 0 || k > 0) ? 1u : 0u);
-        }
-      }
+      const uint64_t bd = smem_desc(b0, b_lbo, 128);
+      const uint64_t a_lo = smem_desc(a0, a_lbo, 128);
+      const uint64_t ad[3] = {a_lo, a_lo + (uint64_t)(kTcHY * kTcHX), a_lo + (uint64_t)(2 * kTcHY * kTcHX)};
+      if (mirror) issue_slice<CN, kTcYT, kTcHY, true>(tbase, ad, bd, idesc, s > 0);
+      else issue_slice<CN, kTcYT, kTcHY, false>(tbase, ad, bd, idesc, s > 0);
       mma_commit(bar_a);
     }
   }
@@ -393,17 +405,10 @@ __global__ void __launch_bounds__(kTcThreads) k_conv3_tc_bf16(const __grid_const
         break;
       }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-      for (int k = 0; k < 27; ++k) {
-        int dz, dy, dx;
-        tap_off(k, &dz, &dy, &dx);
-        const uint64_t bd = smem_desc(b0 + (uint32_t)(k * CN * 16), 27 * CN * 16, 128);
-#pragma unroll
-        for (int m = 0; m < kTcYT; ++m) {
-          const int h = ((1 + dz) * kTcHY + (m + 1 + dy)) * kTcHX + (1 + dx);
-          const uint64_t ad = smem_desc(a0 + (uint32_t)(h * 16), kTcPlaneBytes, 128);
-          mma_bf16_ss(tbase + (uint32_t)(m * CN), ad, bd, idesc, (s > 0 || k > 0) ? 1u : 0u);
-        }
-      }
+      const uint64_t bd = smem_desc(b0, 27 * CN * 16, 128);
+      const uint64_t a_lo = smem_desc(a0, kTcPlaneBytes, 128);
+      const uint64_t ad[3] = {a_lo, a_lo + (uint64_t)(kTcHY * kTcHX), a_lo + (uint64_t)(2 * kTcHY * kTcHX)};
+      issue_slice<CN, kTcYT, kTcHY, false>(tbase, ad, bd, idesc, s > 0);
       mma_commit(bar_mma);
       committed = 1;
     }
@@ -463,6 +468,210 @@ __global__ void __launch_bounds__(kTcThreads) k_conv3_tc_bf16(const __grid_const
         }
       }
     }
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  if (warp == 0) {
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tbase), "r"(NCOLS) : "memory");
+  }
+}
+
+// ---------------------------------------------------------------------------
+// z-walking form of the inference convolution, for layers with 16 input
+// channels (the template also takes more slices, NS).  A block keeps one
+// (x-tile of 128 voxels, y-tile of YT rows) column and walks a range of z.
+// Shared memory holds a ring of 3 input slabs (one z-plane each: YT + 2 rows x
+// 130 voxels, every slice in two 8-channel planes, the layout the descriptors
+// read), so each input plane is loaded once per block instead of three times,
+// and the weights of all slices, loaded once per block.  Per output plane z:
+//   thread 0 waits for slab z+1, issues the 27 x YT x slices MMAs into the
+//   tensor-memory accumulator and commits them; once they are done it reuses
+//   slab z-1's slot for slab z+2 (one TMA box per slice and half, completing on
+//   that slot's mbarrier) while all threads drain the accumulator (bias, ReLU,
+//   BF16 store, or the head).  The TMA copy overlaps the epilogue, and a
+//   second block on the SM (16 channels: 89 KB a block) fills the tensor pipe
+//   while this one drains.
+// Every wait is bounded; a wait that runs out sets *err, the block lets its
+// copies and MMAs in flight finish (bounded) and leaves.
+// ---------------------------------------------------------------------------
+template <int YT, int NS>  // x-rows a block, 16-channel slices
+struct TczShape {
+  static constexpr int HY = YT + 2;
+  static constexpr uint32_t BOX = 16u * kTcHX * HY;                 // one 8-channel plane of a slab
+  static constexpr uint32_t PLANE = (BOX + 127u) / 128u * 128u;     // planes 128 bytes apart
+  static constexpr uint32_t SLAB = 2u * NS * PLANE;
+  static constexpr int R = 3;                                        // slabs in the ring
+};
+
+template <int CN, int YT, int NS>
+constexpr size_t tcz_smem() {
+  using S = TczShape<YT, NS>;
+  return 1024 + (size_t)S::R * S::SLAB + (size_t)NS * 2 * 27 * CN * 16 + 64;
+}
+
+template <int CN, bool HEAD, int YT, int NS>
+__global__ void __launch_bounds__(kTcThreads) k_conv3_tcz(const __grid_constant__ CUtensorMap zmap,
+                                                          const __nv_bfloat16* __restrict__ Wp,
+                                                          const float* __restrict__ bias,
+                                                          __nv_bfloat16* __restrict__ Y, int D, int H, int W,
+                                                          int zper, TcHead hd, int* __restrict__ err) {
+  static_assert(CN % 16 == 0 && CN >= 16 && CN <= 64, "N of the MMA");
+  static_assert(!HEAD || CN == 16, "the head takes 16 channels");
+  using S = TczShape<YT, NS>;
+  constexpr uint32_t NCOLS = YT * CN <= 32 ? 32u : YT * CN <= 64 ? 64u : YT * CN <= 128 ? 128u : 256u;
+  constexpr uint32_t BBYTES = 2u * 27u * CN * 16u;  // one slice's weights
+  extern __shared__ unsigned char tzraw[];
+  unsigned char* base = reinterpret_cast<unsigned char*>((reinterpret_cast<uintptr_t>(tzraw) + 1023) & ~uintptr_t(1023));
+  unsigned char* slabs = base;                          // [R][NS][2 planes] of PLANE bytes
+  unsigned char* B0 = slabs + S::R * S::SLAB;           // [NS][2][27 * CN] x 16 B
+  uint64_t* bars = reinterpret_cast<uint64_t*>(B0 + NS * BBYTES);  // [0..2] slabs, [3] weights, [4] MMAs
+  uint32_t* tslot = reinterpret_cast<uint32_t*>(bars + 5);
+  int* s_ok = reinterpret_cast<int*>(tslot + 1);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int nbx = W / kTcX, nby = (H + YT - 1) / YT;
+  const int bx = blockIdx.x % nbx, by = (blockIdx.x / nbx) % nby, zp = blockIdx.x / (nbx * nby);
+  const int x0 = bx * kTcX, y0 = by * YT;
+  const int zb = zp * zper, ze = min(D, zb + zper);
+
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(saddr(tslot)),
+                 "r"(NCOLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  if (tid == 0) {
+    for (int i = 0; i < 5; ++i) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(saddr(bars + i)) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    *s_ok = 1;
+  }
+  asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+  __syncthreads();
+  asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+  const uint32_t tbase = *tslot;
+  const uint32_t idesc = instr_desc(CN);
+  const uint32_t s0 = saddr(slabs), b0 = saddr(B0);
+  uint32_t phase[S::R] = {0u, 0u, 0u};  // thread 0: parity of each slot's next completion
+  bool busy[S::R] = {false, false, false};  // a copy into the slot not yet awaited
+  uint32_t pm = 0;                      // parity of the MMA barrier
+  bool mma_busy = false, w_busy = false;
+  bool ok = true;
+  // slot of the slab of plane z: the ring starts with plane zb - 1 in slot 0
+  auto slot_of = [&](int z) { return (uint32_t)((z - zb + 1) % S::R); };
+  auto load_slab = [&](int z) {  // thread 0
+    const uint32_t sl = slot_of(z);
+    const uint32_t bar = saddr(bars + sl);
+    busy[sl] = true;
+    mbar_expect_tx(bar, 2u * NS * S::BOX);
+#pragma unroll
+    for (int sc = 0; sc < NS; ++sc)
+#pragma unroll
+      for (int p = 0; p < 2; ++p)
+        tma_load_4d(s0 + sl * S::SLAB + (uint32_t)(sc * 2 + p) * S::PLANE, &zmap, 16 * sc + 8 * p, x0 - 1, y0 - 1,
+                    z, bar);
+  };
+  if (tid == 0 && zb < ze) {
+    mbar_expect_tx(saddr(bars + 3), NS * BBYTES);
+    bulk_load(b0, Wp, NS * BBYTES, saddr(bars + 3));
+    w_busy = true;
+    for (int z = zb - 1; z <= zb + 1; ++z) load_slab(z);  // planes outside the volume read as zeros
+    ok = mbar_wait(saddr(bars + 3), 0);
+    w_busy = !ok;
+    for (int z = zb - 1; z <= zb && ok; ++z) {
+      ok = mbar_wait(saddr(bars + slot_of(z)), phase[slot_of(z)]);
+      if (ok) {
+        phase[slot_of(z)] ^= 1u;
+        busy[slot_of(z)] = false;
+      }
+    }
+  }
+  for (int z = zb; z < ze; ++z) {
+    if (tid == 0) {
+      if (ok) {  // slab z+1, the last one this plane reads
+        ok = mbar_wait(saddr(bars + slot_of(z + 1)), phase[slot_of(z + 1)]);
+        if (ok) {
+          phase[slot_of(z + 1)] ^= 1u;
+          busy[slot_of(z + 1)] = false;
+        }
+      }
+      if (ok) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+#pragma unroll
+        for (int sc = 0; sc < NS; ++sc) {
+          uint64_t ad[3];
+#pragma unroll
+          for (int d = 0; d < 3; ++d)
+            ad[d] = smem_desc(s0 + slot_of(z + d - 1) * S::SLAB + (uint32_t)(sc * 2) * S::PLANE, S::PLANE, 128);
+          const uint64_t bd = smem_desc(b0 + (uint32_t)sc * BBYTES, 27 * CN * 16, 128);
+          issue_slice<CN, YT, S::HY, false>(tbase, ad, bd, idesc, sc > 0);
+        }
+        mma_commit(saddr(bars + 4));
+        mma_busy = true;
+        ok = mbar_wait(saddr(bars + 4), pm);
+        if (ok) {
+          pm ^= 1u;
+          mma_busy = false;
+        }
+        // slab z-1 is no longer read: its slot takes slab z+2 for the next plane
+        if (ok && z + 1 < ze) load_slab(z + 2);
+      }
+      if (!ok) *s_ok = 0;
+    }
+    __syncthreads();
+    if (!*s_ok) break;
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const int xx = x0 + warp * 32 + lane;
+#pragma unroll 1
+    for (int m = 0; m < YT; ++m) {
+      const int yy = y0 + m;
+      const long long vox = ((long long)z * H + yy) * W + xx;
+      float zsum = 0.f;
+      if constexpr (HEAD) zsum = hd.w[16];
+#pragma unroll
+      for (int c16 = 0; c16 < CN / 16; ++c16) {
+        float v[16];
+        tmem_ld16(tbase + ((uint32_t)(warp * 32) << 16) + (uint32_t)(m * CN + c16 * 16), v);
+#pragma unroll
+        for (int j = 0; j < 16; ++j) v[j] = fmaxf(v[j] + bias[c16 * 16 + j], 0.f);
+        if constexpr (HEAD) {
+#pragma unroll
+          for (int j = 0; j < 16; ++j) zsum += hd.w[j] * v[j];
+        } else if (yy < H) {
+          uint4 o0, o1;
+          o0.x = pack2(v[0], v[1]);
+          o0.y = pack2(v[2], v[3]);
+          o0.z = pack2(v[4], v[5]);
+          o0.w = pack2(v[6], v[7]);
+          o1.x = pack2(v[8], v[9]);
+          o1.y = pack2(v[10], v[11]);
+          o1.z = pack2(v[12], v[13]);
+          o1.w = pack2(v[14], v[15]);
+          uint4* dst = reinterpret_cast<uint4*>(Y + vox * CN + c16 * 16);
+          dst[0] = o0;
+          dst[1] = o1;
+        }
+      }
+      if constexpr (HEAD) {
+        if (yy < H) {
+          const float g = 1.f / (1.f + expf(-zsum));
+          const float alpha = hd.w[17] * hd.scale;
+          const float2 a = hd.xbp[vox];
+          hd.x0[vox] = make_float2(g * alpha * a.x, g * alpha * a.y);
+        }
+      }
+    }
+    // every thread's accumulator reads come before the next plane's MMAs
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+  }
+  if (tid == 0 && !ok) {
+    atomicExch(err, 1);
+    // a last bounded wait for the copies and MMAs still in flight before the
+    // shared and tensor memory are released
+    if (mma_busy) mbar_wait(saddr(bars + 4), pm);
+    for (int i = 0; i < S::R; ++i)
+      if (busy[i]) mbar_wait(saddr(bars + i), phase[i]);
+    if (w_busy) mbar_wait(saddr(bars + 3), 0);
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
   __syncthreads();
@@ -535,6 +744,82 @@ bool tc_map_encode(TcMap* m, const __nv_bfloat16* X, int C, int D, int H, int W)
   static_assert(sizeof(map) == sizeof(m->bytes), "tensor map size");
   std::memcpy(m->bytes, &map, sizeof(map));
   return true;
+}
+
+// x-rows a block of the z-walking form takes
+int tcz_rows(int) { return 4; }
+
+bool tc_zmap_encode(TcMap* m, const __nv_bfloat16* X, int C, int D, int H, int W, int rows) {
+  const EncodeTiledFn enc = encode_tiled();
+  if (!enc || !X || (reinterpret_cast<uintptr_t>(X) & 15) != 0 || C % 16 != 0 || rows < 1 || rows > 256) return false;
+  CUtensorMap map;
+  std::memset(&map, 0, sizeof(map));
+  const cuuint64_t dims[4] = {(cuuint64_t)C, (cuuint64_t)W, (cuuint64_t)H, (cuuint64_t)D};
+  const cuuint64_t strides[3] = {(cuuint64_t)C * 2, (cuuint64_t)W * C * 2, (cuuint64_t)H * W * C * 2};
+  const cuuint32_t box[4] = {8, (cuuint32_t)kTcHX, (cuuint32_t)rows, 1};
+  const cuuint32_t estr[4] = {1, 1, 1, 1};
+  if (enc(&map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<__nv_bfloat16*>(X), dims, strides, box, estr,
+          CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+    return false;
+  std::memcpy(m->bytes, &map, sizeof(map));
+  return true;
+}
+
+// 16 input channels only: with three slices (48 channels) the ring and the
+// weights fill the shared memory of one block an SM, and that layer measured
+// slower walking z (a block's loads, MMAs and epilogue then have nothing to
+// overlap with) than in the per-tile kernel.
+bool tcz_supported(int W, int Cin, int Cout) {
+  return W % kTcX == 0 && Cin == 16 && (Cout == 16 || Cout == 32) && encode_tiled() != nullptr;
+}
+
+namespace {
+template <int CN, bool HEAD, int YT, int NS>
+cudaError_t tcz_launch(const TcMap& m, const __nv_bfloat16* Wp, const float* bias, __nv_bfloat16* Y, int D, int H,
+                       int W, const TcHead& hd, int* err, cudaStream_t st) {
+  constexpr size_t smem = tcz_smem<CN, YT, NS>();
+  static bool opted = false;
+  if (!opted) {
+    const cudaError_t e = cudaFuncSetAttribute(k_conv3_tcz<CN, HEAD, YT, NS>,
+                                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    opted = true;
+  }
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_conv3_tcz<CN, HEAD, YT, NS>, kTcThreads, smem) !=
+          cudaSuccess ||
+      per_sm < 1) {
+    cudaGetLastError();
+    per_sm = 1;
+  }
+  int dev = 0, sms = 148;
+  if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) !=
+                                                 cudaSuccess) {
+    cudaGetLastError();
+    sms = 148;
+  }
+  // z-ranges per (x, y) column: about four waves of blocks in all
+  const long long xy = (long long)(W / kTcX) * ((H + YT - 1) / YT);
+  const long long target = 4LL * sms * per_sm;
+  const int zsplit = (int)std::max(1LL, std::min<long long>(D, (target + xy - 1) / xy));
+  const int zper = (D + zsplit - 1) / zsplit;
+  const long long blocks = xy * ((D + zper - 1) / zper);
+  if (blocks > 0x7fffffffLL) return cudaErrorInvalidConfiguration;
+  CUtensorMap map;
+  std::memcpy(&map, m.bytes, sizeof(map));
+  k_conv3_tcz<CN, HEAD, YT, NS><<<(unsigned)blocks, kTcThreads, smem, st>>>(map, Wp, bias, Y, D, H, W, zper, hd, err);
+  return cudaGetLastError();
+}
+}  // namespace
+
+cudaError_t conv3_tcz(const TcMap& zmap, int Cin, const __nv_bfloat16* Wp, const float* bias, int Cout,
+                      __nv_bfloat16* Y, int D, int H, int W, const TcHead* head, int* err, cudaStream_t st) {
+  if (!tcz_supported(W, Cin, Cout) || (head && Cout != 16)) return cudaErrorInvalidValue;
+  const TcHead hd = head ? *head : TcHead{};
+  if (head) return tcz_launch<16, true, 4, 1>(zmap, Wp, bias, Y, D, H, W, hd, err, st);
+  return Cout == 16 ? tcz_launch<16, false, 4, 1>(zmap, Wp, bias, Y, D, H, W, hd, err, st)
+                    : tcz_launch<32, false, 4, 1>(zmap, Wp, bias, Y, D, H, W, hd, err, st);
 }
 
 bool conv3_tc_bf16_supported(int D, int H, int W, int Cin, int Cout) {

@@ -38,5 +38,15 @@ cudaError_t tc_weights(const float* w, int Cout, int Cin, __nv_bfloat16* wp, cud
 cudaError_t conv3_tc_bf16(const TcMap& xmap, int Cin, const __nv_bfloat16* Wp, const float* bias, int Cout,
                           __nv_bfloat16* Y, int D, int H, int W, const TcHead* head, int* err, cudaStream_t st);
 
+// The z-walking form of the same convolution (16 input channels, 16 or 32
+// output channels; the head with 16): a block walks z over one (x, y) tile
+// with a ring of three input planes, each loaded once, through a tensor map
+// made by tc_zmap_encode with `rows` = tcz_rows(Cin) + 2.
+bool tcz_supported(int W, int Cin, int Cout);
+int tcz_rows(int Cin);
+bool tc_zmap_encode(TcMap* m, const __nv_bfloat16* X, int C, int D, int H, int W, int rows);
+cudaError_t conv3_tcz(const TcMap& zmap, int Cin, const __nv_bfloat16* Wp, const float* bias, int Cout,
+                      __nv_bfloat16* Y, int D, int H, int W, const TcHead* head, int* err, cudaStream_t st);
+
 }  // namespace unet
 }  // namespace rihvr

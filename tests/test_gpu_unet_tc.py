@@ -127,3 +127,43 @@ def test_small_widths_keep_fp32_activations(rihvr):
         assert net.activation_bits() == 32
     with rihvr.UNet(8, 16, 256) as net:
         assert net.activation_bits() == 32
+
+
+_PREDICT = """
+import sys, importlib, numpy as np
+sys.path.insert(0, sys.argv[1])
+R = importlib.import_module(sys.argv[2])
+shape = tuple(int(v) for v in sys.argv[3:6])
+rng = np.random.default_rng(9)
+xbp = (rng.normal(size=shape) + 1j * rng.normal(size=shape)).astype(np.complex64)
+with R.UNet(*shape, seed=4) as net:
+    assert net.activation_bits() == 16
+    x0 = net.predict(xbp).cpu().numpy()
+np.save(sys.argv[6], x0)
+"""
+
+
+def test_z_walking_convolutions_equal_per_tile_ones(tmp_path):
+    """The z-walking BF16 convolutions (a block walks z over one tile with a
+    ring of three input planes; the layers with 16 input channels) issue the same MMAs
+    in the same order as the per-tile kernel, so the prediction is bit-equal
+    with RIHVR_UNET_ZWALK=0 (separate processes: the choice is read once).
+    Depth 36 splits into ragged z-ranges, and the second level's 22 rows are
+    not a multiple of its 4-row tiles."""
+    from conftest import PKG_NAME, ROOT
+
+    script = tmp_path / "predict.py"
+    script.write_text(_PREDICT)
+    out = {}
+    for mode in ("zwalk", "tile"):
+        env = dict(os.environ)
+        env.pop("RIHVR_UNET_ZWALK", None)
+        if mode == "tile":
+            env["RIHVR_UNET_ZWALK"] = "0"
+        f = tmp_path / f"{mode}.npy"
+        r = subprocess.run([sys.executable, str(script), ROOT, PKG_NAME, "36", "44", "512", str(f)], env=env,
+                           capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0, r.stderr[-2000:]
+        out[mode] = np.load(f)
+    assert np.all(np.isfinite(out["zwalk"]))
+    assert np.array_equal(out["zwalk"].view(np.uint32), out["tile"].view(np.uint32))
