@@ -283,6 +283,20 @@ int rihvr_tuning(const rihvr_ctx* ctx, int* adj_chunks, int* fwd_chunks, int* tv
 /* Restart from x = 0 without changing the hologram. */
 int rihvr_reset(rihvr_ctx* ctx);
 
+/* Checkpoint and resume (no counterpart in the reference, whose voxel CSV,
+ * SparseVolume::saveData at sparse_volume.cu:518-682, keeps intensities only
+ * and cannot restart a solve).  rihvr_save_state writes, between iterations,
+ * everything the next iteration reads: the hologram, the hologram-space
+ * momentum buffers, the last two prox outputs in the storage type, the step,
+ * momentum and restart scalars and the iteration log.  rihvr_load_state
+ * restores them into a context created with the same sizes, storage, mode
+ * and iteration parameters (else RIHVR_ERR_INVALID_FILE, context unchanged);
+ * further rihvr_iterate calls then continue the solve bit for bit as if it
+ * had not stopped (with the same launch shapes: both contexts untuned, or
+ * tuned alike).  The file takes about 2 x Nz x H x W x storage size bytes. */
+int rihvr_save_state(rihvr_ctx* ctx, const char* path);
+int rihvr_load_state(rihvr_ctx* ctx, const char* path);
+
 /* Restart from a given volume instead of x = 0 (a warm start; the reference
  * always starts from 0, sparse_compressive_holo.cu:273): x0 is num_planes x
  * height x width complex interleaved (host or device), stored in the

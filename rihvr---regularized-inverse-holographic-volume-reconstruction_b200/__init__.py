@@ -136,7 +136,7 @@ EXPORTED = (
     "rihvr_iterate",
     "rihvr_iterate_timed",
     "rihvr_iteration_count", "rihvr_objective", "rihvr_get_iterations", "rihvr_get_plane", "rihvr_get_volume",
-    "rihvr_get_volume_ptr",
+    "rihvr_get_volume_ptr", "rihvr_save_state", "rihvr_load_state",
     "rihvr_get_estimate", "rihvr_get_residual", "rihvr_forward", "rihvr_adjoint", "rihvr_prox_step",
     "rihvr_adjoint_noalloc", "rihvr_sparsity", "rihvr_initial_estimate", "rihvr_lipschitz",
     "rihvr_set_hologram_frame", "rihvr_get_hologram", "rihvr_background_mean", "rihvr_background_median5",
@@ -208,6 +208,8 @@ def load_library(path: str = LIB_PATH):
     for n in ("rihvr_get_volume", "rihvr_get_estimate", "rihvr_get_residual"):
         getattr(L, n).argtypes = [vp, vp, ip]
     L.rihvr_get_volume_ptr.argtypes = [vp, P(vp), P(ctypes.c_int)]
+    L.rihvr_save_state.argtypes = [vp, ctypes.c_char_p]
+    L.rihvr_load_state.argtypes = [vp, ctypes.c_char_p]
     L.rihvr_forward.argtypes = [vp, vp, vp, ip]
     L.rihvr_adjoint.argtypes = [vp, vp, vp, ip]
     L.rihvr_prox_step.argtypes = [vp, vp, vp, dp, vp, P(ctypes.c_double), ip]
@@ -755,6 +757,15 @@ class SparseCompressiveHolo:
         out = np.empty((self.depth, self.height, self.width), np.complex64)
         _check(self._L.rihvr_get_volume(self._h, _ptr(out), 0), "rihvr_get_volume")
         return out
+
+    def saveState(self, path: str):
+        """Checkpoint the solve between iterations (rihvr_save_state)."""
+        _check(self._L.rihvr_save_state(self._h, os.fsencode(path)), "rihvr_save_state")
+
+    def loadState(self, path: str):
+        """Resume a checkpointed solve in this solver (rihvr_load_state): same
+        sizes and parameters; later iterations continue it bit for bit."""
+        _check(self._L.rihvr_load_state(self._h, os.fsencode(path)), "rihvr_load_state")
 
     def volume_device(self):
         """The momentum point volume in device memory, without a copy

@@ -13,6 +13,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdint>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -1692,6 +1693,169 @@ int rihvr_reset(rihvr_ctx* c) {
   if (!c) return fail(RIHVR_ERR_INVALID_ARGUMENT, "NULL context");
   if (!c->have_holo) return fail(RIHVR_ERR_MISSING_DATA, "no hologram set");
   return state_reset(c);
+}
+
+}  // extern "C"
+
+namespace {
+
+// Checkpoint file: a fixed header, the iteration log, the hologram-space
+// buffers that carry from one iteration to the next, and the two volumes
+// P_k and P_{k-1} in the context's storage type.
+constexpr char kStateMagic[8] = {'R', 'I', 'H', 'V', 'R', 'S', 'T', '1'};
+struct StateHeader {
+  char magic[8];
+  int32_t version, W, H, Nz, storage, mode, faithful, n_tv, max_backtracks, record_objective;
+  float z0, dz, lambda, dx, l1, tv;
+  double t, alpha1, beta, prev_f_resid;
+  int32_t it, pending_x, nlog, esize;
+};
+
+void state_header_of(const rihvr_ctx* c, StateHeader* h) {
+  std::memset(h, 0, sizeof(*h));
+  std::memcpy(h->magic, kStateMagic, 8);
+  h->version = 1;
+  h->W = c->W;
+  h->H = c->H;
+  h->Nz = c->Nz;
+  h->storage = c->storage;
+  h->mode = c->mode;
+  h->faithful = c->p.faithful;
+  h->n_tv = c->p.num_tv_iterations;
+  h->max_backtracks = c->p.max_backtracks;
+  h->record_objective = c->p.record_objective;
+  h->z0 = c->p.start_plane;
+  h->dz = c->p.plane_stepsize;
+  h->lambda = c->p.wavelength;
+  h->dx = c->p.resolution;
+  h->l1 = c->p.regularization_param;
+  h->tv = c->p.regularization_TV_param;
+  h->esize = (int32_t)c->esize;
+}
+
+struct FileGuard {
+  FILE* f = nullptr;
+  ~FileGuard() {
+    if (f) std::fclose(f);
+  }
+};
+
+struct PinnedGuard {
+  void* p = nullptr;
+  ~PinnedGuard() {
+    if (p) cudaFreeHost(p);
+  }
+};
+
+constexpr size_t kStateChunk = 64u << 20;  // bytes staged through pinned memory at a time
+
+// device buffer <-> file through a pinned staging buffer
+int state_write_dev(rihvr_ctx* c, FILE* f, const void* dev, size_t bytes, void* stage) {
+  for (size_t o = 0; o < bytes; o += kStateChunk) {
+    const size_t n = std::min(kStateChunk, bytes - o);
+    CK(cudaMemcpyAsync(stage, static_cast<const char*>(dev) + o, n, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    if (std::fwrite(stage, 1, n, f) != n) return fail(RIHVR_ERR_BAD_FILENAME, "writing the state file failed");
+  }
+  return RIHVR_OK;
+}
+
+int state_read_dev(rihvr_ctx* c, FILE* f, void* dev, size_t bytes, void* stage) {
+  for (size_t o = 0; o < bytes; o += kStateChunk) {
+    const size_t n = std::min(kStateChunk, bytes - o);
+    if (std::fread(stage, 1, n, f) != n) return fail(RIHVR_ERR_INVALID_FILE, "the state file is truncated");
+    CK(cudaMemcpyAsync(static_cast<char*>(dev) + o, stage, n, cudaMemcpyHostToDevice, c->st));
+    CK(cudaStreamSynchronize(c->st));
+  }
+  return RIHVR_OK;
+}
+
+// the buffers a checkpoint carries, in file order
+template <typename F>
+int each_state_buffer(rihvr_ctx* c, F fn) {
+  const size_t HW = c->HW;
+  RC(fn(c->b, sizeof(float) * HW));
+  RC(fn(c->dnew, sizeof(float) * HW));
+  RC(fn(c->dY0, sizeof(float) * HW));
+  RC(fn(c->dX, sizeof(float) * HW));
+  RC(fn(c->r, sizeof(float) * HW));
+  RC(fn(c->Rs, sizeof(float2) * HW));
+  RC(fn(c->vol[c->iCur], c->esize * c->V));
+  return fn(c->vol[c->iPrev], c->esize * c->V);
+}
+
+}  // namespace
+
+extern "C" {
+
+int rihvr_save_state(rihvr_ctx* c, const char* path) {
+  if (!c || !path) return fail(RIHVR_ERR_INVALID_ARGUMENT, "NULL argument");
+  if (!c->have_holo) return fail(RIHVR_ERR_MISSING_DATA, "no hologram set");
+  StateHeader h;
+  state_header_of(c, &h);
+  h.t = c->t;
+  h.alpha1 = c->alpha1;
+  h.beta = c->beta;
+  h.prev_f_resid = c->prev_f_resid;
+  h.it = c->it;
+  h.pending_x = c->pending_x;
+  h.nlog = (int32_t)c->log.size();
+  FileGuard fg;
+  fg.f = std::fopen(path, "wb");
+  if (!fg.f) return fail(RIHVR_ERR_BAD_FILENAME, std::string("cannot open ") + path + " for writing");
+  if (std::fwrite(&h, sizeof(h), 1, fg.f) != 1 ||
+      (h.nlog > 0 && std::fwrite(c->log.data(), sizeof(rihvr_iter_record), (size_t)h.nlog, fg.f) != (size_t)h.nlog))
+    return fail(RIHVR_ERR_BAD_FILENAME, "writing the state file failed");
+  PinnedGuard stage;
+  CK(cudaMallocHost(&stage.p, kStateChunk));
+  CK(cudaStreamSynchronize(c->st));
+  RC(each_state_buffer(c, [&](const void* dev, size_t bytes) { return state_write_dev(c, fg.f, dev, bytes, stage.p); }));
+  if (std::fflush(fg.f) != 0) return fail(RIHVR_ERR_BAD_FILENAME, "writing the state file failed");
+  return RIHVR_OK;
+}
+
+int rihvr_load_state(rihvr_ctx* c, const char* path) {
+  if (!c || !path) return fail(RIHVR_ERR_INVALID_ARGUMENT, "NULL argument");
+  FileGuard fg;
+  fg.f = std::fopen(path, "rb");
+  if (!fg.f) return fail(RIHVR_ERR_BAD_FILENAME, std::string("cannot open ") + path);
+  StateHeader h, mine;
+  if (std::fread(&h, sizeof(h), 1, fg.f) != 1 || std::memcmp(h.magic, kStateMagic, 8) != 0 || h.version != 1)
+    return fail(RIHVR_ERR_INVALID_FILE, "not a reconstruction state file");
+  state_header_of(c, &mine);
+  // the solve it resumes must be this context's: sizes, storage, mode and the
+  // parameters every iteration reads
+  if (h.W != mine.W || h.H != mine.H || h.Nz != mine.Nz || h.storage != mine.storage || h.mode != mine.mode ||
+      h.faithful != mine.faithful || h.n_tv != mine.n_tv || h.max_backtracks != mine.max_backtracks ||
+      h.record_objective != mine.record_objective || h.esize != mine.esize || h.z0 != mine.z0 || h.dz != mine.dz ||
+      h.lambda != mine.lambda || h.dx != mine.dx || h.l1 != mine.l1 || h.tv != mine.tv)
+    return fail(RIHVR_ERR_INVALID_FILE, "the state file belongs to a solve with other sizes or parameters");
+  if (h.nlog < 0 || h.nlog > (1 << 24) || h.it < 0 || h.pending_x < -1 || h.pending_x >= h.nlog)
+    return fail(RIHVR_ERR_INVALID_FILE, "the state file's iteration log is inconsistent");
+  std::vector<rihvr_iter_record> log((size_t)h.nlog);
+  if (h.nlog > 0 && std::fread(log.data(), sizeof(rihvr_iter_record), (size_t)h.nlog, fg.f) != (size_t)h.nlog)
+    return fail(RIHVR_ERR_INVALID_FILE, "the state file is truncated");
+  PinnedGuard stage;
+  CK(cudaMallocHost(&stage.p, kStateChunk));
+  CK(cudaStreamSynchronize(c->st));
+  c->iPrev = 0;
+  c->iCur = 1;
+  c->iNew = 2;
+  const int rc =
+      each_state_buffer(c, [&](void* dev, size_t bytes) { return state_read_dev(c, fg.f, dev, bytes, stage.p); });
+  if (rc != RIHVR_OK) {
+    c->have_holo = false;  // partly overwritten: the context needs a hologram again
+    return rc;
+  }
+  c->t = h.t;
+  c->alpha1 = h.alpha1;
+  c->beta = h.beta;
+  c->prev_f_resid = h.prev_f_resid;
+  c->it = h.it;
+  c->pending_x = h.pending_x;
+  c->log.swap(log);
+  c->have_holo = true;
+  return RIHVR_OK;
 }
 
 int rihvr_iterate(rihvr_ctx* c, int n) {

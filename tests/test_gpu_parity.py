@@ -351,3 +351,45 @@ def test_volume_device_pointer_is_the_volume(rihvr, synthmod, cache_dir):
         assert V.shape == X.shape
         assert np.array_equal(V, X)
         assert np.abs(X).max() > 0
+
+
+@pytest.mark.parametrize("storage,record", [(0, 1), (2, 0)])
+def test_checkpoint_resumes_bit_for_bit(rihvr, synthmod, cache_dir, tmp_path, storage, record):
+    """rihvr_save_state after 5 iterations and rihvr_load_state into a new
+    context, then 7 more iterations: the same iteration log and volume as 5
+    and then 7 iterations in one context, bit for bit (with and without
+    objective recording, FP32 and FP16 storage).  (Each rihvr_iterate call
+    settles its last record's objective terms with a pass of its own, so the
+    reference is two calls, not one of 12.)  A state file is refused by a
+    context of another size or with other parameters."""
+    cfg = synthmod.small_config(W=64, H=64, Nz=6, seed=17, num_inverse_iterations=12)
+    _, b = synthmod.make_hologram(cfg, cache_dir=cache_dir)
+    p = rihvr.params_from_config(cfg, storage=storage, record_objective=record)
+    with rihvr.SparseCompressiveHolo(p, cfg.W, cfg.H) as s:
+        s.setHologram(b)
+        s.iterate(5)
+        s.iterate(7)
+        log12, X12 = s.iterations(), s.getVolume()
+    path = str(tmp_path / "state.bin")
+    with rihvr.SparseCompressiveHolo(p, cfg.W, cfg.H) as s:
+        s.setHologram(b)
+        s.iterate(5)
+        s.saveState(path)
+    with rihvr.SparseCompressiveHolo(p, cfg.W, cfg.H) as s:
+        s.loadState(path)
+        s.iterate(7)
+        log, X = s.iterations(), s.getVolume()
+    assert log.shape == log12.shape
+    for name in log12.dtype.names:
+        assert np.array_equal(log[name], log12[name]), name
+    assert np.array_equal(X, X12)
+    q = rihvr.params_from_config(cfg, storage=storage, record_objective=record)
+    q.regularization_param = q.regularization_param * 2
+    with rihvr.SparseCompressiveHolo(q, cfg.W, cfg.H) as s:
+        with pytest.raises(rihvr.RihvrError) as e:
+            s.loadState(path)
+        assert e.value.code == rihvr.ERR_INVALID_FILE
+    with rihvr.SparseCompressiveHolo(p, 32, 32) as s:
+        with pytest.raises(rihvr.RihvrError) as e:
+            s.loadState(path)
+        assert e.value.code == rihvr.ERR_INVALID_FILE
