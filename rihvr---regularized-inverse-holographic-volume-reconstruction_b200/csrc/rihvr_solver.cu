@@ -28,6 +28,8 @@
 #include <thread>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>  // header-only; ranges cost nothing without a profiler
+
 #include "../../include/rihvr.h"
 #include "rihvr_frame.cuh"
 #include "rihvr_kernels.cuh"
@@ -70,6 +72,16 @@ namespace {
     int r_ = (call);                 \
     if (r_ != RIHVR_OK) return r_;   \
   } while (0)
+
+// NVTX range over a scope: the solver's phases (iterations, attempts,
+// momentum step, autotuning, hologram set-up, batches) show in a timeline
+// profiler; in graph-captured iterations they mark the host-side launches.
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 enum KernelClass { K_ADJ_COL = 0, K_ADJ_ROW, K_PROX, K_FWD_ROW, K_FWD_COL, K_PLANE, K_NUM };
 const char* kClassNames[K_NUM] = {"adj_col", "adj_row", "prox", "fwd_row", "fwd_col", "plane"};
@@ -382,6 +394,7 @@ int reduce_into(rihvr_ctx* c, int nblocks, int slot) {
 
 // G = A^H r: column pass from the spectrum, then the inverse row pass.
 int adjoint_volume(rihvr_ctx* c) {
+  NvtxRange nvtx_("rihvr: adjoint");
   {
     ProfScope ps(c, K_ADJ_COL);
     const int rec = env_variant("RIHVR_ADJ_COL", {"direct", "recurrence", "recurrence_hoisted", "recurrence_table"},
@@ -398,6 +411,7 @@ int adjoint_volume(rihvr_ctx* c) {
 
 // dnew = A vol (the volume in `kind` layout), sum (dnew - b)^2 into SLOT_FWD.
 int forward_volume(rihvr_ctx* c, int kind, const void* vol) {
+  NvtxRange nvtx_("rihvr: forward");
   {
     ProfScope ps(c, K_FWD_ROW);
     KL(launch_rows(0, kind, vol, ELEM_C32, c->U, c->W, (long long)c->Nz * c->H, 1.0f, c->st));
@@ -452,6 +466,7 @@ ProxArgs prox_args(rihvr_ctx* c, double t, bool device_scalars = false) {
 
 // P_{k+1} = prox(x_k - t G) for the active mode; sums into SLOT_PROX.
 int prox_volume(rihvr_ctx* c, double t, bool device_scalars = false) {
+  NvtxRange nvtx_("rihvr: prox");
   ProxArgs a = prox_args(c, t, device_scalars);
   int nb = 0;
   ProfScope ps(c, K_PROX);
@@ -754,6 +769,7 @@ void rotate(rihvr_ctx* c) {
 }
 
 int run_iterations_dev(rihvr_ctx* c, int n) {
+  NvtxRange nvtx_("rihvr: device-decided iterations");
   for (int done = 0; done < n;) {
     const int m = std::min(n - done, kDevLogCap);
     stage_ctl(c);
@@ -1137,6 +1153,7 @@ int ensure_iter_graphs(rihvr_ctx* c) {
 // One FISTA iteration (:299-611): one host synchronisation per attempt and one
 // after the momentum step.
 int one_iteration(rihvr_ctx* c) {
+  NvtxRange nvtx_("rihvr: iteration (host-decided)");
   double alpha0 = c->alpha1;
   int bt = 0;
   double f_resid = 0, lim = 0, ratio = 0;
@@ -1457,6 +1474,7 @@ void rihvr_destroy(rihvr_ctx* c) {
 }
 
 int rihvr_set_hologram(rihvr_ctx* c, const float* b, int is_device) {
+  NvtxRange nvtx_("rihvr: set hologram");
   if (!c || !b) return fail(RIHVR_ERR_INVALID_ARGUMENT, "NULL argument");
   // A NaN or infinite sample would poison every later iterate.  The reference
   // only prints a warning per bad sample and carries on (check_isnan_mdata,
@@ -1653,6 +1671,7 @@ int rihvr_tuning(const rihvr_ctx* c, int* adj_chunks, int* fwd_chunks, int* tv_r
 }
 
 int rihvr_autotune(rihvr_ctx* c, double* best_ms) {
+  NvtxRange nvtx_("rihvr: autotune");
   if (!c) return fail(RIHVR_ERR_INVALID_ARGUMENT, "NULL context");
   const TuneKey key{c->device, c->W, c->H, c->Nz, c->p.num_tv_iterations, c->mode, c->storage,
                     c->p.record_objective ? 1 : 0};
@@ -1859,6 +1878,7 @@ int rihvr_load_state(rihvr_ctx* c, const char* path) {
 }
 
 int rihvr_iterate(rihvr_ctx* c, int n) {
+  NvtxRange nvtx_("rihvr: iterate");
   if (!c || n < 0) return fail(RIHVR_ERR_INVALID_ARGUMENT, "bad argument");
   return run_iterations(c, n);
 }
@@ -1879,6 +1899,7 @@ int rihvr_iterate_timed(rihvr_ctx* c, int n, float* ms) {
 }
 
 int rihvr_reconstruct(rihvr_ctx* c, double* final_objective) {
+  NvtxRange nvtx_("rihvr: reconstruct");
   if (!c) return fail(RIHVR_ERR_INVALID_ARGUMENT, "NULL context");
   if (!c->have_holo) return fail(RIHVR_ERR_MISSING_DATA, "no hologram set");
   RC(state_reset(c));
@@ -1889,6 +1910,7 @@ int rihvr_reconstruct(rihvr_ctx* c, double* final_objective) {
 
 int rihvr_reconstruct_batch(rihvr_ctx* const* ctxs, int n, const float* const* holograms, int is_device,
                             double* final_objectives, int* statuses) {
+  NvtxRange nvtx_("rihvr: reconstruct batch");
   g_batch_combined = 0;
   if (!ctxs || !holograms || n <= 0) return fail(RIHVR_ERR_INVALID_ARGUMENT, "empty or NULL batch");
   for (int i = 0; i < n; ++i) {
