@@ -597,6 +597,105 @@ def run_unet(args):
     return 0
 
 
+def run_slabs(args):
+    """One hologram of the 1024 x 1024 x 1000 workload split into z-slabs
+    (rihvr_slab_iterate).  On one GPU (`--slabs K` slabs in this process) the
+    line compares the slab group's time per iteration with one context over
+    all planes on the same hologram, i.e. the cost of the host-decided slab
+    loop and its spectrum sums.  Under torchrun each rank holds one slab on
+    its own GPU and the partial spectra are summed by NCCL all-reduce
+    (strong scaling: the total work is one hologram at every N).  Timed with
+    CUDA events on the slabs' streams; the solve is host-decided, so the time
+    includes the host's part of every attempt."""
+    ws, rank, local = dist_env()
+    import torch
+
+    torch.cuda.set_device(local)
+    rihvr = importlib.import_module(PKG)
+    synth = importlib.import_module(PKG + ".synth")
+    frames = importlib.import_module(PKG + ".frames")
+    slabs = importlib.import_module(PKG + ".slabs")
+    pg = None
+    if ws > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+        pg = dist
+    cfg = workload("c2")
+    if args.nz:
+        cfg.num_planes = args.nz
+        cfg.name = f"{cfg.name}_nz{args.nz}"
+    _, b = synth.make_hologram(cfg)
+    storage = {"f32": 0, "bf16": 1, "f16": 2}[args.storage]
+    p = rihvr.params_from_config(cfg, record_objective=0, storage=storage, autotune=1 if args.autotune else 0,
+                                 faithful=0 if storage == 1 else 1)
+    V = cfg.voxels()
+    single_ms = None
+    if ws == 1:
+        with rihvr.SparseCompressiveHolo(p, cfg.W, cfg.H) as s:
+            s.setHologram(b)
+            s.iterate(args.warmup)
+            single_ms = s.iterate_timed(args.steps) / args.steps
+            single_log = s.iterations()
+        n_local = max(1, args.slabs)
+        group = slabs.SlabSolve(p, cfg.W, cfg.H, n_local)
+        solvers, reducer = group.solvers, None
+    else:
+        z0, nz = slabs.slab_bounds(cfg.num_planes, ws, rank)
+        solvers = [rihvr.SparseCompressiveHolo(p, cfg.W, cfg.H, z_first=z0, z_count=nz)]
+        reducer = slabs.torch_reducer()
+    for s in solvers:
+        s.setHologram(b)
+    slabs.slab_iterate(solvers, args.warmup, reducer)
+    streams = [torch.cuda.ExternalStream(s.stream()) for s in solvers]
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = [torch.cuda.Event(enable_timing=True) for _ in solvers]
+    if pg is not None:
+        pg.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        time.sleep(0.5)
+        e0.record(streams[0])
+        slabs.slab_iterate(solvers, args.steps, reducer)
+        for e, st in zip(e1, streams):
+            e.record(st)
+        for e in e1:
+            e.synchronize()
+    ms = max(e0.elapsed_time(e) for e in e1)
+    if pg is not None:
+        pg.barrier()
+    max_ms = frames.reduce_max(ms, device="cuda")
+    log = solvers[0].iterations()
+    line = None
+    if rank == 0:
+        line = {"metric": METRIC, "value": V * args.steps / (max_ms / 1e3), "unit": "voxel-iters/s", "n_gpus": ws,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": max_ms / args.steps,
+                "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+                "dtype": "f32" if storage == 0 else args.storage, "data": "synthetic",
+                "config": {"workload": cfg.name + "_zslabs", "W": cfg.W, "H": cfg.H, "Nz": cfg.num_planes,
+                           "slabs": len(solvers) * ws, "slab_planes": [s.depth for s in solvers],
+                           "parallelism": f"{ws} z-slabs, one per GPU, NCCL spectrum sums" if ws > 1 else
+                           f"{len(solvers)} z-slabs on one GPU",
+                           "l2": "inputs larger than L2", "storage": args.storage},
+                "single_context_ms_per_step": single_ms,
+                "slab_overhead": (max_ms / args.steps / single_ms) if single_ms else None,
+                "same_decisions_as_single_context": (
+                    bool(np.array_equal(log["backtracks"], single_log["backtracks"][:len(log)]) and
+                         np.array_equal(log["restarted"], single_log["restarted"][:len(log)]))
+                    if single_ms else None),
+                "clocks": clk.summary()}
+        print(json.dumps(line), flush=True)
+    for s in solvers:
+        s.destroy()
+    if pg is not None:
+        pg.barrier()
+        pg.destroy_process_group()
+    return 0
+
+
 def run_ours(args):
     ws, rank, local = dist_env()
     import torch
@@ -746,7 +845,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c2",
-                    choices=["c2", "c1", "c5", "series", "segment", "warmstart", "warmstart4", "unet"])
+                    choices=["c2", "c1", "c5", "series", "segment", "warmstart", "warmstart4", "unet", "slabs"])
+    ap.add_argument("--slabs", type=int, default=2,
+                    help="z-slabs of the hologram on one GPU (--config slabs; one per rank under torchrun)")
     ap.add_argument("--frames", type=int, default=0,
                     help="frames of the uneven series (--config series, default 64) or of the warm-start set "
                          "(default 16; 256 for warmstart4)")
@@ -772,6 +873,8 @@ def main():
         return run_warmstart4(args)
     if args.config == "unet":
         return run_unet(args)
+    if args.config == "slabs":
+        return run_slabs(args)
     return run_ours(args)
 
 

@@ -283,6 +283,57 @@ int rihvr_tuning(const rihvr_ctx* ctx, int* adj_chunks, int* fwd_chunks, int* tv
 /* Restart from x = 0 without changing the hologram. */
 int rihvr_reset(rihvr_ctx* ctx);
 
+/* Z-slab sharding of one hologram (no counterpart in the reference, whose
+ * volume lives on one GPU).  A slab context holds planes
+ * [z_first, z_first + z_count) of the params' plane list; params, sizes and
+ * step rules are those of the whole volume (the first step is still
+ * 1 / num_planes).  Modes 5 and 7 only: their prox is separable by plane,
+ * which 3-D TV (mode 6) is not.  Give every slab the same hologram
+ * (rihvr_set_hologram), then run rihvr_slab_iterate; each slab returns its
+ * own planes (rihvr_get_volume, rihvr_get_plane with z counted from
+ * z_first) and the whole solve's iteration log (rihvr_get_iterations).
+ * Calls that need every plane (rihvr_iterate, rihvr_reconstruct and its batch
+ * form, rihvr_objective, rihvr_set_initial_volume, rihvr_warm_start,
+ * rihvr_initial_estimate, rihvr_lipschitz, rihvr_segment) return
+ * RIHVR_ERR_INVALID_STATE on a slab that holds fewer than num_planes planes;
+ * rihvr_forward on one returns its planes' contribution to the hologram. */
+int rihvr_create_slab(const rihvr_params* params, int width, int height, int z_first, int z_count,
+                      rihvr_ctx** out);
+
+/* The planes a context holds (0 and num_planes for rihvr_create's). */
+int rihvr_slab_range(const rihvr_ctx* ctx, int* z_first, int* z_count);
+
+enum rihvr_dtype { RIHVR_DTYPE_F32 = 0, RIHVR_DTYPE_F64 = 1 };
+
+/* Sum over the processes that hold the other slabs of the solve (one slab a
+ * process, e.g. one process per GPU).  sum(user, data, count, dtype,
+ * on_device) must replace the count values at data by their sum over all
+ * processes, identical bit for bit in every process (an NCCL or MPI
+ * all-reduce is), and return 0 when done; data is device memory of the
+ * slab's device when on_device is 1, host memory when 0.  With host_staged
+ * set, the partial spectrum is passed through pinned host memory too, for
+ * process groups that reduce host buffers only. */
+typedef struct rihvr_slab_reducer {
+  int (*sum)(void* user, void* data, long long count, int dtype, int on_device);
+  void* user;
+  int host_staged;
+} rihvr_slab_reducer;
+
+/* `iterations` FISTA iterations (inverseReconstruct's loop, :299-611) of one
+ * hologram whose planes are split over slab contexts.  Without a reducer the
+ * n contexts (1..16, on one device or several with peer access, which is
+ * enabled here) must tile the plane list in order; the partial spectra are
+ * summed on every slab's device by peer reads, in slab order.  With a reducer,
+ * n is 1 and the other slabs belong to other processes, which call this
+ * function at the same time with the same iteration count.  Each attempt
+ * exchanges one H x W complex FP32 plane (the partial spectrum) and 8 FP64
+ * sums; the backtracking, restart and momentum decisions are made on the sums
+ * and agree in every slab.  The objective and iterates equal those of one
+ * context over all planes up to the order of the FP32 spectrum and FP64
+ * sums; a single slab holding every plane reproduces rihvr_iterate bit for
+ * bit. */
+int rihvr_slab_iterate(rihvr_ctx* const* ctxs, int n, int iterations, const rihvr_slab_reducer* reducer);
+
 /* Checkpoint and resume (no counterpart in the reference, whose voxel CSV,
  * SparseVolume::saveData at sparse_volume.cu:518-682, keeps intensities only
  * and cannot restart a solve).  rihvr_save_state writes, between iterations,

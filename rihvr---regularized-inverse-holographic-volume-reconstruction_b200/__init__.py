@@ -24,6 +24,7 @@ OK = 0
 ERR_INVALID_ARGUMENT = 7
 ERR_UNKNOWN_MODE = 6
 ERR_MISSING_DATA = 3
+ERR_INVALID_STATE = 4
 ERR_INVALID_FILE = 9
 ERR_INVALID_DATA = 10
 ERR_BAD_FILENAME = 2
@@ -137,6 +138,7 @@ EXPORTED = (
     "rihvr_iterate_timed",
     "rihvr_iteration_count", "rihvr_objective", "rihvr_get_iterations", "rihvr_get_plane", "rihvr_get_volume",
     "rihvr_get_volume_ptr", "rihvr_save_state", "rihvr_load_state",
+    "rihvr_create_slab", "rihvr_slab_range", "rihvr_slab_iterate",
     "rihvr_get_estimate", "rihvr_get_residual", "rihvr_forward", "rihvr_adjoint", "rihvr_prox_step",
     "rihvr_adjoint_noalloc", "rihvr_sparsity", "rihvr_initial_estimate", "rihvr_lipschitz",
     "rihvr_set_hologram_frame", "rihvr_get_hologram", "rihvr_background_mean", "rihvr_background_median5",
@@ -180,6 +182,9 @@ def load_library(path: str = LIB_PATH):
     L.rihvr_read_param_file.argtypes = [ctypes.c_char_p, P(RihvrParams), P(FileParams)]
     L.rihvr_plane_list.argtypes = [P(RihvrParams), P(ctypes.c_double)]
     L.rihvr_create.argtypes = [P(RihvrParams), ip, ip, P(vp)]
+    L.rihvr_create_slab.argtypes = [P(RihvrParams), ip, ip, ip, ip, P(vp)]
+    L.rihvr_slab_range.argtypes = [vp, P(ctypes.c_int), P(ctypes.c_int)]
+    L.rihvr_slab_iterate.argtypes = [P(vp), ip, ip, vp]
     L.rihvr_destroy.argtypes = [vp]
     L.rihvr_debug_fail_allocations_after.argtypes = [ip]
     L.rihvr_destroy.restype = None
@@ -613,15 +618,26 @@ class SparseCompressiveHolo:
     padded ``height x width`` hologram; ``inverseReconstruct(b)`` runs the
     configured number of FISTA iterations from x = 0 and returns the objective
     at the final momentum point; ``getPlane(z)`` returns a plane of the volume.
+    With ``z_first``/``z_count`` the solver holds only those planes of the
+    plane list (a z-slab, rihvr_create_slab; whole solves of slabs run through
+    ``slabs.slab_iterate``), and ``depth`` is ``z_count``.
     """
 
-    def __init__(self, params: RihvrParams, width: int, height: int):
+    def __init__(self, params: RihvrParams, width: int, height: int, z_first: int | None = None,
+                 z_count: int | None = None):
         L = load_library()
         self._L = L
         self.params = params
-        self.width, self.height, self.depth = int(width), int(height), int(params.num_planes)
+        self.width, self.height = int(width), int(height)
         h = ctypes.c_void_p()
-        _check(L.rihvr_create(ctypes.byref(params), self.width, self.height, ctypes.byref(h)), "rihvr_create")
+        if z_first is None and z_count is None:
+            self.z_first, self.depth = 0, int(params.num_planes)
+            _check(L.rihvr_create(ctypes.byref(params), self.width, self.height, ctypes.byref(h)), "rihvr_create")
+        else:
+            self.z_first = int(z_first or 0)
+            self.depth = int(params.num_planes) - self.z_first if z_count is None else int(z_count)
+            _check(L.rihvr_create_slab(ctypes.byref(params), self.width, self.height, self.z_first, self.depth,
+                                       ctypes.byref(h)), "rihvr_create_slab")
         self._h = h
 
     # lifecycle ---------------------------------------------------------------

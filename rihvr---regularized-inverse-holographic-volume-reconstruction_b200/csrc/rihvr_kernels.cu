@@ -1330,6 +1330,29 @@ cudaError_t launch_sum_chunks(const float2* Spart, int nchunks, float2* S, long 
   return cudaGetLastError();
 }
 
+struct SlabSources {
+  const float2* p[kMaxSlabs];
+};
+
+__global__ void k_sum_slabs(SlabSources s, int n, float2* __restrict__ dst, long long count) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < count;
+       i += (long long)gridDim.x * blockDim.x) {
+    float2 a = s.p[0][i];
+    for (int k = 1; k < n; ++k) a = cadd(a, s.p[k][i]);
+    dst[i] = a;
+  }
+}
+
+cudaError_t launch_sum_slabs(const float2* const* src, int n, float2* dst, long long count, cudaStream_t st) {
+  if (n < 1 || n > kMaxSlabs) return cudaErrorInvalidValue;
+  SlabSources s{};
+  for (int k = 0; k < n; ++k) s.p[k] = src[k];
+  int blocks = (int)((count + 255) / 256);
+  if (blocks > 4 * num_sms()) blocks = 4 * num_sms();
+  k_sum_slabs<<<blocks, 256, 0, st>>>(s, n, dst, count);
+  return cudaGetLastError();
+}
+
 // ---------------------------------------------------------------------------
 // block reduction of kNumSums doubles into partials[block]
 // ---------------------------------------------------------------------------

@@ -105,6 +105,11 @@ int fwd_col_chunks(int W, int H, int Nz);
 cudaError_t launch_plane_col(int inverse, const float2* in, float2* out, int W, int H, float scale,
                              cudaStream_t st);
 cudaError_t launch_sum_chunks(const float2* Spart, int nchunks, float2* S, long long n, cudaStream_t st);
+// Partial spectra of the z-slabs of one hologram summed in slab order,
+// dst = ((src[0] + src[1]) + src[2]) + ...; sources on other devices are read
+// through peer mappings with plain loads.
+constexpr int kMaxSlabs = 16;
+cudaError_t launch_sum_slabs(const float2* const* src, int n, float2* dst, long long count, cudaStream_t st);
 cudaError_t launch_prox_tv2d(int storage, const ProxArgs& a, int* nblocks_out, cudaStream_t st);
 cudaError_t launch_prox_l1(int storage, const ProxArgs& a, int* nblocks_out, cudaStream_t st);
 cudaError_t launch_reduce_partials(const double* partials, int nblocks, double* scratch, double* out,

@@ -184,6 +184,7 @@ __global__ void k_ctl_post(IterCtl* s, const double* sums, DevRec* log) {
 struct rihvr_ctx {
   rihvr_params p{};
   int W = 0, H = 0, Nz = 0;
+  int z_first = 0;  // first plane held, of p.num_planes (z-slab contexts hold Nz < p.num_planes)
   size_t HW = 0, V = 0;
   int mode = 7;
   int storage = 0;
@@ -269,6 +270,8 @@ struct rihvr_ctx {
   long long launches = 0;  // kernels launched by this context
   unsigned long long uid = 0;  // unique for the process (a reused address gets a new one)
   unsigned graph_gen = 0;      // advanced whenever the context's captured graphs are dropped
+  cudaEvent_t slab_ev = nullptr;  // end of the slab's partial spectrum (rihvr_slab_iterate)
+  float2* slab_stage_h = nullptr; // pinned copy of the spectrum for host-staged reducers
   std::vector<void*> allocs;
 };
 
@@ -409,9 +412,9 @@ int adjoint_volume(rihvr_ctx* c) {
   return RIHVR_OK;
 }
 
-// dnew = A vol (the volume in `kind` layout), sum (dnew - b)^2 into SLOT_FWD.
-int forward_volume(rihvr_ctx* c, int kind, const void* vol) {
-  NvtxRange nvtx_("rihvr: forward");
+// S = sum over the context's planes of H'_z FFT2(vol_z) (the volume in `kind`
+// layout): the row and column passes and the sum of the z-chunks.
+int forward_partial(rihvr_ctx* c, int kind, const void* vol) {
   {
     ProfScope ps(c, K_FWD_ROW);
     KL(launch_rows(0, kind, vol, ELEM_C32, c->U, c->W, (long long)c->Nz * c->H, 1.0f, c->st));
@@ -425,11 +428,24 @@ int forward_volume(rihvr_ctx* c, int kind, const void* vol) {
   }
   ProfScope ps(c, K_PLANE);
   KL(launch_sum_chunks(c->Spart, c->nchunks, c->S, (long long)c->HW, c->st));
-  KL(launch_plane_col(1, c->S, c->pc1, c->W, c->H, 1.0f, c->st));
+  return RIHVR_OK;
+}
+
+// dnew = Re(IFFT2(S_all)) / (W H) from a summed spectrum; sum (dnew - b)^2 into SLOT_FWD.
+int forward_from_spectrum(rihvr_ctx* c, const float2* S_all) {
+  ProfScope ps(c, K_PLANE);
+  KL(launch_plane_col(1, S_all, c->pc1, c->W, c->H, 1.0f, c->st));
   KL(launch_rows(1, ELEM_C32, c->pc1, ELEM_C32, c->pc2, c->W, c->H, 1.0f / (float)c->HW, c->st));
   int nb = 0;
   KL(launch_finish_forward(c->pc2, c->b, c->dnew, (long long)c->HW, c->partials, &nb, c->st));
   return reduce_into(c, nb, SLOT_FWD);
+}
+
+// dnew = A vol (the volume in `kind` layout), sum (dnew - b)^2 into SLOT_FWD.
+int forward_volume(rihvr_ctx* c, int kind, const void* vol) {
+  NvtxRange nvtx_("rihvr: forward");
+  RC(forward_partial(c, kind, vol));
+  return forward_from_spectrum(c, c->S);
 }
 
 ProxArgs prox_args(rihvr_ctx* c, double t, bool device_scalars = false) {
@@ -1265,7 +1281,17 @@ int check_col_waits(rihvr_ctx* c) {
   return RIHVR_OK;
 }
 
+// Whole-volume operations refuse a context that holds only some planes.
+int whole_volume(const rihvr_ctx* c, const char* what) {
+  if (c->Nz < c->p.num_planes)
+    return fail(RIHVR_ERR_INVALID_STATE, std::string(what) + " needs every plane; this z-slab context holds " +
+                                             std::to_string(c->Nz) + " of " + std::to_string(c->p.num_planes) +
+                                             " (whole solves of slabs go through rihvr_slab_iterate)");
+  return RIHVR_OK;
+}
+
 int run_iterations(rihvr_ctx* c, int n) {
+  RC(whole_volume(c, "iterating"));
   if (!c->have_holo) return fail(RIHVR_ERR_MISSING_DATA, "no hologram set");
   int i = 0;
   RC(eager_start(c, n, &i));
@@ -1368,10 +1394,13 @@ const char* rihvr_status_string(int s) {
 
 int rihvr_debug_fail_allocations_after(int n) { return g_alloc_budget.exchange(n < 0 ? -1 : n); }
 
-int rihvr_create(const rihvr_params* params, int width, int height, rihvr_ctx** out) {
-  if (!out) return fail(RIHVR_ERR_INVALID_ARGUMENT, "out is NULL");
-  *out = nullptr;
-  RC(validate(params, width, height));
+}  // extern "C"
+
+namespace {
+
+// A context for planes [z_first, z_first + z_count) of the plane list
+// (all of them for rihvr_create); params and sizes already validated.
+int create_ctx(const rihvr_params* params, int width, int height, int z_first, int z_count, rihvr_ctx** out) {
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
     cudaGetLastError();
@@ -1384,7 +1413,8 @@ int rihvr_create(const rihvr_params* params, int width, int height, rihvr_ctx** 
   c->p = *params;
   c->W = width;
   c->H = height;
-  c->Nz = params->num_planes;
+  c->Nz = z_count;
+  c->z_first = z_first;
   c->HW = (size_t)width * height;
   c->V = c->HW * c->Nz;
   // No TV regularisation means the L1 prox (:187-195)
@@ -1442,8 +1472,9 @@ int rihvr_create(const rihvr_params* params, int width, int height, rihvr_ctx** 
     return cleanup(RIHVR_ERR_OUT_OF_MEMORY);
   std::vector<double> ct;
   phase_turns(height, width, (double)params->resolution, (double)params->wavelength, ct);
-  std::vector<double> zl((size_t)c->Nz);
-  rihvr_plane_list(params, zl.data());
+  std::vector<double> zall((size_t)params->num_planes);
+  rihvr_plane_list(params, zall.data());
+  const std::vector<double> zl(zall.begin() + z_first, zall.begin() + z_first + z_count);
   // evenly spaced planes (exactly, in FP64) let the adjoint advance H'_z by a recurrence
   c->dz_uniform = c->Nz > 1 ? zl[1] - zl[0] : 1.0;
   for (int k = 1; k + 1 < c->Nz && c->dz_uniform != 0; ++k)
@@ -1454,6 +1485,32 @@ int rihvr_create(const rihvr_params* params, int width, int height, rihvr_ctx** 
     return cleanup(fail(RIHVR_ERR_CUDA, "initial copies failed"));
   *out = c;
   return RIHVR_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int rihvr_create(const rihvr_params* params, int width, int height, rihvr_ctx** out) {
+  if (!out) return fail(RIHVR_ERR_INVALID_ARGUMENT, "out is NULL");
+  *out = nullptr;
+  RC(validate(params, width, height));
+  return create_ctx(params, width, height, 0, params->num_planes, out);
+}
+
+int rihvr_create_slab(const rihvr_params* params, int width, int height, int z_first, int z_count,
+                      rihvr_ctx** out) {
+  if (!out) return fail(RIHVR_ERR_INVALID_ARGUMENT, "out is NULL");
+  *out = nullptr;
+  RC(validate(params, width, height));
+  if (z_first < 0 || z_count < 1 || z_count > params->num_planes - z_first)
+    return fail(RIHVR_ERR_INVALID_ARGUMENT, "planes [" + std::to_string(z_first) + ", " +
+                                                std::to_string((long long)z_first + z_count) + ") are not within 0.." +
+                                                std::to_string(params->num_planes));
+  // 3-D TV (mode 6) couples each plane to its neighbours across slab boundaries
+  if (params->regularization_TV_param != 0.f && params->mode == 6)
+    return fail(RIHVR_ERR_UNKNOWN_MODE, "z-slabs need a plane-separable prox (mode 5 or 7), not 3-D TV (mode 6)");
+  return create_ctx(params, width, height, z_first, z_count, out);
 }
 
 void rihvr_destroy(rihvr_ctx* c) {
@@ -1469,6 +1526,8 @@ void rihvr_destroy(rihvr_ctx* c) {
   if (c->ctl_h) cudaFreeHost(c->ctl_h);
   if (c->dlog_h) cudaFreeHost(c->dlog_h);
   for (cudaEvent_t e : c->ev_pool) cudaEventDestroy(e);
+  if (c->slab_ev) cudaEventDestroy(c->slab_ev);
+  if (c->slab_stage_h) cudaFreeHost(c->slab_stage_h);
   if (c->st) cudaStreamDestroy(c->st);
   delete c;
 }
@@ -1877,6 +1936,283 @@ int rihvr_load_state(rihvr_ctx* c, const char* path) {
   return RIHVR_OK;
 }
 
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Z-slab sharding of one hologram.  A slab context holds planes
+// [z_first, z_first + Nz) of the volume and its own copy of every
+// hologram-space buffer.  The gradient, the prox and the forward pass up to
+// the partial spectrum S_s = sum over the slab's planes of H'_z FFT2(P_z) are
+// the slab's own; one attempt exchanges S_s (summed over the slabs in slab
+// order, so that every slab holds the same total) and the slabs' FP64 prox
+// sums.  After the sum every slab runs the same arithmetic on the same values
+// (the plane pass, d, r, the residual spectrum, the decisions), so no other
+// exchange is needed.  The decisions are those of one_iteration.
+// ---------------------------------------------------------------------------
+
+namespace {
+
+struct DeviceScope {
+  int prev = -1;
+  explicit DeviceScope(int d) {
+    if (cudaGetDevice(&prev) == cudaSuccess && prev != d) cudaSetDevice(d);
+  }
+  ~DeviceScope() {
+    int cur = -1;
+    if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+  }
+};
+
+struct SlabGroup {
+  rihvr_ctx* const* cs;
+  int n;
+  const rihvr_slab_reducer* red;  // other processes' slabs, or NULL
+
+  int sum_over_processes(void* data, long long count, int dtype, int on_device) const {
+    if (!red) return RIHVR_OK;
+    const int rc = red->sum(red->user, data, count, dtype, on_device);
+    if (rc != 0) return fail(RIHVR_ERR_UNKNOWN_ERROR, "the slab reducer failed with " + std::to_string(rc));
+    return RIHVR_OK;
+  }
+};
+
+// The group must tile the plane list in order (in-process slabs), share
+// sizes and parameters, hold a hologram and stand at the same iteration.
+int check_slab_group(const SlabGroup& g) {
+  if (!g.cs || g.n < 1 || g.n > kMaxSlabs)
+    return fail(RIHVR_ERR_INVALID_ARGUMENT, "1.." + std::to_string(kMaxSlabs) + " slab contexts expected");
+  if (g.red && (g.n != 1 || !g.red->sum))
+    return fail(RIHVR_ERR_INVALID_ARGUMENT, "a reducer takes exactly one local slab and a sum function");
+  const rihvr_ctx* c0 = g.cs[0];
+  int next = 0;
+  for (int i = 0; i < g.n; ++i) {
+    const rihvr_ctx* c = g.cs[i];
+    if (!c) return fail(RIHVR_ERR_INVALID_ARGUMENT, "NULL slab context");
+    if (c->W != c0->W || c->H != c0->H || std::memcmp(&c->p, &c0->p, sizeof(rihvr_params)) != 0)
+      return fail(RIHVR_ERR_INVALID_ARGUMENT, "slab contexts differ in size or parameters");
+    if (!c->have_holo) return fail(RIHVR_ERR_MISSING_DATA, "no hologram set on slab " + std::to_string(i));
+    if (c->it != c0->it || c->iCur != c0->iCur || c->prev_f_resid != c0->prev_f_resid)
+      return fail(RIHVR_ERR_INVALID_STATE, "slab " + std::to_string(i) +
+                                               " holds another hologram or stands at another iteration");
+    if (!g.red && c->z_first != next)
+      return fail(RIHVR_ERR_INVALID_ARGUMENT, "slab " + std::to_string(i) + " starts at plane " +
+                                                  std::to_string(c->z_first) + ", expected " + std::to_string(next));
+    next = c->z_first + c->Nz;
+  }
+  if (!g.red && next != c0->p.num_planes)
+    return fail(RIHVR_ERR_INVALID_ARGUMENT, "the slabs end at plane " + std::to_string(next) + " of " +
+                                                std::to_string(c0->p.num_planes));
+  return RIHVR_OK;
+}
+
+// Peer mappings between the devices of an in-process group.
+int enable_slab_peers(const SlabGroup& g) {
+  for (int i = 0; i < g.n; ++i)
+    for (int j = 0; j < g.n; ++j) {
+      const int a = g.cs[i]->device, b = g.cs[j]->device;
+      if (a == b) continue;
+      int ok = 0;
+      CK(cudaDeviceCanAccessPeer(&ok, a, b));
+      if (!ok)
+        return fail(RIHVR_ERR_CUDA, "device " + std::to_string(a) + " cannot read device " + std::to_string(b));
+      DeviceScope ds(a);
+      const cudaError_t e = cudaDeviceEnablePeerAccess(b, 0);
+      if (e == cudaErrorPeerAccessAlreadyEnabled)
+        cudaGetLastError();
+      else if (e != cudaSuccess)
+        return fail(RIHVR_ERR_CUDA, std::string("cudaDeviceEnablePeerAccess: ") + cudaGetErrorString(e));
+    }
+  for (int i = 0; i < g.n; ++i) {
+    rihvr_ctx* c = g.cs[i];
+    DeviceScope ds(c->device);
+    if (!c->slab_ev) CK(cudaEventCreateWithFlags(&c->slab_ev, cudaEventDisableTiming));
+    if (g.red && g.red->host_staged && !c->slab_stage_h && halloc(&c->slab_stage_h, sizeof(float2) * c->HW) != RIHVR_OK)
+      return fail(RIHVR_ERR_OUT_OF_MEMORY, "pinned staging buffer");
+  }
+  return RIHVR_OK;
+}
+
+// One attempt over the group: per slab the gradient (first attempt), the prox
+// and the partial spectrum; the spectra summed; per slab the rest of the
+// forward pass.  sp receives the prox sums over all slabs, *f_resid the
+// residual term of the new prox output.
+int slab_attempt(const SlabGroup& g, bool first, double* sp, double* f_resid) {
+  for (int i = 0; i < g.n; ++i) {
+    rihvr_ctx* c = g.cs[i];
+    DeviceScope ds(c->device);
+    CK(cudaMemcpyAsync(c->scal_d, c->scal_h, 5 * sizeof(float), cudaMemcpyHostToDevice, c->st));
+    if (first) RC(adjoint_volume(c));
+    RC(prox_volume(c, c->t, true));
+    {
+      NvtxRange nvtx_("rihvr: forward (slab part)");
+      RC(forward_partial(c, elem_kind(c->storage), c->vol[c->iNew]));
+    }
+    CK(cudaEventRecord(c->slab_ev, c->st));
+  }
+  std::vector<const float2*> total((size_t)g.n);
+  if (!g.red) {
+    std::vector<const float2*> src((size_t)g.n);
+    for (int i = 0; i < g.n; ++i) src[(size_t)i] = g.cs[i]->S;
+    for (int i = 0; i < g.n; ++i) {
+      rihvr_ctx* c = g.cs[i];
+      DeviceScope ds(c->device);
+      for (int j = 0; j < g.n; ++j)
+        if (j != i) CK(cudaStreamWaitEvent(c->st, g.cs[j]->slab_ev, 0));
+      KL(launch_sum_slabs(src.data(), g.n, c->Spart, (long long)c->HW, c->st));
+      total[(size_t)i] = c->Spart;
+    }
+  } else {
+    rihvr_ctx* c = g.cs[0];
+    DeviceScope ds(c->device);
+    NvtxRange nvtx_("rihvr: slab spectrum exchange");
+    if (g.red->host_staged) {
+      CK(cudaMemcpyAsync(c->slab_stage_h, c->S, sizeof(float2) * c->HW, cudaMemcpyDeviceToHost, c->st));
+      CK(cudaStreamSynchronize(c->st));
+      RC(g.sum_over_processes(c->slab_stage_h, 2 * (long long)c->HW, RIHVR_DTYPE_F32, 0));
+      CK(cudaMemcpyAsync(c->S, c->slab_stage_h, sizeof(float2) * c->HW, cudaMemcpyHostToDevice, c->st));
+    } else {
+      CK(cudaStreamSynchronize(c->st));
+      RC(g.sum_over_processes(c->S, 2 * (long long)c->HW, RIHVR_DTYPE_F32, 1));
+    }
+    total[0] = c->S;
+  }
+  for (int i = 0; i < g.n; ++i) {
+    rihvr_ctx* c = g.cs[i];
+    DeviceScope ds(c->device);
+    RC(forward_from_spectrum(c, total[(size_t)i]));
+    CK(cudaMemcpyAsync(c->sums_h, c->sums_d, sizeof(double) * kNumSums * NUM_SLOTS, cudaMemcpyDeviceToHost, c->st));
+  }
+  for (int i = 0; i < g.n; ++i) {
+    DeviceScope ds(g.cs[i]->device);
+    CK(cudaStreamSynchronize(g.cs[i]->st));
+  }
+  for (int k = 0; k < kNumSums; ++k) {
+    double v = 0;
+    for (int i = 0; i < g.n; ++i) v += g.cs[i]->sums_h[SLOT_PROX * kNumSums + k];
+    sp[k] = v;
+  }
+  RC(g.sum_over_processes(sp, kNumSums, RIHVR_DTYPE_F64, 0));
+  *f_resid = 0.5 * g.cs[0]->sums_h[SLOT_FWD * kNumSums + SUM_RR];
+  return RIHVR_OK;
+}
+
+// One FISTA iteration of the group (one_iteration's decisions on the summed
+// values; every slab takes the same step, momentum and record).
+int slab_iteration(const SlabGroup& g) {
+  NvtxRange nvtx_("rihvr: iteration (z-slabs)");
+  rihvr_ctx* c0 = g.cs[0];
+  double alpha0 = c0->alpha1;
+  int bt = 0;
+  double f_resid = 0, lim = 0, ratio = 0;
+  double sp[kNumSums];
+  for (;;) {
+    for (int i = 0; i < g.n; ++i) {
+      rihvr_ctx* c = g.cs[i];
+      const ProxArgs a = prox_args(c, c->t);
+      c->scal_h[0] = a.beta;
+      c->scal_h[1] = a.t;
+      c->scal_h[2] = a.mu;
+      c->scal_h[3] = a.s;
+      c->scal_h[4] = a.thr;
+    }
+    RC(slab_attempt(g, bt == 0, sp, &f_resid));
+    if (bt == 0 && c0->p.record_objective)
+      for (int i = 0; i < g.n; ++i) settle_x_terms(g.cs[i], sp);
+    lim = sp[SUM_LIM1] + sp[SUM_LIM2] / (2.0 * c0->t);
+    ratio = f_resid / (c0->prev_f_resid + lim);
+    if (((ratio > 1.0) || (ratio < 0.0)) && bt < c0->p.max_backtracks) {
+      for (int i = 0; i < g.n; ++i) g.cs[i]->t *= 0.5;  // stepsize_shrinkage (:63)
+      ++bt;
+      continue;
+    }
+    break;
+  }
+  rihvr_iter_record rec{};
+  rec.f_resid_prox = f_resid;
+  rec.lim = lim;
+  rec.ratio = ratio;
+  rec.t = c0->t;
+  rec.backtracks = bt;
+  rec.restart_sum = sp[SUM_RS];
+  rec.f_prox = f_resid + (double)c0->p.regularization_param * sp[SUM_L1P] + tv_weight(c0) * sp[SUM_TVP];
+  const bool restarted = sp[SUM_RS] > 0.0;  // fistaRestart (:471-475)
+  if (restarted) alpha0 = 1.0;
+  const double alpha1 = (1.0 + std::sqrt(1.0 + 4.0 * alpha0 * alpha0)) / 2.0;
+  const double beta = (alpha0 - 1.0) / alpha1;
+  rec.beta = beta;
+  rec.restarted = restarted ? 1 : 0;
+  for (int i = 0; i < g.n; ++i) {
+    rihvr_ctx* c = g.cs[i];
+    DeviceScope ds(c->device);
+    c->scal_h[8] = (float)beta;
+    RC(enqueue_momentum(c));
+  }
+  for (int i = 0; i < g.n; ++i) {
+    rihvr_ctx* c = g.cs[i];
+    DeviceScope ds(c->device);
+    CK(cudaStreamSynchronize(c->st));
+    const int old_prev = c->iPrev;
+    c->iPrev = c->iCur;
+    c->iCur = c->iNew;
+    c->iNew = old_prev;
+    c->alpha1 = alpha1;
+    c->beta = beta;
+    c->prev_f_resid = 0.5 * c->sums_h[SLOT_MOM * kNumSums + SUM_RR];
+    rihvr_iter_record r = rec;
+    r.f_resid_x = c->prev_f_resid;
+    r.f_x = r.f_resid_x;
+    c->log.push_back(r);
+    c->pending_x = (int)c->log.size() - 1;
+    c->it++;
+    c->warm = true;
+  }
+  return RIHVR_OK;
+}
+
+// The momentum-point terms of the last record from the norms over all slabs.
+int slab_settle_pending(const SlabGroup& g) {
+  rihvr_ctx* c0 = g.cs[0];
+  if (!c0->p.record_objective || c0->pending_x < 0) return RIHVR_OK;
+  double s[kNumSums] = {0};
+  for (int i = 0; i < g.n; ++i) {
+    rihvr_ctx* c = g.cs[i];
+    DeviceScope ds(c->device);
+    double l1x, tvx;
+    RC(norms_at_x(c, &l1x, &tvx));
+    s[SUM_L1X] += l1x;
+    s[SUM_TVX] += tvx;
+  }
+  RC(g.sum_over_processes(s, kNumSums, RIHVR_DTYPE_F64, 0));
+  for (int i = 0; i < g.n; ++i) settle_x_terms(g.cs[i], s);
+  return RIHVR_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int rihvr_slab_iterate(rihvr_ctx* const* ctxs, int n, int iterations, const rihvr_slab_reducer* reducer) {
+  NvtxRange nvtx_("rihvr: slab iterate");
+  if (iterations < 0) return fail(RIHVR_ERR_INVALID_ARGUMENT, "iterations must be >= 0");
+  const SlabGroup g{ctxs, n, reducer};
+  RC(check_slab_group(g));
+  RC(enable_slab_peers(g));
+  for (int k = 0; k < iterations; ++k) RC(slab_iteration(g));
+  RC(slab_settle_pending(g));
+  for (int i = 0; i < n; ++i) {
+    DeviceScope ds(ctxs[i]->device);
+    RC(check_col_waits(ctxs[i]));
+  }
+  return RIHVR_OK;
+}
+
+int rihvr_slab_range(const rihvr_ctx* c, int* z_first, int* z_count) {
+  if (!c) return fail(RIHVR_ERR_INVALID_ARGUMENT, "NULL context");
+  if (z_first) *z_first = c->z_first;
+  if (z_count) *z_count = c->Nz;
+  return RIHVR_OK;
+}
+
 int rihvr_iterate(rihvr_ctx* c, int n) {
   NvtxRange nvtx_("rihvr: iterate");
   if (!c || n < 0) return fail(RIHVR_ERR_INVALID_ARGUMENT, "bad argument");
@@ -1901,6 +2237,7 @@ int rihvr_iterate_timed(rihvr_ctx* c, int n, float* ms) {
 int rihvr_reconstruct(rihvr_ctx* c, double* final_objective) {
   NvtxRange nvtx_("rihvr: reconstruct");
   if (!c) return fail(RIHVR_ERR_INVALID_ARGUMENT, "NULL context");
+  RC(whole_volume(c, "rihvr_reconstruct"));
   if (!c->have_holo) return fail(RIHVR_ERR_MISSING_DATA, "no hologram set");
   RC(state_reset(c));
   RC(run_iterations(c, c->p.num_inverse_iterations));
@@ -1918,6 +2255,7 @@ int rihvr_reconstruct_batch(rihvr_ctx* const* ctxs, int n, const float* const* h
     for (int j = 0; j < i; ++j)
       if (ctxs[j] == ctxs[i]) return fail(RIHVR_ERR_INVALID_ARGUMENT, "a context appears twice in the batch");
   }
+  for (int i = 0; i < n; ++i) RC(whole_volume(ctxs[i], "rihvr_reconstruct_batch"));
   std::vector<int> st(n, RIHVR_OK), ran(n, 0);
   std::vector<std::string> msg(n);
   // run fn on every frame still without error, one host thread per frame
@@ -2021,6 +2359,7 @@ int rihvr_iteration_count(const rihvr_ctx* c) { return c ? c->it : -1; }
 
 int rihvr_objective(rihvr_ctx* c, double* f, double* terms3) {
   if (!c || !f) return fail(RIHVR_ERR_INVALID_ARGUMENT, "NULL argument");
+  RC(whole_volume(c, "rihvr_objective"));
   if (!c->have_holo) return fail(RIHVR_ERR_MISSING_DATA, "no hologram set");
   double l1x, tvx;
   RC(norms_at_x(c, &l1x, &tvx));
@@ -2044,6 +2383,7 @@ int rihvr_sparsity(rihvr_ctx* c, double* fraction) {
 
 int rihvr_initial_estimate(rihvr_ctx* c, float* out, int is_device) {
   if (!c || !out) return fail(RIHVR_ERR_INVALID_ARGUMENT, "NULL argument");
+  RC(whole_volume(c, "rihvr_initial_estimate"));
   if (!c->have_holo) return fail(RIHVR_ERR_MISSING_DATA, "no hologram set");
   // gradient.reconstruct(measured) then backPropagateInitial: A (t A^H b), t = 1/Nz
   CK(cudaMemcpyAsync(c->r, c->b, sizeof(float) * c->HW, cudaMemcpyDeviceToDevice, c->st));
@@ -2100,6 +2440,7 @@ extern "C" {
 
 int rihvr_set_initial_volume(rihvr_ctx* c, const float* x0, int is_device) {
   if (!c || !x0) return fail(RIHVR_ERR_INVALID_ARGUMENT, "NULL argument");
+  RC(whole_volume(c, "rihvr_set_initial_volume"));
   if (!c->have_holo) return fail(RIHVR_ERR_MISSING_DATA, "no hologram set");
   RC(state_reset(c));
   RC(copy_in(c, c->U, x0, sizeof(float2) * c->V, is_device));
@@ -2118,6 +2459,7 @@ int rihvr_backpropagate(rihvr_ctx* c, float* out, int is_device) {
 
 int rihvr_warm_start(rihvr_ctx* c, rihvr_unet* net) {
   if (!c || !net) return fail(RIHVR_ERR_INVALID_ARGUMENT, "NULL argument");
+  RC(whole_volume(c, "rihvr_warm_start"));
   if (!c->have_holo) return fail(RIHVR_ERR_MISSING_DATA, "no hologram set");
   int D, H, W;
   unet_dims(net, &D, &H, &W);
@@ -2162,6 +2504,7 @@ int rihvr_get_volume_ptr(rihvr_ctx* c, const void** dev_ptr, int* dtype) {
 int rihvr_segment(rihvr_ctx* c, const rihvr_segment_params* sp, rihvr_object* objects, int max_objects,
                   int* num_objects, rihvr_segment_info* info) {
   if (!c) return fail(RIHVR_ERR_INVALID_ARGUMENT, "NULL context");
+  RC(whole_volume(c, "rihvr_segment"));
   // the volume rihvr_get_volume returns, read in place
   if (!c->seg_ws) c->seg_ws = seg_workspace_create();
   rihvr_segment_info local{};
@@ -2195,6 +2538,7 @@ int rihvr_get_residual(rihvr_ctx* c, float* out, int is_device) {
 int rihvr_lipschitz(rihvr_ctx* c, int iterations, unsigned long long seed, double* L_out, double* history) {
   if (!c || !L_out) return fail(RIHVR_ERR_INVALID_ARGUMENT, "NULL argument");
   if (iterations < 1 || iterations > 100000) return fail(RIHVR_ERR_INVALID_ARGUMENT, "iterations must be 1..100000");
+  RC(whole_volume(c, "rihvr_lipschitz"));
   if (!c->have_holo) return fail(RIHVR_ERR_MISSING_DATA, "no hologram set");
   // FP64 sum of squares of n floats on the device, read back
   auto sumsq = [&](const float* x, long long n, double* out) -> int {
