@@ -340,8 +340,9 @@ int rihvr_slab_iterate(rihvr_ctx* const* ctxs, int n, int iterations, const rihv
  * everything the next iteration reads: the hologram, the hologram-space
  * momentum buffers, the last two prox outputs in the storage type, the step,
  * momentum and restart scalars and the iteration log.  rihvr_load_state
- * restores them into a context created with the same sizes, storage, mode
- * and iteration parameters (else RIHVR_ERR_INVALID_FILE, context unchanged);
+ * restores them into a context created with the same sizes, plane range
+ * (z-slabs), storage, mode and iteration parameters (else
+ * RIHVR_ERR_INVALID_FILE, context unchanged);
  * further rihvr_iterate calls then continue the solve bit for bit as if it
  * had not stopped (with the same launch shapes: both contexts untuned, or
  * tuned alike).  The file takes about 2 x Nz x H x W x storage size bytes. */

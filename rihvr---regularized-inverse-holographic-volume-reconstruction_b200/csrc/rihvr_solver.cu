@@ -1787,12 +1787,13 @@ struct StateHeader {
   float z0, dz, lambda, dx, l1, tv;
   double t, alpha1, beta, prev_f_resid;
   int32_t it, pending_x, nlog, esize;
+  int32_t z_first, num_planes;  // the planes held, of the whole volume's (z-slabs)
 };
 
 void state_header_of(const rihvr_ctx* c, StateHeader* h) {
   std::memset(h, 0, sizeof(*h));
   std::memcpy(h->magic, kStateMagic, 8);
-  h->version = 1;
+  h->version = 2;
   h->W = c->W;
   h->H = c->H;
   h->Nz = c->Nz;
@@ -1809,6 +1810,8 @@ void state_header_of(const rihvr_ctx* c, StateHeader* h) {
   h->l1 = c->p.regularization_param;
   h->tv = c->p.regularization_TV_param;
   h->esize = (int32_t)c->esize;
+  h->z_first = c->z_first;
+  h->num_planes = c->p.num_planes;
 }
 
 struct FileGuard {
@@ -1898,7 +1901,7 @@ int rihvr_load_state(rihvr_ctx* c, const char* path) {
   fg.f = std::fopen(path, "rb");
   if (!fg.f) return fail(RIHVR_ERR_BAD_FILENAME, std::string("cannot open ") + path);
   StateHeader h, mine;
-  if (std::fread(&h, sizeof(h), 1, fg.f) != 1 || std::memcmp(h.magic, kStateMagic, 8) != 0 || h.version != 1)
+  if (std::fread(&h, sizeof(h), 1, fg.f) != 1 || std::memcmp(h.magic, kStateMagic, 8) != 0 || h.version != 2)
     return fail(RIHVR_ERR_INVALID_FILE, "not a reconstruction state file");
   state_header_of(c, &mine);
   // the solve it resumes must be this context's: sizes, storage, mode and the
@@ -1906,7 +1909,8 @@ int rihvr_load_state(rihvr_ctx* c, const char* path) {
   if (h.W != mine.W || h.H != mine.H || h.Nz != mine.Nz || h.storage != mine.storage || h.mode != mine.mode ||
       h.faithful != mine.faithful || h.n_tv != mine.n_tv || h.max_backtracks != mine.max_backtracks ||
       h.record_objective != mine.record_objective || h.esize != mine.esize || h.z0 != mine.z0 || h.dz != mine.dz ||
-      h.lambda != mine.lambda || h.dx != mine.dx || h.l1 != mine.l1 || h.tv != mine.tv)
+      h.lambda != mine.lambda || h.dx != mine.dx || h.l1 != mine.l1 || h.tv != mine.tv ||
+      h.z_first != mine.z_first || h.num_planes != mine.num_planes)
     return fail(RIHVR_ERR_INVALID_FILE, "the state file belongs to a solve with other sizes or parameters");
   if (h.nlog < 0 || h.nlog > (1 << 24) || h.it < 0 || h.pending_x < -1 || h.pending_x >= h.nlog)
     return fail(RIHVR_ERR_INVALID_FILE, "the state file's iteration log is inconsistent");

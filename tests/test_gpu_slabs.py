@@ -259,3 +259,36 @@ def test_nccl_reducer_sums_the_spectrum_in_device_memory(rihvr, synthmod, cache_
     assert staged == 0
     assert recs == _records_bits(rec)
     assert np.array_equal(vol, X)
+
+
+def test_slab_checkpoints_resume_the_group(rihvr, synthmod, cache_dir, tmp_path):
+    """Each slab saves its own state (rihvr_save_state); new slab contexts
+    loading them continue the group's solve bit for bit.  A state file names
+    its plane range, so slab 1's file does not load into slab 0 although their
+    sizes agree."""
+    c = synthmod.small_config(W=64, H=64, Nz=8, seed=36, num_inverse_iterations=9)
+    b = synthmod.make_hologram(c, cache_dir=cache_dir)[1]
+    p = rihvr.params_from_config(c)
+    ref = _slabs().SlabSolve(p, c.W, c.H, 2)
+    g = _slabs().SlabSolve(p, c.W, c.H, 2)
+    h = _slabs().SlabSolve(p, c.W, c.H, 2)
+    try:
+        ref.setHologram(b)
+        ref.iterate(4)
+        ref.iterate(5)
+        g.setHologram(b)
+        g.iterate(4)
+        files = [str(tmp_path / f"slab{i}.state") for i in range(2)]
+        for s, f in zip(g.solvers, files):
+            s.saveState(f)
+        with pytest.raises(rihvr.RihvrError) as e:
+            h.solvers[0].loadState(files[1])
+        assert e.value.code == rihvr.ERR_INVALID_FILE
+        for s, f in zip(h.solvers, files):
+            s.loadState(f)
+        h.iterate(5)
+        assert _records_bits(h.iterations()) == _records_bits(ref.iterations())
+        assert np.array_equal(h.getVolume(), ref.getVolume())
+    finally:
+        for x in (ref, g, h):
+            x.destroy()
