@@ -86,3 +86,121 @@ def test_two_gloo_ranks_sum_slab_buffers():
     for rank, rc1, rc2, staged, spec, sums in res:
         assert (rc1, rc2, staged) == (0, 0, 1)
         assert np.array_equal(spec, want_spec) and np.array_equal(sums, want_sums)
+
+
+def _oracle_slab_solve(rank, world, cfg, b, n_iter, sum_fn):
+    """FISTA of one z-slab with the FP64 oracle as the compute: the exchange
+    rihvr_slab_iterate makes (the slab's share of the forward operator and
+    the line-search and restart sums, summed over the slabs), the decisions of
+    inverseReconstruct (sparse_compressive_holo.cu:299-611) on the sums."""
+    import oracle as O
+
+    slabs = _slabs()
+    z0, nz = slabs.slab_bounds(cfg.num_planes, world, rank)
+    z = cfg.plane_list()
+    p = O.OracleParams(W=cfg.W, H=cfg.H, z=z[z0:z0 + nz], dx=cfg.dx(), lam=cfg.lam(), l1=cfg.l1(), tv=cfg.tv(),
+                       n_tv=cfg.num_tv_iterations, mode=7, faithful=1, n_threads=1)
+    b = b.astype(np.float64)
+    X = np.zeros((nz, cfg.H, cfg.W), np.complex128)
+    Y0 = np.zeros_like(X)
+    dX = np.zeros_like(b)
+    dY0 = np.zeros_like(b)
+    r = dX - b
+    prev_f = 0.5 * float(np.sum(r * r))
+    t = 1.0 / cfg.num_planes  # the whole volume's first step
+    alpha1 = 1.0
+    log = []
+    for _ in range(n_iter):
+        alpha0, bt = alpha1, 0
+        while True:
+            P, s3 = O.prox_from(p, X, Y0, r, t)
+            d = sum_fn(O.forward(p, P))  # the slab's share of A P, summed over the slabs
+            s3 = sum_fn(s3)
+            f_resid = 0.5 * float(np.sum((d - b) ** 2))
+            lim = s3[0] + s3[1] / (2.0 * t)
+            ratio = f_resid / (prev_f + lim)
+            if (ratio > 1.0 or ratio < 0.0) and bt < p.max_backtracks:
+                t *= 0.5
+                bt += 1
+                continue
+            break
+        restarted = s3[2] > 0.0
+        if restarted:
+            alpha0 = 1.0
+        alpha1 = (1.0 + np.sqrt(1.0 + 4.0 * alpha0 * alpha0)) / 2.0
+        beta = (alpha0 - 1.0) / alpha1
+        X = P + beta * (P - Y0)
+        Y0 = P
+        dX = d + beta * (d - dY0)
+        dY0 = d
+        r = dX - b
+        prev_f = 0.5 * float(np.sum(r * r))
+        log.append((bt, int(restarted), f_resid, prev_f))
+    return log, Y0
+
+
+def _oracle_slab_worker(rank, world, port, out):
+    import sys
+
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    for p in (root, os.path.join(root, "oracle"), os.path.join(root, "tests")):
+        sys.path.insert(0, p)
+    import torch
+    import torch.distributed as dist
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    try:
+        cfg, b = _tiny_case()
+
+        def sum_fn(a):
+            t = torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64).copy())
+            dist.all_reduce(t)
+            return t.numpy()
+
+        out.put((rank,) + _oracle_slab_solve(rank, world, cfg, b, 8, sum_fn))
+    finally:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def _tiny_case():
+    synth = importlib.import_module(PKG_NAME + ".synth")
+    cfg = synth.small_config(W=32, H=32, Nz=7, seed=41, num_inverse_iterations=8)
+    _, b = synth.make_hologram(cfg)
+    return cfg, b
+
+
+def test_two_gloo_ranks_solve_one_hologram_by_slabs():
+    """Two ranks hold 4 and 3 of the 7 planes and exchange per attempt only
+    the forward share and three sums (FP64 oracle compute, gloo sums); their
+    solve is the single-process oracle solve of all planes: the same
+    backtracking and restart decisions, objective terms within 1e-9 and the
+    volume within 1e-9 (only the order of FP64 sums differs)."""
+    import oracle as O
+    import torch.multiprocessing as mp
+
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = free_port()
+    procs = [ctx.Process(target=_oracle_slab_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = sorted((q.get(timeout=300) for _ in procs), key=lambda t: t[0])
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    (_, log0, P0), (_, log1, P1) = res
+    assert log0 == log1  # every rank takes the same decisions on the same sums
+    cfg, b = _tiny_case()
+    op = O.OracleParams(W=cfg.W, H=cfg.H, z=cfg.plane_list(), dx=cfg.dx(), lam=cfg.lam(), l1=cfg.l1(), tv=cfg.tv(),
+                        n_tv=cfg.num_tv_iterations, mode=7, faithful=1, n_threads=1)
+    ref, _, P, _, _ = O.solve(op, b.astype(np.float64), 8)
+    assert [x[0] for x in log0] == list(ref["backtracks"])
+    assert [x[1] for x in log0] == list(ref["restarted"])
+    assert np.allclose([x[2] for x in log0], ref["f_resid_prox"], rtol=1e-9, atol=0)
+    assert np.allclose([x[3] for x in log0], ref["f_resid_x"], rtol=1e-9, atol=0)
+    Ps = np.concatenate([P0, P1])
+    assert Ps.shape == P.shape
+    assert np.linalg.norm(Ps - P) <= 1e-9 * np.linalg.norm(P)
