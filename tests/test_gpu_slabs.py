@@ -46,9 +46,12 @@ def test_one_slab_of_every_plane_equals_iterate(rihvr, synthmod, cache_dir):
         assert np.array_equal(s.getVolume(), X)
 
 
-@pytest.mark.parametrize("storage,tv,n_slabs", [(0, None, 3), (2, None, 2), (0, 0.0, 4)])
-def test_slabs_match_one_context(rihvr, synthmod, cache_dir, storage, tv, n_slabs):
-    kw = dict(W=128, H=128, Nz=25, seed=32, num_inverse_iterations=20)
+@pytest.mark.parametrize("storage,tv,n_slabs,n_tv", [(0, None, 3, 5), (2, None, 2, 5), (0, 0.0, 4, 5),
+                                                     (0, None, 2, 7)])
+def test_slabs_match_one_context(rihvr, synthmod, cache_dir, storage, tv, n_slabs, n_tv):
+    """Mode 7 in FP32 and FP16 storage, mode 5 (no TV), and 7 TV iterations
+    (the prox in two launches with its dual stored in each slab's buffers)."""
+    kw = dict(W=128, H=128, Nz=25, seed=32, num_inverse_iterations=20, num_tv_iterations=n_tv)
     if tv is not None:
         kw["regularization_TV_param"] = tv
     c = synthmod.small_config(**kw)
