@@ -139,3 +139,24 @@ def test_batch_mode_setting(rihvr):
     assert L.rihvr_batch_last_combined() == 0
     assert L.rihvr_set_batch_mode(2) == rihvr.OK
     assert L.rihvr_set_batch_mode(0) == rihvr.OK
+
+
+def test_header_compiles_as_plain_c(tmp_path):
+    """include/rihvr.h is a C header: a C99 translation unit that includes it
+    and names its types builds with -pedantic -Werror."""
+    import shutil
+    import subprocess
+
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    src = tmp_path / "use.c"
+    src.write_text('#include "rihvr.h"\n'
+                   "static int sum(void* u, void* d, long long n, int t, int dev) {\n"
+                   "  (void)u; (void)d; (void)n; (void)t; (void)dev; return 0;\n}\n"
+                   "int use(void) {\n"
+                   "  rihvr_params p; rihvr_iter_record r; rihvr_slab_reducer red = {sum, 0, 1};\n"
+                   "  (void)p; (void)r; (void)red; return RIHVR_OK + RIHVR_DTYPE_F64;\n}\n")
+    res = subprocess.run([cc, "-std=c99", "-Wall", "-Wextra", "-pedantic", "-Werror", f"-I{os.path.dirname(HEADER)}",
+                          "-c", str(src), "-o", str(tmp_path / "use.o")], capture_output=True, text=True)
+    assert res.returncode == 0, res.stderr
